@@ -1,0 +1,231 @@
+"""bellhopcuda_b200 — B200-native BELLHOP beam tracer (2-D field modes).
+
+Python mirror of the reference's library flow (include/bhc/bhc.hpp):
+
+    bhc::setup(init, params, outputs)   ->  Tracer(...).setup(file_root)
+    bhc::run(params, outputs)           ->  Tracer.run()
+    outputs.uAllSources                 ->  Tracer.field(env, ifreq)
+    bhc::writeout(params, outputs, fr)  ->  Tracer.writeout(file_root)
+    bhc::finalize(params, outputs)      ->  Tracer.close()
+
+All compute happens in libbhcb.so (hand-written sm_100a kernels) through the C
+ABI declared in include/bhcb.h. There is no CPU fallback: if the native
+library is missing or no GPU is present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbhcb.so")
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+ERR_NAMES = {
+    2: "BHC_ERR_RAYINIT", 3: "BHC_ERR_BOUNDARY_SEG_CONTAINS_NAN",
+    4: "BHC_ERR_BOUNDARY_CONDITION_TYPE", 5: "BHC_ERR_INVALID_SSP_TYPE",
+    6: "BHC_ERR_OUTSIDE_ALTIMETRY", 7: "BHC_ERR_OUTSIDE_BATHYMETRY", 31: "segment buffer overflow",
+}
+
+
+class BhcbError(RuntimeError):
+    def __init__(self, code: int, msg: str, err_bits: int = 0):
+        super().__init__("bhcb error %d: %s" % (code, msg))
+        self.code = code
+        self.err_bits = err_bits
+
+
+class Init(C.Structure):
+    _fields_ = [("gpu_index", C.c_int32), ("precision", C.c_int32), ("max_memory", C.c_uint64),
+                ("share_trajectory", C.c_int32), ("reserved", C.c_int32),
+                ("output_callback", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("steps", C.c_uint64), ("segments", C.c_uint64),
+                ("evals", C.c_uint64), ("err_bits", C.c_uint32), ("warn_bits", C.c_uint32),
+                ("groups", C.c_int32), ("fields", C.c_int32), ("trace_ms", C.c_double),
+                ("influence_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+class EnvInfo(C.Structure):
+    _fields_ = [("nsz", C.c_int32), ("nrz", C.c_int32), ("nrz_per_range", C.c_int32),
+                ("nrr", C.c_int32), ("nalpha", C.c_int32), ("ssp_type", C.c_int32),
+                ("freq", C.c_double), ("deltas", C.c_double), ("run_type", C.c_char * 8),
+                ("beam_type", C.c_char * 8)]
+
+
+_lib = None
+
+# (name, restype, argtypes) for every entry point of include/bhcb.h
+SIGNATURES = [
+    ("bhcb_open", C.c_int, [C.POINTER(Init), C.POINTER(C.c_void_p)]),
+    ("bhcb_close", None, [C.c_void_p]),
+    ("bhcb_setup", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("bhcb_add_env", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]),
+    ("bhcb_clear", C.c_int, [C.c_void_p]),
+    ("bhcb_set_frequencies", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    ("bhcb_run", C.c_int, [C.c_void_p]),
+    ("bhcb_prepare", C.c_int, [C.c_void_p]),
+    ("bhcb_launch", C.c_int, [C.c_void_p]),
+    ("bhcb_sync", C.c_int, [C.c_void_p]),
+    ("bhcb_field_shape", C.c_int, [C.c_void_p, C.c_int32] + [C.POINTER(C.c_int32)] * 4),
+    ("bhcb_copy_field", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),
+    ("bhcb_field_device", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("bhcb_receivers", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_int32,
+                                 C.POINTER(C.c_float), C.c_int32]),
+    ("bhcb_writeout", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_char_p]),
+    ("bhcb_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    ("bhcb_last_error", C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32)]),
+    ("bhcb_check_env", C.c_int, [C.c_char_p, C.POINTER(EnvInfo), C.c_char_p, C.c_size_t]),
+    ("bhcb_version", C.c_char_p, []),
+]
+
+
+def load_library():
+    """Load libbhcb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libbhcb.so is missing: run `python -m bellhopcuda_b200.build` "
+                               "(there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check_env(file_root: str) -> dict:
+    """Read and validate an environment on the host only (no GPU needed)."""
+    lib = load_library()
+    info = EnvInfo()
+    msg = C.create_string_buffer(512)
+    rc = lib.bhcb_check_env(file_root.encode(), C.byref(info), msg, 512)
+    if rc != 0:
+        raise BhcbError(rc, msg.value.decode(errors="replace"))
+    return dict(nsz=info.nsz, nrz=info.nrz, nrz_per_range=info.nrz_per_range, nrr=info.nrr,
+                nalpha=info.nalpha, ssp_type=info.ssp_type, freq=info.freq, deltas=info.deltas,
+                run_type=info.run_type.decode(), beam_type=info.beam_type.decode())
+
+
+class Tracer:
+    """One bhcb context (one GPU, one stream)."""
+
+    def __init__(self, gpu: int = 0, precision: int = PREC_MIXED, max_memory: int = 0,
+                 share_trajectory: bool = True):
+        self._lib = load_library()
+        init = Init(gpu, precision, max_memory, 1 if share_trajectory else 0, 0, None)
+        h = C.c_void_p()
+        rc = self._lib.bhcb_open(C.byref(init), C.byref(h))
+        if rc != 0:
+            raise BhcbError(rc, "bhcb_open failed (no usable CUDA device?)")
+        self._h = h
+        self.precision = precision
+
+    # -- error helper
+    def _check(self, rc):
+        if rc != 0:
+            msg = C.create_string_buffer(1024)
+            eb, wb = C.c_uint32(), C.c_uint32()
+            self._lib.bhcb_last_error(self._h, msg, 1024, C.byref(eb), C.byref(wb))
+            raise BhcbError(rc, msg.value.decode(errors="replace"), eb.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bhcb_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- bhc::setup
+    def setup(self, file_root: str):
+        self._check(self._lib.bhcb_setup(self._h, file_root.encode()))
+        return self
+
+    def add_env(self, file_root: str) -> int:
+        idx = C.c_int32()
+        self._check(self._lib.bhcb_add_env(self._h, file_root.encode(), C.byref(idx)))
+        return idx.value
+
+    def clear(self):
+        self._check(self._lib.bhcb_clear(self._h))
+
+    def set_frequencies(self, env: int, freqs: Sequence[float]):
+        arr = (C.c_double * len(freqs))(*[float(f) for f in freqs])
+        self._check(self._lib.bhcb_set_frequencies(self._h, env, len(freqs), arr))
+
+    # -- bhc::run
+    def run(self):
+        self._check(self._lib.bhcb_run(self._h))
+        return self
+
+    def prepare(self):
+        self._check(self._lib.bhcb_prepare(self._h))
+
+    def launch(self):
+        self._check(self._lib.bhcb_launch(self._h))
+
+    def sync(self):
+        self._check(self._lib.bhcb_sync(self._h))
+
+    # -- outputs
+    def field_shape(self, env: int = 0):
+        v = [C.c_int32() for _ in range(4)]
+        self._check(self._lib.bhcb_field_shape(self._h, env, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def field(self, env: int = 0, ifreq: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Scaled complex pressure, shape (NSz, NRz_per_range, NRr), complex64."""
+        _, nsz, nrz, nrr = self.field_shape(env)
+        if out is None:
+            out = np.empty((nsz, nrz, nrr), np.complex64)
+        self._check(self._lib.bhcb_copy_field(self._h, env, ifreq, out.ctypes.data, out.nbytes))
+        return out
+
+    def field_device_ptr(self, env: int = 0, ifreq: int = 0) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.bhcb_field_device(self._h, env, ifreq, C.byref(p)))
+        return p.value
+
+    def receivers(self, env: int = 0):
+        _, _, _, nrr = self.field_shape(env)
+        info_rz = self.field_shape(env)[2]
+        rr = np.zeros(nrr, np.float64)
+        rz = np.zeros(max(info_rz, 1), np.float32)
+        self._check(self._lib.bhcb_receivers(self._h, env, rr.ctypes.data_as(C.POINTER(C.c_double)),
+                                             nrr, rz.ctypes.data_as(C.POINTER(C.c_float)), rz.size))
+        return rr, rz
+
+    def writeout(self, file_root: str, env: int = 0, ifreq: int = 0):
+        self._check(self._lib.bhcb_writeout(self._h, env, ifreq, file_root.encode()))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self._lib.bhcb_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+def tl_db(p: np.ndarray) -> np.ndarray:
+    """Transmission loss -20 log10 |p| (dB), +inf where p == 0."""
+    a = np.abs(p).astype(np.float64)
+    with np.errstate(divide="ignore"):
+        return -20.0 * np.log10(a)

@@ -1,0 +1,709 @@
+// Runtime behind the bhcb C ABI: context, environment batch, device arena,
+// kernel sequencing and output access. See include/bhcb.h for the contract.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/bhcb.h"
+#include "bhcb_internal.h"
+#include "host/env2d.h"
+
+namespace bhcb {
+template<typename R> cudaError_t launch_trace(const GroupDev *, int, long long, void *,
+                                              unsigned long long, RunCounters *,
+                                              unsigned long long *, int, int, cudaStream_t);
+template<typename R> cudaError_t launch_influence(const void *, unsigned long long,
+                                                  const GroupDev *, int, const double *, float2 *,
+                                                  RunCounters *, bool, bool, int, cudaStream_t);
+cudaError_t launch_scale(const float2 *, float2 *, const GroupDev *, int, int, cudaStream_t);
+size_t seg_record_bytes(bool fp64);
+} // namespace bhcb
+
+using namespace bhcb;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct MemError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                           \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if(e_ != cudaSuccess)                                                           \
+            throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));           \
+    } while(0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t n)
+    {
+        if(n <= bytes) return;
+        release();
+        CK(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    void release()
+    {
+        if(p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+struct EnvSlot {
+    std::string root;
+    EnvInput in;
+    std::vector<double> freqs;   // evaluation frequencies (default: file frequency)
+    // filled by prepare
+    std::vector<EnvTables> tables;    // per frequency
+    std::vector<int> field_of_freq;   // global field index per frequency
+};
+
+struct Field {
+    int env, ifreq;
+    int64_t base;        // complex-element offset in acc/out
+    int nsz, nrzp, nrr;
+};
+
+} // namespace
+
+struct bhcb_ctx {
+    int device = 0;
+    int precision = BHCB_PREC_MIXED;
+    bool share = true;
+    uint64_t max_memory = 16ull << 30;
+    void (*output_cb)(const char *) = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int sm_count = 148;
+
+    std::vector<EnvSlot> envs;
+    bool prepared = false;
+
+    // prepared state
+    std::vector<GroupDev> groups_h;
+    std::vector<Field> fields;
+    std::vector<double> freqs_h;
+    int64_t total_field = 0;
+    long long njobs = 0;
+    unsigned long long seg_cap = 0;
+    bool any_gauss = false, any_coherent = false, mixed_types = false;
+    bool gauss = false, coherent = true;
+
+    DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
+    RunCounters last{};
+    bhcb_stats stats{};
+    std::string last_error;
+    uint32_t err_bits = 0, warn_bits = 0;
+
+    void msg(const std::string &s) const
+    {
+        if(output_cb) output_cb(s.c_str());
+    }
+};
+
+namespace {
+
+int fail(bhcb_ctx *c, int code, const std::string &m)
+{
+    if(c) {
+        c->last_error = m;
+        c->msg(m);
+    }
+    return code;
+}
+
+template<typename F> int guarded(bhcb_ctx *c, F &&fn)
+{
+    if(!c) return BHCB_ERR_ARG;
+    try {
+        c->last_error.clear();
+        return fn();
+    } catch(const CudaError &e) {
+        return fail(c, BHCB_ERR_CUDA, e.what());
+    } catch(const StateError &e) {
+        return fail(c, BHCB_ERR_STATE, e.what());
+    } catch(const MemError &e) {
+        return fail(c, BHCB_ERR_MEMORY, e.what());
+    } catch(const std::exception &e) {
+        return fail(c, BHCB_ERR_INPUT, e.what());
+    }
+}
+
+// ------------------------------------------------------------------ arena
+struct Arena {
+    std::vector<uint8_t> bytes;
+    template<typename T> size_t put(const std::vector<T> &v)
+    {
+        size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 8));
+        if(!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+    size_t put_raw(const void *p, size_t n)
+    {
+        size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + n);
+        std::memcpy(bytes.data() + off, p, n);
+        return off;
+    }
+};
+
+template<typename T> T *dptr(void *base, size_t off)
+{
+    return reinterpret_cast<T *>(reinterpret_cast<uint8_t *>(base) + off);
+}
+
+void do_prepare(bhcb_ctx *c)
+{
+    if(c->envs.empty()) throw StateError("no environment: call bhcb_setup or bhcb_add_env first");
+    CK(cudaSetDevice(c->device));
+    c->groups_h.clear();
+    c->fields.clear();
+    c->freqs_h.clear();
+    c->total_field = 0;
+    c->njobs = 0;
+    bool fp64 = c->precision == BHCB_PREC_FP64;
+    // --- preprocess every (env, frequency) and form trace groups
+    struct GroupPlan { int env; std::vector<int> ifreqs; };
+    std::vector<GroupPlan> plan;
+    int nG = 0, nC = 0;
+    for(int e = 0; e < (int)c->envs.size(); ++e) {
+        EnvSlot &S = c->envs[e];
+        S.tables.clear();
+        for(double f : S.freqs) S.tables.push_back(preprocess(S.in, f));
+        for(const auto &w : S.tables[0].warnings) c->msg("warning: " + w);
+        std::vector<bool> done(S.freqs.size(), false);
+        for(size_t i = 0; i < S.freqs.size(); ++i) {
+            if(done[i]) continue;
+            GroupPlan gp{e, {(int)i}};
+            done[i] = true;
+            if(!fp64 && c->share) {
+                for(size_t j = i + 1; j < S.freqs.size(); ++j)
+                    if(!done[j] && S.tables[i].same_trajectory_tables(S.tables[j])
+                       && S.tables[i].alpha == S.tables[j].alpha) {
+                        gp.ifreqs.push_back((int)j);
+                        done[j] = true;
+                    }
+            }
+            plan.push_back(gp);
+        }
+        const EnvTables &T0 = S.tables[0];
+        char bt = T0.beam_type[0];
+        (bt == 'B' ? nG : nC) += 1;
+    }
+    // one launch handles a single influence flavour; mixed batches are split by the caller
+    c->gauss = c->envs[0].tables[0].beam_type[0] == 'B';
+    c->coherent = c->envs[0].tables[0].run_type[0] == 'C';
+    for(auto &S : c->envs) {
+        const EnvTables &T0 = S.tables[0];
+        if((T0.beam_type[0] == 'B') != c->gauss || (T0.run_type[0] == 'C') != c->coherent)
+            throw std::runtime_error("a batch must use one beam type and one coherence mode");
+        char r0 = T0.run_type[0];
+        if(!(r0 == 'C' || r0 == 'S' || r0 == 'I'))
+            throw std::runtime_error("only TL runs (C, S, I) are supported by this entry point");
+    }
+    // --- build device tables
+    Arena A;
+    struct EnvOffsets { size_t z, rho, c, cz, n2, n2z, coef, btop, bbot, rr, rz, sz, alpha, sbp; };
+    std::vector<EnvOffsets> offs;
+    std::vector<EnvDev> envdev;
+    for(const GroupPlan &gp : plan) {
+        const EnvSlot &S = c->envs[gp.env];
+        const EnvTables &T = S.tables[gp.ifreqs[0]];
+        EnvOffsets o;
+        o.z = A.put(T.z); o.rho = A.put(T.rho); o.c = A.put(T.c); o.cz = A.put(T.cz);
+        o.n2 = A.put(T.n2); o.n2z = A.put(T.n2z); o.coef = A.put(T.coef);
+        o.btop = A.put(T.btop); o.bbot = A.put(T.bbot);
+        o.rr = A.put(T.rr); o.rz = A.put(T.rz); o.sz = A.put(T.sz); o.alpha = A.put(T.alpha);
+        o.sbp = A.put(T.sbp);
+        offs.push_back(o);
+        EnvDev d{};
+        d.ssp_type = T.ssp_type;
+        d.nssp = (int)T.z.size();
+        d.top = T.top;
+        d.bot = T.bot;
+        d.ntop = (int)T.btop.size();
+        d.nbot = (int)T.bbot.size();
+        d.top_curv = T.top_curv; d.bot_curv = T.bot_curv;
+        d.top_long = T.top_long; d.bot_long = T.bot_long;
+        d.nrr = (int)T.rr.size();
+        d.nrz = (int)T.rz.size();
+        d.nrz_per_range = T.nrz_per_range;
+        d.nsz = (int)T.sz.size();
+        d.nalpha = (int)T.alpha.size();
+        d.isingle = T.isingle;
+        d.dalpha = T.dalpha;
+        d.delta_r = T.delta_r;
+        d.deltas = T.deltas;
+        d.box_x = T.box_x;
+        d.box_y = T.box_y;
+        d.freq0 = T.freq0;
+        d.run0 = T.run_type[0];
+        d.beam0 = T.beam_type[0];
+        d.beam2 = T.beam_type[2];
+        d.gaussian = T.beam_type[0] == 'B';
+        d.coherent = T.run_type[0] == 'C';
+        d.line_source = T.run_type[3] == 'X';
+        d.irregular = T.run_type[4] == 'I';
+        d.q_zero_init = T.run_type[1] == 'G';
+        d.nsbp = (int)(T.sbp.size() / 2);
+        envdev.push_back(d);
+    }
+    size_t env_off = A.put(envdev);
+    c->arena.ensure(A.bytes.size());
+    void *ab = c->arena.p;
+    // patch device pointers
+    for(size_t g = 0; g < plan.size(); ++g) {
+        EnvDev &d = *reinterpret_cast<EnvDev *>(A.bytes.data() + env_off + g * sizeof(EnvDev));
+        const EnvOffsets &o = offs[g];
+        d.z = dptr<double>(ab, o.z); d.rho = dptr<double>(ab, o.rho);
+        d.c = dptr<double>(ab, o.c); d.cz = dptr<double>(ab, o.cz);
+        d.n2 = dptr<double>(ab, o.n2); d.n2z = dptr<double>(ab, o.n2z);
+        d.coef = dptr<double>(ab, o.coef);
+        d.btop = dptr<BdryPtDev>(ab, o.btop); d.bbot = dptr<BdryPtDev>(ab, o.bbot);
+        d.rr = dptr<double>(ab, o.rr); d.rz = dptr<float>(ab, o.rz); d.sz = dptr<float>(ab, o.sz);
+        d.alpha = dptr<double>(ab, o.alpha); d.sbp = dptr<double>(ab, o.sbp);
+    }
+    CK(cudaMemcpyAsync(ab, A.bytes.data(), A.bytes.size(), cudaMemcpyHostToDevice, c->stream));
+    // --- groups, fields, frequencies
+    for(auto &S : c->envs) S.field_of_freq.assign(S.freqs.size(), -1);
+    for(size_t g = 0; g < plan.size(); ++g) {
+        const GroupPlan &gp = plan[g];
+        EnvSlot &S = c->envs[gp.env];
+        const EnvTables &T = S.tables[gp.ifreqs[0]];
+        GroupDev G{};
+        G.env = dptr<EnvDev>(ab, env_off + g * sizeof(EnvDev));
+        int nal = T.isingle > 0 ? 1 : (int)T.alpha.size();
+        G.job_base = c->njobs;
+        G.njobs = (int)(nal * T.sz.size());
+        G.nfreq = (int)gp.ifreqs.size();
+        G.freq_base = (int)c->freqs_h.size();
+        G.field_stride_f = (int)(T.sz.size() * T.nrz_per_range * T.rr.size());
+        G.field_base = c->total_field;
+        for(size_t k = 0; k < gp.ifreqs.size(); ++k) {
+            int fi = gp.ifreqs[k];
+            c->freqs_h.push_back(S.freqs[fi]);
+            Field F{gp.env, fi, c->total_field + (int64_t)k * G.field_stride_f, (int)T.sz.size(),
+                    T.nrz_per_range, (int)T.rr.size()};
+            S.field_of_freq[fi] = (int)c->fields.size();
+            c->fields.push_back(F);
+        }
+        c->total_field += (int64_t)G.nfreq * G.field_stride_f;
+        c->njobs += G.njobs;
+        c->groups_h.push_back(G);
+    }
+    c->groups_d.ensure(c->groups_h.size() * sizeof(GroupDev));
+    CK(cudaMemcpyAsync(c->groups_d.p, c->groups_h.data(), c->groups_h.size() * sizeof(GroupDev),
+                       cudaMemcpyHostToDevice, c->stream));
+    c->freqs_d.ensure(c->freqs_h.size() * sizeof(double));
+    CK(cudaMemcpyAsync(c->freqs_d.p, c->freqs_h.data(), c->freqs_h.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, c->stream));
+    size_t fbytes = (size_t)c->total_field * sizeof(float2);
+    c->acc.ensure(fbytes);
+    c->out.ensure(fbytes);
+    c->counters.ensure(sizeof(RunCounters) + 64);
+    // segment buffer: grows on overflow
+    size_t rec = seg_record_bytes(fp64);
+    size_t budget = c->max_memory > 3 * fbytes ? c->max_memory - 3 * fbytes : 0;
+    unsigned long long want = std::max<unsigned long long>(c->seg_cap, (unsigned long long)c->njobs * 1024ull);
+    unsigned long long maxcap = budget / rec;
+    if(maxcap < 1024) throw MemError("max_memory too small for the segment buffer");
+    c->seg_cap = std::min(want, maxcap);
+    c->segs.ensure(c->seg_cap * rec);
+    c->prepared = true;
+}
+
+void do_launch(bhcb_ctx *c)
+{
+    if(!c->prepared) throw StateError("bhcb_launch before bhcb_prepare");
+    bool fp64 = c->precision == BHCB_PREC_FP64;
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(RunCounters) + 64, c->stream));
+    RunCounters *ctr = (RunCounters *)c->counters.p;
+    unsigned long long init_overflow = 0xffffffffull;
+    CK(cudaMemcpyAsync(&ctr->overflow_job, &init_overflow, 4, cudaMemcpyHostToDevice, c->stream));
+    unsigned long long *jobc = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
+    CK(cudaMemsetAsync(c->acc.p, 0, (size_t)c->total_field * sizeof(float2), c->stream));
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    int tblock = 32;
+    long long tgrid = std::min<long long>((c->njobs + tblock - 1) / tblock, (long long)c->sm_count * 16);
+    if(tgrid < 1) tgrid = 1;
+    const GroupDev *G = (const GroupDev *)c->groups_d.p;
+    int ng = (int)c->groups_h.size();
+    if(fp64)
+        CK(launch_trace<double>(G, ng, c->njobs, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
+    else
+        CK(launch_trace<float>(G, ng, c->njobs, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    // the influence grid covers the buffer capacity; chunks past the stored
+    // count are skipped by reading the count on the device
+    int igrid = c->sm_count * 8;
+    if(fp64)
+        CK(launch_influence<double>(c->segs.p, c->seg_cap, G, ng, (const double *)c->freqs_d.p,
+                                    (float2 *)c->acc.p, ctr, c->gauss, c->coherent, igrid, c->stream));
+    else
+        CK(launch_influence<float>(c->segs.p, c->seg_cap, G, ng, (const double *)c->freqs_d.p,
+                                   (float2 *)c->acc.p, ctr, c->gauss, c->coherent, igrid, c->stream));
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(launch_scale((const float2 *)c->acc.p, (float2 *)c->out.p, G, ng, c->sm_count * 2, c->stream));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+}
+
+int do_sync(bhcb_ctx *c)
+{
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(&c->last, c->counters.p, sizeof(RunCounters), cudaMemcpyDeviceToHost));
+    float t0 = 0, t1 = 0, t2 = 0;
+    CK(cudaEventElapsedTime(&t0, c->ev[0], c->ev[1]));
+    CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&t2, c->ev[0], c->ev[3]));
+    c->stats.rays = (uint64_t)c->njobs;
+    c->stats.steps = c->last.nsteps;
+    c->stats.segments = c->last.nseg;
+    c->stats.evals = c->last.nevals;
+    c->stats.err_bits = c->last.err_bits;
+    c->stats.warn_bits = c->last.warn_bits;
+    c->stats.groups = (int)c->groups_h.size();
+    c->stats.fields = (int)c->fields.size();
+    c->stats.trace_ms = t0;
+    c->stats.influence_ms = t1;
+    c->stats.total_ms = t2;
+    c->err_bits = c->last.err_bits;
+    c->warn_bits = c->last.warn_bits;
+    return 0;
+}
+
+int run_checked(bhcb_ctx *c)
+{
+    for(int attempt = 0; attempt < 8; ++attempt) {
+        do_launch(c);
+        do_sync(c);
+        if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
+            // grow the segment buffer and run again
+            size_t rec = seg_record_bytes(c->precision == BHCB_PREC_FP64);
+            size_t fbytes = (size_t)c->total_field * sizeof(float2);
+            size_t budget = c->max_memory > 3 * fbytes ? c->max_memory - 3 * fbytes : 0;
+            unsigned long long maxcap = budget / rec;
+            if(c->seg_cap >= maxcap)
+                throw MemError("segment buffer exceeds max_memory; raise bhcb_init.max_memory");
+            c->seg_cap = std::min(maxcap, std::max(c->seg_cap * 2, (unsigned long long)(c->last.nseg * 1.25)));
+            c->segs.ensure(c->seg_cap * rec);
+            continue;
+        }
+        if(c->last.err_bits) {
+            char b[96];
+            snprintf(b, sizeof b, "tracer error bits 0x%x", c->last.err_bits);
+            return fail(c, BHCB_ERR_RUN, b);
+        }
+        return BHCB_OK;
+    }
+    return fail(c, BHCB_ERR_MEMORY, "segment buffer overflow persisted");
+}
+
+const Field *find_field(bhcb_ctx *c, int env, int ifreq)
+{
+    if(!c->prepared) throw StateError("no run has been prepared");
+    if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
+    const EnvSlot &S = c->envs[env];
+    if(ifreq < 0 || ifreq >= (int)S.field_of_freq.size()) throw std::invalid_argument("ifreq out of range");
+    return &c->fields[S.field_of_freq[ifreq]];
+}
+
+} // namespace
+
+extern "C" {
+
+int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
+{
+    if(!out) return BHCB_ERR_ARG;
+    *out = nullptr;
+    auto c = std::make_unique<bhcb_ctx>();
+    if(init) {
+        c->device = init->gpu_index;
+        c->precision = init->precision == BHCB_PREC_FP64 ? BHCB_PREC_FP64 : BHCB_PREC_MIXED;
+        if(init->max_memory) c->max_memory = init->max_memory;
+        c->share = init->share_trajectory != 0;
+        c->output_cb = init->output_callback;
+    }
+    int ndev = 0;
+    if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return BHCB_ERR_CUDA;
+    }
+    if(c->device < 0 || c->device >= ndev) return BHCB_ERR_ARG;
+    if(cudaSetDevice(c->device) != cudaSuccess) return BHCB_ERR_CUDA;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return BHCB_ERR_CUDA;
+    for(auto &e : c->ev)
+        if(cudaEventCreate(&e) != cudaSuccess) return BHCB_ERR_CUDA;
+    *out = c.release();
+    return BHCB_OK;
+}
+
+void bhcb_close(bhcb_ctx *c)
+{
+    if(!c) return;
+    cudaSetDevice(c->device);
+    if(c->stream) cudaStreamSynchronize(c->stream);
+    for(DevBuf *b : {&c->arena, &c->groups_d, &c->freqs_d, &c->acc, &c->out, &c->segs, &c->counters})
+        b->release();
+    for(auto &e : c->ev)
+        if(e) cudaEventDestroy(e);
+    if(c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int bhcb_clear(bhcb_ctx *c)
+{
+    return guarded(c, [&]() -> int {
+        c->envs.clear();
+        c->prepared = false;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_add_env(bhcb_ctx *c, const char *root, int32_t *idx)
+{
+    return guarded(c, [&]() -> int {
+        if(!root) throw std::invalid_argument("file_root is NULL");
+        EnvSlot S;
+        S.root = root;
+        S.in = read_env_files(root);
+        S.freqs = {S.in.freq0};
+        preprocess(S.in, S.in.freq0);   // validate now, like bhc::setup's Validate pass
+        c->envs.push_back(std::move(S));
+        c->prepared = false;
+        if(idx) *idx = (int32_t)c->envs.size() - 1;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_setup(bhcb_ctx *c, const char *root)
+{
+    int r = bhcb_clear(c);
+    if(r) return r;
+    return bhcb_add_env(c, root, nullptr);
+}
+
+int bhcb_set_frequencies(bhcb_ctx *c, int32_t env, int32_t n, const double *f)
+{
+    return guarded(c, [&]() -> int {
+        if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
+        if(n <= 0 || !f) throw std::invalid_argument("need at least one frequency");
+        for(int i = 0; i < n; ++i)
+            if(!(f[i] > 0.0)) throw std::invalid_argument("frequencies must be positive");
+        c->envs[env].freqs.assign(f, f + n);
+        c->prepared = false;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_prepare(bhcb_ctx *c)
+{
+    return guarded(c, [&]() -> int {
+        do_prepare(c);
+        return BHCB_OK;
+    });
+}
+
+int bhcb_launch(bhcb_ctx *c)
+{
+    return guarded(c, [&]() -> int {
+        do_launch(c);
+        return BHCB_OK;
+    });
+}
+
+int bhcb_sync(bhcb_ctx *c)
+{
+    return guarded(c, [&]() -> int {
+        do_sync(c);
+        if(c->last.err_bits) {
+            char b[96];
+            snprintf(b, sizeof b, "tracer error bits 0x%x", c->last.err_bits);
+            return fail(c, (c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) ? BHCB_ERR_MEMORY : BHCB_ERR_RUN, b);
+        }
+        return BHCB_OK;
+    });
+}
+
+int bhcb_run(bhcb_ctx *c)
+{
+    return guarded(c, [&]() -> int {
+        if(!c->prepared) do_prepare(c);
+        return run_checked(c);
+    });
+}
+
+int bhcb_field_shape(bhcb_ctx *c, int32_t env, int32_t *nfreq, int32_t *nsz, int32_t *nrzp, int32_t *nrr)
+{
+    return guarded(c, [&]() -> int {
+        if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
+        const EnvSlot &S = c->envs[env];
+        EnvTables T = S.tables.empty() ? preprocess(S.in, S.freqs[0]) : S.tables[0];
+        if(nfreq) *nfreq = (int32_t)S.freqs.size();
+        if(nsz) *nsz = (int32_t)T.sz.size();
+        if(nrzp) *nrzp = T.nrz_per_range;
+        if(nrr) *nrr = (int32_t)T.rr.size();
+        return BHCB_OK;
+    });
+}
+
+int bhcb_copy_field(bhcb_ctx *c, int32_t env, int32_t ifreq, void *dst, size_t bytes)
+{
+    return guarded(c, [&]() -> int {
+        const Field *F = find_field(c, env, ifreq);
+        size_t need = (size_t)F->nsz * F->nrzp * F->nrr * sizeof(float2);
+        if(!dst || bytes < need) throw std::invalid_argument("destination too small");
+        CK(cudaMemcpyAsync(dst, (float2 *)c->out.p + F->base, need, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return BHCB_OK;
+    });
+}
+
+int bhcb_field_device(bhcb_ctx *c, int32_t env, int32_t ifreq, void **dptr_out)
+{
+    return guarded(c, [&]() -> int {
+        const Field *F = find_field(c, env, ifreq);
+        if(!dptr_out) throw std::invalid_argument("dptr is NULL");
+        *dptr_out = (float2 *)c->out.p + F->base;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_receivers(bhcb_ctx *c, int32_t env, double *rr, int32_t nrr, float *rz, int32_t nrz)
+{
+    return guarded(c, [&]() -> int {
+        if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
+        const EnvSlot &S = c->envs[env];
+        EnvTables T = S.tables.empty() ? preprocess(S.in, S.freqs[0]) : S.tables[0];
+        if(rr) std::memcpy(rr, T.rr.data(), std::min<size_t>(nrr, T.rr.size()) * sizeof(double));
+        if(rz) std::memcpy(rz, T.rz.data(), std::min<size_t>(nrz, T.rz.size()) * sizeof(float));
+        return BHCB_OK;
+    });
+}
+
+int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
+{
+    return guarded(c, [&]() -> int {
+        const Field *F = find_field(c, env, ifreq);
+        const EnvSlot &S = c->envs[env];
+        const EnvTables &T = S.tables[ifreq];
+        std::vector<float2> u((size_t)F->nsz * F->nrzp * F->nrr);
+        CK(cudaMemcpyAsync(u.data(), (float2 *)c->out.p + F->base, u.size() * sizeof(float2),
+                           cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        // .shd layout: src/mode/tl.cpp:38-101 (header), 195-248 (records)
+        int nsz = F->nsz, nrz = (int)T.rz.size(), nrr = F->nrr;
+        int32_t lrecl = 84;
+        lrecl = std::max<int32_t>(lrecl, 2 * 1 * 8);
+        lrecl = std::max<int32_t>(lrecl, 1 * 8);
+        lrecl = std::max<int32_t>(lrecl, nsz * 4);
+        lrecl = std::max<int32_t>(lrecl, nrz * 4);
+        lrecl = std::max<int32_t>(lrecl, nrr * 8);
+        int nrec = 10 + nsz * F->nrzp;
+        std::vector<uint8_t> buf((size_t)lrecl * nrec, 0);
+        auto rec = [&](int r) { return buf.data() + (size_t)r * lrecl; };
+        int32_t lw = lrecl / 4;
+        std::memcpy(rec(0), &lw, 4);
+        std::string title = S.in.title;
+        title.resize(80, ' ');
+        std::memcpy(rec(0) + 4, title.data(), 80);
+        const char *pt = T.run_type[4] == 'I' ? "irregular " : "rectilin  ";
+        std::memcpy(rec(1), pt, 10);
+        int32_t hdr[7] = {1, 1, 1, 1, nsz, nrz, nrr};
+        std::memcpy(rec(2), hdr, sizeof hdr);
+        double f0 = S.freqs[ifreq], atten = 0.0;
+        std::memcpy(rec(2) + 28, &f0, 8);
+        std::memcpy(rec(2) + 36, &atten, 8);
+        std::memcpy(rec(3), &f0, 8);
+        double zero = 0.0;
+        std::memcpy(rec(4), &zero, 8);
+        std::memcpy(rec(5), &zero, 8); std::memcpy(rec(5) + 8, &zero, 8);
+        std::memcpy(rec(6), &zero, 8); std::memcpy(rec(6) + 8, &zero, 8);
+        std::memcpy(rec(7), T.sz.data(), nsz * 4);
+        std::memcpy(rec(8), T.rz.data(), nrz * 4);
+        std::memcpy(rec(9), T.rr.data(), nrr * 8);
+        for(int isz = 0; isz < nsz; ++isz)
+            for(int iz = 0; iz < F->nrzp; ++iz)
+                std::memcpy(rec(10 + isz * F->nrzp + iz), &u[((size_t)isz * F->nrzp + iz) * nrr],
+                            (size_t)nrr * 8);
+        std::ofstream o(std::string(root) + ".shd", std::ios::binary);
+        if(!o.good()) throw std::runtime_error(std::string("cannot open ") + root + ".shd");
+        o.write((const char *)buf.data(), buf.size());
+        return BHCB_OK;
+    });
+}
+
+int bhcb_get_stats(bhcb_ctx *c, bhcb_stats *s)
+{
+    if(!c || !s) return BHCB_ERR_ARG;
+    *s = c->stats;
+    return BHCB_OK;
+}
+
+int bhcb_last_error(bhcb_ctx *c, char *msg, size_t n, uint32_t *eb, uint32_t *wb)
+{
+    if(!c) return BHCB_ERR_ARG;
+    if(msg && n) {
+        size_t l = std::min(n - 1, c->last_error.size());
+        std::memcpy(msg, c->last_error.data(), l);
+        msg[l] = 0;
+    }
+    if(eb) *eb = c->err_bits;
+    if(wb) *wb = c->warn_bits;
+    return BHCB_OK;
+}
+
+int bhcb_check_env(const char *root, bhcb_env_info *info, char *msg, size_t n)
+{
+    try {
+        if(!root) throw std::invalid_argument("file_root is NULL");
+        EnvInput in = read_env_files(root);
+        EnvTables T = preprocess(in, in.freq0);
+        if(info) {
+            std::memset(info, 0, sizeof(*info));
+            info->nsz = (int32_t)T.sz.size();
+            info->nrz = (int32_t)T.rz.size();
+            info->nrz_per_range = T.nrz_per_range;
+            info->nrr = (int32_t)T.rr.size();
+            info->nalpha = (int32_t)T.alpha.size();
+            info->ssp_type = T.ssp_type;
+            info->freq = T.freq0;
+            info->deltas = T.deltas;
+            std::memcpy(info->run_type, T.run_type, 7);
+            std::memcpy(info->beam_type, T.beam_type, 4);
+        }
+        if(msg && n) msg[0] = 0;
+        return BHCB_OK;
+    } catch(const std::exception &e) {
+        if(msg && n) {
+            size_t l = std::min(n - 1, std::strlen(e.what()));
+            std::memcpy(msg, e.what(), l);
+            msg[l] = 0;
+        }
+        return BHCB_ERR_INPUT;
+    }
+}
+
+const char *bhcb_version(void) { return "bhcb 0.1 (sm_100a)"; }
+
+} // extern "C"

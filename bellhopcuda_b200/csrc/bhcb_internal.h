@@ -1,0 +1,117 @@
+// Internal data layout shared by the host runtime and the sm_100a kernels.
+//
+// One "environment" (EnvDev) is the preprocessed, device-resident form of one
+// bhcParams set (reference: include/bhc/structs.hpp:548-563) for one trace
+// frequency. A "group" is one environment plus the list of frequencies whose
+// fields are evaluated from its trajectories (1 for a plain run; N when the
+// environment's tables are frequency independent and frequencies share one
+// trajectory). A launch processes a batch of groups; its rays ("jobs") are
+// numbered group-major, then source depth, then launch angle, matching the
+// reference's job order within a group (src/common.hpp:347-391).
+#pragma once
+#include <stdint.h>
+
+namespace bhcb {
+
+// SSP interpolation types (reference: src/runtype.hpp:52-75)
+enum SspType : int32_t { SSP_N2LINEAR = 0, SSP_CLINEAR = 1, SSP_CUBIC = 2, SSP_PCHIP = 3,
+                         SSP_ANALYTIC = 4 };
+
+// error / warning bits: same numbering as the reference's ErrState
+// (src/util/errors.hpp:61-93); BHCB_ERR_SEG_OVERFLOW is this runtime's own.
+enum : uint32_t {
+    ERR_RAYINIT = 2, ERR_BOUNDARY_SEG_NAN = 3, ERR_BOUNDARY_CONDITION_TYPE = 4,
+    ERR_INVALID_SSP_TYPE = 5, ERR_OUTSIDE_ALTIMETRY = 6, ERR_OUTSIDE_BATHYMETRY = 7,
+    ERR_SEG_OVERFLOW = 31,
+};
+enum : uint32_t {
+    WARN_ONERAY_OUTOFMEMORY = 1, WARN_TOO_FEW_BEAMS = 3, WARN_SOURCE_OUTSIDE_BOUNDARIES = 4,
+    WARN_STEP_NEGATIVE_H = 8, WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17,
+};
+
+struct HsDev {          // halfspace (include/bhc/structs.hpp:93-101)
+    double cPr, cPi, cSr, cSi, rho;
+    int32_t bc;         // 'V','R','A','G'
+    int32_t pad;
+};
+
+struct BdryPtDev {      // 2-D boundary node (include/bhc/structs.hpp:147-170)
+    double x[2], t[2], n[2], Noden[2], Nodet[2];
+    double Len, kappa;
+    double cPr, cPi, cSr, cSi, rho;   // per-segment halfspace (long format 'L')
+};
+
+struct EnvDev {
+    // SSP tables (reference SSPStructure, include/bhc/structs.hpp:73-91)
+    int32_t ssp_type, nssp;
+    const double *z, *rho;
+    const double *c, *cz;      // complex, interleaved re/im, [nssp]
+    const double *n2, *n2z;    // complex [nssp]
+    const double *coef;        // complex [4][nssp]: spline (S) or pchip (P) coefficients
+    HsDev top, bot;
+    // boundaries
+    int32_t ntop, nbot;
+    int32_t top_curv, bot_curv;      // type[0] == 'C'
+    int32_t top_long, bot_long;      // type[1] == 'L'
+    const BdryPtDev *btop, *bbot;
+    // receivers / sources / angles (include/bhc/structs.hpp:278-321)
+    int32_t nrr, nrz, nrz_per_range, nsz, nalpha, isingle;
+    const double *rr;
+    const float *rz, *sz;
+    const double *alpha;
+    double dalpha, delta_r;
+    // beam (include/bhc/structs.hpp:331-341)
+    double deltas, box_x, box_y, freq0;
+    int32_t run0;                    // RunType[0]
+    int32_t beam0;                   // Beam->Type[0] after MoveBeamType
+    int32_t beam2;                   // Beam->Type[2] curvature option
+    int32_t gaussian, coherent, line_source, irregular, q_zero_init;
+    // source beam pattern: pairs (angle deg, linear level)
+    int32_t nsbp, pad0;
+    const double *sbp;
+};
+
+struct GroupDev {
+    const EnvDev *env;       // device pointer
+    int64_t job_base;        // first job index of this group
+    int32_t njobs;           // nsz_or_1 * nalpha_or_1
+    int32_t nfreq;           // frequencies evaluated from this group's trajectories
+    int32_t freq_base;       // index of first frequency slot in the launch's freq list
+    int32_t field_stride_f;  // complex elements per frequency field of this group
+    int64_t field_base;      // offset (complex elements) of this group's first field
+};
+
+// One influence segment (point0 -> point1 of Step_InfluenceGeoCart,
+// src/influence.hpp:1201-1406), with the receiver-column walk already done.
+template<typename R> struct SegRec {
+    double x0r, x0z;      // point0.x
+    double tau0r;         // point0.tau.real()
+    R dtaur, tau0i, dtaui;
+    R tx, tz;             // unit ray tangent (rayt)
+    R rlen;               // segment length
+    R q0, dq;             // point0.q.x, point1.q.x - point0.q.x
+    R rcp_q0;             // Dalpha / c0 of the ray
+    R cnst_num;           // Ratio1 * sqrt(point1.c) * point1.Amp
+    R phase_a;            // (Gaussian ? point1 : point0).Phase + inflray.phase
+    R phase_b;            // inflray.phase + pi/2 (caustic branch of FinalPhase)
+    R sigma_seg;          // max|q| * rcp_q0 / |rayt.x| before AdjustSigma
+    R c0;                 // point0.c (Gaussian AdjustSigma wavelength)
+    R tau1r;              // point1.tau.real() (Gaussian AdjustSigma)
+    R zlo, zhi;           // min / max depth of the segment
+    R rcvr_decl;          // receiver declination angle (deg)
+    int32_t ir_lo, ir_hi; // receiver columns evaluated (inclusive), ir_lo <= ir_hi
+    int32_t job;          // global job (ray) index
+    int32_t is;           // step index along the ray
+    int32_t ntop, nbot;   // bounce counts of point1
+};
+
+struct RunCounters {
+    unsigned long long nseg;      // segments appended
+    unsigned long long nsteps;    // ray steps taken
+    unsigned long long nevals;    // beam-receiver contributions applied
+    unsigned int err_bits, warn_bits;
+    unsigned int overflow_job;    // first job that could not store its segments
+    unsigned int pad;
+};
+
+} // namespace bhcb

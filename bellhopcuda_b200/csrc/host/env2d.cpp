@@ -1,0 +1,664 @@
+#include "env2d.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "ldi.h"
+
+namespace bhcb {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+inline double FLT(float f) { return (double)f; }   // reference FL() literal
+
+[[noreturn]] void env_error(const std::string &m) { throw std::runtime_error(m); }
+
+// ------------------------------------------------------------------ reading
+// vector read with the -999.9 sub-tabulation markers preset
+// (src/common_setup.hpp:370-381 ReadVector)
+template<typename T> void read_vector(LdiReader &f, int32_t &n, std::vector<T> &x)
+{
+    f.record();
+    f.read(n);
+    if(n <= 0) env_error("vector length must be positive");
+    x.assign(std::max(3, n), (T)0);
+    x[1] = x[2] = (T)(-999.9f);
+    f.record();
+    for(int i = 0; i < n; ++i) f.read(x[i]);
+}
+
+void read_bdry_file(const std::string &path, BdryIn &b)
+{
+    LdiReader f(path);
+    if(!f.good()) env_error("unable to open boundary file " + path);
+    f.record();
+    f.read_chars(b.type, 2);
+    int32_t n = 0;
+    f.record();
+    f.read(n);
+    if(n < 1) env_error("boundary file " + path + ": bad point count");
+    b.r_km.assign(n, 0.0);
+    b.z.assign(n, 0.0);
+    b.geo.assign(b.type[1] == 'L' ? n : 0, {0, 0, 0, 0, 0});
+    for(int i = 0; i < n; ++i) {
+        f.record();
+        f.read(b.r_km[i]);
+        f.read(b.z[i]);
+        if(b.type[1] == 'L')
+            for(int k = 0; k < 5; ++k) f.read(b.geo[i][k]);
+    }
+    b.file = true;
+}
+
+// ------------------------------------------------------------- preprocessing
+double franc_garr(double f, const double fg[4])
+{
+    double T = fg[0], S = fg[1], pH = fg[2], zb = fg[3];
+    double c = FLT(1412.0) + FLT(3.21) * T + FLT(1.19) * S + FLT(0.0167) * zb;
+    double a1 = FLT(8.86) / c * std::pow(FLT(10.0), FLT(0.78) * pH - FLT(5.0));
+    double p1 = FLT(1.0);
+    double f1 = FLT(2.8) * std::sqrt(S / 35) * std::pow(FLT(1.0), FLT(4.0) - FLT(1245.0) / (T + FLT(273.0)));
+    double a2 = FLT(21.44) * S / c * (FLT(1.0) + FLT(0.025) * T);
+    double p2 = FLT(1.0) - 1.37e-4 * zb + 6.2e-9 * zb * zb;
+    double f2 = FLT(8.17) * std::pow(FLT(10.0), FLT(8.0) - FLT(1990.0) / (T + 273))
+        / (FLT(1.0) + FLT(0.0018) * (S - FLT(35.0)));
+    double p3 = FLT(1.0) - 3.83e-5 * zb + 4.9e-10 * zb * zb;
+    double a3 = (T < FLT(20.0))
+        ? 4.937e-4 - 2.59e-5 * T + 9.11e-7 * T * T - 1.5e-8 * T * T * T
+        : 3.964e-4 - 1.146e-5 * T + 1.45e-7 * T * T - 6.5e-10 * T * T * T;
+    return a1 * p1 * (f1 * f * f) / (f1 * f1 + f * f) + a2 * p2 * (f2 * f * f) / (f2 * f2 + f * f)
+        + a3 * p3 * f * f;
+}
+
+// attenuation -> complex sound speed (src/module/atten.cpp:99-194)
+cpxd crci(const EnvInput &in, double freq, double fT, double z, double c, double alpha, char au0,
+          char au1)
+{
+    double freq0 = freq;
+    double omega = FLT(2.0) * kPi * freq;
+    double aT = 0.0;
+    switch(au0) {
+    case 'N': aT = alpha; break;
+    case 'M': aT = alpha / 8.6858896; break;
+    case 'm':
+        aT = alpha / 8.6858896;
+        if(freq < fT) aT *= std::pow(freq / freq0, 1.0);
+        else aT *= (freq / freq0) * std::pow(fT / freq0, 1.0 - FLT(1.0));
+        break;
+    case 'F': aT = alpha * freq / 8685.8896; break;
+    case 'W': if(std::fabs(c) >= DBL_EPSILON) aT = alpha * freq / (8.6858896 * c); break;
+    case 'Q': if(std::fabs(c * alpha) >= DBL_EPSILON) aT = omega / (FLT(2.0) * c * alpha); break;
+    case 'L': if(std::fabs(c) >= DBL_EPSILON) aT = alpha * omega / c; break;
+    }
+    if(au1 == 'T') {
+        double f2 = (freq / FLT(1000.0)) * (freq / FLT(1000.0));
+        double th = FLT(3.3e-3) + FLT(0.11) * f2 / (FLT(1.0) + f2) + FLT(44.0) * f2 / (FLT(4100.0) + f2)
+            + FLT(3e-4) * f2;
+        aT += th / FLT(8685.8896);
+    } else if(au1 == 'F') {
+        aT += franc_garr(freq / FLT(1000.0), in.fg) / FLT(8685.8896);
+    } else if(au1 == 'B') {
+        for(const auto &b : in.bio) {
+            if(z >= b[0] && z <= b[1]) {
+                double q = 1.0 - (b[2] * b[2]) / (freq * freq);
+                aT += (b[4] / (q * q + 1.0 / (b[3] * b[3]))) / FLT(8685.8896);
+            }
+        }
+    }
+    aT *= (c * c) / omega;
+    return cpxd(c, aT);
+}
+
+// de Boor cubic spline with complex ordinates (src/curves.hpp:76-188)
+void cspline(const double *tau, cpxd *c1, cpxd *c2, cpxd *c3, cpxd *c4, int n, int ibcbeg, int ibcend)
+{
+    cpxd g = 0.0;
+    int l = n - 1;
+    for(int m = 1; m < n; ++m) {
+        c3[m] = cpxd(tau[m] - tau[m - 1], FLT(0.0));
+        c4[m] = (c1[m] - c1[m - 1]) / c3[m];
+    }
+    if(ibcbeg == 0) {
+        if(n > 2) {
+            c4[0] = c3[2];
+            c3[0] = c3[1] + c3[2];
+            c2[0] = ((c3[1] + FLT(2.0) * c3[0]) * c4[1] * c3[2] + (c3[1] * c3[1]) * c4[2]) / c3[0];
+        } else {
+            c4[0] = cpxd(1.0, 0.0);
+            c3[0] = cpxd(1.0, 0.0);
+            c2[0] = FLT(2.0) * c4[1];
+        }
+    } else if(ibcbeg == 1) {
+        c4[0] = cpxd(1.0, 0.0);
+        c3[0] = cpxd(0.0, 0.0);
+    } else if(ibcbeg == 2) {
+        c4[0] = cpxd(2.0, 0.0);
+        c3[0] = cpxd(1.0, 0.0);
+        c2[0] = FLT(3.0) * c4[1] - c2[0] * c3[1] * FLT(0.5);
+    }
+    for(int m = 1; m < l; ++m) {
+        g = -c3[m + 1] / c4[m - 1];
+        c2[m] = g * c2[m - 1] + FLT(3.0) * (c3[m] * c4[m + 1] + c3[m + 1] * c4[m]);
+        c4[m] = g * c3[m - 1] + FLT(2.0) * (c3[m] + c3[m + 1]);
+    }
+    if(ibcend != 1) {
+        if(ibcend == 0) {
+            if(n == 2 && ibcbeg == 0) {
+                c2[n - 1] = c4[n - 1];
+            } else if((n == 3 && ibcbeg == 0) || n == 2) {
+                c2[n - 1] = FLT(2.0) * c4[n - 1];
+                c4[n - 1] = cpxd(1.0, 0.0);
+                g = FLT(1.0) / -c4[n - 2];
+            } else {
+                g = c3[n - 2] + c3[n - 1];
+                c2[n - 1] = ((c3[n - 1] + FLT(2.0) * g) * c4[n - 1] * c3[n - 2]
+                             + (c3[n - 1] * c3[n - 1]) * (c1[n - 2] - c1[n - 3]) / c3[n - 2]) / g;
+                g = -g / c4[n - 2];
+                c4[n - 1] = c3[n - 2];
+            }
+        } else if(ibcend == 2) {
+            c2[n - 1] = FLT(3.0) * c4[n - 1] + c2[n - 1] * c3[n - 1] * FLT(0.5);
+            c4[n - 1] = cpxd(2.0, 0.0);
+            g = FLT(1.0) / -c4[n - 2];
+        }
+        if(ibcbeg > 0 || n > 2) {
+            c4[n - 1] += g * c3[n - 2];
+            c2[n - 1] = (g * c2[n - 2] + c2[n - 1]) / c4[n - 1];
+        }
+    }
+    for(int j = l - 1; j >= 0; --j) c2[j] = (c2[j] - c3[j] * c2[j + 1]) / c4[j];
+    for(int i = 1; i < n; ++i) {
+        cpxd dtau = c3[i];
+        cpxd divdf1 = (c1[i] - c1[i - 1]) / dtau;
+        cpxd divdf3 = c2[i - 1] + c2[i] - FLT(2.0) * divdf1;
+        c3[i - 1] = FLT(2.0) * (divdf1 - c2[i - 1] - divdf3) / dtau;
+        c4[i - 1] = (divdf3 / dtau) * (FLT(6.0) / dtau);
+    }
+    c3[n - 1] = c3[l - 1] + (tau[n - 1] - tau[l - 1]) * c4[l - 1];
+    c4[n - 1] = cpxd(0.0, 0.0);
+    for(int i = 0; i < l; ++i) {
+        double dt = tau[i + 1] - tau[i];
+        c4[n - 1] += dt * (c1[i] + dt * (c2[i] * FLT(0.5) + dt * (c3[i] / FLT(6.0) + dt * c4[i] / FLT(24.0))));
+    }
+    c4[n - 1] /= tau[n - 1] - tau[0];
+}
+
+double fp_interior(double d1, double d2, double fp)
+{
+    if(d1 * d2 > FLT(0.0)) {
+        if(d1 > FLT(0.0)) return std::min(std::max(fp, 0.0), 3.0 * std::min(d1, d2));
+        return std::max(std::min(fp, 0.0), 3.0 * std::max(d1, d2));
+    }
+    return 0.0;
+}
+double fp_left(double d1, double d2, double fp)
+{
+    if(d1 * fp <= 0.0) return FLT(0.0);
+    if((d1 * d2 <= 0.0) && (std::fabs(fp) > std::fabs(3.0 * d1))) return 3.0 * d1;
+    return fp;
+}
+
+// monotone PCHIP coefficients (src/curves.hpp:206-372)
+void pchip(const double *x, const cpxd *y, int n, cpxd *p1, cpxd *p2, cpxd *p3, cpxd *p4)
+{
+    if(n == 2) {
+        p1[0] = y[0];
+        p2[0] = (y[1] - y[0]) / (x[1] - x[0]);
+        p3[0] = 0.0;
+        p4[0] = 0.0;
+        return;
+    }
+    std::vector<cpxd> w1(n), w2(n), w3(n), w4(n);
+    for(int i = 0; i < n; ++i) p1[i] = y[i];
+    auto hdel = [&](int ix, double &h1, double &h2, cpxd &d1, cpxd &d2) {
+        h1 = x[ix] - x[ix - 1];
+        h2 = x[ix + 1] - x[ix];
+        d1 = (y[ix] - y[ix - 1]) / h1;
+        d2 = (y[ix + 1] - y[ix]) / h2;
+    };
+    double h1, h2;
+    cpxd d1, d2, ft;
+    hdel(1, h1, h2, d1, d2);
+    ft = ((2.0 * h1 + h2) * d1 - h1 * d2) / (h1 + h2);
+    p2[0] = cpxd(fp_left(d1.real(), d2.real(), ft.real()), fp_left(d1.imag(), d2.imag(), ft.imag()));
+    hdel(n - 2, h1, h2, d1, d2);
+    ft = (-h2 * d1 + (h1 + 2.0 * h2) * d2) / (h1 + h2);
+    p2[n - 1] = cpxd(fp_left(d2.real(), d1.real(), ft.real()), fp_left(d2.imag(), d1.imag(), ft.imag()));
+    for(int i = 0; i < n; ++i) w1[i] = p1[i];
+    w2[0] = p2[0];
+    w2[n - 1] = p2[n - 1];
+    cspline(x, w1.data(), w2.data(), w3.data(), w4.data(), n, 1, 1);
+    for(int ix = 1; ix < n - 1; ++ix) {
+        hdel(ix, h1, h2, d1, d2);
+        p2[ix] = cpxd(fp_interior(d1.real(), d2.real(), w2[ix].real()),
+                      fp_interior(d1.imag(), d2.imag(), w2[ix].imag()));
+    }
+    for(int ix = 0; ix < n - 1; ++ix) {
+        double h = x[ix + 1] - x[ix];
+        cpxd f1 = p1[ix], f2 = p1[ix + 1], f1p = p2[ix], f2p = p2[ix + 1];
+        p3[ix] = (3.0 * (f2 - f1) - h * (2.0 * f1p + f2p)) / (h * h);
+        p4[ix] = (h * (f1p + f2p) - 2.0 * (f2 - f1)) / (h * h * h);
+    }
+}
+
+// SubTab (src/common_setup.hpp:306-334): FMA sub-tabulation
+template<typename T> void subtab(std::vector<T> &x, int n)
+{
+    const T m999 = (T)(sizeof(T) == 4 ? -999.9f : -999.9);
+    const T p01 = (T)(sizeof(T) == 4 ? 0.01f : 0.01);
+    if(n >= 3 && std::fabs(x[2] - m999) < p01) {
+        if(std::fabs(x[1] - m999) < p01) x[1] = x[0];
+        T dx = (x[1] - x[0]) / (T)(n - 1), x0 = x[0];
+        for(int i = 0; i < n; ++i) x[i] = std::fma((T)i, dx, x0);
+    }
+}
+
+HsDev make_hs(const EnvInput &in, double freq, double fT, const HsIn &h)
+{
+    HsDev d{};
+    d.bc = h.bc;
+    char au0 = in.top_opt[2], au1 = in.top_opt[3];
+    if(h.bc == 'A') {
+        cpxd cP = crci(in, freq, fT, h.zTemp, h.alphaR, h.alphaI, au0, au1);
+        cpxd cS = crci(in, freq, fT, h.zTemp, h.betaR, h.betaI, au0, au1);
+        d.cPr = cP.real(); d.cPi = cP.imag();
+        d.cSr = cS.real(); d.cSi = cS.imag();
+        d.rho = h.rho;
+    } else if(h.bc == 'G') {   // grain size (src/module/boundarycond.hpp:179-224)
+        double Mz = h.Mz, vr, a2f, rho;
+        if(Mz >= FLT(-1.0) && Mz < FLT(1.0)) {
+            vr = FLT(0.002709) * Mz * Mz - FLT(0.056452) * Mz + FLT(1.2778);
+            rho = FLT(0.007797) * Mz * Mz - FLT(0.17057) * Mz + FLT(2.3139);
+        } else if(Mz >= FLT(1.0) && Mz < FLT(5.3)) {
+            vr = FLT(-0.0014881) * Mz * Mz * Mz + FLT(0.0213937) * Mz * Mz - FLT(0.1382798) * Mz + FLT(1.3425);
+            rho = FLT(-0.0165406) * Mz * Mz * Mz + FLT(0.2290201) * Mz * Mz - FLT(1.1069031) * Mz + FLT(3.0455);
+        } else {
+            vr = FLT(-0.0024324) * Mz + FLT(1.0019);
+            rho = FLT(-0.0012973) * Mz + FLT(1.1565);
+        }
+        if(Mz >= FLT(-1.0) && Mz < FLT(0.0)) a2f = FLT(0.4556);
+        else if(Mz >= FLT(0.0) && Mz < FLT(2.6)) a2f = FLT(0.4556) + FLT(0.0245) * Mz;
+        else if(Mz >= FLT(2.6) && Mz < FLT(4.5)) a2f = FLT(0.1978) + FLT(0.1245) * Mz;
+        else if(Mz >= FLT(4.5) && Mz < FLT(6.0)) a2f = FLT(8.0399) - FLT(2.5228) * Mz + FLT(0.20098) * Mz * Mz;
+        else if(Mz >= FLT(6.0) && Mz < FLT(9.5)) a2f = FLT(0.9431) - FLT(0.2041) * Mz + FLT(0.0117) * Mz * Mz;
+        else a2f = FLT(0.0601);
+        double aR = vr * FLT(1500.0);
+        double aI = a2f * (vr / FLT(1000.0)) * FLT(1500.0) * std::log(FLT(10.0)) / (FLT(40.0) * kPi);
+        cpxd cP = crci(in, freq, fT, h.zTemp, aR, aI, 'L', ' ');
+        d.cPr = cP.real(); d.cPi = cP.imag();
+        d.rho = rho;
+    }
+    return d;
+}
+
+// src/module/boundary.hpp:180-226 (extension), 600-896 (2-D tangents/normals/curvature)
+std::vector<BdryPtDev> build_bdry(const EnvInput &in, double freq, const BdryIn &b, bool istop,
+                                  double depth, int32_t &curv, int32_t &islong)
+{
+    const double big = std::sqrt(DBL_MAX) / 1.0e5;
+    std::vector<BdryPtDev> bd;
+    char type0 = 'L', type1 = 'S';
+    if(!b.file) {
+        bd.assign(2, BdryPtDev{});
+        bd[0].x[0] = -big; bd[0].x[1] = depth;
+        bd[1].x[0] = big;  bd[1].x[1] = depth;
+    } else {
+        type0 = b.type[0];
+        type1 = b.type[1];
+        int n = (int)b.r_km.size() + 2;
+        bd.assign(n, BdryPtDev{});
+        for(int i = 1; i < n - 1; ++i) {
+            bd[i].x[0] = b.r_km[i - 1];
+            bd[i].x[1] = b.z[i - 1];
+            if(type1 == 'L') {
+                const auto &g = b.geo[i - 1];
+                cpxd cP = crci(in, freq, 0, 1.0e20, g[0], g[3], 'W', ' ');
+                cpxd cS = crci(in, freq, 0, 1.0e20, g[1], g[4], 'W', ' ');
+                bd[i].cPr = cP.real(); bd[i].cPi = cP.imag();
+                bd[i].cSr = cS.real(); bd[i].cSi = cS.imag();
+                bd[i].rho = g[2];
+            }
+        }
+        bd[0] = bd[1];
+        bd[0].x[0] = -big * 0.001;
+        bd[n - 1] = bd[n - 2];
+        bd[n - 1].x[0] = big * 0.001;
+        for(auto &p : bd) { std::memset(p.t, 0, sizeof(p.t)); }
+    }
+    for(auto &p : bd) p.x[0] *= 1000.0;   // km -> m
+    int n = (int)bd.size();
+    for(int i = 1; i < n; ++i)
+        if(!(bd[i].x[0] > bd[i - 1].x[0]))
+            env_error(std::string(istop ? "altimetry" : "bathymetry") + " ranges are not monotonically increasing");
+    double negtop = istop ? -1.0 : 1.0;
+    std::vector<double> Dx(n, 0.0);
+    for(int i = 0; i < n - 1; ++i) {
+        double tx = bd[i + 1].x[0] - bd[i].x[0], tz = bd[i + 1].x[1] - bd[i].x[1];
+        Dx[i] = tz / tx;
+        double len = std::sqrt(tx * tx + tz * tz);
+        bd[i].Len = len;
+        bd[i].t[0] = tx / len;
+        bd[i].t[1] = tz / len;
+        bd[i].n[0] = -negtop * bd[i].t[1];
+        bd[i].n[1] = negtop * bd[i].t[0];
+    }
+    curv = type0 == 'C';
+    islong = type1 == 'L';
+    if(type0 == 'C') {
+        for(int i = 1; i < n - 1; ++i) {
+            double sss = FLT(0.5);
+            bd[i].Nodet[0] = (FLT(1.0) - sss) * bd[i - 1].t[0] + sss * bd[i].t[0];
+            bd[i].Nodet[1] = (FLT(1.0) - sss) * bd[i - 1].t[1] + sss * bd[i].t[1];
+        }
+        bd[0].Nodet[0] = 1.0; bd[0].Nodet[1] = 0.0;
+        bd[n - 1].Nodet[0] = 1.0; bd[n - 1].Nodet[1] = 0.0;
+        for(int i = 0; i < n; ++i) {
+            bd[i].Noden[0] = -negtop * bd[i].Nodet[1];
+            bd[i].Noden[1] = negtop * bd[i].Nodet[0];
+        }
+        for(int i = 0; i < n - 1; ++i) {
+            double Dxx = (Dx[i + 1] - Dx[i]) / (bd[i + 1].x[0] - bd[i].x[0]);
+            bd[i].kappa = Dxx * bd[i].t[0] * bd[i].t[0] * bd[i].t[0];
+        }
+    } else {
+        for(auto &p : bd) p.kappa = 0.0;
+    }
+    if(type0 != 'L' && type0 != 'C') env_error("unknown boundary interpolation type");
+    return bd;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------- read_env
+EnvInput read_env_files(const std::string &root)
+{
+    EnvInput in;
+    LdiReader f(root + ".env");
+    if(!f.good()) env_error("unable to open environment file " + root + ".env");
+    f.record(); f.read(in.title);                               // Title
+    f.record(); f.read(in.freq0);                               // Freq0
+    int32_t nmedia = 1;
+    f.record(); f.read(nmedia);                                 // NMedia
+    if(nmedia != 1) env_error("only NMEDIA = 1 is supported");
+    f.record(); f.read_chars(in.top_opt, 6);                    // TopOpt
+    if(in.top_opt[3] == 'F') {
+        f.record();
+        for(int k = 0; k < 4; ++k) f.read(in.fg[k]);
+    } else if(in.top_opt[3] == 'B') {
+        int32_t nb = 0;
+        f.record(); f.read(nb);
+        in.bio.assign(nb, {0, 0, 0, 0, 0});
+        for(int i = 0; i < nb; ++i) {
+            f.record();
+            for(int k = 0; k < 5; ++k) f.read(in.bio[i][k]);
+        }
+    }
+    if(in.top_opt[5] == 'B') env_error("broadband option 'B' is not supported by the reference either");
+    // values recycled from the top halfspace to the SSP and the bottom halfspace
+    // (src/api.cpp:254-260)
+    double rec[5] = {FLT(1500.0), FLT(0.0), FLT(1.0), FLT(0.0), FLT(0.0)};
+    in.top.bc = in.top_opt[1];
+    if(in.top.bc == 'A') {                                      // BoundaryCondTop
+        f.record(); f.read(in.top.zTemp);
+        for(int k = 0; k < 5; ++k) f.read(rec[k]);
+        in.top.alphaR = rec[0]; in.top.betaR = rec[1]; in.top.rho = rec[2];
+        in.top.alphaI = rec[3]; in.top.betaI = rec[4];
+    } else if(in.top.bc == 'G') {
+        f.record(); f.read(in.top.zTemp); f.read(in.top.Mz);
+    }
+    {                                                           // SSP
+        int32_t npts = 0;
+        double sigma = 0;
+        f.record(); f.read(npts); f.read(sigma); f.read(in.bot_depth);
+        char st = in.top_opt[0];
+        if(st != 'A') {
+            for(int guard = 0;; ++guard) {
+                if(guard > 100001) env_error("number of SSP points exceeds limit");
+                double z = 0;
+                f.record();
+                f.read(z);
+                for(int k = 0; k < 5; ++k) f.read(rec[k]);
+                in.ssp_z.push_back(z);
+                in.alphaR.push_back(rec[0]); in.betaR.push_back(rec[1]); in.rho.push_back(rec[2]);
+                in.alphaI.push_back(rec[3]); in.betaI.push_back(rec[4]);
+                if(std::fabs(z - in.bot_depth) < FLT(100.0) * FLT_EPSILON) break;
+            }
+        } else {
+            in.ssp_z = {0.0, in.bot_depth};
+        }
+    }
+    f.record(); f.read_chars(in.bot_opt, 6);                    // BotOpt
+    double bsigma = 0;
+    f.read(bsigma);
+    in.bot.bc = in.bot_opt[0];
+    if(in.bot.bc == 'A') {                                      // BoundaryCondBot
+        f.record(); f.read(in.bot.zTemp);
+        for(int k = 0; k < 5; ++k) f.read(rec[k]);
+        in.bot.alphaR = rec[0]; in.bot.betaR = rec[1]; in.bot.rho = rec[2];
+        in.bot.alphaI = rec[3]; in.bot.betaI = rec[4];
+    } else if(in.bot.bc == 'G') {
+        f.record(); f.read(in.bot.zTemp); f.read(in.bot.Mz);
+    }
+    read_vector(f, in.nsz, in.sz);                              // SzRz
+    read_vector(f, in.nrz, in.rz);
+    read_vector(f, in.nrr, in.rr_km);                           // RcvrRanges
+    f.record(); f.read_chars(in.run_type, 7);                   // RunType
+    {                                                           // RayAnglesElevation
+        f.record();
+        f.read(in.nalpha);
+        if(in.top_opt[5] == 'I') f.read(in.isingle);
+        int n = in.nalpha;
+        in.alpha_deg.assign(std::max(3, std::max(n, 2)), 0.0);
+        if(n > 2) in.alpha_deg[2] = FLT(-999.9);
+        f.record();
+        int nread = n == 0 ? 2 : n;
+        for(int i = 0; i < nread; ++i) f.read(in.alpha_deg[i]);
+    }
+    f.record();                                                 // BeamInfo
+    f.read(in.deltas); f.read(in.box_z); f.read(in.box_r_km);
+    if(in.run_type[1] == 'C' || in.run_type[1] == 'R')
+        env_error("Cerveny beams are not supported by this build");
+    if(in.top_opt[4] == '~' || in.top_opt[4] == '*') read_bdry_file(root + ".ati", in.ati);
+    if(in.bot_opt[1] == '~' || in.bot_opt[1] == '*') read_bdry_file(root + ".bty", in.bty);
+    if(in.run_type[2] == '*') {                                 // SBP
+        LdiReader s(root + ".sbp");
+        if(!s.good()) env_error("unable to open source beam pattern file");
+        int32_t n = 0;
+        s.record(); s.read(n);
+        in.sbp.assign(n, {0, 0});
+        for(int i = 0; i < n; ++i) { s.record(); s.read(in.sbp[i][0]); s.read(in.sbp[i][1]); }
+    }
+    return in;
+}
+
+// -------------------------------------------------------------- preprocess
+EnvTables preprocess(const EnvInput &in, double freq)
+{
+    EnvTables t;
+    t.freq0 = freq;
+    std::memcpy(t.run_type, in.run_type, 7);
+    // RunType validation / normalisation (src/module/runtype.hpp:53-78)
+    switch(t.run_type[0]) {
+    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'V': case 'v': break;
+    case 'R': env_error("ray-trace runs ('R') are not a field mode");
+    default: env_error("unknown RunType");
+    }
+    switch(t.run_type[1]) {
+    case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
+    default: t.run_type[1] = 'G';
+    }
+    if(t.run_type[3] != 'X') t.run_type[3] = 'R';
+    if(t.run_type[4] != 'I') t.run_type[4] = 'R';
+    if(t.run_type[5] != ' ' && t.run_type[5] != '2') env_error("3-D environment given to the 2-D reader");
+    std::memcpy(t.beam_type, "G S ", 4);                       // MoveBeamType (module/beaminfo.hpp:240-244)
+    t.beam_type[0] = t.run_type[1];
+    t.beam_type[3] = t.run_type[6];
+    char bt = t.beam_type[0];
+    if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
+        env_error(std::string("beam type '") + bt + "' is not supported by this build");
+    if(t.beam_type[3] == 'S') env_error("beam shift ('S') is not supported by this build");
+
+    char st = in.top_opt[0];
+    switch(st) {
+    case 'N': t.ssp_type = SSP_N2LINEAR; break;
+    case 'C': t.ssp_type = SSP_CLINEAR; break;
+    case 'S': t.ssp_type = SSP_CUBIC; break;
+    case 'P': t.ssp_type = SSP_PCHIP; break;
+    case 'A': t.ssp_type = SSP_ANALYTIC; break;
+    case 'Q': env_error("quad SSP ('Q') is not supported by this build");
+    default: env_error("unknown SSP type");
+    }
+    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G')
+        env_error("top boundary condition not supported by this build");
+    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G')
+        env_error("bottom boundary condition not supported by this build");
+    // fT: 1000 once an 'A' bottom halfspace has been read (module/boundarycond.hpp:37-58)
+    double fT = in.bot.bc == 'A' ? FLT(1000.0) : 1.0e20;
+    int n = (int)in.ssp_z.size();
+    if(n < 2) env_error("the SSP must have at least 2 points");
+    for(int i = 1; i < n; ++i)
+        if(!(in.ssp_z[i] > in.ssp_z[i - 1])) env_error("SSP depths must be monotone increasing");
+    t.z = in.ssp_z;
+    t.rho = in.rho.empty() ? std::vector<double>(n, 1.0) : in.rho;
+    t.c.assign(2 * n, 0.0);
+    t.cz.assign(2 * n, 0.0);
+    t.n2.assign(2 * n, 0.0);
+    t.n2z.assign(2 * n, 0.0);
+    t.coef.assign(8 * n, 0.0);
+    if(st != 'A') {
+        std::vector<cpxd> c(n), cz(n, cpxd(NAN, NAN));
+        for(int i = 0; i < n; ++i) {
+            c[i] = crci(in, freq, fT, in.ssp_z[i], in.alphaR[i], in.alphaI[i], in.top_opt[2], in.top_opt[3]);
+            if(i > 0) cz[i - 1] = (c[i] - c[i - 1]) / (in.ssp_z[i] - in.ssp_z[i - 1]);
+        }
+        for(int i = 0; i < n; ++i) {
+            t.c[2 * i] = c[i].real(); t.c[2 * i + 1] = c[i].imag();
+            t.cz[2 * i] = cz[i].real(); t.cz[2 * i + 1] = cz[i].imag();
+        }
+        if(st == 'N') {
+            std::vector<cpxd> n2(n);
+            for(int i = 0; i < n; ++i) n2[i] = FLT(1.0) / (c[i] * c[i]);
+            for(int i = 0; i < n; ++i) { t.n2[2 * i] = n2[i].real(); t.n2[2 * i + 1] = n2[i].imag(); }
+            for(int i = 1; i < n; ++i) {
+                cpxd d = (n2[i] - n2[i - 1]) / (in.ssp_z[i] - in.ssp_z[i - 1]);
+                t.n2z[2 * (i - 1)] = d.real(); t.n2z[2 * (i - 1) + 1] = d.imag();
+            }
+        } else if(st == 'S' || st == 'P') {
+            std::vector<cpxd> k0(n), k1(n), k2(n), k3(n);
+            if(st == 'S') {
+                for(int i = 0; i < n; ++i) k0[i] = c[i];
+                cspline(in.ssp_z.data(), k0.data(), k1.data(), k2.data(), k3.data(), n, 0, 0);
+            } else {
+                pchip(in.ssp_z.data(), c.data(), n, k0.data(), k1.data(), k2.data(), k3.data());
+            }
+            const std::vector<cpxd> *K[4] = {&k0, &k1, &k2, &k3};
+            for(int k = 0; k < 4; ++k)
+                for(int i = 0; i < n; ++i) {
+                    t.coef[2 * (k * n + i)] = (*K[k])[i].real();
+                    t.coef[2 * (k * n + i) + 1] = (*K[k])[i].imag();
+                }
+        }
+    }
+    double top_depth = in.ssp_z[0], bot_depth = in.bot_depth;
+    if(std::fabs(in.ssp_z[n - 1] - bot_depth) >= FLT(100.0) * FLT_EPSILON)
+        t.warnings.push_back("Ocean bottom must be at last SSP depth");
+    t.top = make_hs(in, freq, fT, in.top);
+    t.bot = make_hs(in, freq, fT, in.bot);
+    t.btop = build_bdry(in, freq, in.ati, true, top_depth, t.top_curv, t.top_long);
+    t.bbot = build_bdry(in, freq, in.bty, false, bot_depth, t.bot_curv, t.bot_long);
+    for(const auto &p : t.bbot)
+        if(p.x[1] > bot_depth) env_error("bathymetry drops below lowest point in the sound speed profile");
+    for(const auto &p : t.btop)
+        if(p.x[1] < top_depth) env_error("altimetry rises above highest point in the sound speed profile");
+
+    // sources / receivers (module/szrz.hpp:64-125, module/rcvrranges.hpp:74-85)
+    t.sz = in.sz;
+    subtab(t.sz, in.nsz);
+    t.sz.resize(in.nsz);
+    std::sort(t.sz.begin(), t.sz.end());
+    t.rz = in.rz;
+    subtab(t.rz, in.nrz);
+    t.rz.resize(in.nrz);
+    std::sort(t.rz.begin(), t.rz.end());
+    for(auto &v : t.sz) { if(v < top_depth) v = (float)top_depth; if(v > bot_depth) v = (float)bot_depth; }
+    for(auto &v : t.rz) { if(v < top_depth) v = (float)top_depth; if(v > bot_depth) v = (float)bot_depth; }
+    std::vector<double> rr = in.rr_km;
+    subtab(rr, in.nrr);
+    rr.resize(in.nrr);
+    std::sort(rr.begin(), rr.end());
+    for(auto &v : rr) v *= FLT(1000.0);
+    for(int i = 1; i < in.nrr; ++i)
+        if(!(rr[i] > rr[i - 1])) env_error("receiver ranges are not monotonically increasing");
+    t.rr = rr;
+    t.delta_r = in.nrr >= 2 ? rr[in.nrr - 1] - rr[in.nrr - 2] : FLT(0.0);
+    t.nrz_per_range = t.run_type[4] == 'I' ? 1 : in.nrz;
+    if(t.run_type[4] == 'I' && in.nrz != in.nrr)
+        t.warnings.push_back("Irregular grid option selected with NRz not equal to Nr");
+    if(t.run_type[4] == 'I' && in.nrz < in.nrr)   // receiver ir sits at depth Rz[ir]
+        env_error("irregular grid needs at least as many receiver depths as ranges");
+
+    // angles (module/rayangles.hpp:66-190)
+    int na = in.nalpha;
+    std::vector<double> al = in.alpha_deg;
+    if(na == 0) {
+        double c0 = FLT(1500.0);
+        na = std::max((int)(FLT(0.3) * rr[in.nrr - 1] * freq / c0), 300);
+        double dth = std::atan((bot_depth - top_depth) / (FLT(10.0) * rr[in.nrr - 1]));
+        na = std::max((int)(kPi / dth), na);
+        std::vector<double> a(std::max(3, na), 0.0);
+        a[0] = al[0];
+        a[1] = al[1];
+        if(na > 2) a[2] = FLT(-999.9);
+        al = a;
+    }
+    subtab(al, na);
+    al.resize(na);
+    std::sort(al.begin(), al.end());
+    if(na > 1 && std::fabs(std::fmod(al[na - 1] - al[0], FLT(360.0)))
+                     < FLT(10.0) * std::fabs(std::nextafter(360.0, 0.0) - 360.0))
+        --na;
+    al.resize(na);
+    for(int i = 1; i < na; ++i)
+        if(!(al[i] > al[i - 1])) env_error("beam angles are not monotonically increasing");
+    for(auto &v : al) v *= kPi / 180.0;
+    t.alpha = al;
+    t.dalpha = na != 1 ? (al[na - 1] - al[0]) / (na - 1) : FLT(0.0);
+    t.isingle = in.top_opt[5] == 'I' ? in.isingle : 0;
+    if(t.isingle != 0 && (t.isingle < 1 || t.isingle > na)) env_error("selected beam iSingle not in [1, n]");
+
+    // beam box and step (module/beaminfo.hpp:220-237)
+    t.box_x = in.box_r_km * FLT(1000.0);
+    t.box_y = in.box_z;
+    if(t.box_x <= 0.0 || t.box_y <= 0.0) env_error("beam box not set up correctly");
+    t.deltas = in.deltas;
+    if(std::fabs(t.deltas) < DBL_EPSILON) t.deltas = (bot_depth - top_depth) / FLT(10.0);
+
+    // source beam pattern (module/sbp.hpp:58-67,148-157)
+    if(!in.sbp.empty()) {
+        for(const auto &p : in.sbp) {
+            t.sbp.push_back(p[0]);
+            t.sbp.push_back(std::pow(FLT(10.0), p[1] / FLT(20.0)));
+        }
+    } else {
+        t.sbp = {FLT(-180.0), std::pow(FLT(10.0), 0.0 / FLT(20.0)), FLT(180.0), std::pow(FLT(10.0), 0.0 / FLT(20.0))};
+    }
+    return t;
+}
+
+bool EnvTables::same_trajectory_tables(const EnvTables &o) const
+{
+    auto eqhs = [](const HsDev &a, const HsDev &b) { return std::memcmp(&a, &b, sizeof(HsDev)) == 0; };
+    auto eqbd = [](const std::vector<BdryPtDev> &a, const std::vector<BdryPtDev> &b) {
+        return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(BdryPtDev)) == 0;
+    };
+    // reflection phase/amplitude from a halfspace depend only on cP, cS, rho
+    // (the omega factors cancel in the 2-D coefficient, src/reflect.hpp:316-350)
+    return c == o.c && cz == o.cz && n2 == o.n2 && n2z == o.n2z && coef == o.coef && eqhs(top, o.top)
+        && eqhs(bot, o.bot) && eqbd(btop, o.btop) && eqbd(bbot, o.bbot) && run_type[0] != 'S';
+}
+
+} // namespace bhcb

@@ -1,0 +1,74 @@
+// 2-D environment: file reading (EnvInput) and preprocessing into the tables
+// the kernels consume (EnvTables).
+//
+// EnvInput holds the values as the reference's modules hold them after Read
+// (src/api.cpp:253-277 runs Title, Freq0, NMedia, TopOpt, BoundaryCondTop,
+// SSP, BotOpt, BoundaryCondBot, SzRz, RcvrRanges, RunType, RayAngles,
+// BeamInfo, Altimetry, Bathymetry, SBP in this order). preprocess() restates
+// the modules' Validate/Preprocess steps (src/module/*.hpp) for one frequency.
+#pragma once
+#include <array>
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../bhcb_internal.h"
+
+namespace bhcb {
+
+using cpxd = std::complex<double>;
+
+struct HsIn {
+    char bc = 'V';
+    double zTemp = 0, alphaR = 0, betaR = 0, rho = 0, alphaI = 0, betaI = 0, Mz = 0;
+};
+
+struct BdryIn {
+    bool file = false;
+    char type[2] = {'L', 'S'};
+    std::vector<double> r_km, z;
+    std::vector<std::array<double, 5>> geo;   // long format: alphaR betaR rho alphaI betaI
+};
+
+struct EnvInput {
+    std::string title;
+    double freq0 = 50.0;
+    char top_opt[6] = {'C', 'V', 'W', ' ', ' ', ' '};
+    char bot_opt[6] = {'R', ' ', ' ', ' ', ' ', ' '};
+    double fg[4] = {20.0, 35.0, 8.0, 0.0};     // Francois-Garrison T S pH z_bar
+    std::vector<std::array<double, 5>> bio;    // z1 z2 f0 q a0
+    HsIn top, bot;
+    std::vector<double> ssp_z, alphaR, betaR, rho, alphaI, betaI;
+    double bot_depth = 5000.0;
+    BdryIn ati, bty;
+    std::vector<std::array<double, 2>> sbp;    // angle (deg), level (dB)
+    int32_t nsz = 1, nrz = 1, nrr = 1, nalpha = 0, isingle = 0;
+    std::vector<float> sz, rz;                 // as read, before SubTab
+    std::vector<double> rr_km, alpha_deg;
+    char run_type[7] = {'C', 'G', ' ', 'R', 'R', ' ', ' '};
+    double deltas = 0, box_z = 0, box_r_km = 0;
+};
+
+struct EnvTables {
+    double freq0 = 0;
+    int32_t ssp_type = SSP_CLINEAR;
+    std::vector<double> z, rho, c, cz, n2, n2z, coef;   // complex tables interleaved
+    HsDev top{}, bot{};
+    int32_t top_curv = 0, bot_curv = 0, top_long = 0, bot_long = 0;
+    std::vector<BdryPtDev> btop, bbot;
+    std::vector<double> rr, alpha, sbp;
+    std::vector<float> rz, sz;
+    double dalpha = 0, delta_r = 0, deltas = 0, box_x = 0, box_y = 0;
+    char run_type[7];
+    char beam_type[4];
+    int32_t nrz_per_range = 1, isingle = 0;
+    std::vector<std::string> warnings;
+    // true when every frequency-dependent table is identical to other's
+    bool same_trajectory_tables(const EnvTables &o) const;
+};
+
+EnvInput read_env_files(const std::string &fileroot);
+EnvTables preprocess(const EnvInput &in, double freq);
+
+} // namespace bhcb

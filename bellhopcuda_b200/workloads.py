@@ -1,0 +1,91 @@
+"""Seeded synthetic workloads (2-D) used by the tests and the benchmark.
+
+No public dataset is involved: every environment is generated from a numpy
+PCG64 seed, written as ordinary BELLHOP input files, and fed identically to
+the reference, the oracle and this library.
+
+* ``munk_tl``   — deep-water Munk profile, coherent hat-beam TL
+                  (51 c-linear nodes, 2001 rays, 201 x 1001 receivers).
+* ``rd_gauss``  — range-dependent Gaussian-beam TL: PCHIP Munk + smoothed
+                  N(0, 2 m/s) perturbation on 64 nodes, 200-point bathymetry
+                  uniform in 3000-5000 m over 100 km, 10 log-spaced frequencies
+                  50-500 Hz, 20001 rays over +-30 deg, 501 x 2001 receivers.
+* ``batch_envs`` — many small uneven spline-SSP environments for batched runs.
+"""
+from __future__ import annotations
+
+import math
+from typing import List
+
+import numpy as np
+
+from .envfile import EnvSpec
+
+
+def munk_c(z, eps=0.00737):
+    """Canonical Munk profile c(z) = 1500 (1 + eps (eta - 1 + exp(-eta)))."""
+    z = np.asarray(z, dtype=np.float64)
+    eta = 2.0 * (z - 1300.0) / 1300.0
+    return 1500.0 * (1.0 + eps * (eta - 1.0 + np.exp(-eta)))
+
+
+def munk_tl(nalpha=2001, nrz=201, nrr=1001, freq=50.0, beam="G") -> EnvSpec:
+    z = np.arange(0.0, 5000.0 + 1e-9, 100.0)
+    return EnvSpec(
+        title="Munk coherent TL", freq=freq, ssp_type="C", top_bc="V", atten_unit="W",
+        ssp_z=z, ssp_cp=munk_c(z), bot_bc="A", bot_hs=(5000.0, 1600.0, 0.0, 1.8, 0.8, 0.0),
+        nsz=1, sz=(1000.0,), nrz=nrz, rz=(0.0, 5000.0), nrr=nrr, rr_km=(0.0, 100.0),
+        run_type="C%s RR " % beam, nalpha=nalpha, alpha=(-20.0, 20.0), deltas=0.0,
+        box_z=5500.0, box_r_km=101.0)
+
+
+def rd_gauss_freqs(n=10):
+    return [float(f) for f in np.logspace(math.log10(50.0), math.log10(500.0), n)]
+
+
+def rd_gauss(seed=1002, freq=None, nalpha=20001, nrz=501, nrr=2001, nbty=200) -> EnvSpec:
+    """Range-dependent Gaussian-beam case; ``freq`` None -> the first frequency."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    z = np.linspace(0.0, 5000.0, 64)
+    pert = rng.normal(0.0, 2.0, z.size)
+    k = np.exp(-0.5 * (np.arange(-2, 3) / 1.0) ** 2)
+    k /= k.sum()
+    pert = np.convolve(np.pad(pert, 2, mode="edge"), k, mode="valid")
+    c = munk_c(z) + pert
+    br = np.linspace(0.0, 100.0, nbty)
+    bz = rng.uniform(3000.0, 5000.0, nbty)
+    zmax = float(bz.max())
+    # the SSP must reach the deepest bathymetry point (module/boundary.hpp:419-425)
+    z = z * (zmax / 5000.0)
+    return EnvSpec(
+        title="range-dependent Gaussian TL", freq=rd_gauss_freqs()[0] if freq is None else freq,
+        ssp_type="P", top_bc="V", atten_unit="W", ssp_z=z, ssp_cp=c, bot_bc="A",
+        bot_hs=(zmax, 1600.0, 0.0, 1.8, 0.8, 0.0), bty_r=br, bty_z=bz, bty_type="LS",
+        nsz=1, sz=(1000.0,), nrz=nrz, rz=(0.0, zmax), nrr=nrr, rr_km=(0.0, 100.0),
+        run_type="CB RR ", nalpha=nalpha, alpha=(-30.0, 30.0), deltas=0.0,
+        box_z=zmax + 500.0, box_r_km=101.0)
+
+
+def batch_envs(n=256, seed=1003, scale=1.0) -> List[EnvSpec]:
+    """Uneven spline-SSP environments; ``scale`` < 1 shrinks rays/receivers."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(n):
+        nn = int(rng.integers(20, 201))
+        depth = float(rng.uniform(200.0, 5000.0))
+        z = np.linspace(0.0, depth, nn)
+        c = munk_c(z) + rng.normal(0.0, 3.0, nn)
+        cp = float(rng.uniform(1500.0, 1800.0))
+        rho = float(rng.uniform(1.5, 2.0))
+        f = float(math.exp(rng.uniform(math.log(25.0), math.log(1000.0))))
+        na = max(16, int(int(rng.integers(500, 20001)) * scale))
+        nrz = max(8, int(int(rng.integers(100, 501)) * scale))
+        nrr = max(8, int(int(rng.integers(200, 2001)) * scale))
+        rmax = float(rng.uniform(10.0, 100.0))
+        out.append(EnvSpec(
+            title="batch env %d" % i, freq=f, ssp_type="S", top_bc="V", atten_unit="W",
+            ssp_z=z, ssp_cp=c, bot_bc="A", bot_hs=(depth, cp, 0.0, rho, 0.5, 0.0),
+            nsz=1, sz=(float(rng.uniform(0.05, 0.95)) * depth,), nrz=nrz, rz=(0.0, depth),
+            nrr=nrr, rr_km=(0.0, rmax), run_type="CB RR ", nalpha=na, alpha=(-30.0, 30.0),
+            deltas=0.0, box_z=depth + 100.0, box_r_km=rmax + 1.0))
+    return out

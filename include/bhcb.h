@@ -1,0 +1,131 @@
+/*
+ * bhcb — C ABI of the B200 beam tracer (libbhcb.so).
+ *
+ * The reference exposes its tracer as C++ templates in include/bhc/bhc.hpp
+ * (bhc::setup / run / writeout / finalize over bhcParams / bhcOutputs). Its
+ * internal seam for the field modes is RunFieldModesImpl
+ * (src/mode/fieldimpl.hpp:27-28). This header is the plain-C surface that a
+ * host binding (C++, ctypes, cgo, JNI) calls instead; each entry point names
+ * the reference call it replaces.
+ *
+ * Conventions: every function returns 0 on success and a non-zero status on
+ * failure (never throws, never resets the device); the message is available
+ * from bhcb_last_error. A context is bound to one GPU and one CUDA stream and
+ * is not thread-safe; separate contexts are independent (the reference's
+ * "multiple instances" rule, include/bhc/bhc.hpp:41-43).
+ */
+#ifndef BHCB_H
+#define BHCB_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bhcb_ctx bhcb_ctx;
+
+enum {
+    BHCB_OK = 0,
+    BHCB_ERR_ARG = 1,        /* invalid argument */
+    BHCB_ERR_INPUT = 2,      /* invalid or unsupported environment */
+    BHCB_ERR_CUDA = 3,       /* CUDA runtime error (context stays usable) */
+    BHCB_ERR_RUN = 4,        /* tracer reported an error bit (see err_bits) */
+    BHCB_ERR_MEMORY = 5,     /* max_memory budget exceeded */
+    BHCB_ERR_STATE = 6       /* call out of order (e.g. run before setup) */
+};
+
+enum { BHCB_PREC_FP64 = 0, BHCB_PREC_MIXED = 1 };
+
+/* Context options; mirrors bhcInit (include/bhc/structs.hpp:490-546). */
+typedef struct bhcb_init {
+    int32_t gpu_index;        /* bhcInit::gpuIndex */
+    int32_t precision;        /* BHCB_PREC_FP64 or BHCB_PREC_MIXED */
+    uint64_t max_memory;      /* bhcInit::maxMemory (device bytes); 0 = 16 GiB */
+    int32_t share_trajectory; /* frequencies share one trace when tables allow (mixed only) */
+    int32_t reserved;
+    void (*output_callback)(const char *message); /* bhcInit::outputCallback */
+} bhcb_init;
+
+/* Counters of the last run. */
+typedef struct bhcb_stats {
+    uint64_t rays, steps, segments, evals;
+    uint32_t err_bits, warn_bits;   /* reference ErrState bit numbering (src/util/errors.hpp:61-93) */
+    int32_t groups, fields;         /* trace groups launched, TL fields produced */
+    double trace_ms, influence_ms, total_ms;
+} bhcb_stats;
+
+/* Create a context; replaces the bhcInternal construction in bhc::setup
+   (src/api.cpp:194-215, setupGPU src/api.cpp:144-189). init may be NULL. */
+int bhcb_open(const bhcb_init *init, bhcb_ctx **out);
+
+/* bhc::finalize (src/api.cpp:830-855): release every resource. */
+void bhcb_close(bhcb_ctx *ctx);
+
+/* bhc::setup with bhcInit::FileRoot set (src/api.cpp:194-291): read
+   FileRoot.env (+ .bty/.ati/.sbp) as the context's single environment. */
+int bhcb_setup(bhcb_ctx *ctx, const char *file_root);
+
+/* Batched extension (no reference counterpart: the reference needs one
+   bhcParams per environment): append one more environment; returns its index
+   in *env_index. bhcb_setup is bhcb_clear + bhcb_add_env. */
+int bhcb_add_env(bhcb_ctx *ctx, const char *file_root, int32_t *env_index);
+int bhcb_clear(bhcb_ctx *ctx);
+
+/* Multi-frequency extension (no reference counterpart: the reference traces
+   one freq0 per bhc::run, include/bhc/bhc.hpp:174-179): evaluate env_index at
+   the nfreq given frequencies instead of its file frequency. */
+int bhcb_set_frequencies(bhcb_ctx *ctx, int32_t env_index, int32_t nfreq, const double *freqs);
+
+/* bhc::run (src/api.cpp:384-418): preprocess, trace, accumulate and
+   post-process (ScalePressure) every field, synchronously. */
+int bhcb_run(bhcb_ctx *ctx);
+
+/* Split form of bhcb_run for callers that manage timing / streams:
+   bhcb_prepare uploads the tables and sizes the buffers; bhcb_launch enqueues
+   the kernels on the context stream without synchronising; bhcb_sync waits
+   and checks the run's error bits. */
+int bhcb_prepare(bhcb_ctx *ctx);
+int bhcb_launch(bhcb_ctx *ctx);
+int bhcb_sync(bhcb_ctx *ctx);
+
+/* Output description: outputs.uAllSources layout per field is
+   [NSz][NRz_per_range][NRr] complex float (GetFieldAddr, src/common.hpp:393-405). */
+int bhcb_field_shape(bhcb_ctx *ctx, int32_t env_index, int32_t *nfreq, int32_t *nsz,
+                     int32_t *nrz_per_range, int32_t *nrr);
+/* Copy field (env_index, ifreq) to host memory dst (bytes >= its size). */
+int bhcb_copy_field(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void *dst, size_t bytes);
+/* Device pointer of field (env_index, ifreq); valid until the next run/close. */
+int bhcb_field_device(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void **dptr);
+/* Receiver grid as used by the run (ranges in m, depths in m). */
+int bhcb_receivers(bhcb_ctx *ctx, int32_t env_index, double *rr, int32_t nrr, float *rz,
+                   int32_t nrz);
+
+/* bhc::writeout (src/api.cpp:465-486) for TL runs: write FileRoot.shd of
+   (env_index, ifreq) in the reference's .shd layout (src/mode/tl.cpp:38-248). */
+int bhcb_writeout(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, const char *file_root);
+
+/* Counters of the last run. */
+int bhcb_get_stats(bhcb_ctx *ctx, bhcb_stats *stats);
+
+/* Last error message (NUL-terminated, truncated to n) and ErrState bits. */
+int bhcb_last_error(bhcb_ctx *ctx, char *msg, size_t n, uint32_t *err_bits,
+                    uint32_t *warn_bits);
+
+/* Host-only validation (no GPU needed): read FileRoot.env (+ side files) and
+   run the preprocessing that bhc::setup's Validate/Echo pass performs
+   (src/api.cpp:278-281); report the sizes the run would use. */
+typedef struct bhcb_env_info {
+    int32_t nsz, nrz, nrz_per_range, nrr, nalpha, ssp_type;
+    double freq, deltas;
+    char run_type[8], beam_type[8];
+} bhcb_env_info;
+int bhcb_check_env(const char *file_root, bhcb_env_info *info, char *msg, size_t n);
+
+/* Library version string. */
+const char *bhcb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
