@@ -50,7 +50,7 @@ class Stats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("steps", C.c_uint64), ("segments", C.c_uint64),
                 ("evals", C.c_uint64), ("err_bits", C.c_uint32), ("warn_bits", C.c_uint32),
                 ("groups", C.c_int32), ("fields", C.c_int32), ("trace_ms", C.c_double),
-                ("influence_ms", C.c_double), ("total_ms", C.c_double)]
+                ("influence_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_uint64)]
 
 
 class EnvInfo(C.Structure):
@@ -83,6 +83,8 @@ SIGNATURES = [
     ("bhcb_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("bhcb_last_error", C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_uint32)]),
+    ("bhcb_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("bhcb_probe_fp_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("bhcb_check_env", C.c_int, [C.c_char_p, C.POINTER(EnvInfo), C.c_char_p, C.c_size_t]),
     ("bhcb_version", C.c_char_p, []),
 ]
@@ -102,6 +104,16 @@ def load_library():
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+def probe_fp_peak(gpu: int = 0):
+    """Measured (FP32, FP64) FMA throughput in TFLOP/s."""
+    lib = load_library()
+    a, b = C.c_double(), C.c_double()
+    rc = lib.bhcb_probe_fp_peak(gpu, C.byref(a), C.byref(b))
+    if rc != 0:
+        raise BhcbError(rc, "peak probe failed")
+    return a.value, b.value
 
 
 def check_env(file_root: str) -> dict:
@@ -217,6 +229,11 @@ class Tracer:
 
     def writeout(self, file_root: str, env: int = 0, ifreq: int = 0):
         self._check(self._lib.bhcb_writeout(self._h, env, ifreq, file_root.encode()))
+
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.bhcb_stream(self._h, C.byref(p)))
+        return p.value or 0
 
     def stats(self) -> dict:
         s = Stats()

@@ -158,13 +158,6 @@ struct Arena {
         if(!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
         return off;
     }
-    size_t put_raw(const void *p, size_t n)
-    {
-        size_t off = (bytes.size() + 255) & ~size_t(255);
-        bytes.resize(off + n);
-        std::memcpy(bytes.data() + off, p, n);
-        return off;
-    }
 };
 
 template<typename T> T *dptr(void *base, size_t off)
@@ -284,6 +277,7 @@ void do_prepare(bhcb_ctx *c)
         d.alpha = dptr<double>(ab, o.alpha); d.sbp = dptr<double>(ab, o.sbp);
     }
     CK(cudaMemcpyAsync(ab, A.bytes.data(), A.bytes.size(), cudaMemcpyHostToDevice, c->stream));
+    c->stats.h2d_bytes = A.bytes.size();
     // --- groups, fields, frequencies
     for(auto &S : c->envs) S.field_of_freq.assign(S.freqs.size(), -1);
     for(size_t g = 0; g < plan.size(); ++g) {
@@ -314,6 +308,7 @@ void do_prepare(bhcb_ctx *c)
     c->groups_d.ensure(c->groups_h.size() * sizeof(GroupDev));
     CK(cudaMemcpyAsync(c->groups_d.p, c->groups_h.data(), c->groups_h.size() * sizeof(GroupDev),
                        cudaMemcpyHostToDevice, c->stream));
+    c->stats.h2d_bytes += c->groups_h.size() * sizeof(GroupDev) + c->freqs_h.size() * sizeof(double);
     c->freqs_d.ensure(c->freqs_h.size() * sizeof(double));
     CK(cudaMemcpyAsync(c->freqs_d.p, c->freqs_h.data(), c->freqs_h.size() * sizeof(double),
                        cudaMemcpyHostToDevice, c->stream));
@@ -651,6 +646,13 @@ int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
         o.write((const char *)buf.data(), buf.size());
         return BHCB_OK;
     });
+}
+
+int bhcb_stream(bhcb_ctx *c, void **stream)
+{
+    if(!c || !stream) return BHCB_ERR_ARG;
+    *stream = (void *)c->stream;
+    return BHCB_OK;
 }
 
 int bhcb_get_stats(bhcb_ctx *c, bhcb_stats *s)

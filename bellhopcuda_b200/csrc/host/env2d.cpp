@@ -651,14 +651,42 @@ EnvTables preprocess(const EnvInput &in, double freq)
 
 bool EnvTables::same_trajectory_tables(const EnvTables &o) const
 {
-    auto eqhs = [](const HsDev &a, const HsDev &b) { return std::memcmp(&a, &b, sizeof(HsDev)) == 0; };
-    auto eqbd = [](const std::vector<BdryPtDev> &a, const std::vector<BdryPtDev> &b) {
-        return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(BdryPtDev)) == 0;
+    // Tables converted from attenuation units by crci differ between
+    // frequencies only by rounding when the units are frequency independent
+    // (e.g. dB/wavelength); a relative tolerance of 1e-12 accepts exactly
+    // those cases and rejects genuinely frequency-dependent attenuation.
+    auto close = [](double a, double b) {
+        if(a == b) return true;
+        if(std::isnan(a) && std::isnan(b)) return true;
+        return std::fabs(a - b) <= 1e-12 * std::max(std::fabs(a), std::fabs(b));
     };
-    // reflection phase/amplitude from a halfspace depend only on cP, cS, rho
-    // (the omega factors cancel in the 2-D coefficient, src/reflect.hpp:316-350)
-    return c == o.c && cz == o.cz && n2 == o.n2 && n2z == o.n2z && coef == o.coef && eqhs(top, o.top)
-        && eqhs(bot, o.bot) && eqbd(btop, o.btop) && eqbd(bbot, o.bbot) && run_type[0] != 'S';
+    auto vclose = [&](const std::vector<double> &a, const std::vector<double> &b) {
+        if(a.size() != b.size()) return false;
+        for(size_t i = 0; i < a.size(); ++i)
+            if(!close(a[i], b[i])) return false;
+        return true;
+    };
+    auto hclose = [&](const HsDev &a, const HsDev &b) {
+        return a.bc == b.bc && close(a.cPr, b.cPr) && close(a.cPi, b.cPi) && close(a.cSr, b.cSr)
+            && close(a.cSi, b.cSi) && close(a.rho, b.rho);
+    };
+    auto bclose = [&](const std::vector<BdryPtDev> &a, const std::vector<BdryPtDev> &b) {
+        if(a.size() != b.size()) return false;
+        for(size_t i = 0; i < a.size(); ++i) {
+            const double *x = reinterpret_cast<const double *>(&a[i]);
+            const double *y = reinterpret_cast<const double *>(&b[i]);
+            for(size_t k = 0; k < sizeof(BdryPtDev) / sizeof(double); ++k)
+                if(!close(x[k], y[k])) return false;
+        }
+        return true;
+    };
+    // The 2-D halfspace reflection coefficient depends on omega only through
+    // cP, cS (the omega factors cancel, src/reflect.hpp:316-350), and the
+    // semi-coherent Lloyd-mirror source amplitude depends on omega
+    // (src/trace.hpp:148-152), so 'S' runs never share.
+    return vclose(c, o.c) && vclose(cz, o.cz) && vclose(n2, o.n2) && vclose(n2z, o.n2z)
+        && vclose(coef, o.coef) && hclose(top, o.top) && hclose(bot, o.bot) && bclose(btop, o.btop)
+        && bclose(bbot, o.bbot) && alpha == o.alpha && run_type[0] != 'S';
 }
 
 } // namespace bhcb

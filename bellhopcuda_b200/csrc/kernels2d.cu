@@ -16,14 +16,10 @@
 //                   transpose of the accumulator into the reference layout
 //                   [field][isz][iz][ir] (src/common.hpp:393-405).
 #include <cuda_runtime.h>
-#include <cooperative_groups.h>
-#include <cooperative_groups/scan.h>
 
 #include "bhcb_internal.h"
 #include "device_math.cuh"
 #include "trace2d.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace bhcb {
 
@@ -69,18 +65,6 @@ struct InflState {   // the carried part of InfluenceRayInfo (include/bhc/struct
     V2<double> x;
     int ir;
 };
-
-// Append `emit` segments from the converged lanes of this warp; returns the
-// first slot index for this lane (or ~0ull when the buffer is full).
-__device__ __forceinline__ unsigned long long warp_append(unsigned long long *counter, int emit)
-{
-    cg::coalesced_group g = cg::coalesced_threads();
-    int incl = cg::inclusive_scan(g, emit);
-    unsigned long long base = 0;
-    if(g.thread_rank() == g.size() - 1) base = atomicAdd(counter, (unsigned long long)incl);
-    base = g.shfl(base, g.size() - 1);
-    return base + (unsigned long long)(incl - emit);
-}
 
 // Sequential prologue of Step_InfluenceGeoCart (2-D): returns true when the
 // segment has receiver columns to evaluate and fills rec.
@@ -154,18 +138,34 @@ template<typename R> __device__ __forceinline__ bool infl_prologue(
     return true;
 }
 
+// Segment slots are handed out to each ray in blocks of SEG_BLOCK (one global
+// atomic per block); a ray's segments are therefore stored in step order.
+constexpr int SEG_BLOCK = 32;
+
+struct SlotCursor {
+    unsigned long long next = 0, end = 0;   // [next, end) free slots of the current block
+};
+
 template<typename R> __device__ __forceinline__ void emit_seg(
-    const SegRec<R> &rec, bool emit, SegRec<R> *segs, unsigned long long cap, RunCounters *ctr,
+    const SegRec<R> &rec, SegRec<R> *segs, unsigned long long cap, RunCounters *ctr, SlotCursor &cur,
     bool &overflow)
 {
-    unsigned long long slot = warp_append(&ctr->nseg, emit ? 1 : 0);
-    if(emit) {
-        if(slot < cap) {
-            segs[slot] = rec;
-        } else {
+    if(cur.next == cur.end) {
+        unsigned long long b = atomicAdd(&ctr->nseg, (unsigned long long)SEG_BLOCK);
+        if(b + SEG_BLOCK > cap) {
             overflow = true;
+            return;
         }
+        cur.next = b;
+        cur.end = b + SEG_BLOCK;
     }
+    segs[cur.next++] = rec;
+}
+
+// mark the unused tail of the ray's last block as empty
+template<typename R> __device__ __forceinline__ void close_block(SegRec<R> *segs, SlotCursor &cur)
+{
+    for(; cur.next < cur.end; ++cur.next) segs[cur.next].job = -1;
 }
 
 template<typename R> __global__ void __launch_bounds__(64) trace_kernel(
@@ -242,8 +242,10 @@ template<typename R> __global__ void __launch_bounds__(64) trace_kernel(
         int small = 0, is = 0;
         bool overflow = false;
         unsigned long long nsteps = 0;
+        SlotCursor cur;
         for(;;) {
-            if(__ldcg(&ctr->err_bits) != 0u) break;
+            // another ray's error stops the run (src/trace.hpp:559); polled every 32 steps
+            if((nsteps & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) break;
             bool tr = false, br = false;
             step2d(p0, p1, top, bot, e, iSeg, small, tr, br, ctr);
             ++nsteps;
@@ -271,12 +273,12 @@ template<typename R> __global__ void __launch_bounds__(64) trace_kernel(
                 distances(p2.x, top, bot, dEndTop, dEndBot);
             }
             SegRec<R> rec;
-            bool em = infl_prologue(p0, p1, inf, e, rcp_q0, ratio1, (int)job, is, rec);
-            emit_seg(rec, em, segs, cap, ctr, overflow);
+            if(infl_prologue(p0, p1, inf, e, rcp_q0, ratio1, (int)job, is, rec))
+                emit_seg(rec, segs, cap, ctr, cur, overflow);
             ++is;
             if(two) {
-                em = infl_prologue(p1, p2, inf, e, rcp_q0, ratio1, (int)job, is, rec);
-                emit_seg(rec, em, segs, cap, ctr, overflow);
+                if(infl_prologue(p1, p2, inf, e, rcp_q0, ratio1, (int)job, is, rec))
+                    emit_seg(rec, segs, cap, ctr, cur, overflow);
                 p0 = p2;
                 ++is;
             } else {
@@ -299,6 +301,7 @@ template<typename R> __global__ void __launch_bounds__(64) trace_kernel(
             dBegTop = dEndTop;
             dBegBot = dEndBot;
         }
+        close_block(segs, cur);
         atomicAdd(&ctr->nsteps, nsteps);
     }
 }
@@ -324,38 +327,67 @@ __device__ __forceinline__ int upper_f(const float *a, int n, double v)
     return lo;
 }
 
-template<typename R> struct alignas(16) SegShared {
-    SegRec<R> rec;
-};
-
-// Reduce the phase (double) to [-pi, pi] before the bulk-precision sincos.
+// Reduce an angle to [-pi, pi].
 __device__ __forceinline__ double reduce_2pi(double a)
 {
     const double inv2pi = 0.15915494309189533577, twopi = 6.28318530717958647692;
     return a - twopi * rint(a * inv2pi);
 }
+__device__ __forceinline__ float reduce_2pi(float a)
+{
+    const float inv2pi = 0.159154943f, twopi_hi = 6.28318548f, twopi_lo = -1.7484555e-7f;
+    float k = rintf(a * inv2pi);
+    return fmaf(-k, twopi_lo, fmaf(-k, twopi_hi, a));
+}
+
+// Math used per beam-receiver contribution: IEEE in the FP64 kernel, the SFU
+// approximations (after explicit range reduction) in the mixed kernel.
+template<typename R> struct EvalMath;
+template<> struct EvalMath<double> {
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double exp_(double a) { return exp(a); }
+    static __device__ __forceinline__ double rsqrt_(double a) { return 1.0 / sqrt(a); }
+    static __device__ __forceinline__ void sincos_(double a, double *s, double *c) { sincos(a, s, c); }
+};
+template<> struct EvalMath<float> {
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float exp_(float a) { return __expf(a); }
+    static __device__ __forceinline__ float rsqrt_(float a) { return rsqrtf(a); }
+    static __device__ __forceinline__ void sincos_(float a, float *s, float *c) { __sincosf(a, s, c); }
+};
 
 constexpr int WARPS_PER_CTA = 4;
+
+// Per (segment, frequency) values computed once by the segment's owner lane.
+template<typename R> struct SegFreq {
+    R sigfloor;    // AdjustSigma lower bound (Gaussian)
+    R ph0;         // omega * tau0.real reduced to [-pi, pi]
+    R omdt;        // omega * dtau.real
+    R att0, att1;  // omega * tau0.imag, omega * dtau.imag
+    int izlo, niz;
+};
 
 template<typename R, bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
 influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                  const GroupDev *__restrict__ groups, int ngroups, const double *__restrict__ freqs,
                  float2 *__restrict__ acc, RunCounters *ctr)
 {
-    // the trace kernel's append counter may exceed the capacity on overflow
+    using M = EvalMath<R>;
+    // the trace kernel's slot counter may exceed the capacity on overflow
     const unsigned long long nseg = min(__ldcg(&ctr->nseg), cap);
     __shared__ SegRec<R> s_rec[WARPS_PER_CTA][32];
+    __shared__ SegFreq<R> s_sf[WARPS_PER_CTA][32];
+    __shared__ long long s_base[WARPS_PER_CTA][32];       // field offset of (isz, ir=0, iz=0), f=0
+    __shared__ const double *s_rr[WARPS_PER_CTA][32];
+    __shared__ const float *s_rz[WARPS_PER_CTA][32];
+    __shared__ int s_stride[WARPS_PER_CTA][32];           // per-frequency field stride
+    __shared__ int s_nrzp[WARPS_PER_CTA][32];             // 0 -> irregular grid
     __shared__ int s_pre[WARPS_PER_CTA][33];
-    __shared__ int s_izlo[WARPS_PER_CTA][32];
-    __shared__ int s_niz[WARPS_PER_CTA][32];
-    __shared__ float s_sig[WARPS_PER_CTA][32];   // sigma lower bound for the frequency (Gaussian)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned long long nchunks = (nseg + 31) / 32;
     unsigned long long evals = 0;
     for(unsigned long long ch = (unsigned long long)blockIdx.x * WARPS_PER_CTA + w; ch < nchunks;
         ch += (unsigned long long)gridDim.x * WARPS_PER_CTA) {
-        unsigned long long si = ch * 32 + lane;
-        bool valid = si < nseg;
         // stage this chunk's segment records (coalesced 4-byte words)
         {
             const int words = sizeof(SegRec<R>) / 4;
@@ -363,48 +395,63 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
             uint32_t *dst = reinterpret_cast<uint32_t *>(&s_rec[w][0]);
             int nvalid = (int)min(32ull, nseg - ch * 32);
             for(int k = lane; k < nvalid * words; k += 32) dst[k] = __ldcs(src + k);
+            if(lane >= nvalid) s_rec[w][lane].job = -1;
         }
         __syncwarp();
         const SegRec<R> &my = s_rec[w][lane];
-        const GroupDev *G = nullptr;
+        const bool valid = my.job >= 0;
         const EnvDev *e = nullptr;
-        int nfreq = 0;
+        int nfreq = 0, freq_base = 0;
         if(valid) {
-            int job = my.job;
-            G = &groups[find_group(groups, ngroups, job)];
-            e = G->env;
-            nfreq = G->nfreq;
+            const GroupDev &G = groups[find_group(groups, ngroups, my.job)];
+            e = G.env;
+            nfreq = G.nfreq;
+            freq_base = G.freq_base;
+            int local = (int)((long long)my.job - G.job_base);
+            int nal = e->isingle > 0 ? 1 : e->nalpha;
+            int isz = local / nal;
+            s_base[w][lane] = G.field_base + (long long)isz * e->nrr * e->nrz_per_range;
+            s_rr[w][lane] = e->rr;
+            s_rz[w][lane] = e->rz;
+            s_stride[w][lane] = G.field_stride_f;
+            s_nrzp[w][lane] = e->irregular ? 0 : e->nrz_per_range;
         }
         int maxf = nfreq;
         for(int o = 16; o > 0; o >>= 1) maxf = max(maxf, __shfl_xor_sync(0xffffffffu, maxf, o));
         for(int f = 0; f < maxf; ++f) {
-            // ---- per-segment work count for frequency f
-            int cnt = 0, izlo = 0, niz = 0;
-            float sigfloor = 0.f;
-            double freq = 0.0;
+            // ---- per-segment work count for frequency f (owner lane)
+            int cnt = 0;
             if(valid && f < nfreq) {
-                freq = freqs[G->freq_base + f];
+                double freq = freqs[freq_base + f];
+                double omega = 2.0 * BHCB_PI * freq;
+                SegFreq<R> sf;
                 R sig = my.sigma_seg;
-                if(GAUSS) {
+                sf.sigfloor = (R)0;
+                if(GAUSS) {   // AdjustSigma (src/influence.hpp:91-100)
                     R lam = my.c0 / (R)freq;
                     R fl = min((R)FLTD(0.2) * (R)freq * my.tau1r, (R)BHCB_PI * lam);
-                    sigfloor = (float)fl;
+                    sf.sigfloor = fl;
                     sig = max(sig, fl);
                 }
                 double rmax = (GAUSS ? 4.0 : 1.0) * (double)sig;
                 int ncol = my.ir_hi - my.ir_lo + 1;
                 if(e->irregular) {
-                    niz = 1;
-                    izlo = 0;
+                    sf.niz = 1;
+                    sf.izlo = 0;
                 } else if(fabs((double)my.tx) > FLTD(0.50001)) {
                     double zmin = (double)my.zlo - rmax, zmax = (double)my.zhi + rmax;
-                    izlo = lower_f(e->rz, e->nrz, zmin);
-                    niz = upper_f(e->rz, e->nrz, zmax) - izlo;
+                    sf.izlo = lower_f(e->rz, e->nrz, zmin);
+                    sf.niz = upper_f(e->rz, e->nrz, zmax) - sf.izlo;
                 } else {
-                    izlo = 0;
-                    niz = e->nrz;
+                    sf.izlo = 0;
+                    sf.niz = e->nrz;
                 }
-                cnt = niz > 0 ? ncol * niz : 0;
+                sf.ph0 = (R)reduce_2pi(omega * my.tau0r);
+                sf.omdt = (R)(omega * (double)my.dtaur);
+                sf.att0 = (R)(omega * (double)my.tau0i);
+                sf.att1 = (R)(omega * (double)my.dtaui);
+                s_sf[w][lane] = sf;
+                cnt = sf.niz > 0 ? ncol * sf.niz : 0;
             }
             // warp exclusive scan of counts
             int incl = cnt;
@@ -415,11 +462,7 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
             int total = __shfl_sync(0xffffffffu, incl, 31);
             s_pre[w][lane + 1] = incl;
             if(lane == 0) s_pre[w][0] = 0;
-            s_izlo[w][lane] = izlo;
-            s_niz[w][lane] = niz;
-            s_sig[w][lane] = sigfloor;
             __syncwarp();
-            evals += (lane == 0) ? (unsigned long long)total : 0ull;
             for(int ev = lane; ev < total; ev += 32) {
                 // owning segment: largest k with s_pre[k] <= ev
                 int k = 0;
@@ -427,69 +470,55 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                 for(int step = 16; step > 0; step >>= 1)
                     if(s_pre[w][k + step] <= ev) k += step;
                 const SegRec<R> &S = s_rec[w][k];
+                const SegFreq<R> &F = s_sf[w][k];
                 int j = ev - s_pre[w][k];
-                int nz = s_niz[w][k];
-                int col = j / nz;
-                int izi = j - col * nz;
+                int col = 0;
+                while(j >= F.niz) { j -= F.niz; ++col; }   // few columns per segment
                 int ir = S.ir_lo + col;
-                int iz = s_izlo[w][k] + izi;
-                const GroupDev &GG = groups[find_group(groups, ngroups, S.job)];
-                const EnvDev &E = *GG.env;
-                double fq = freqs[GG.freq_base + f];
-                double zr = E.irregular ? (double)E.rz[ir] : (double)E.rz[iz];
-                R dr = (R)(E.rr[ir] - S.x0r), dz = (R)(zr - S.x0z);
-                R s = (dr * S.tx + dz * S.tz) / S.rlen;
-                R n1 = fabs(dr * (-S.tz) + dz * S.tx);
+                int iz = F.izlo + j;
+                int nrzp = s_nrzp[w][k];
+                double zr = (double)s_rz[w][k][nrzp ? iz : ir];
+                R dr = (R)(s_rr[w][k][ir] - S.x0r), dz = (R)(zr - S.x0z);
+                // InfluenceGeoCore (src/influence.hpp:897-1024), 2-D Cartesian
+                R s = M::div(dr * S.tx + dz * S.tz, S.rlen);
+                R n1 = fabs(dz * S.tx - dr * S.tz);
                 R qF = S.q0 + s * S.dq;
                 R sigma = fabs(qF * S.rcp_q0);
                 R sig0 = sigma;
-                if(GAUSS) sigma = max(sigma, (R)s_sig[w][k]);
-                R window = (GAUSS ? (R)4 : (R)1) * sigma;
-                if(n1 >= window) continue;   // outside the beam (n > W sigma or n == W sigma)
-                double delr = S.tau0r + (double)s * (double)S.dtaur;
-                R deli = S.tau0i + s * S.dtaui;
-                R cnst = S.cnst_num / sqrt(fabs(qF));
+                if(GAUSS) sigma = max(sigma, F.sigfloor);
+                if(n1 >= (GAUSS ? (R)4 : (R)1) * sigma) continue;   // outside the beam window
+                R cnst = S.cnst_num * M::rsqrt_(fabs(qF));
                 R wgt;
                 if(GAUSS) {
-                    R a = n1 / sigma;
-                    wgt = exp((R)FLTD(-0.5) * a * a) * (sig0 / sigma);
+                    R a = M::div(n1, sigma);
+                    wgt = M::exp_((R)FLTD(-0.5) * a * a) * M::div(sig0, sigma);
                 } else {
-                    wgt = (sigma - n1) / sigma;
+                    wgt = M::div(sigma - n1, sigma);
                 }
                 bool caustic = (qF <= (R)0 && S.q0 > (R)0) || (qF >= (R)0 && S.q0 < (R)0);
                 R ph = caustic ? S.phase_b : S.phase_a;
-                double omega = 2.0 * BHCB_PI * fq;
                 float2 v;
-                if(COHERENT) {
-                    R amp = cnst * wgt * exp((R)omega * deli);
-                    double ang = reduce_2pi(omega * delr - (double)ph);
+                if(COHERENT) {   // ApplyContribution (src/influence.hpp:455-459)
+                    R amp = cnst * wgt * M::exp_(F.att0 + s * F.att1);
+                    R ang = reduce_2pi(F.ph0 + s * F.omdt - ph);
                     R sn, cs;
-                    if(sizeof(R) == 4) {
-                        float sf, cf;
-                        sincosf((float)ang, &sf, &cf);
-                        sn = (R)sf; cs = (R)cf;
-                    } else {
-                        double sd, cd;
-                        sincos(ang, &sd, &cd);
-                        sn = (R)sd; cs = (R)cd;
-                    }
+                    M::sincos_(ang, &sn, &cs);
                     v = make_float2((float)(amp * cs), (float)(-amp * sn));
-                } else {
-                    R vv = cnst * exp((R)omega * deli);
+                } else {         // incoherent / semi-coherent (src/influence.hpp:460-468)
+                    R vv = cnst * M::exp_(F.att0 + s * F.att1);
                     vv = vv * vv * wgt;
                     if(GAUSS) vv *= (R)sqrt(FLTD(2.0) * BHCB_PI);
                     v = make_float2((float)vv, 0.f);
                 }
-                int local = (int)((long long)S.job - GG.job_base);
-                int nal = E.isingle > 0 ? 1 : E.nalpha;
-                int isz = local / nal;
-                size_t addr = (size_t)GG.field_base + (size_t)f * GG.field_stride_f
-                    + ((size_t)isz * E.nrr + ir) * E.nrz_per_range + (E.irregular ? 0 : iz);
+                size_t addr = (size_t)(s_base[w][k] + (long long)f * s_stride[w][k])
+                    + (size_t)ir * (nrzp ? nrzp : 1) + (nrzp ? iz : 0);
                 atomicAdd(&acc[addr], v);
+                ++evals;
             }
             __syncwarp();
         }
     }
+    for(int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
     if(lane == 0 && evals) atomicAdd(&ctr->nevals, evals);
 }
 

@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark: TL fields/s on one B200 for the range-dependent Gaussian-beam
+workload (2-D, PCHIP SSP, 200-point bathymetry, 20001 rays over +-30 deg,
+501 x 2001 receivers, 10 log-spaced frequencies 50-500 Hz).
+
+A step is one pass of the hot path over the batch: trace every ray, evaluate
+every beam-receiver contribution for all 10 frequencies, post-process the 10
+TL fields. Our arm runs the mixed-precision tracer (FP32 bulk, FP64 positions /
+travel time / crossing solves) with the 10 frequencies sharing one trajectory;
+the FP64 per-frequency tracer is timed beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank owns a different environment of the same
+shape (seed + rank); there is no data-path collective ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TL fields/s on 1 B200: mixed vs FP64 trace, surrogate vs plain, <=0.5 dB TL err"
+UNIT = "TL fields/s"
+WORKLOAD = "rd_gauss"
+
+# Algorithmic work per unit, frozen before the first GPU timing: one 2-D
+# oracle ray step (Step + RayUpdate + RayTerminate for a 1-D SSP) and one
+# applied beam-receiver contribution (InfluenceGeoCore + ApplyContribution).
+F_STEP = 320.0
+F_INFL = 40.0
+# Oracle counts for this workload (oracle/count_work.py rd_gauss): trajectories
+# do not depend on frequency, so steps are per trace; contributions are summed
+# over the 10 frequencies.
+ORACLE_STEPS_PER_TRACE = 20993289
+ORACLE_EVALS_ALL_FREQS = 6440570521
+# DRAM traffic of one influence launch (10 frequencies), from the ncu capture
+# summarised in profiles/influence_kernel_rd_gauss.md (None until captured).
+INFLUENCE_DRAM_BYTES = None
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                      "-lms", "200", "-i", str(self.gpu)], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- environment
+def make_env(tmp, rank):
+    from bellhopcuda_b200 import workloads as W
+    from bellhopcuda_b200.envfile import write_env
+    spec = W.rd_gauss(seed=1002 + rank)
+    root = write_env(spec, os.path.join(tmp, "rd_gauss_%d" % rank))
+    return spec, root, W.rd_gauss_freqs()
+
+
+def tl_rms(a, b):
+    import numpy as np
+    from bellhopcuda_b200 import tl_db
+    ta, tb = tl_db(a), tl_db(b)
+    m = tb < 100.0
+    d = np.abs(ta[m] - tb[m])
+    d = np.where(np.isfinite(d), d, 1e3)
+    return float(np.sqrt(np.mean(d ** 2)))
+
+
+# ------------------------------------------------------------- our arm
+def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush):
+    """Device time per step of the prepared run (tables resident in HBM)."""
+    t = B.Tracer(gpu=gpu, precision=precision)
+    t.setup(root)
+    t.set_frequencies(0, freqs)
+    t.prepare()
+    s = torch.cuda.ExternalStream(t.stream_ptr(), device=gpu)
+    for _ in range(warmup):
+        t.launch()
+        t.sync()
+    times, stats = [], []
+    for _ in range(steps):
+        with torch.cuda.stream(s):
+            flush.zero_()          # evict L2 (256 MiB > 126 MB) outside the timed window
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        t.launch()
+        e1.record(s)
+        t.sync()
+        times.append(e0.elapsed_time(e1))
+        stats.append(t.stats())
+    fields = [t.field(0, i)[0] for i in range(len(freqs))]
+    return t, times, stats, fields
+
+
+def time_e2e(B, torch, root, freqs, steps, gpu):
+    """Same metric through the public C ABI with host buffers: setup reads the
+    files, prepare uploads the tables, run, and every field copied back to
+    pinned host memory, all inside the timed window."""
+    t = B.Tracer(gpu=gpu, precision=B.PREC_MIXED)
+    nf = len(freqs)
+    t.setup(root)
+    t.set_frequencies(0, freqs)
+    t.run()
+    _, nsz, nrz, nrr = t.field_shape(0)
+    host = [torch.empty((nsz, nrz, nrr), dtype=torch.complex64, pin_memory=True) for _ in range(nf)]
+    s = torch.cuda.ExternalStream(t.stream_ptr(), device=gpu)
+    times = []
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        t.setup(root)
+        t.set_frequencies(0, freqs)
+        t.run()
+        for i in range(nf):
+            arr = host[i].numpy()
+            t.field(0, i, out=arr)
+        e1.record(s)
+        torch.cuda.synchronize(gpu)
+        times.append(e0.elapsed_time(e1))
+    st = t.stats()
+    d2h = nf * nsz * nrz * nrr * 8
+    t.close()
+    return times, st["h2d_bytes"], d2h
+
+
+# ------------------------------------------------------- reference CPU arm
+_libc = ctypes.CDLL(None)
+_libc.fma.restype = ctypes.c_double
+_libc.fma.argtypes = [ctypes.c_double] * 3
+
+
+def sampled_angles(n, a0, a1, first, m):
+    """The reference's sub-tabulated launch angles (SubTab, FMA form) first..first+m-1."""
+    dx = (a1 - a0) / (n - 1)
+    return [_libc.fma(float(i), dx, a0) for i in range(first, first + m)]
+
+
+def reference_sample(spec, freqs, m, tmp):
+    """Run the reference's own bellhopcxx (all host cores) on m consecutive rays
+    of every frequency; returns (estimated seconds per full step, detail)."""
+    import copy
+    from bellhopcuda_b200.envfile import write_env
+    exe = os.path.join(ROOT, "oracle", "_ref", "bellhopcxx")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/bellhopcxx not built"
+    n = spec.nalpha
+    total_ms, detail = 0.0, []
+    for k, f in enumerate(freqs):
+        first = int((k + 0.5) * (n - m) / len(freqs))
+        s2 = copy.deepcopy(spec)
+        s2.freq = f
+        s2.nalpha = m
+        s2.alpha = sampled_angles(n, spec.alpha[0], spec.alpha[1], first, m)
+        root = write_env(s2, os.path.join(tmp, "refsample_%d" % k))
+        out = subprocess.run([exe, "-2", root], capture_output=True, text=True, timeout=600)
+        mm = re.search(r"Run:\s*([0-9.eE+-]+)\s*ms", out.stdout)
+        if out.returncode != 0 or not mm:
+            return None, "bellhopcxx failed: " + (out.stdout + out.stderr)[-200:]
+        ms = float(mm.group(1))
+        total_ms += ms
+        detail.append(ms)
+    est_s = total_ms * (n / m) / 1000.0
+    return est_s, detail
+
+
+def cpu_baseline(spec, freqs, tmp, m=300):
+    est_s, detail = reference_sample(spec, freqs, m, tmp)
+    if est_s is None:
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": detail}
+    return {"value": len(freqs) / est_s, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": "reference bellhopcxx (unmodified sources, all %d host threads), %d consecutive "
+                      "rays of the %d-ray fan for each of the %d frequencies, Run time scaled by "
+                      "%d/%d" % (os.cpu_count(), m, spec.nalpha, len(freqs), spec.nalpha, m),
+            "sample_run_ms": detail}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from bellhopcuda_b200 import workloads as W
+    with tempfile.TemporaryDirectory() as tmp:
+        spec = W.rd_gauss()
+        freqs = W.rd_gauss_freqs()
+        vals = []
+        for _ in range(max(args.warmup, 0)):
+            reference_sample(spec, freqs, args.ref_rays, tmp)
+        for _ in range(args.steps):
+            est_s, detail = reference_sample(spec, freqs, args.ref_rays, tmp)
+            if est_s is None:
+                print(json.dumps({"impl": "reference", "unavailable": str(detail)}))
+                return 0
+            vals.append(len(freqs) / est_s)
+        v = statistics.mean(vals)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * len(freqs) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "rd_gauss: 2-D Gaussian-beam TL, PCHIP SSP 64 nodes, 200-pt bathymetry, "
+                                   "20001 rays +-30 deg, 501x2001 receivers, 10 freqs 50-500 Hz",
+                       "sample": "%d rays per frequency" % args.ref_rays},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": "%d consecutive rays per frequency of the %d-ray fan, scaled"
+                                       % (args.ref_rays, spec.nalpha)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-rays", type=int, default=300)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    import bellhopcuda_b200 as B
+    from bellhopcuda_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    fp32_peak, fp64_peak = B.probe_fp_peak(local)
+    with tempfile.TemporaryDirectory() as tmp:
+        spec, root, freqs = make_env(tmp, rank)
+        nf = len(freqs)
+        # ---- headline: mixed precision, shared trajectory
+        barrier()
+        with ClockSampler(local) as clk:
+            t, times, stats, fields_mixed = time_arm(B, torch, root, freqs, B.PREC_MIXED, args.steps,
+                                                     args.warmup, local, flush)
+            barrier()
+        clocks = clk.summary()
+        total_s = max_over_ranks(sum(times) / 1000.0)
+        ms_per_step = 1000.0 * total_s / args.steps
+        value = world * nf * args.steps / total_s
+        st = stats[-1]
+        t.close()
+        # ---- FP64 per-frequency tracer (the plain GPU trace)
+        fp64 = None
+        if not args.no_fp64:
+            t64, times64, stats64, fields64 = time_arm(B, torch, root, freqs, B.PREC_FP64,
+                                                       max(1, args.steps // 2), 1, local, flush)
+            t64.close()
+            ms64 = max_over_ranks(statistics.mean(times64))
+            errs = [tl_rms(fields_mixed[i], fields64[i]) for i in range(nf)]
+            fp64 = {"value": world * nf * 1000.0 / ms64, "ms_per_step": ms64,
+                    "mixed_speedup": (world * nf * 1000.0 / ms64) and value / (world * nf * 1000.0 / ms64),
+                    "tl_rms_err_db_mixed_vs_fp64_max_over_freqs": max(errs),
+                    "trace_ms": stats64[-1]["trace_ms"], "influence_ms": stats64[-1]["influence_ms"]}
+        # ---- end to end through the C ABI with host buffers
+        e2e_times, h2d, d2h = time_e2e(B, torch, root, freqs, max(1, args.steps), local)
+        e2e_s = max_over_ranks(sum(e2e_times) / 1000.0)
+        e2e = {"value": world * nf * len(e2e_times) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+        # ---- roofline of the dominant kernel
+        infl_ms = statistics.mean(s_["influence_ms"] for s_ in stats)
+        trace_ms = statistics.mean(s_["trace_ms"] for s_ in stats)
+        dom = "influence_kernel" if infl_ms >= trace_ms else "trace_kernel"
+        if dom == "influence_kernel":
+            work = F_INFL * ORACLE_EVALS_ALL_FREQS
+            dur = infl_ms
+        else:
+            work = F_STEP * ORACLE_STEPS_PER_TRACE
+            dur = trace_ms
+        achieved = work / (dur * 1e-3) / 1e12
+        roofline = {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": fp32_peak,
+                    "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
+                    "traffic": INFLUENCE_DRAM_BYTES if dom == "influence_kernel" else None,
+                    "peak_source": "bhcb_probe_fp_peak FP32 FMA probe measured in this run "
+                                   "(MEASURED_PEAKS.json has no FP32 figure)",
+                    "work": "%s x %d oracle units per launch" % (
+                        ("F_infl=%g flop" % F_INFL, ORACLE_EVALS_ALL_FREQS) if dom == "influence_kernel"
+                        else ("F_step=%g flop" % F_STEP, ORACLE_STEPS_PER_TRACE)),
+                    "kernel_ms": dur,
+                    "other_kernel": {"trace_kernel_ms": trace_ms, "trace_achieved_tflops":
+                                     F_STEP * ORACLE_STEPS_PER_TRACE / (trace_ms * 1e-3) / 1e12,
+                                     "influence_kernel_ms": infl_ms},
+                    "fp64_peak_tflops": fp64_peak}
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(spec, freqs, tmp, m=args.ref_rays)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 bulk / f64 phase+position", "data": "synthetic",
+        "config": {"workload": "rd_gauss: 2-D Gaussian-beam TL, PCHIP SSP 64 nodes, 200-pt bathymetry, "
+                               "20001 rays +-30 deg, 501x2001 receivers, 10 freqs 50-500 Hz, "
+                               "frequencies share one trajectory",
+                   "fields_per_step": nf, "rays": int(st["rays"]), "steps_traced": int(st["steps"]),
+                   "contributions": int(st["evals"]), "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas per GPU (one environment per rank)"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": 3 * args.steps, "fp64_trace": fp64,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

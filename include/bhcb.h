@@ -53,6 +53,7 @@ typedef struct bhcb_stats {
     uint32_t err_bits, warn_bits;   /* reference ErrState bit numbering (src/util/errors.hpp:61-93) */
     int32_t groups, fields;         /* trace groups launched, TL fields produced */
     double trace_ms, influence_ms, total_ms;
+    uint64_t h2d_bytes;             /* table bytes uploaded by the last bhcb_prepare */
 } bhcb_stats;
 
 /* Create a context; replaces the bhcInternal construction in bhc::setup
@@ -104,6 +105,14 @@ int bhcb_receivers(bhcb_ctx *ctx, int32_t env_index, double *rr, int32_t nrr, fl
 /* bhc::writeout (src/api.cpp:465-486) for TL runs: write FileRoot.shd of
    (env_index, ifreq) in the reference's .shd layout (src/mode/tl.cpp:38-248). */
 int bhcb_writeout(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, const char *file_root);
+
+/* The context's CUDA stream (cudaStream_t), for callers that time or order
+   their own work against the tracer's kernels. */
+int bhcb_stream(bhcb_ctx *ctx, void **stream);
+
+/* Measured FP32 / FP64 FMA throughput of the device (TFLOP/s), the roofline
+   denominators of the tracer's pipe-bound kernels. */
+int bhcb_probe_fp_peak(int32_t gpu_index, double *fp32_tflops, double *fp64_tflops);
 
 /* Counters of the last run. */
 int bhcb_get_stats(bhcb_ctx *ctx, bhcb_stats *stats);

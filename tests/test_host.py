@@ -1,0 +1,137 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every
+entry point of include/bhcb.h; the native reader / preprocessing agrees with
+the oracle on sizes and rejects invalid inputs with the reference's messages."""
+import os
+import re
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import bellhopcuda_b200 as B  # noqa: E402
+import oracle_ctypes  # noqa: E402
+from cases import CASES  # noqa: E402
+from bellhopcuda_b200.envfile import EnvSpec, write_env  # noqa: E402
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "bhcb.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(bhcb_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = B.load_library()
+    names = header_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding declares every one of them
+    bound = {n for n, _, _ in B.SIGNATURES}
+    assert set(names) <= bound, set(names) - bound
+
+
+def test_version_string():
+    assert b"sm_100a" in B.load_library().bhcb_version()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reader_sizes_match_oracle(name, workdir):
+    spec = CASES[name]()
+    root = write_env(spec, os.path.join(workdir, "sz_" + name))
+    info = B.check_env(root)
+    o = oracle_ctypes.run(spec)
+    assert info["nsz"] == o["NSz"]
+    assert info["nrz"] == o["NRz"]
+    assert info["nrr"] == o["NRr"]
+    assert info["nalpha"] == o["Nalpha"]
+
+
+def test_reader_list_directed_syntax(workdir):
+    """Repeat counts, commas, '/' terminators and quoted strings."""
+    root = os.path.join(workdir, "ld")
+    open(root + ".env", "w").write(
+        "'list, directed test' ! title\n"
+        "100.0\n1\n'CVW'\n"
+        "3  0.0  1000.0\n"
+        "0.0 1500.0 /\n500.0,1510.0,0.0,1.0 /\n1000.0 1520.0 /\n"
+        "'A' 0.0\n1000.0 1600.0 0.0 1.8 0.8 0.0 /\n"
+        "1\n500.0 /\n"
+        "3\n100.0 2*900.0 /\n"
+        "11\n0.0 10.0 /\n"
+        "'CG'\n"
+        "21\n-10.0 10.0 /\n"
+        "0.0 1100.0 10.5\n")
+    info = B.check_env(root)
+    assert info["nrz"] == 3 and info["nrr"] == 11 and info["nalpha"] == 21
+    assert info["freq"] == 100.0 and abs(info["deltas"] - 100.0) < 1e-12
+
+
+def _write(workdir, name, **kw):
+    from bellhopcuda_b200 import workloads as W
+    spec = W.munk_tl(nalpha=11, nrz=5, nrr=5)
+    for k, v in kw.items():
+        setattr(spec, k, v)
+    return write_env(spec, os.path.join(workdir, name))
+
+
+def test_reader_rejects_nonmonotone_ssp(workdir):
+    z = np.arange(0.0, 5001.0, 100.0)
+    z[10], z[11] = z[11], z[10]
+    root = _write(workdir, "nonmono", ssp_z=list(z))
+    with pytest.raises(B.BhcbError, match="monotone"):
+        B.check_env(root)
+
+
+def test_reader_rejects_bathymetry_below_ssp(workdir):
+    root = _write(workdir, "deep", bty_r=[0.0, 50.0, 100.0], bty_z=[4000.0, 6000.0, 4000.0])
+    with pytest.raises(B.BhcbError, match="bathymetry drops below"):
+        B.check_env(root)
+
+
+def test_reader_rejects_bad_box(workdir):
+    root = _write(workdir, "box", box_z=0.0)
+    with pytest.raises(B.BhcbError, match="beam box"):
+        B.check_env(root)
+
+
+def test_reader_rejects_unsupported_beam(workdir):
+    root = _write(workdir, "cerveny", run_type="CC RR ")
+    with pytest.raises(B.BhcbError, match="not supported"):
+        B.check_env(root)
+
+
+def test_reader_missing_file(workdir):
+    with pytest.raises(B.BhcbError, match="unable to open"):
+        B.check_env(os.path.join(workdir, "does_not_exist"))
+
+
+def test_open_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(B.BhcbError):
+        B.Tracer()
+
+
+REFERENCE_INPUTS = "/root/reference/test/in"
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_INPUTS), reason="reference inputs not present")
+@pytest.mark.parametrize("name", ["Munk", "MunkB_Coh", "MunkB_gb", "DickinsB", "DickinsFlatB", "free"])
+def test_reader_accepts_reference_inputs(name, workdir):
+    src = os.path.join(REFERENCE_INPUTS, name)
+    if not os.path.exists(src + ".env"):
+        pytest.skip("no such input")
+    import shutil
+    for ext in (".env", ".bty", ".ati", ".ssp", ".sbp"):
+        if os.path.exists(src + ext):
+            shutil.copy(src + ext, os.path.join(workdir, name + ext))
+    try:
+        B.check_env(os.path.join(workdir, name))
+    except B.BhcbError as e:
+        assert "not supported" in str(e) or "not a field mode" in str(e), str(e)

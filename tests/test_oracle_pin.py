@@ -1,0 +1,76 @@
+"""The oracle (C restatement) against the reference itself.
+
+Golden fixtures in tests/golden/ were produced by the reference's own
+bellhopcxx, compiled from its unmodified sources (tests/golden/make_golden.py).
+The oracle must reproduce them bit-for-bit. When the reference build is present
+(oracle/_ref), a second check runs it live on a fresh randomised case.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import oracle_ctypes  # noqa: E402
+from cases import CASES  # noqa: E402
+from bellhopcuda_b200.envfile import write_env  # noqa: E402
+from bellhopcuda_b200.shdfile import read_shd  # noqa: E402
+
+REF_EXE = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "bellhopcxx")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_reference_golden(name):
+    gold = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    res = oracle_ctypes.run(CASES[name]())
+    assert res["err_bits"] == 0
+    got = res["field"]
+    ref = gold["field"]
+    assert got.shape == ref.shape
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(res["rr"], gold["rr"])
+    np.testing.assert_array_equal(res["rz"], gold["rz"])
+
+
+@pytest.mark.skipif(not os.path.exists(REF_EXE), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("seed", [1, 2])
+def test_oracle_matches_reference_live(seed, workdir):
+    from bellhopcuda_b200 import workloads as W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    spec = W.rd_gauss(seed=100 + seed, nalpha=int(rng.integers(51, 201)), nrz=int(rng.integers(11, 41)),
+                      nrr=int(rng.integers(21, 121)), nbty=int(rng.integers(5, 60)))
+    spec.freq = float(rng.uniform(30, 400))
+    spec.run_type = ["CG RR ", "CB RR ", "IB RR "][seed % 3]
+    root = write_env(spec, os.path.join(workdir, "live%d" % seed))
+    subprocess.run([REF_EXE, "-2", "-1", root], check=True, capture_output=True)
+    ref = read_shd(root + ".shd")["field"][0, 0, 0]
+    got = oracle_ctypes.run(spec)["field"]
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_oracle_arrivals_match_reference_counts(workdir):
+    if not os.path.exists(REF_EXE):
+        pytest.skip("reference build (oracle/_ref) not present")
+    import re
+    from bellhopcuda_b200 import workloads as W
+    from bellhopcuda_b200.arrfile import read_arr_binary
+    spec = W.rd_gauss(nalpha=151, nrz=7, nrr=15, nbty=20)
+    spec.run_type = "aG RR "
+    root = write_env(spec, os.path.join(workdir, "arr"))
+    subprocess.run([REF_EXE, "-2", "-1", root], check=True, capture_output=True)
+    A = read_arr_binary(root + ".arr")
+    mx = int(re.search(r"Maximum # of arrivals = *(\d+)", open(root + ".prt").read()).group(1))
+    o = oracle_ctypes.run(spec, max_narr=mx, allow_merging=1)
+    for k, arrs in enumerate(A["sources"][0]["arrivals"]):
+        iz, ir = divmod(k, spec.nrr)
+        n = o["narr"][0, iz, ir]
+        assert n == len(arrs)
+        oa = o["arr"][0, iz, ir, :n]
+        np.testing.assert_array_equal(oa["a"], arrs[:, 0])
+        np.testing.assert_array_equal(oa["delay_re"], arrs[:, 2])
+        np.testing.assert_array_equal(oa["NTopBnc"].astype(np.float32), arrs[:, 6])
+        np.testing.assert_array_equal(oa["NBotBnc"].astype(np.float32), arrs[:, 7])
