@@ -85,6 +85,8 @@ SIGNATURES = [
                                   C.POINTER(C.c_uint32)]),
     ("bhcb_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("bhcb_probe_fp_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("bhcb_run_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
+                                   C.c_char_p, C.c_size_t]),
     ("bhcb_check_env", C.c_int, [C.c_char_p, C.POINTER(EnvInfo), C.c_char_p, C.c_size_t]),
     ("bhcb_version", C.c_char_p, []),
 ]
@@ -229,6 +231,14 @@ class Tracer:
 
     def writeout(self, file_root: str, env: int = 0, ifreq: int = 0):
         self._check(self._lib.bhcb_writeout(self._h, env, ifreq, file_root.encode()))
+
+    def run_noalloc(self, field_dev_ptr: int, nbytes: int, env: int = 0, ifreq: int = 0):
+        """Allocation-free run of one field into a caller-owned device buffer
+        (see bhcb_run_noalloc in include/bhcb.h); the context must be prepared."""
+        msg = C.create_string_buffer(256)
+        rc = self._lib.bhcb_run_noalloc(self._h, env, ifreq, C.c_void_p(field_dev_ptr), nbytes, msg, 256)
+        if rc != 0:
+            raise BhcbError(rc, msg.value.decode(errors="replace"))
 
     def stream_ptr(self) -> int:
         p = C.c_void_p()

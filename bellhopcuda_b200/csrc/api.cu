@@ -17,6 +17,7 @@
 #include "../../include/bhcb.h"
 #include "bhcb_internal.h"
 #include "host/env2d.h"
+#include "noalloc.h"
 
 namespace bhcb {
 template<typename R> cudaError_t launch_trace(const GroupDev *, int, long long, void *,
@@ -423,6 +424,36 @@ const Field *find_field(bhcb_ctx *c, int env, int ifreq)
 }
 
 } // namespace
+
+namespace bhcb {
+int noalloc_job_from_ctx(bhcb_ctx *c, int32_t env, int32_t ifreq, NoAllocJob *job, const char **why)
+{
+    if(!c->prepared) { *why = "context not prepared: call bhcb_prepare (or bhcb_run) first"; return BHCB_ERR_STATE; }
+    if(env < 0 || env >= (int)c->envs.size()) { *why = "env_index out of range"; return BHCB_ERR_ARG; }
+    const EnvSlot &S = c->envs[env];
+    if(ifreq < 0 || ifreq >= (int)S.field_of_freq.size()) { *why = "ifreq out of range"; return BHCB_ERR_ARG; }
+    const Field &F = c->fields[S.field_of_freq[ifreq]];
+    for(const GroupDev &G : c->groups_h) {
+        int64_t span = (int64_t)G.nfreq * G.field_stride_f;
+        if(F.base >= G.field_base && F.base < G.field_base + span) {
+            int k = (int)((F.base - G.field_base) / G.field_stride_f);
+            job->group = G;
+            job->freq = c->freqs_h[G.freq_base + k];
+            job->precision = c->precision;
+            job->gaussian = c->gauss;
+            job->coherent = c->coherent;
+            job->nsz = F.nsz;
+            job->nrzp = F.nrzp;
+            job->nrr = F.nrr;
+            job->sm_count = c->sm_count;
+            job->stream = c->stream;
+            return BHCB_OK;
+        }
+    }
+    *why = "field not found in the prepared groups";
+    return BHCB_ERR_STATE;
+}
+} // namespace bhcb
 
 extern "C" {
 

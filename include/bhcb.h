@@ -131,6 +131,25 @@ typedef struct bhcb_env_info {
 } bhcb_env_info;
 int bhcb_check_env(const char *file_root, bhcb_env_info *info, char *msg, size_t n);
 
+/* Allocation-free run (no counterpart in the reference). For callers that
+   must not allocate device memory once running — work inside a budget owned
+   by another allocator, allocation-free real-time loops, issuing work while a
+   stream is being captured. Computes field (env_index, ifreq) of a context
+   prepared earlier (bhcb_prepare / bhcb_run, which allocate) into the
+   caller's device buffer field_dev ([NSz][NRz_per_range][NRr] complex float,
+   bytes >= its size) on the context stream, then synchronises. It calls no
+   cudaMalloc / cudaFree: its scratch (accumulator, counters, field
+   descriptor) is a static device array the library reserves on every GPU
+   that loads it, limited to BHCB_NOALLOC_MAX_FIELD receivers per field; larger
+   fields are rejected with BHCB_ERR_ARG. The first call on a device looks up
+   the array's address (cudaGetSymbolAddress) and should come before any
+   stream capture. All calls on a device share the array: calls whose GPU
+   work overlaps race and must be serialised. msg (may be NULL) receives the
+   reason of a failure. */
+#define BHCB_NOALLOC_MAX_FIELD (1 << 21)
+int bhcb_run_noalloc(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void *field_dev, size_t bytes,
+                     char *msg, size_t msg_len);
+
 /* Library version string. */
 const char *bhcb_version(void);
 
