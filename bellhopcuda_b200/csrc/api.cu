@@ -351,7 +351,7 @@ void do_launch(bhcb_ctx *c)
     CK(cudaEventRecord(c->ev[1], c->stream));
     // the influence grid covers the buffer capacity; chunks past the stored
     // count are skipped by reading the count on the device
-    int igrid = c->sm_count * 8;
+    int igrid = c->sm_count * 8;   // persistent warps draining the chunk queue
     if(fp64)
         CK(launch_influence<double>(c->segs.p, c->seg_cap, G, ng, (const double *)c->freqs_d.p,
                                     (float2 *)c->acc.p, ctr, c->gauss, c->coherent, igrid, c->stream));

@@ -112,6 +112,7 @@ struct RunCounters {
     unsigned int err_bits, warn_bits;
     unsigned int overflow_job;    // first job that could not store its segments
     unsigned int pad;
+    unsigned long long chunk_counter;   // influence work queue (32-segment chunks)
 };
 
 } // namespace bhcb

@@ -200,15 +200,109 @@ template<typename R> struct SegFreq {
     R ph0;         // omega * tau0.real reduced to [-pi, pi]
     R omdt;        // omega * dtau.real
     R att0, att1;  // omega * tau0.imag, omega * dtau.imag
+    double zmin, zmax;   // receiver depth window of the segment
     int izlo, niz;
 };
 
-template<typename R, bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
+// One beam-receiver contribution of segment S at (column ir, depth index
+// zidx); returns false when the receiver is outside the beam window.
+// InfluenceGeoCore + ApplyContribution (src/influence.hpp:423-473,897-1024).
+// The FP64 kernel keeps the reference's operation order; the mixed kernel
+// uses the per-column constants A = dr tx / rlen, Bz = tz / rlen, Cn = dr tz.
+template<typename R, bool GAUSS, bool COHERENT> struct Contribution;
+
+template<bool GAUSS, bool COHERENT> struct Contribution<double, GAUSS, COHERENT> {
+    double dr;
+    __device__ __forceinline__ void column(const SegRec<double> &S, double rr) { dr = rr - S.x0r; }
+    __device__ __forceinline__ bool eval(const SegRec<double> &S, const SegFreq<double> &F, float zr_f,
+                                         float2 &v) const
+    {
+        double dz = (double)zr_f - S.x0z;
+        double s = (dr * S.tx + dz * S.tz) / S.rlen;
+        double n1 = fabs(dz * S.tx - dr * S.tz);
+        double qF = S.q0 + s * S.dq;
+        double sigma = fabs(qF * S.rcp_q0), sig0 = sigma;
+        if(GAUSS) sigma = max(sigma, F.sigfloor);
+        if(n1 >= (GAUSS ? 4.0 : 1.0) * sigma) return false;
+        double cnst = S.cnst_num / sqrt(fabs(qF));
+        double wgt;
+        if(GAUSS) wgt = exp(FLTD(-0.5) * (n1 / sigma) * (n1 / sigma)) * (sig0 / sigma);
+        else wgt = (sigma - n1) / sigma;
+        bool caustic = (qF <= 0.0 && S.q0 > 0.0) || (qF >= 0.0 && S.q0 < 0.0);
+        double ph = caustic ? S.phase_b : S.phase_a;
+        if(COHERENT) {
+            double amp = cnst * wgt * exp(F.att0 + s * F.att1);
+            double ang = reduce_2pi(F.ph0 + s * F.omdt - ph), sn, cs;
+            sincos(ang, &sn, &cs);
+            v = make_float2((float)(amp * cs), (float)(-amp * sn));
+        } else {
+            double vv = cnst * exp(F.att0 + s * F.att1);
+            vv = vv * vv * wgt;
+            if(GAUSS) vv *= sqrt(FLTD(2.0) * BHCB_PI);
+            v = make_float2((float)vv, 0.f);
+        }
+        return true;
+    }
+};
+
+template<bool GAUSS, bool COHERENT> struct Contribution<float, GAUSS, COHERENT> {
+    float A, Bz, Cn, x0z;
+    __device__ __forceinline__ void column(const SegRec<float> &S, double rr)
+    {
+        float dr = (float)(rr - S.x0r);
+        float inv = __fdividef(1.0f, S.rlen);
+        A = dr * S.tx * inv;
+        Bz = S.tz * inv;
+        Cn = dr * S.tz;
+        x0z = (float)S.x0z;
+    }
+    __device__ __forceinline__ bool eval(const SegRec<float> &S, const SegFreq<float> &F, float zr,
+                                         float2 &v) const
+    {
+        float dz = zr - x0z;
+        float s = fmaf(dz, Bz, A);
+        float n1 = fabsf(fmaf(dz, S.tx, -Cn));
+        float qF = fmaf(s, S.dq, S.q0);
+        float sigma = fabsf(qF * S.rcp_q0), sig0 = sigma;
+        if(GAUSS) sigma = fmaxf(sigma, F.sigfloor);
+        if(n1 >= (GAUSS ? 4.f : 1.f) * sigma) return false;
+        float rs = __fdividef(1.0f, sigma);
+        float cnst = S.cnst_num * rsqrtf(fabsf(qF));
+        float wgt;
+        if(GAUSS) {
+            float a = n1 * rs;
+            wgt = __expf(-0.5f * a * a) * (sig0 * rs);
+        } else {
+            wgt = (sigma - n1) * rs;
+        }
+        bool caustic = (qF <= 0.f && S.q0 > 0.f) || (qF >= 0.f && S.q0 < 0.f);
+        float ph = caustic ? S.phase_b : S.phase_a;
+        float att = fmaf(s, F.att1, F.att0);
+        if(COHERENT) {
+            float amp = cnst * wgt * (att != 0.f ? __expf(att) : 1.f);
+            float ang = reduce_2pi(fmaf(s, F.omdt, F.ph0) - ph), sn, cs;
+            __sincosf(ang, &sn, &cs);
+            v = make_float2(amp * cs, -amp * sn);
+        } else {
+            float vv = cnst * (att != 0.f ? __expf(att) : 1.f);
+            vv = vv * vv * wgt;
+            if(GAUSS) vv *= 2.50662827463100050242f;   // sqrt(2 pi)
+            v = make_float2(vv, 0.f);
+        }
+        return true;
+    }
+};
+
+// Warp-cooperative influence: each warp stages 32 segment records, then for
+// every frequency splits itself into sub-groups of g lanes (g = 4..32, chosen
+// from the chunk's average work per segment); a group takes one segment at a
+// time, keeps its fields in registers and strides its lanes over the depths of
+// each receiver column, so consecutive lanes reduce into consecutive addresses.
+template<typename R, bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(32 * WARPS_PER_CTA, 6)
 influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                  const GroupDev *__restrict__ groups, int ngroups, const double *__restrict__ freqs,
                  float2 *__restrict__ acc, RunCounters *ctr)
 {
-    using M = EvalMath<R>;
     // the trace kernel's slot counter may exceed the capacity on overflow
     const unsigned long long nseg = min(__ldcg(&ctr->nseg), cap);
     __shared__ SegRec<R> s_rec[WARPS_PER_CTA][32];
@@ -218,19 +312,23 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
     __shared__ const float *s_rz[WARPS_PER_CTA][32];
     __shared__ int s_stride[WARPS_PER_CTA][32];           // per-frequency field stride
     __shared__ int s_nrzp[WARPS_PER_CTA][32];             // 0 -> irregular grid
-    __shared__ int s_pre[WARPS_PER_CTA][33];
+    __shared__ int s_nf[WARPS_PER_CTA][32];               // frequencies of the segment's group
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned long long nchunks = (nseg + 31) / 32;
-    unsigned long long evals = 0;
-    for(unsigned long long ch = (unsigned long long)blockIdx.x * WARPS_PER_CTA + w; ch < nchunks;
-        ch += (unsigned long long)gridDim.x * WARPS_PER_CTA) {
-        // stage this chunk's segment records (coalesced 4-byte words)
+    unsigned int evals = 0;
+    for(;;) {
+        // dynamic work queue: chunks differ widely in work
+        unsigned long long ch = 0;
+        if(lane == 0) ch = atomicAdd(&ctr->chunk_counter, 1ull);
+        ch = __shfl_sync(0xffffffffu, ch, 0);
+        if(ch >= nchunks) break;
         {
             const int words = sizeof(SegRec<R>) / 4;
             const uint32_t *src = reinterpret_cast<const uint32_t *>(segs + ch * 32);
             uint32_t *dst = reinterpret_cast<uint32_t *>(&s_rec[w][0]);
             int nvalid = (int)min(32ull, nseg - ch * 32);
             for(int k = lane; k < nvalid * words; k += 32) dst[k] = __ldcs(src + k);
+            __syncwarp();
             if(lane >= nvalid) s_rec[w][lane].job = -1;
         }
         __syncwarp();
@@ -252,10 +350,10 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
             s_stride[w][lane] = G.field_stride_f;
             s_nrzp[w][lane] = e->irregular ? 0 : e->nrz_per_range;
         }
+        s_nf[w][lane] = nfreq;
         int maxf = nfreq;
         for(int o = 16; o > 0; o >>= 1) maxf = max(maxf, __shfl_xor_sync(0xffffffffu, maxf, o));
         for(int f = 0; f < maxf; ++f) {
-            // ---- per-segment work count for frequency f (owner lane)
             int cnt = 0;
             if(valid && f < nfreq) {
                 double freq = freqs[freq_base + f];
@@ -270,92 +368,89 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                     sig = max(sig, fl);
                 }
                 double rmax = (GAUSS ? 4.0 : 1.0) * (double)sig;
-                int ncol = my.ir_hi - my.ir_lo + 1;
+                if(fabs((double)my.tx) > FLTD(0.50001)) {
+                    sf.zmin = (double)my.zlo - rmax;
+                    sf.zmax = (double)my.zhi + rmax;
+                } else {   // steep segment: every depth (src/influence.hpp:1285-1292)
+                    sf.zmin = -1.7976931348623157e308;
+                    sf.zmax = 1.7976931348623157e308;
+                }
                 if(e->irregular) {
                     sf.niz = 1;
                     sf.izlo = 0;
-                } else if(fabs((double)my.tx) > FLTD(0.50001)) {
-                    double zmin = (double)my.zlo - rmax, zmax = (double)my.zhi + rmax;
-                    sf.izlo = lower_f(e->rz, e->nrz, zmin);
-                    sf.niz = upper_f(e->rz, e->nrz, zmax) - sf.izlo;
                 } else {
-                    sf.izlo = 0;
-                    sf.niz = e->nrz;
+                    sf.izlo = lower_f(e->rz, e->nrz, sf.zmin);
+                    sf.niz = upper_f(e->rz, e->nrz, sf.zmax) - sf.izlo;
                 }
                 sf.ph0 = (R)reduce_2pi(omega * my.tau0r);
                 sf.omdt = (R)(omega * (double)my.dtaur);
                 sf.att0 = (R)(omega * (double)my.tau0i);
                 sf.att1 = (R)(omega * (double)my.dtaui);
                 s_sf[w][lane] = sf;
-                cnt = sf.niz > 0 ? ncol * sf.niz : 0;
+                cnt = sf.niz > 0 ? (my.ir_hi - my.ir_lo + 1) * sf.niz : 0;
             }
-            // warp exclusive scan of counts
-            int incl = cnt;
-            for(int o = 1; o < 32; o <<= 1) {
-                int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if(lane >= o) incl += v;
-            }
-            int total = __shfl_sync(0xffffffffu, incl, 31);
-            s_pre[w][lane + 1] = incl;
-            if(lane == 0) s_pre[w][0] = 0;
+            int tot = cnt;
+            for(int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            if(tot == 0) continue;
             __syncwarp();
-            for(int ev = lane; ev < total; ev += 32) {
-                // owning segment: largest k with s_pre[k] <= ev
-                int k = 0;
-#pragma unroll
-                for(int step = 16; step > 0; step >>= 1)
-                    if(s_pre[w][k + step] <= ev) k += step;
+            // group size from the average depth-run length of the chunk
+            int avg = tot >> 5;
+            int g = avg >= 24 ? 32 : avg >= 12 ? 16 : avg >= 6 ? 8 : 4;
+            int ngrp = 32 / g, gid = lane / g, lig = lane & (g - 1);
+            for(int k = gid; k < 32; k += ngrp) {
                 const SegRec<R> &S = s_rec[w][k];
-                const SegFreq<R> &F = s_sf[w][k];
-                int j = ev - s_pre[w][k];
-                int col = 0;
-                while(j >= F.niz) { j -= F.niz; ++col; }   // few columns per segment
-                int ir = S.ir_lo + col;
-                int iz = F.izlo + j;
-                int nrzp = s_nrzp[w][k];
-                double zr = (double)s_rz[w][k][nrzp ? iz : ir];
-                R dr = (R)(s_rr[w][k][ir] - S.x0r), dz = (R)(zr - S.x0z);
-                // InfluenceGeoCore (src/influence.hpp:897-1024), 2-D Cartesian
-                R s = M::div(dr * S.tx + dz * S.tz, S.rlen);
-                R n1 = fabs(dz * S.tx - dr * S.tz);
-                R qF = S.q0 + s * S.dq;
-                R sigma = fabs(qF * S.rcp_q0);
-                R sig0 = sigma;
-                if(GAUSS) sigma = max(sigma, F.sigfloor);
-                if(n1 >= (GAUSS ? (R)4 : (R)1) * sigma) continue;   // outside the beam window
-                R cnst = S.cnst_num * M::rsqrt_(fabs(qF));
-                R wgt;
-                if(GAUSS) {
-                    R a = M::div(n1, sigma);
-                    wgt = M::exp_((R)FLTD(-0.5) * a * a) * M::div(sig0, sigma);
+                if(S.job < 0) continue;
+                const SegFreq<R> F = s_sf[w][k];
+                const long long base = s_base[w][k] + (long long)f * s_stride[w][k];
+                const double *rr = s_rr[w][k];
+                const float *rz = s_rz[w][k];
+                const int nrzp = s_nrzp[w][k];
+                if(f >= s_nf[w][k]) continue;   // its group has fewer frequencies
+                if(nrzp) {
+                    // rectilinear grid: the group walks the flattened (column, depth)
+                    // pairs of the segment, depth fastest, so the idle tail is paid
+                    // once per segment; a lane recomputes its column constants only
+                    // when it moves to the next column.
+                    const int niz = F.niz, total = (S.ir_hi - S.ir_lo + 1) * niz;
+                    const float *zp = rz + F.izlo;
+                    int col = lig / niz, j = lig - col * niz, ccol = -1;
+                    Contribution<R, GAUSS, COHERENT> C;
+                    float2 *colp = nullptr;
+                    for(int e = lig; e < total; e += g) {
+                        if(col != ccol) {
+                            ccol = col;
+                            int ir = S.ir_lo + col;
+                            C.column(S, rr[ir]);
+                            colp = acc + base + (long long)ir * nrzp + F.izlo;
+                        }
+                        float2 v;
+                        if(C.eval(S, F, zp[j], v)) {
+                            atomicAdd(colp + j, v);
+                            ++evals;
+                        }
+                        j += g;
+                        while(j >= niz) { j -= niz; ++col; }
+                    }
                 } else {
-                    wgt = M::div(sigma - n1, sigma);
+                    // irregular grid: one receiver per column, at depth rz[ir]
+                    for(int ir = S.ir_lo + lig; ir <= S.ir_hi; ir += g) {
+                        double zr = (double)rz[ir];
+                        if(zr < F.zmin || zr > F.zmax) continue;
+                        Contribution<R, GAUSS, COHERENT> C;
+                        C.column(S, rr[ir]);
+                        float2 v;
+                        if(C.eval(S, F, rz[ir], v)) {
+                            atomicAdd(acc + base + ir, v);
+                            ++evals;
+                        }
+                    }
                 }
-                bool caustic = (qF <= (R)0 && S.q0 > (R)0) || (qF >= (R)0 && S.q0 < (R)0);
-                R ph = caustic ? S.phase_b : S.phase_a;
-                float2 v;
-                if(COHERENT) {   // ApplyContribution (src/influence.hpp:455-459)
-                    R amp = cnst * wgt * M::exp_(F.att0 + s * F.att1);
-                    R ang = reduce_2pi(F.ph0 + s * F.omdt - ph);
-                    R sn, cs;
-                    M::sincos_(ang, &sn, &cs);
-                    v = make_float2((float)(amp * cs), (float)(-amp * sn));
-                } else {         // incoherent / semi-coherent (src/influence.hpp:460-468)
-                    R vv = cnst * M::exp_(F.att0 + s * F.att1);
-                    vv = vv * vv * wgt;
-                    if(GAUSS) vv *= (R)sqrt(FLTD(2.0) * BHCB_PI);
-                    v = make_float2((float)vv, 0.f);
-                }
-                size_t addr = (size_t)(s_base[w][k] + (long long)f * s_stride[w][k])
-                    + (size_t)ir * (nrzp ? nrzp : 1) + (nrzp ? iz : 0);
-                atomicAdd(&acc[addr], v);
-                ++evals;
             }
             __syncwarp();
         }
     }
     for(int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
-    if(lane == 0 && evals) atomicAdd(&ctr->nevals, evals);
+    if(lane == 0 && evals) atomicAdd(&ctr->nevals, (unsigned long long)evals);
 }
 
 // ScalePressure (src/influence.hpp:1556-1627, 2-D) fused with the transpose

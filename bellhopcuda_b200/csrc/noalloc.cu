@@ -75,12 +75,17 @@ template<typename R, bool GAUSS, bool COHERENT> __device__ __forceinline__ void 
         sig = max(sig, sigfloor);
     }
     double rmax = (GAUSS ? 4.0 : 1.0) * (double)sig;
+    double zmin = -1.7976931348623157e308, zmax = 1.7976931348623157e308;
+    if(fabs((double)S.tx) > FLTD(0.50001)) {   // steep segments take every depth
+        zmin = (double)S.zlo - rmax;
+        zmax = (double)S.zhi + rmax;
+    }
     int izlo = 0, niz = e.nrz;
     if(e.irregular) {
         niz = 1;
-    } else if(fabs((double)S.tx) > FLTD(0.50001)) {
-        izlo = lower_f(e.rz, e.nrz, (double)S.zlo - rmax);
-        niz = upper_f(e.rz, e.nrz, (double)S.zhi + rmax) - izlo;
+    } else {
+        izlo = lower_f(e.rz, e.nrz, zmin);
+        niz = upper_f(e.rz, e.nrz, zmax) - izlo;
     }
     R ph0 = (R)reduce_2pi(omega * S.tau0r);
     R omdt = (R)(omega * (double)S.dtaur);
@@ -90,6 +95,7 @@ template<typename R, bool GAUSS, bool COHERENT> __device__ __forceinline__ void 
         for(int j = 0; j < niz; ++j) {
             int iz = izlo + j;
             double zr = (double)e.rz[nrzp ? iz : ir];
+            if(!nrzp && (zr < zmin || zr > zmax)) continue;   // depth window, irregular grid
             R dr = (R)(e.rr[ir] - S.x0r), dz = (R)(zr - S.x0z);
             R s = M::div(dr * S.tx + dz * S.tz, S.rlen);
             R n1 = fabs(dz * S.tx - dr * S.tz);

@@ -62,8 +62,10 @@ __device__ __forceinline__ void update_seg(double x, bool tpos, const double *a,
     }
 }
 
-// src/ssp.hpp:53-152,309-375 (1-D profile types evaluated in 2-D)
-template<typename R> __device__ __forceinline__ void eval_ssp(
+// src/ssp.hpp:53-152,309-375 (1-D profile types evaluated in 2-D). The
+// density (LinInterpDensity) is only used by reflections, so it is evaluated
+// when NEED_RHO is set.
+template<typename R, bool NEED_RHO = false> __device__ __forceinline__ void eval_ssp(
     V2<double> x, V2<R> t, SSPOut<R> &o, const EnvDev &e, SegState &s, RunCounters *ctr)
 {
     o.crr = o.crz = o.czz = (R)0;
@@ -82,10 +84,15 @@ template<typename R> __device__ __forceinline__ void eval_ssp(
     }
     update_seg(x.y, t.y >= (R)0, e.z, e.nssp, s.z);
     int iz = s.z;
-    double z0 = e.z[iz], z1 = e.z[iz + 1];
+    double z0 = e.z[iz];
     double dz = x.y - z0;
-    R w = (R)(dz / (z1 - z0));
-    o.rho = ((R)1 - w) * (R)e.rho[iz] + w * (R)e.rho[iz + 1];
+    R w = (R)0;
+    if(NEED_RHO || e.ssp_type == SSP_N2LINEAR) {
+        w = (R)(dz / (e.z[iz + 1] - z0));
+        o.rho = ((R)1 - w) * (R)e.rho[iz] + w * (R)e.rho[iz + 1];
+    } else {
+        o.rho = (R)0;
+    }
     switch(e.ssp_type) {
     case SSP_CLINEAR: {
         o.c = (R)e.c[2 * iz] + (R)dz * (R)e.cz[2 * iz];
@@ -331,8 +338,11 @@ template<typename R> __device__ __forceinline__ void step2d(
     double hw0 = h * w0, hw1 = h * w1;
     ray2.t = sub2(sub2(ray0.t, div2(scl2((R)hw0, o0.gradc), csq0)), div2(scl2((R)hw1, o1.gradc), csq1));
     // travel time in FP64: tau += hw0 / c0 + hw1 / c1 (complex sound speed)
-    Cx<double> d0 = rdivc(hw0, cx<double>((double)o0.c, (double)o0.ci));
-    Cx<double> d1 = rdivc(hw1, cx<double>((double)o1.c, (double)o1.ci));
+    // (a real divisor is divided directly; cdiv gives the same value for it)
+    Cx<double> d0 = o0.ci == (R)0 ? cx<double>(hw0 / (double)o0.c, 0.0)
+                                  : rdivc(hw0, cx<double>((double)o0.c, (double)o0.ci));
+    Cx<double> d1 = o1.ci == (R)0 ? cx<double>(hw1 / (double)o1.c, 0.0)
+                                  : rdivc(hw1, cx<double>((double)o1.c, (double)o1.ci));
     ray2.taur = ray0.taur + d0.r + d1.r;
     ray2.taui = ray0.taui + d0.i + d1.i;
     ray2.p = add2(add2(ray0.p, scl2((R)hw0, pq0p)), scl2((R)hw1, pq1p));
@@ -365,7 +375,7 @@ template<typename R> __device__ __forceinline__ void reflect2d(
     np.x = old.x;
     np.t = sub2(old.t, scl2((R)2 * Th, nB));
     SSPOut<R> o;
-    eval_ssp(old.x, old.t, o, e, iSeg, ctr);
+    eval_ssp<R, true>(old.x, old.t, o, e, iSeg, ctr);
     R c = o.c;
     np.c = c;
     np.taur = old.taur;

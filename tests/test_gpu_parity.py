@@ -38,7 +38,22 @@ def run_product(spec, root, precision, freqs=None):
         return out, t.stats()
 
 
+def _irregular(beam):
+    s = W.munk_tl(nalpha=301, nrz=201, nrr=201, beam=beam)
+    s.run_type = "C%s RI " % beam
+    return s
+
+
+def _steep():
+    s = W.munk_tl(nalpha=301, nrz=51, nrr=201, beam="B")
+    s.alpha = (-75.0, 75.0)
+    return s
+
+
 CASES = {
+    "munk_irregular_hat": _irregular("G"),
+    "munk_irregular_gauss": _irregular("B"),
+    "munk_steep_gauss": _steep(),
     "munk_hat": W.munk_tl(nalpha=301, nrz=51, nrr=201),
     "munk_gauss": W.munk_tl(nalpha=301, nrz=51, nrr=201, beam="B"),
     "rd_pchip_gauss": W.rd_gauss(nalpha=401, nrz=61, nrr=201, nbty=60),
