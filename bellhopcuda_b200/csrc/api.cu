@@ -104,6 +104,7 @@ struct bhcb_ctx {
     std::vector<Field> fields;
     std::vector<double> freqs_h;
     int64_t total_field = 0;
+    int64_t total_acc = 0;       // accumulator elements (padded rows)
     long long njobs = 0;
     unsigned long long seg_cap = 0;
     bool any_gauss = false, any_coherent = false, mixed_types = false;
@@ -174,6 +175,7 @@ void do_prepare(bhcb_ctx *c)
     c->fields.clear();
     c->freqs_h.clear();
     c->total_field = 0;
+    c->total_acc = 0;
     c->njobs = 0;
     bool fp64 = c->precision == BHCB_PREC_FP64;
     // --- preprocess every (env, frequency) and form trace groups
@@ -227,7 +229,10 @@ void do_prepare(bhcb_ctx *c)
         o.z = A.put(T.z); o.rho = A.put(T.rho); o.c = A.put(T.c); o.cz = A.put(T.cz);
         o.n2 = A.put(T.n2); o.n2z = A.put(T.n2z); o.coef = A.put(T.coef);
         o.btop = A.put(T.btop); o.bbot = A.put(T.bbot);
-        o.rr = A.put(T.rr); o.rz = A.put(T.rz); o.sz = A.put(T.sz); o.alpha = A.put(T.alpha);
+        // depths padded to an even count: the mixed influence kernel reads them in pairs
+        std::vector<float> rz_even = T.rz;
+        if(rz_even.size() & 1) rz_even.push_back(rz_even.back());
+        o.rr = A.put(T.rr); o.rz = A.put(rz_even); o.sz = A.put(T.sz); o.alpha = A.put(T.alpha);
         o.sbp = A.put(T.sbp);
         offs.push_back(o);
         EnvDev d{};
@@ -294,6 +299,11 @@ void do_prepare(bhcb_ctx *c)
         G.freq_base = (int)c->freqs_h.size();
         G.field_stride_f = (int)(T.sz.size() * T.nrz_per_range * T.rr.size());
         G.field_base = c->total_field;
+        G.acc_nz = T.run_type[4] == 'I' ? T.nrz_per_range : (T.nrz_per_range + 1) & ~1;
+        G.acc_stride_f = (int64_t)T.sz.size() * T.rr.size() * G.acc_nz;
+        c->total_acc = (c->total_acc + 1) & ~int64_t(1);
+        G.acc_base = c->total_acc;
+        c->total_acc += (int64_t)G.nfreq * G.acc_stride_f;
         for(size_t k = 0; k < gp.ifreqs.size(); ++k) {
             int fi = gp.ifreqs[k];
             c->freqs_h.push_back(S.freqs[fi]);
@@ -314,12 +324,13 @@ void do_prepare(bhcb_ctx *c)
     CK(cudaMemcpyAsync(c->freqs_d.p, c->freqs_h.data(), c->freqs_h.size() * sizeof(double),
                        cudaMemcpyHostToDevice, c->stream));
     size_t fbytes = (size_t)c->total_field * sizeof(float2);
-    c->acc.ensure(fbytes);
+    size_t abytes = (size_t)c->total_acc * sizeof(float2);
+    c->acc.ensure(abytes);
     c->out.ensure(fbytes);
     c->counters.ensure(sizeof(RunCounters) + 64);
     // segment buffer: grows on overflow
     size_t rec = seg_record_bytes(fp64);
-    size_t budget = c->max_memory > 3 * fbytes ? c->max_memory - 3 * fbytes : 0;
+    size_t budget = c->max_memory > 2 * fbytes + abytes ? c->max_memory - 2 * fbytes - abytes : 0;
     unsigned long long want = std::max<unsigned long long>(c->seg_cap, (unsigned long long)c->njobs * 1024ull);
     unsigned long long maxcap = budget / rec;
     if(maxcap < 1024) throw MemError("max_memory too small for the segment buffer");
@@ -337,7 +348,7 @@ void do_launch(bhcb_ctx *c)
     unsigned long long init_overflow = 0xffffffffull;
     CK(cudaMemcpyAsync(&ctr->overflow_job, &init_overflow, 4, cudaMemcpyHostToDevice, c->stream));
     unsigned long long *jobc = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
-    CK(cudaMemsetAsync(c->acc.p, 0, (size_t)c->total_field * sizeof(float2), c->stream));
+    CK(cudaMemsetAsync(c->acc.p, 0, (size_t)c->total_acc * sizeof(float2), c->stream));
     CK(cudaEventRecord(c->ev[0], c->stream));
     int tblock = 32;
     long long tgrid = std::min<long long>((c->njobs + tblock - 1) / tblock, (long long)c->sm_count * 16);
@@ -396,7 +407,8 @@ int run_checked(bhcb_ctx *c)
             // grow the segment buffer and run again
             size_t rec = seg_record_bytes(c->precision == BHCB_PREC_FP64);
             size_t fbytes = (size_t)c->total_field * sizeof(float2);
-            size_t budget = c->max_memory > 3 * fbytes ? c->max_memory - 3 * fbytes : 0;
+            size_t abytes = (size_t)c->total_acc * sizeof(float2);
+            size_t budget = c->max_memory > 2 * fbytes + abytes ? c->max_memory - 2 * fbytes - abytes : 0;
             unsigned long long maxcap = budget / rec;
             if(c->seg_cap >= maxcap)
                 throw MemError("segment buffer exceeds max_memory; raise bhcb_init.max_memory");

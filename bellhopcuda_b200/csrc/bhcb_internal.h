@@ -79,11 +79,20 @@ struct GroupDev {
     int32_t freq_base;       // index of first frequency slot in the launch's freq list
     int32_t field_stride_f;  // complex elements per frequency field of this group
     int64_t field_base;      // offset (complex elements) of this group's first field
+    // influence accumulator layout [field][isz][ir][iz], depth rows acc_nz long
+    // (rectilinear grids: nrz rounded up to even, so depth pairs are 16-byte
+    // aligned); acc_base is even
+    int64_t acc_base;
+    int64_t acc_stride_f;    // accumulator elements per frequency field
+    int32_t acc_nz;
+    int32_t pad;
 };
 
 // One influence segment (point0 -> point1 of Step_InfluenceGeoCart,
 // src/influence.hpp:1201-1406), with the receiver-column walk already done.
-template<typename R> struct SegRec {
+// 16-byte aligned (128 B mixed, 192 B FP64) so that a record is written with
+// full 16-byte stores.
+template<typename R> struct alignas(16) SegRec {
     double x0r, x0z;      // point0.x
     double tau0r;         // point0.tau.real()
     R dtaur, tau0i, dtaui;

@@ -62,6 +62,39 @@ template<typename T> __device__ __forceinline__ Cx<T> csqrt_(Cx<T> z)
     return {fabs(z.i) / (t + t), copysign(t, z.i)};
 }
 
+// Hardware approximations (PTX .approx.ftz forms) for the mixed-precision
+// contribution math; arguments of sin/cos are range-reduced by the caller.
+__device__ __forceinline__ float ex2_ftz(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sin_ftz(float x)
+{
+    float y;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float cos_ftz(float x)
+{
+    float y;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ double spacing_d(double v)
 {
     return fabs(nextafter(v, 0.0) - v);

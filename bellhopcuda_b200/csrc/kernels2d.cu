@@ -45,7 +45,11 @@ template<typename R> __device__ __forceinline__ void emit_seg(
         cur.next = b;
         cur.end = b + SEG_BLOCK;
     }
-    segs[cur.next++] = rec;
+    static_assert(sizeof(SegRec<R>) % 16 == 0, "segment records are written in 16-byte words");
+    const uint4 *src = reinterpret_cast<const uint4 *>(&rec);
+    uint4 *dst = reinterpret_cast<uint4 *>(segs + cur.next++);
+#pragma unroll
+    for(int k = 0; k < (int)(sizeof(SegRec<R>) / 16); ++k) dst[k] = src[k];
 }
 
 // mark the unused tail of the ray's last block as empty
@@ -204,18 +208,25 @@ template<typename R> struct SegFreq {
     int izlo, niz;
 };
 
-// One beam-receiver contribution of segment S at (column ir, depth index
-// zidx); returns false when the receiver is outside the beam window.
-// InfluenceGeoCore + ApplyContribution (src/influence.hpp:423-473,897-1024).
-// The FP64 kernel keeps the reference's operation order; the mixed kernel
-// uses the per-column constants A = dr tx / rlen, Bz = tz / rlen, Cn = dr tz.
+// Beam-receiver contributions of one segment for one frequency
+// (InfluenceGeoCore + ApplyContribution, src/influence.hpp:423-473,897-1024):
+// constructed once per (segment, frequency), column() once per receiver
+// column, eval() per receiver depth; eval returns false outside the beam window.
+// The FP64 policy keeps the reference's operation order. The mixed policy keeps
+// the segment constants in registers, uses the per-column constants
+// A = dr tx / rlen, Cn = dr tz, folds the Gaussian weight and the attenuation
+// into one base-2 exponential, and evaluates the phase with the hardware
+// sin/cos after an explicit 2 pi reduction.
 template<typename R, bool GAUSS, bool COHERENT> struct Contribution;
 
 template<bool GAUSS, bool COHERENT> struct Contribution<double, GAUSS, COHERENT> {
+    const SegRec<double> &S;
+    const SegFreq<double> &F;
     double dr;
-    __device__ __forceinline__ void column(const SegRec<double> &S, double rr) { dr = rr - S.x0r; }
-    __device__ __forceinline__ bool eval(const SegRec<double> &S, const SegFreq<double> &F, float zr_f,
-                                         float2 &v) const
+    __device__ __forceinline__ Contribution(const SegRec<double> &S_, const SegFreq<double> &F_)
+        : S(S_), F(F_) {}
+    __device__ __forceinline__ void column(double rr) { dr = rr - S.x0r; }
+    __device__ __forceinline__ bool eval(float zr_f, float2 &v) const
     {
         double dz = (double)zr_f - S.x0z;
         double s = (dr * S.tx + dz * S.tz) / S.rlen;
@@ -246,50 +257,127 @@ template<bool GAUSS, bool COHERENT> struct Contribution<double, GAUSS, COHERENT>
 };
 
 template<bool GAUSS, bool COHERENT> struct Contribution<float, GAUSS, COHERENT> {
-    float A, Bz, Cn, x0z;
-    __device__ __forceinline__ void column(const SegRec<float> &S, double rr)
+    static constexpr float LOG2E = 1.44269504088896340736f;
+    double x0r;
+    float tx, tz, inv_rlen, Bz, x0z, dq, q0, rcpq, sfl, sgq, cA, cB, omdt, lg0, lg1, cn;
+    float A, Cn;
+    __device__ __forceinline__ Contribution(const SegRec<float> &S, const SegFreq<float> &F)
     {
-        float dr = (float)(rr - S.x0r);
-        float inv = __fdividef(1.0f, S.rlen);
-        A = dr * S.tx * inv;
-        Bz = S.tz * inv;
-        Cn = dr * S.tz;
+        x0r = S.x0r;
+        tx = S.tx;
+        tz = S.tz;
+        inv_rlen = rcp_ftz(S.rlen);
+        Bz = tz * inv_rlen;
         x0z = (float)S.x0z;
+        dq = S.dq;
+        q0 = S.q0;
+        rcpq = S.rcp_q0;
+        sfl = F.sigfloor;
+        // caustic branch of the phase: (q <= 0 && q0 > 0) || (q >= 0 && q0 < 0)
+        // is sign(q0) * q <= 0 with sign(q0) != 0
+        sgq = q0 > 0.f ? 1.f : (q0 < 0.f ? -1.f : 0.f);
+        cA = F.ph0 - S.phase_a;
+        cB = sgq != 0.f ? F.ph0 - S.phase_b : cA;
+        omdt = F.omdt;
+        lg0 = F.att0 * LOG2E;
+        lg1 = F.att1 * LOG2E;
+        cn = S.cnst_num;
     }
-    __device__ __forceinline__ bool eval(const SegRec<float> &S, const SegFreq<float> &F, float zr,
-                                         float2 &v) const
+    __device__ __forceinline__ void column(double rr)
+    {
+        float dr = (float)(rr - x0r);
+        A = dr * tx * inv_rlen;
+        Cn = dr * tz;
+    }
+    __device__ __forceinline__ bool eval(float zr, float2 &v) const
     {
         float dz = zr - x0z;
         float s = fmaf(dz, Bz, A);
-        float n1 = fabsf(fmaf(dz, S.tx, -Cn));
-        float qF = fmaf(s, S.dq, S.q0);
-        float sigma = fabsf(qF * S.rcp_q0), sig0 = sigma;
-        if(GAUSS) sigma = fmaxf(sigma, F.sigfloor);
+        float n1 = fabsf(fmaf(dz, tx, -Cn));
+        float qF = fmaf(s, dq, q0);
+        float sig0 = fabsf(qF * rcpq);
+        float sigma = GAUSS ? fmaxf(sig0, sfl) : sig0;
         if(n1 >= (GAUSS ? 4.f : 1.f) * sigma) return false;
-        float rs = __fdividef(1.0f, sigma);
-        float cnst = S.cnst_num * rsqrtf(fabsf(qF));
-        float wgt;
+        float rs = rcp_ftz(sigma);
+        float la = fmaf(s, lg1, lg0);           // log2 of the attenuation factor
+        float lgs = 0.f, w;
         if(GAUSS) {
             float a = n1 * rs;
-            wgt = __expf(-0.5f * a * a) * (sig0 * rs);
+            lgs = (a * a) * (-0.5f * LOG2E);    // log2 of the Gaussian weight
+            w = sig0 * rs;
         } else {
-            wgt = (sigma - n1) * rs;
+            w = (sigma - n1) * rs;
         }
-        bool caustic = (qF <= 0.f && S.q0 > 0.f) || (qF >= 0.f && S.q0 < 0.f);
-        float ph = caustic ? S.phase_b : S.phase_a;
-        float att = fmaf(s, F.att1, F.att0);
+        float cnst = cn * rsqrt_ftz(fabsf(qF));
         if(COHERENT) {
-            float amp = cnst * wgt * (att != 0.f ? __expf(att) : 1.f);
-            float ang = reduce_2pi(fmaf(s, F.omdt, F.ph0) - ph), sn, cs;
-            __sincosf(ang, &sn, &cs);
-            v = make_float2(amp * cs, -amp * sn);
+            float amp = cnst * w * ex2_ftz(la + lgs);
+            float ang = fmaf(s, omdt, sgq * qF <= 0.f ? cB : cA);
+            // nearest integer of ang / 2 pi by the 1.5 * 2^23 shifter (|ang| << 2^22)
+            float k = fmaf(ang, 0.159154943f, 12582912.f) - 12582912.f;
+            ang = fmaf(-k, 6.28318548f, ang);
+            ang = fmaf(-k, -1.7484555e-7f, ang);
+            v = make_float2(amp * cos_ftz(ang), -amp * sin_ftz(ang));
         } else {
-            float vv = cnst * (att != 0.f ? __expf(att) : 1.f);
-            vv = vv * vv * wgt;
+            float vv = cnst * cnst * w * ex2_ftz(la + la + lgs);
             if(GAUSS) vv *= 2.50662827463100050242f;   // sqrt(2 pi)
             v = make_float2(vv, 0.f);
         }
         return true;
+    }
+    // The same for the two receivers of one column at depths zr.x, zr.y (an
+    // even/odd pair of depth indices), with Blackwell's paired FP32 operations;
+    // ok0 / ok1 say which of the two lie in the segment's depth window. v holds
+    // both contributions (zero outside the beam); returns how many are inside.
+    __device__ __forceinline__ int eval_pair(float2 zr, bool ok0, bool ok1, float4 &v) const
+    {
+        const float2 dz = __fadd2_rn(zr, make_float2(-x0z, -x0z));
+        const float2 s = __ffma2_rn(dz, make_float2(Bz, Bz), make_float2(A, A));
+        const float2 nr = __ffma2_rn(dz, make_float2(tx, tx), make_float2(-Cn, -Cn));
+        const float2 qF = __ffma2_rn(s, make_float2(dq, dq), make_float2(q0, q0));
+        const float2 sq = __fmul2_rn(qF, make_float2(rcpq, rcpq));
+        const float n0 = fabsf(nr.x), n1 = fabsf(nr.y);
+        const float g0 = fabsf(sq.x), g1 = fabsf(sq.y);
+        const float sg0 = GAUSS ? fmaxf(g0, sfl) : g0, sg1 = GAUSS ? fmaxf(g1, sfl) : g1;
+        const float W = GAUSS ? 4.f : 1.f;
+        const bool in0 = ok0 && !(n0 >= W * sg0), in1 = ok1 && !(n1 >= W * sg1);
+        if(!(in0 || in1)) return 0;
+        const float2 rs = make_float2(rcp_ftz(sg0), rcp_ftz(sg1));
+        float2 lg = __ffma2_rn(s, make_float2(lg1, lg1), make_float2(lg0, lg0));
+        if(!COHERENT) lg = __fadd2_rn(lg, lg);
+        float2 w;
+        if(GAUSS) {
+            const float2 a = __fmul2_rn(make_float2(n0, n1), rs);
+            lg = __ffma2_rn(__fmul2_rn(a, a), make_float2(-0.5f * LOG2E, -0.5f * LOG2E), lg);
+            w = __fmul2_rn(make_float2(g0, g1), rs);
+        } else {
+            w = __fmul2_rn(make_float2(sg0 - n0, sg1 - n1), rs);
+        }
+        const float2 r = make_float2(rsqrt_ftz(fabsf(qF.x)), rsqrt_ftz(fabsf(qF.y)));
+        const float2 e = make_float2(ex2_ftz(lg.x), ex2_ftz(lg.y));
+        if(COHERENT) {
+            float2 amp = __fmul2_rn(__fmul2_rn(r, w), __fmul2_rn(e, make_float2(cn, cn)));
+            amp.x = in0 ? amp.x : 0.f;
+            amp.y = in1 ? amp.y : 0.f;
+            const float2 sgn = __fmul2_rn(qF, make_float2(sgq, sgq));
+            float2 ang = __ffma2_rn(s, make_float2(omdt, omdt),
+                                    make_float2(sgn.x <= 0.f ? cB : cA, sgn.y <= 0.f ? cB : cA));
+            // -round(ang / 2 pi) by the 1.5 * 2^23 shifter, then ang mod 2 pi
+            const float SH = 12582912.f, I2P = 0.159154943f;
+            const float2 nk = __fadd2_rn(__ffma2_rn(ang, make_float2(-I2P, -I2P), make_float2(-SH, -SH)),
+                                         make_float2(SH, SH));
+            ang = __ffma2_rn(nk, make_float2(6.28318548f, 6.28318548f), ang);
+            ang = __ffma2_rn(nk, make_float2(-1.7484555e-7f, -1.7484555e-7f), ang);
+            const float2 cs = make_float2(cos_ftz(ang.x), cos_ftz(ang.y));
+            const float2 sn = make_float2(sin_ftz(ang.x), sin_ftz(ang.y));
+            const float2 re = __fmul2_rn(amp, cs);
+            const float2 im = __fmul2_rn(make_float2(-amp.x, -amp.y), sn);
+            v = make_float4(re.x, im.x, re.y, im.y);
+        } else {
+            const float k = GAUSS ? cn * cn * 2.50662827463100050242f : cn * cn;   // sqrt(2 pi)
+            float2 vv = __fmul2_rn(__fmul2_rn(__fmul2_rn(r, r), w), __fmul2_rn(e, make_float2(k, k)));
+            v = make_float4(in0 ? vv.x : 0.f, 0.f, in1 ? vv.y : 0.f, 0.f);
+        }
+        return (int)in0 + (int)in1;
     }
 };
 
@@ -310,7 +398,7 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
     __shared__ long long s_base[WARPS_PER_CTA][32];       // field offset of (isz, ir=0, iz=0), f=0
     __shared__ const double *s_rr[WARPS_PER_CTA][32];
     __shared__ const float *s_rz[WARPS_PER_CTA][32];
-    __shared__ int s_stride[WARPS_PER_CTA][32];           // per-frequency field stride
+    __shared__ long long s_stride[WARPS_PER_CTA][32];     // per-frequency accumulator stride
     __shared__ int s_nrzp[WARPS_PER_CTA][32];             // 0 -> irregular grid
     __shared__ int s_nf[WARPS_PER_CTA][32];               // frequencies of the segment's group
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -322,10 +410,13 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
         if(lane == 0) ch = atomicAdd(&ctr->chunk_counter, 1ull);
         ch = __shfl_sync(0xffffffffu, ch, 0);
         if(ch >= nchunks) break;
+        // segments are stored in trace order, so the last chunks hold the
+        // far-range segments with the widest beams: take the heaviest first
+        ch = nchunks - 1 - ch;
         {
-            const int words = sizeof(SegRec<R>) / 4;
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(segs + ch * 32);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&s_rec[w][0]);
+            const int words = sizeof(SegRec<R>) / 16;
+            const uint4 *src = reinterpret_cast<const uint4 *>(segs + ch * 32);
+            uint4 *dst = reinterpret_cast<uint4 *>(&s_rec[w][0]);
             int nvalid = (int)min(32ull, nseg - ch * 32);
             for(int k = lane; k < nvalid * words; k += 32) dst[k] = __ldcs(src + k);
             __syncwarp();
@@ -344,11 +435,11 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
             int local = (int)((long long)my.job - G.job_base);
             int nal = e->isingle > 0 ? 1 : e->nalpha;
             int isz = local / nal;
-            s_base[w][lane] = G.field_base + (long long)isz * e->nrr * e->nrz_per_range;
+            s_base[w][lane] = G.acc_base + (long long)isz * e->nrr * G.acc_nz;
             s_rr[w][lane] = e->rr;
             s_rz[w][lane] = e->rz;
-            s_stride[w][lane] = G.field_stride_f;
-            s_nrzp[w][lane] = e->irregular ? 0 : e->nrz_per_range;
+            s_stride[w][lane] = G.acc_stride_f;
+            s_nrzp[w][lane] = e->irregular ? 0 : G.acc_nz;
         }
         s_nf[w][lane] = nfreq;
         int maxf = nfreq;
@@ -387,7 +478,12 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                 sf.att0 = (R)(omega * (double)my.tau0i);
                 sf.att1 = (R)(omega * (double)my.dtaui);
                 s_sf[w][lane] = sf;
-                cnt = sf.niz > 0 ? (my.ir_hi - my.ir_lo + 1) * sf.niz : 0;
+                // work units: depth pairs on a rectilinear grid in the mixed
+                // kernel, single depths otherwise
+                int units = sf.niz;
+                if(sizeof(R) == 4 && !e->irregular && sf.niz > 0)
+                    units = ((sf.izlo + sf.niz + 1) >> 1) - (sf.izlo >> 1);
+                cnt = sf.niz > 0 ? (my.ir_hi - my.ir_lo + 1) * units : 0;
             }
             int tot = cnt;
             for(int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
@@ -406,6 +502,48 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                 const float *rz = s_rz[w][k];
                 const int nrzp = s_nrzp[w][k];
                 if(f >= s_nf[w][k]) continue;   // its group has fewer frequencies
+                if constexpr(sizeof(R) == 4) {
+                    if(nrzp) {
+                        if(F.niz <= 0) continue;
+                        // rectilinear grid, mixed kernel: the group walks the
+                        // flattened (column, depth pair) units of the segment,
+                        // pairs fastest; a unit is the depth indices (2P, 2P+1)
+                        // (rows are acc_nz long, acc_nz even, so the pair's
+                        // accumulator entries are one aligned 16-byte word) and
+                        // is reduced with one vector atomic.
+                        const int izlo = F.izlo, izhi = F.izlo + F.niz;
+                        const int p0 = izlo >> 1, npair = ((izhi + 1) >> 1) - p0;
+                        const int ncols = S.ir_hi - S.ir_lo + 1;
+                        const float2 *zp2 = reinterpret_cast<const float2 *>(rz) + p0;
+                        float4 *acc4 = reinterpret_cast<float4 *>(acc + base) + p0;
+                        const int q = g / npair, rq = g - q * npair;
+                        int col = lig / npair, jp = lig - col * npair, ccol = -1;
+                        Contribution<float, GAUSS, COHERENT> C(S, F);
+                        float4 *colp = nullptr;
+                        while(col < ncols) {
+                            if(col != ccol) {
+                                ccol = col;
+                                const int ir = S.ir_lo + col;
+                                C.column(rr[ir]);
+                                colp = acc4 + (long long)ir * (nrzp >> 1);
+                            }
+                            const int d0 = 2 * (p0 + jp);
+                            float4 v;
+                            const int n = C.eval_pair(zp2[jp], d0 >= izlo, d0 + 1 < izhi, v);
+                            if(n) {
+                                atomicAdd(colp + jp, v);
+                                evals += n;
+                            }
+                            jp += rq;
+                            col += q;
+                            if(jp >= npair) {
+                                jp -= npair;
+                                ++col;
+                            }
+                        }
+                        continue;
+                    }
+                }
                 if(nrzp) {
                     // rectilinear grid: the group walks the flattened (column, depth)
                     // pairs of the segment, depth fastest, so the idle tail is paid
@@ -414,17 +552,17 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                     const int niz = F.niz, total = (S.ir_hi - S.ir_lo + 1) * niz;
                     const float *zp = rz + F.izlo;
                     int col = lig / niz, j = lig - col * niz, ccol = -1;
-                    Contribution<R, GAUSS, COHERENT> C;
+                    Contribution<R, GAUSS, COHERENT> C(S, F);
                     float2 *colp = nullptr;
                     for(int e = lig; e < total; e += g) {
                         if(col != ccol) {
                             ccol = col;
                             int ir = S.ir_lo + col;
-                            C.column(S, rr[ir]);
+                            C.column(rr[ir]);
                             colp = acc + base + (long long)ir * nrzp + F.izlo;
                         }
                         float2 v;
-                        if(C.eval(S, F, zp[j], v)) {
+                        if(C.eval(zp[j], v)) {
                             atomicAdd(colp + j, v);
                             ++evals;
                         }
@@ -433,13 +571,13 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                     }
                 } else {
                     // irregular grid: one receiver per column, at depth rz[ir]
+                    Contribution<R, GAUSS, COHERENT> C(S, F);
                     for(int ir = S.ir_lo + lig; ir <= S.ir_hi; ir += g) {
                         double zr = (double)rz[ir];
                         if(zr < F.zmin || zr > F.zmax) continue;
-                        Contribution<R, GAUSS, COHERENT> C;
-                        C.column(S, rr[ir]);
+                        C.column(rr[ir]);
                         float2 v;
-                        if(C.eval(S, F, rz[ir], v)) {
+                        if(C.eval(rz[ir], v)) {
                             atomicAdd(acc + base + ir, v);
                             ++evals;
                         }
@@ -454,7 +592,7 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
 }
 
 // ScalePressure (src/influence.hpp:1556-1627, 2-D) fused with the transpose
-// acc[f][isz][ir][iz] -> out[f][isz][iz][ir].
+// acc[f][isz][ir][iz] (rows acc_nz long) -> out[f][isz][iz][ir].
 __global__ void scale_kernel(const float2 *__restrict__ acc, float2 *__restrict__ out,
                              const GroupDev *__restrict__ groups, int ngroups)
 {
@@ -470,10 +608,11 @@ __global__ void scale_kernel(const float2 *__restrict__ acc, float2 *__restrict_
         int rem = t - plane * tiles_r * tiles_z;
         int tr = rem / tiles_z, tz = rem - tr * tiles_z;
         size_t base = (size_t)G.field_base + (size_t)plane * nr * nz;
+        size_t abase = (size_t)G.acc_base + (size_t)plane * nr * G.acc_nz;
         // load: rows ir, contiguous iz
         for(int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
             int ir = tr * 32 + yy, iz = tz * 32 + threadIdx.x;
-            if(ir < nr && iz < nz) tile[yy][threadIdx.x] = acc[base + (size_t)ir * nz + iz];
+            if(ir < nr && iz < nz) tile[yy][threadIdx.x] = acc[abase + (size_t)ir * G.acc_nz + iz];
         }
         __syncthreads();
         for(int yy = threadIdx.y; yy < 32; yy += blockDim.y) {

@@ -332,6 +332,9 @@ extern "C" int bhcb_run_noalloc(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq,
     h.group.freq_base = 0;
     h.group.field_base = 0;
     h.group.field_stride_f = (int)nelem;
+    h.group.acc_base = 0;                  // this path's accumulator rows are not padded
+    h.group.acc_stride_f = (int64_t)nelem;
+    h.group.acc_nz = J.nrzp;
     unsigned char *sc = (unsigned char *)scratch;
     if(cudaMemcpyAsync(sc, &h, sizeof h, cudaMemcpyHostToDevice, J.stream) != cudaSuccess
        || cudaMemsetAsync(sc + kHeaderBytes, 0, nelem * sizeof(float2), J.stream) != cudaSuccess)
