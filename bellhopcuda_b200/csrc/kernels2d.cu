@@ -256,131 +256,6 @@ template<bool GAUSS, bool COHERENT> struct Contribution<double, GAUSS, COHERENT>
     }
 };
 
-template<bool GAUSS, bool COHERENT> struct Contribution<float, GAUSS, COHERENT> {
-    static constexpr float LOG2E = 1.44269504088896340736f;
-    double x0r;
-    float tx, tz, inv_rlen, Bz, x0z, dq, q0, rcpq, sfl, sgq, cA, cB, omdt, lg0, lg1, cn;
-    float A, Cn;
-    __device__ __forceinline__ Contribution(const SegRec<float> &S, const SegFreq<float> &F)
-    {
-        x0r = S.x0r;
-        tx = S.tx;
-        tz = S.tz;
-        inv_rlen = rcp_ftz(S.rlen);
-        Bz = tz * inv_rlen;
-        x0z = (float)S.x0z;
-        dq = S.dq;
-        q0 = S.q0;
-        rcpq = S.rcp_q0;
-        sfl = F.sigfloor;
-        // caustic branch of the phase: (q <= 0 && q0 > 0) || (q >= 0 && q0 < 0)
-        // is sign(q0) * q <= 0 with sign(q0) != 0
-        sgq = q0 > 0.f ? 1.f : (q0 < 0.f ? -1.f : 0.f);
-        cA = F.ph0 - S.phase_a;
-        cB = sgq != 0.f ? F.ph0 - S.phase_b : cA;
-        omdt = F.omdt;
-        lg0 = F.att0 * LOG2E;
-        lg1 = F.att1 * LOG2E;
-        cn = S.cnst_num;
-    }
-    __device__ __forceinline__ void column(double rr)
-    {
-        float dr = (float)(rr - x0r);
-        A = dr * tx * inv_rlen;
-        Cn = dr * tz;
-    }
-    __device__ __forceinline__ bool eval(float zr, float2 &v) const
-    {
-        float dz = zr - x0z;
-        float s = fmaf(dz, Bz, A);
-        float n1 = fabsf(fmaf(dz, tx, -Cn));
-        float qF = fmaf(s, dq, q0);
-        float sig0 = fabsf(qF * rcpq);
-        float sigma = GAUSS ? fmaxf(sig0, sfl) : sig0;
-        if(n1 >= (GAUSS ? 4.f : 1.f) * sigma) return false;
-        float rs = rcp_ftz(sigma);
-        float la = fmaf(s, lg1, lg0);           // log2 of the attenuation factor
-        float lgs = 0.f, w;
-        if(GAUSS) {
-            float a = n1 * rs;
-            lgs = (a * a) * (-0.5f * LOG2E);    // log2 of the Gaussian weight
-            w = sig0 * rs;
-        } else {
-            w = (sigma - n1) * rs;
-        }
-        float cnst = cn * rsqrt_ftz(fabsf(qF));
-        if(COHERENT) {
-            float amp = cnst * w * ex2_ftz(la + lgs);
-            float ang = fmaf(s, omdt, sgq * qF <= 0.f ? cB : cA);
-            // nearest integer of ang / 2 pi by the 1.5 * 2^23 shifter (|ang| << 2^22)
-            float k = fmaf(ang, 0.159154943f, 12582912.f) - 12582912.f;
-            ang = fmaf(-k, 6.28318548f, ang);
-            ang = fmaf(-k, -1.7484555e-7f, ang);
-            v = make_float2(amp * cos_ftz(ang), -amp * sin_ftz(ang));
-        } else {
-            float vv = cnst * cnst * w * ex2_ftz(la + la + lgs);
-            if(GAUSS) vv *= 2.50662827463100050242f;   // sqrt(2 pi)
-            v = make_float2(vv, 0.f);
-        }
-        return true;
-    }
-    // The same for the two receivers of one column at depths zr.x, zr.y (an
-    // even/odd pair of depth indices), with Blackwell's paired FP32 operations;
-    // ok0 / ok1 say which of the two lie in the segment's depth window. v holds
-    // both contributions (zero outside the beam); returns how many are inside.
-    __device__ __forceinline__ int eval_pair(float2 zr, bool ok0, bool ok1, float4 &v) const
-    {
-        const float2 dz = __fadd2_rn(zr, make_float2(-x0z, -x0z));
-        const float2 s = __ffma2_rn(dz, make_float2(Bz, Bz), make_float2(A, A));
-        const float2 nr = __ffma2_rn(dz, make_float2(tx, tx), make_float2(-Cn, -Cn));
-        const float2 qF = __ffma2_rn(s, make_float2(dq, dq), make_float2(q0, q0));
-        const float2 sq = __fmul2_rn(qF, make_float2(rcpq, rcpq));
-        const float n0 = fabsf(nr.x), n1 = fabsf(nr.y);
-        const float g0 = fabsf(sq.x), g1 = fabsf(sq.y);
-        const float sg0 = GAUSS ? fmaxf(g0, sfl) : g0, sg1 = GAUSS ? fmaxf(g1, sfl) : g1;
-        const float W = GAUSS ? 4.f : 1.f;
-        const bool in0 = ok0 && !(n0 >= W * sg0), in1 = ok1 && !(n1 >= W * sg1);
-        if(!(in0 || in1)) return 0;
-        const float2 rs = make_float2(rcp_ftz(sg0), rcp_ftz(sg1));
-        float2 lg = __ffma2_rn(s, make_float2(lg1, lg1), make_float2(lg0, lg0));
-        if(!COHERENT) lg = __fadd2_rn(lg, lg);
-        float2 w;
-        if(GAUSS) {
-            const float2 a = __fmul2_rn(make_float2(n0, n1), rs);
-            lg = __ffma2_rn(__fmul2_rn(a, a), make_float2(-0.5f * LOG2E, -0.5f * LOG2E), lg);
-            w = __fmul2_rn(make_float2(g0, g1), rs);
-        } else {
-            w = __fmul2_rn(make_float2(sg0 - n0, sg1 - n1), rs);
-        }
-        const float2 r = make_float2(rsqrt_ftz(fabsf(qF.x)), rsqrt_ftz(fabsf(qF.y)));
-        const float2 e = make_float2(ex2_ftz(lg.x), ex2_ftz(lg.y));
-        if(COHERENT) {
-            float2 amp = __fmul2_rn(__fmul2_rn(r, w), __fmul2_rn(e, make_float2(cn, cn)));
-            amp.x = in0 ? amp.x : 0.f;
-            amp.y = in1 ? amp.y : 0.f;
-            const float2 sgn = __fmul2_rn(qF, make_float2(sgq, sgq));
-            float2 ang = __ffma2_rn(s, make_float2(omdt, omdt),
-                                    make_float2(sgn.x <= 0.f ? cB : cA, sgn.y <= 0.f ? cB : cA));
-            // -round(ang / 2 pi) by the 1.5 * 2^23 shifter, then ang mod 2 pi
-            const float SH = 12582912.f, I2P = 0.159154943f;
-            const float2 nk = __fadd2_rn(__ffma2_rn(ang, make_float2(-I2P, -I2P), make_float2(-SH, -SH)),
-                                         make_float2(SH, SH));
-            ang = __ffma2_rn(nk, make_float2(6.28318548f, 6.28318548f), ang);
-            ang = __ffma2_rn(nk, make_float2(-1.7484555e-7f, -1.7484555e-7f), ang);
-            const float2 cs = make_float2(cos_ftz(ang.x), cos_ftz(ang.y));
-            const float2 sn = make_float2(sin_ftz(ang.x), sin_ftz(ang.y));
-            const float2 re = __fmul2_rn(amp, cs);
-            const float2 im = __fmul2_rn(make_float2(-amp.x, -amp.y), sn);
-            v = make_float4(re.x, im.x, re.y, im.y);
-        } else {
-            const float k = GAUSS ? cn * cn * 2.50662827463100050242f : cn * cn;   // sqrt(2 pi)
-            float2 vv = __fmul2_rn(__fmul2_rn(__fmul2_rn(r, r), w), __fmul2_rn(e, make_float2(k, k)));
-            v = make_float4(in0 ? vv.x : 0.f, 0.f, in1 ? vv.y : 0.f, 0.f);
-        }
-        return (int)in0 + (int)in1;
-    }
-};
-
 // Warp-cooperative influence: each warp stages 32 segment records, then for
 // every frequency splits itself into sub-groups of g lanes (g = 4..32, chosen
 // from the chunk's average work per segment); a group takes one segment at a
@@ -478,12 +353,7 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                 sf.att0 = (R)(omega * (double)my.tau0i);
                 sf.att1 = (R)(omega * (double)my.dtaui);
                 s_sf[w][lane] = sf;
-                // work units: depth pairs on a rectilinear grid in the mixed
-                // kernel, single depths otherwise
-                int units = sf.niz;
-                if(sizeof(R) == 4 && !e->irregular && sf.niz > 0)
-                    units = ((sf.izlo + sf.niz + 1) >> 1) - (sf.izlo >> 1);
-                cnt = sf.niz > 0 ? (my.ir_hi - my.ir_lo + 1) * units : 0;
+                cnt = sf.niz > 0 ? (my.ir_hi - my.ir_lo + 1) * sf.niz : 0;
             }
             int tot = cnt;
             for(int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
@@ -502,48 +372,6 @@ influence_kernel(const SegRec<R> *__restrict__ segs, unsigned long long cap,
                 const float *rz = s_rz[w][k];
                 const int nrzp = s_nrzp[w][k];
                 if(f >= s_nf[w][k]) continue;   // its group has fewer frequencies
-                if constexpr(sizeof(R) == 4) {
-                    if(nrzp) {
-                        if(F.niz <= 0) continue;
-                        // rectilinear grid, mixed kernel: the group walks the
-                        // flattened (column, depth pair) units of the segment,
-                        // pairs fastest; a unit is the depth indices (2P, 2P+1)
-                        // (rows are acc_nz long, acc_nz even, so the pair's
-                        // accumulator entries are one aligned 16-byte word) and
-                        // is reduced with one vector atomic.
-                        const int izlo = F.izlo, izhi = F.izlo + F.niz;
-                        const int p0 = izlo >> 1, npair = ((izhi + 1) >> 1) - p0;
-                        const int ncols = S.ir_hi - S.ir_lo + 1;
-                        const float2 *zp2 = reinterpret_cast<const float2 *>(rz) + p0;
-                        float4 *acc4 = reinterpret_cast<float4 *>(acc + base) + p0;
-                        const int q = g / npair, rq = g - q * npair;
-                        int col = lig / npair, jp = lig - col * npair, ccol = -1;
-                        Contribution<float, GAUSS, COHERENT> C(S, F);
-                        float4 *colp = nullptr;
-                        while(col < ncols) {
-                            if(col != ccol) {
-                                ccol = col;
-                                const int ir = S.ir_lo + col;
-                                C.column(rr[ir]);
-                                colp = acc4 + (long long)ir * (nrzp >> 1);
-                            }
-                            const int d0 = 2 * (p0 + jp);
-                            float4 v;
-                            const int n = C.eval_pair(zp2[jp], d0 >= izlo, d0 + 1 < izhi, v);
-                            if(n) {
-                                atomicAdd(colp + jp, v);
-                                evals += n;
-                            }
-                            jp += rq;
-                            col += q;
-                            if(jp >= npair) {
-                                jp -= npair;
-                                ++col;
-                            }
-                        }
-                        continue;
-                    }
-                }
                 if(nrzp) {
                     // rectilinear grid: the group walks the flattened (column, depth)
                     // pairs of the segment, depth fastest, so the idle tail is paid
@@ -644,23 +472,31 @@ template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroup
     return cudaGetLastError();
 }
 
+cudaError_t launch_influence_mixed(const void *segs, unsigned long long cap, const GroupDev *groups, int ngroups,
+                                   const double *freqs, float2 *acc, RunCounters *ctr, bool gauss,
+                                   bool coherent, int grid, cudaStream_t st);
+
 template<typename R> cudaError_t launch_influence(const void *segs, unsigned long long nseg,
                                                   const GroupDev *groups, int ngroups,
                                                   const double *freqs, float2 *acc,
                                                   RunCounters *ctr, bool gauss, bool coherent,
                                                   int grid, cudaStream_t st)
 {
-    const SegRec<R> *s = (const SegRec<R> *)segs;
-    int block = 32 * WARPS_PER_CTA;
-    if(gauss && coherent)
-        influence_kernel<R, true, true><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
-    else if(gauss)
-        influence_kernel<R, true, false><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
-    else if(coherent)
-        influence_kernel<R, false, true><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
-    else
-        influence_kernel<R, false, false><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
-    return cudaGetLastError();
+    if constexpr(sizeof(R) == 4) {
+        return launch_influence_mixed(segs, nseg, groups, ngroups, freqs, acc, ctr, gauss, coherent, grid, st);
+    } else {
+        const SegRec<R> *s = (const SegRec<R> *)segs;
+        int block = 32 * WARPS_PER_CTA;
+        if(gauss && coherent)
+            influence_kernel<R, true, true><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
+        else if(gauss)
+            influence_kernel<R, true, false><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
+        else if(coherent)
+            influence_kernel<R, false, true><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
+        else
+            influence_kernel<R, false, false><<<grid, block, 0, st>>>(s, nseg, groups, ngroups, freqs, acc, ctr);
+        return cudaGetLastError();
+    }
 }
 
 cudaError_t launch_scale(const float2 *acc, float2 *out, const GroupDev *groups, int ngroups,
