@@ -60,6 +60,13 @@ class EnvInfo(C.Structure):
                 ("beam_type", C.c_char * 8)]
 
 
+# bhcb_arrival / bhcb_eigen_hit (the reference's Arrival and EigenHit records)
+ARRIVAL_DTYPE = np.dtype([("NTopBnc", "<i4"), ("NBotBnc", "<i4"), ("SrcDeclAngle", "<f4"),
+                          ("SrcAzimAngle", "<f4"), ("RcvrDeclAngle", "<f4"), ("RcvrAzimAngle", "<f4"),
+                          ("a", "<f4"), ("Phase", "<f4"), ("delay_re", "<f4"), ("delay_im", "<f4")])
+EIGEN_HIT_DTYPE = np.dtype([(n, "<i4") for n in ("is", "itheta", "ir", "iz", "isx", "isy", "isz",
+                                                 "ialpha", "ibeta")])
+
 _lib = None
 
 # (name, restype, argtypes) for every entry point of include/bhcb.h
@@ -88,6 +95,12 @@ SIGNATURES = [
     ("bhcb_run_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
                                    C.c_char_p, C.c_size_t]),
     ("bhcb_check_env", C.c_int, [C.c_char_p, C.POINTER(EnvInfo), C.c_char_p, C.c_size_t]),
+    ("bhcb_set_arrival_options", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    ("bhcb_arrivals_shape", C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 4),
+    ("bhcb_copy_arrivals", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
+                                     C.c_size_t]),
+    ("bhcb_eigen_hits", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
+                                  C.POINTER(C.c_int64)]),
     ("bhcb_version", C.c_char_p, []),
 ]
 
@@ -231,6 +244,30 @@ class Tracer:
 
     def writeout(self, file_root: str, env: int = 0, ifreq: int = 0):
         self._check(self._lib.bhcb_writeout(self._h, env, ifreq, file_root.encode()))
+
+    def set_arrival_options(self, max_narr: int = 0, allow_merging: bool = True):
+        """ArrInfo::MaxNArr (0: sized from max_memory) and AllowMerging for arrivals runs."""
+        self._check(self._lib.bhcb_set_arrival_options(self._h, int(max_narr), int(bool(allow_merging))))
+
+    def arrivals(self, env: int = 0, ifreq: int = 0):
+        """(narr [NSz, NRz_per_range, NRr] int32, arr [..., max_narr] ARRIVAL_DTYPE) of an arrivals run."""
+        v = [C.c_int32() for _ in range(4)]
+        self._check(self._lib.bhcb_arrivals_shape(self._h, env, ifreq, *[C.byref(x) for x in v]))
+        nsz, nrzp, nrr, mx = (x.value for x in v)
+        narr = np.zeros((nsz, nrzp, nrr), dtype=np.int32)
+        arr = np.zeros((nsz, nrzp, nrr, mx), dtype=ARRIVAL_DTYPE)
+        self._check(self._lib.bhcb_copy_arrivals(self._h, env, ifreq, narr.ctypes.data, narr.nbytes,
+                                                 arr.ctypes.data, arr.nbytes))
+        return narr, arr
+
+    def eigen_hits(self, env: int = 0, ifreq: int = 0) -> np.ndarray:
+        """Eigenray hits (EIGEN_HIT_DTYPE) of an eigen run, in the reference's order."""
+        n = C.c_int64()
+        self._check(self._lib.bhcb_eigen_hits(self._h, env, ifreq, None, 0, C.byref(n)))
+        hits = np.zeros(n.value, dtype=EIGEN_HIT_DTYPE)
+        if n.value:
+            self._check(self._lib.bhcb_eigen_hits(self._h, env, ifreq, hits.ctypes.data, n.value, C.byref(n)))
+        return hits
 
     def run_noalloc(self, field_dev_ptr: int, nbytes: int, env: int = 0, ifreq: int = 0):
         """Allocation-free run of one field into a caller-owned device buffer

@@ -28,6 +28,18 @@ template<typename R> cudaError_t launch_influence(const void *, unsigned long lo
                                                   RunCounters *, bool, bool, int, cudaStream_t);
 cudaError_t launch_scale(const float2 *, float2 *, const GroupDev *, int, int, cudaStream_t);
 size_t seg_record_bytes(bool fp64);
+template<typename R> cudaError_t launch_arr_gather(const void *, unsigned long long, const GroupDev *, int,
+                                                   const double *, bool, bool, ArrCand *, uint64_t *, uint32_t *,
+                                                   unsigned long long, unsigned long long *, RunCounters *,
+                                                   ArrKeyBits, int, cudaStream_t);
+size_t radix_sort_hist_entries(unsigned long long n);
+cudaError_t radix_sort_pairs(uint64_t *, uint32_t *, uint64_t *, uint32_t *, unsigned long long, int, uint32_t *,
+                             int *, cudaStream_t);
+cudaError_t launch_arr_replay(const uint64_t *, const uint32_t *, const ArrCand *, unsigned long long,
+                              const GroupDev *, int, const double *, long long, int, int, int, int32_t *,
+                              ArrivalRec *, int, cudaStream_t);
+cudaError_t launch_eigen_emit(const uint32_t *, const ArrCand *, unsigned long long, EigenHitRec *, int32_t *, int,
+                              const uint64_t *, int, cudaStream_t);
 } // namespace bhcb
 
 using namespace bhcb;
@@ -80,9 +92,28 @@ struct EnvSlot {
 
 struct Field {
     int env, ifreq;
-    int64_t base;        // complex-element offset in acc/out
+    int64_t base;        // complex-element offset in out (and receiver-cell offset of arrivals)
     int nsz, nrzp, nrr;
 };
+
+enum { MODE_TL = 0, MODE_ARR = 1, MODE_EIGEN = 2 };
+constexpr unsigned long long MAXN_STEPS_HOST = 100000;   // steps per ray (include/bhc/structs.hpp:66)
+
+int run_mode_of(char r0)
+{
+    if(r0 == 'A' || r0 == 'a') return MODE_ARR;
+    if(r0 == 'E') return MODE_EIGEN;
+    if(r0 == 'C' || r0 == 'S' || r0 == 'I') return MODE_TL;
+    throw std::runtime_error(std::string("RunType '") + r0 + "' is not supported by this entry point "
+                             "(TL 'C'/'S'/'I', arrivals 'A'/'a', eigen hits 'E')");
+}
+
+int bits_for(unsigned long long n)   // bits to hold values 0..n-1 (at least 1)
+{
+    int b = 1;
+    while(b < 63 && (1ull << b) < n) ++b;
+    return b;
+}
 
 } // namespace
 
@@ -111,6 +142,18 @@ struct bhcb_ctx {
     bool gauss = false, coherent = true;
 
     DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
+
+    // arrivals / eigen runs (RunType 'A', 'a', 'E')
+    int mode = MODE_TL;
+    int32_t opt_max_narr = 0, allow_merging = 1;
+    int32_t max_narr = 0;
+    ArrKeyBits kb{};
+    unsigned long long ncand = 0;
+    DevBuf cand, keys0, keys1, vals0, vals1, hist, narr_d, arr_d, hits_d, hitfield_d;
+    const uint64_t *sorted_keys = nullptr;
+    const uint32_t *sorted_vals = nullptr;
+    std::vector<EigenHitRec> hits_h;      // eigen hits of the last run, in reference order
+    std::vector<int64_t> hit_begin;       // per field: first hit (size nfields + 1)
     RunCounters last{};
     bhcb_stats stats{};
     std::string last_error;
@@ -167,6 +210,51 @@ template<typename T> T *dptr(void *base, size_t off)
     return reinterpret_cast<T *>(reinterpret_cast<uint8_t *>(base) + off);
 }
 
+// Key layout and arrival storage of an arrivals / eigen run.
+void prepare_arrivals(bhcb_ctx *c)
+{
+    int max_njobs = 1, max_nrr = 1, max_nrzp = 1;
+    for(const GroupDev &G : c->groups_h) max_njobs = std::max(max_njobs, G.njobs);
+    for(const Field &F : c->fields) {
+        max_nrr = std::max(max_nrr, F.nrr);
+        max_nrzp = std::max(max_nrzp, F.nrzp);
+    }
+    ArrKeyBits kb{};
+    const int bis = bits_for(MAXN_STEPS_HOST), bjob = bits_for((unsigned long long)max_njobs);
+    if(c->mode == MODE_ARR) {
+        kb.eigen = 0;
+        kb.sh_walk = 0;
+        kb.sh_is = 0;
+        kb.sh_job = bis;
+        kb.sh_cell = bis + bjob;
+        kb.total_bits = kb.sh_cell + bits_for((unsigned long long)c->total_field);
+    } else {
+        kb.eigen = 1;
+        kb.sh_walk = bits_for((unsigned long long)max_nrzp);
+        kb.sh_is = kb.sh_walk + bits_for((unsigned long long)max_nrr);
+        kb.sh_job = kb.sh_is + bis;
+        kb.sh_cell = kb.sh_job + bjob;
+        kb.total_bits = kb.sh_cell + bits_for((unsigned long long)c->fields.size());
+    }
+    if(kb.total_bits > 64)
+        throw MemError("arrival ordering key needs more than 64 bits; split the run");
+    c->kb = kb;
+    if(c->mode == MODE_ARR) {
+        size_t cells = (size_t)c->total_field;
+        int32_t mx = c->opt_max_narr;
+        if(mx <= 0) {
+            // like the reference (src/mode/arr.hpp:80-98): as many arrivals per
+            // receiver as a quarter of max_memory holds, at most 1000
+            uint64_t m = (c->max_memory / 4) / (cells * sizeof(ArrivalRec) + 1);
+            mx = (int32_t)std::min<uint64_t>(m, 1000);
+        }
+        if(mx <= 0) throw MemError("insufficient memory to allocate arrivals");
+        c->max_narr = mx;
+        c->narr_d.ensure(cells * sizeof(int32_t));
+        c->arr_d.ensure(cells * (size_t)mx * sizeof(ArrivalRec));
+    }
+}
+
 void do_prepare(bhcb_ctx *c)
 {
     if(c->envs.empty()) throw StateError("no environment: call bhcb_setup or bhcb_add_env first");
@@ -178,6 +266,10 @@ void do_prepare(bhcb_ctx *c)
     c->total_acc = 0;
     c->njobs = 0;
     bool fp64 = c->precision == BHCB_PREC_FP64;
+    c->mode = run_mode_of(c->envs[0].in.run_type[0]);
+    for(auto &S : c->envs)
+        if(run_mode_of(S.in.run_type[0]) != c->mode)
+            throw std::runtime_error("a batch must use one run mode (TL, arrivals or eigen hits)");
     // --- preprocess every (env, frequency) and form trace groups
     struct GroupPlan { int env; std::vector<int> ifreqs; };
     std::vector<GroupPlan> plan;
@@ -192,7 +284,7 @@ void do_prepare(bhcb_ctx *c)
             if(done[i]) continue;
             GroupPlan gp{e, {(int)i}};
             done[i] = true;
-            if(!fp64 && c->share) {
+            if(!fp64 && c->share && c->mode == MODE_TL) {   // arrivals and hits are per frequency
                 for(size_t j = i + 1; j < S.freqs.size(); ++j)
                     if(!done[j] && S.tables[i].same_trajectory_tables(S.tables[j])
                        && S.tables[i].alpha == S.tables[j].alpha) {
@@ -213,9 +305,6 @@ void do_prepare(bhcb_ctx *c)
         const EnvTables &T0 = S.tables[0];
         if((T0.beam_type[0] == 'B') != c->gauss || (T0.run_type[0] == 'C') != c->coherent)
             throw std::runtime_error("a batch must use one beam type and one coherence mode");
-        char r0 = T0.run_type[0];
-        if(!(r0 == 'C' || r0 == 'S' || r0 == 'I'))
-            throw std::runtime_error("only TL runs (C, S, I) are supported by this entry point");
     }
     // --- build device tables
     Arena A;
@@ -265,6 +354,7 @@ void do_prepare(bhcb_ctx *c)
         d.irregular = T.run_type[4] == 'I';
         d.q_zero_init = T.run_type[1] == 'G';
         d.nsbp = (int)(T.sbp.size() / 2);
+        d.arrivals = c->mode == MODE_ARR;
         envdev.push_back(d);
     }
     size_t env_off = A.put(envdev);
@@ -304,6 +394,7 @@ void do_prepare(bhcb_ctx *c)
         c->total_acc = (c->total_acc + 1) & ~int64_t(1);
         G.acc_base = c->total_acc;
         c->total_acc += (int64_t)G.nfreq * G.acc_stride_f;
+        G.field_index = (int32_t)c->fields.size();
         for(size_t k = 0; k < gp.ifreqs.size(); ++k) {
             int fi = gp.ifreqs[k];
             c->freqs_h.push_back(S.freqs[fi]);
@@ -336,6 +427,7 @@ void do_prepare(bhcb_ctx *c)
     if(maxcap < 1024) throw MemError("max_memory too small for the segment buffer");
     c->seg_cap = std::min(want, maxcap);
     c->segs.ensure(c->seg_cap * rec);
+    if(c->mode != MODE_TL) prepare_arrivals(c);
     c->prepared = true;
 }
 
@@ -360,6 +452,7 @@ void do_launch(bhcb_ctx *c)
     else
         CK(launch_trace<float>(G, ng, c->njobs, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
     CK(cudaEventRecord(c->ev[1], c->stream));
+    if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
     // the influence grid covers the buffer capacity; chunks past the stored
     // count are skipped by reading the count on the device
     int igrid = c->sm_count * 8;   // persistent warps draining the chunk queue
@@ -380,8 +473,12 @@ int do_sync(bhcb_ctx *c)
     CK(cudaMemcpy(&c->last, c->counters.p, sizeof(RunCounters), cudaMemcpyDeviceToHost));
     float t0 = 0, t1 = 0, t2 = 0;
     CK(cudaEventElapsedTime(&t0, c->ev[0], c->ev[1]));
-    CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
-    CK(cudaEventElapsedTime(&t2, c->ev[0], c->ev[3]));
+    if(c->mode == MODE_TL) {
+        CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
+        CK(cudaEventElapsedTime(&t2, c->ev[0], c->ev[3]));
+    } else {
+        t2 = t0;
+    }
     c->stats.rays = (uint64_t)c->njobs;
     c->stats.steps = c->last.nsteps;
     c->stats.segments = c->last.nseg;
@@ -396,6 +493,88 @@ int do_sync(bhcb_ctx *c)
     c->err_bits = c->last.err_bits;
     c->warn_bits = c->last.warn_bits;
     return 0;
+}
+
+// Arrivals / eigen hits of the traced segments: count, gather, order, replay.
+void run_arrivals(bhcb_ctx *c)
+{
+    const bool fp64 = c->precision == BHCB_PREC_FP64;
+    const GroupDev *G = (const GroupDev *)c->groups_d.p;
+    const int ng = (int)c->groups_h.size();
+    const double *fq = (const double *)c->freqs_d.p;
+    RunCounters *ctr = (RunCounters *)c->counters.p;
+    unsigned long long *cursor = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
+    const int grid = c->sm_count * 16;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    // 1. count
+    CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), c->stream));
+    if(fp64)
+        CK(launch_arr_gather<double>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, true, nullptr, nullptr, nullptr, 0,
+                                     cursor, ctr, c->kb, grid, c->stream));
+    else
+        CK(launch_arr_gather<float>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, true, nullptr, nullptr, nullptr, 0,
+                                    cursor, ctr, c->kb, grid, c->stream));
+    unsigned long long n = 0;
+    CK(cudaMemcpyAsync(&n, &ctr->nevals, sizeof n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if(n >= (1ull << 32)) throw MemError("more than 2^32 arrival candidates; split the run");
+    const size_t per = sizeof(ArrCand) + 2 * sizeof(uint64_t) + 2 * sizeof(uint32_t);
+    if(n * per > c->max_memory) throw MemError("arrival candidates exceed max_memory; raise bhcb_init.max_memory");
+    c->ncand = n;
+    size_t nn = std::max<size_t>(n, 1);
+    c->cand.ensure(nn * sizeof(ArrCand));
+    c->keys0.ensure(nn * sizeof(uint64_t));
+    c->keys1.ensure(nn * sizeof(uint64_t));
+    c->vals0.ensure(nn * sizeof(uint32_t));
+    c->vals1.ensure(nn * sizeof(uint32_t));
+    c->hist.ensure(radix_sort_hist_entries(nn) * sizeof(uint32_t));
+    // 2. gather
+    CK(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), c->stream));
+    if(fp64)
+        CK(launch_arr_gather<double>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, false, (ArrCand *)c->cand.p,
+                                     (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, c->kb, grid,
+                                     c->stream));
+    else
+        CK(launch_arr_gather<float>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, false, (ArrCand *)c->cand.p,
+                                    (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, c->kb, grid,
+                                    c->stream));
+    // 3. order
+    int in1 = 0;
+    CK(radix_sort_pairs((uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, (uint64_t *)c->keys1.p,
+                        (uint32_t *)c->vals1.p, n, c->kb.total_bits, (uint32_t *)c->hist.p, &in1, c->stream));
+    c->sorted_keys = (const uint64_t *)(in1 ? c->keys1.p : c->keys0.p);
+    c->sorted_vals = (const uint32_t *)(in1 ? c->vals1.p : c->vals0.p);
+    // 4. replay / emit
+    if(c->mode == MODE_ARR) {
+        const size_t cells = (size_t)c->total_field;
+        CK(cudaMemsetAsync(c->arr_d.p, 0, cells * (size_t)c->max_narr * sizeof(ArrivalRec), c->stream));
+        CK(launch_arr_replay(c->sorted_keys, c->sorted_vals, (const ArrCand *)c->cand.p, n, G, ng, fq,
+                             (long long)cells, c->kb.sh_cell, c->max_narr, c->allow_merging, (int32_t *)c->narr_d.p,
+                             (ArrivalRec *)c->arr_d.p, c->sm_count, c->stream));
+    } else {
+        c->hits_d.ensure(nn * sizeof(EigenHitRec));
+        c->hitfield_d.ensure(nn * sizeof(int32_t));
+        CK(launch_eigen_emit(c->sorted_vals, (const ArrCand *)c->cand.p, n, (EigenHitRec *)c->hits_d.p,
+                             (int32_t *)c->hitfield_d.p, c->kb.sh_cell, c->sorted_keys, c->sm_count, c->stream));
+        c->hits_h.resize(n);
+        std::vector<int32_t> fld(n);
+        if(n) {
+            CK(cudaMemcpyAsync(c->hits_h.data(), c->hits_d.p, n * sizeof(EigenHitRec), cudaMemcpyDeviceToHost,
+                               c->stream));
+            CK(cudaMemcpyAsync(fld.data(), c->hitfield_d.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        }
+        CK(cudaStreamSynchronize(c->stream));
+        c->hit_begin.assign(c->fields.size() + 1, 0);
+        for(size_t k = 0; k < n; ++k) c->hit_begin[fld[k] + 1]++;
+        for(size_t f = 0; f < c->fields.size(); ++f) c->hit_begin[f + 1] += c->hit_begin[f];
+    }
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float t1 = 0;
+    CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
+    c->stats.influence_ms = t1;
+    c->stats.total_ms = c->stats.trace_ms + t1;
+    c->stats.evals = n;
 }
 
 int run_checked(bhcb_ctx *c)
@@ -421,6 +600,7 @@ int run_checked(bhcb_ctx *c)
             snprintf(b, sizeof b, "tracer error bits 0x%x", c->last.err_bits);
             return fail(c, BHCB_ERR_RUN, b);
         }
+        if(c->mode != MODE_TL) run_arrivals(c);
         return BHCB_OK;
     }
     return fail(c, BHCB_ERR_MEMORY, "segment buffer overflow persisted");
@@ -467,6 +647,110 @@ int noalloc_job_from_ctx(bhcb_ctx *c, int32_t env, int32_t ifreq, NoAllocJob *jo
 }
 } // namespace bhcb
 
+namespace {
+// Fortran sequential unformatted records: [int32 n][n bytes][int32 n]
+struct RecWriter {
+    std::vector<uint8_t> cur;
+    std::ofstream &o;
+    explicit RecWriter(std::ofstream &o_) : o(o_) {}
+    template<typename T> void put(const T &v)
+    {
+        const uint8_t *p = reinterpret_cast<const uint8_t *>(&v);
+        cur.insert(cur.end(), p, p + sizeof(T));
+    }
+    void put_bytes(const void *p, size_t n)
+    {
+        const uint8_t *q = reinterpret_cast<const uint8_t *>(p);
+        cur.insert(cur.end(), q, q + n);
+    }
+    void end()
+    {
+        int32_t n = (int32_t)cur.size();
+        o.write((const char *)&n, 4);
+        o.write((const char *)cur.data(), cur.size());
+        o.write((const char *)&n, 4);
+        cur.clear();
+    }
+};
+
+// WriteOutArrivals (src/mode/arr.cpp:88-239), 2-D: binary for RunType 'a',
+// list-directed text for 'A'.
+void write_arrivals(bhcb_ctx *c, const Field &F, const EnvSlot &S, const EnvTables &T, double freq,
+                    const std::string &path)
+{
+    size_t cells = (size_t)F.nsz * F.nrzp * F.nrr;
+    std::vector<int32_t> narr(cells);
+    std::vector<ArrivalRec> arr(cells * (size_t)c->max_narr);
+    CK(cudaMemcpyAsync(narr.data(), (int32_t *)c->narr_d.p + F.base, cells * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(arr.data(), (ArrivalRec *)c->arr_d.p + (size_t)F.base * c->max_narr,
+                       arr.size() * sizeof(ArrivalRec), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double RadDeg = 180.0 / 3.14159265358979323846;
+    const bool ascii = T.run_type[0] == 'A';
+    std::ofstream o(path, std::ios::binary);
+    if(!o.good()) throw std::runtime_error("cannot open " + path);
+    int nrz = (int)T.rz.size(), nrr = F.nrr, nsz = F.nsz;
+    if(ascii) {
+        char b[64];
+        o << "'2D'\n";
+        snprintf(b, sizeof b, "%.9g\n", freq);
+        o << b;
+        o << nsz;
+        for(float v : T.sz) { snprintf(b, sizeof b, " %.9g", v); o << b; }
+        o << "\n" << nrz;
+        for(float v : T.rz) { snprintf(b, sizeof b, " %.9g", v); o << b; }
+        o << "\n" << nrr;
+        for(double v : T.rr) { snprintf(b, sizeof b, " %.17g", v); o << b; }
+        o << "\n";
+    } else {
+        RecWriter w(o);
+        w.put_bytes("'2D'", 4); w.end();
+        w.put((float)freq); w.end();
+        w.put((int32_t)nsz); w.put_bytes(T.sz.data(), T.sz.size() * 4); w.end();
+        w.put((int32_t)nrz); w.put_bytes(T.rz.data(), T.rz.size() * 4); w.end();
+        w.put((int32_t)nrr); w.put_bytes(T.rr.data(), T.rr.size() * 8); w.end();
+    }
+    RecWriter w(o);
+    for(int isz = 0; isz < nsz; ++isz) {
+        // MaxNPerSource (src/mode/arr.cpp:24-74): the largest count of this source
+        int32_t maxn = 0;
+        size_t cb = (size_t)isz * F.nrzp * nrr;
+        for(size_t k = 0; k < (size_t)F.nrzp * nrr; ++k) maxn = std::max(maxn, narr[cb + k]);
+        if(ascii) o << maxn << "\n";
+        else { w.put(maxn); w.end(); }
+        for(int iz = 0; iz < F.nrzp; ++iz)
+            for(int ir = 0; ir < nrr; ++ir) {
+                size_t base = cb + (size_t)iz * nrr + ir;
+                int32_t n = narr[base];
+                if(ascii) o << n << "\n";
+                else { w.put(n); w.end(); }
+                for(int a = 0; a < n; ++a) {
+                    const ArrivalRec &A = arr[base * c->max_narr + a];
+                    float ph = (float)RadDeg * A.Phase;
+                    if(ascii) {
+                        char b[256];
+                        snprintf(b, sizeof b, "%.9g %.9g %.9g %.9g %.9g %.9g %d %d\n", A.a, ph, A.delay_re,
+                                 A.delay_im, A.SrcDeclAngle, A.RcvrDeclAngle, A.NTopBnc, A.NBotBnc);
+                        o << b;
+                    } else {
+                        w.put(A.a);
+                        w.put((float)(RadDeg * A.Phase));
+                        w.put(A.delay_re);
+                        w.put(A.delay_im);
+                        w.put(A.SrcDeclAngle);
+                        w.put(A.RcvrDeclAngle);
+                        w.put((float)A.NTopBnc);
+                        w.put((float)A.NBotBnc);
+                        w.end();
+                    }
+                }
+            }
+    }
+    (void)S;
+}
+} // namespace
+
 extern "C" {
 
 int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
@@ -501,7 +785,9 @@ void bhcb_close(bhcb_ctx *c)
     if(!c) return;
     cudaSetDevice(c->device);
     if(c->stream) cudaStreamSynchronize(c->stream);
-    for(DevBuf *b : {&c->arena, &c->groups_d, &c->freqs_d, &c->acc, &c->out, &c->segs, &c->counters})
+    for(DevBuf *b : {&c->arena, &c->groups_d, &c->freqs_d, &c->acc, &c->out, &c->segs, &c->counters, &c->cand,
+                     &c->keys0, &c->keys1, &c->vals0, &c->vals1, &c->hist, &c->narr_d, &c->arr_d, &c->hits_d,
+                     &c->hitfield_d})
         b->release();
     for(auto &e : c->ev)
         if(e) cudaEventDestroy(e);
@@ -579,6 +865,7 @@ int bhcb_sync(bhcb_ctx *c)
             snprintf(b, sizeof b, "tracer error bits 0x%x", c->last.err_bits);
             return fail(c, (c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) ? BHCB_ERR_MEMORY : BHCB_ERR_RUN, b);
         }
+        if(c->mode != MODE_TL) run_arrivals(c);
         return BHCB_OK;
     });
 }
@@ -608,6 +895,7 @@ int bhcb_field_shape(bhcb_ctx *c, int32_t env, int32_t *nfreq, int32_t *nsz, int
 int bhcb_copy_field(bhcb_ctx *c, int32_t env, int32_t ifreq, void *dst, size_t bytes)
 {
     return guarded(c, [&]() -> int {
+        if(c->mode != MODE_TL) throw StateError("not a TL run: use bhcb_copy_arrivals / bhcb_eigen_hits");
         const Field *F = find_field(c, env, ifreq);
         size_t need = (size_t)F->nsz * F->nrzp * F->nrr * sizeof(float2);
         if(!dst || bytes < need) throw std::invalid_argument("destination too small");
@@ -639,9 +927,85 @@ int bhcb_receivers(bhcb_ctx *c, int32_t env, double *rr, int32_t nrr, float *rz,
     });
 }
 
+int bhcb_set_arrival_options(bhcb_ctx *c, int32_t max_narr, int32_t allow_merging)
+{
+    return guarded(c, [&]() -> int {
+        if(max_narr < 0) throw std::invalid_argument("max_narr must be >= 0 (0 = sized from max_memory)");
+        c->opt_max_narr = max_narr;
+        c->allow_merging = allow_merging != 0;
+        c->prepared = false;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_arrivals_shape(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *nsz, int32_t *nrzp, int32_t *nrr,
+                        int32_t *max_narr)
+{
+    return guarded(c, [&]() -> int {
+        if(c->mode != MODE_ARR || !c->prepared) throw StateError("no prepared arrivals run");
+        const Field *F = find_field(c, env, ifreq);
+        if(nsz) *nsz = F->nsz;
+        if(nrzp) *nrzp = F->nrzp;
+        if(nrr) *nrr = F->nrr;
+        if(max_narr) *max_narr = c->max_narr;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_copy_arrivals(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *narr, size_t narr_bytes,
+                       bhcb_arrival *arr, size_t arr_bytes)
+{
+    static_assert(sizeof(bhcb_arrival) == sizeof(ArrivalRec), "arrival record layout");
+    return guarded(c, [&]() -> int {
+        if(c->mode != MODE_ARR || !c->prepared) throw StateError("no arrivals run");
+        const Field *F = find_field(c, env, ifreq);
+        size_t cells = (size_t)F->nsz * F->nrzp * F->nrr;
+        if(narr) {
+            if(narr_bytes < cells * sizeof(int32_t)) throw std::invalid_argument("narr buffer too small");
+            CK(cudaMemcpyAsync(narr, (int32_t *)c->narr_d.p + F->base, cells * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, c->stream));
+        }
+        if(arr) {
+            size_t need = cells * (size_t)c->max_narr * sizeof(ArrivalRec);
+            if(arr_bytes < need) throw std::invalid_argument("arrival buffer too small");
+            CK(cudaMemcpyAsync(arr, (ArrivalRec *)c->arr_d.p + (size_t)F->base * c->max_narr, need,
+                               cudaMemcpyDeviceToHost, c->stream));
+        }
+        CK(cudaStreamSynchronize(c->stream));
+        return BHCB_OK;
+    });
+}
+
+int bhcb_eigen_hits(bhcb_ctx *c, int32_t env, int32_t ifreq, bhcb_eigen_hit *hits, int64_t max_hits,
+                    int64_t *nhits)
+{
+    static_assert(sizeof(bhcb_eigen_hit) == sizeof(EigenHitRec), "eigen hit layout");
+    return guarded(c, [&]() -> int {
+        if(c->mode != MODE_EIGEN || !c->prepared) throw StateError("no eigen-hit run");
+        if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
+        const EnvSlot &S = c->envs[env];
+        if(ifreq < 0 || ifreq >= (int)S.field_of_freq.size()) throw std::invalid_argument("ifreq out of range");
+        int fi = S.field_of_freq[ifreq];
+        if(c->hit_begin.size() != c->fields.size() + 1) throw StateError("no hits: run first");
+        int64_t b = c->hit_begin[fi], e = c->hit_begin[fi + 1];
+        if(nhits) *nhits = e - b;
+        if(hits && max_hits > 0)
+            std::memcpy(hits, c->hits_h.data() + b, (size_t)std::min<int64_t>(max_hits, e - b) * sizeof(EigenHitRec));
+        return BHCB_OK;
+    });
+}
+
 int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
 {
     return guarded(c, [&]() -> int {
+        if(c->mode == MODE_EIGEN)
+            throw StateError("eigenray .ray output (re-trace of the hit rays) is not built; use bhcb_eigen_hits");
+        if(c->mode == MODE_ARR) {
+            const Field *F = find_field(c, env, ifreq);
+            const EnvSlot &S = c->envs[env];
+            write_arrivals(c, *F, S, S.tables[ifreq], S.freqs[ifreq], std::string(root) + ".arr");
+            return BHCB_OK;
+        }
         const Field *F = find_field(c, env, ifreq);
         const EnvSlot &S = c->envs[env];
         const EnvTables &T = S.tables[ifreq];

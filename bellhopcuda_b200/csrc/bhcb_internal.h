@@ -67,7 +67,8 @@ struct EnvDev {
     int32_t beam2;                   // Beam->Type[2] curvature option
     int32_t gaussian, coherent, line_source, irregular, q_zero_init;
     // source beam pattern: pairs (angle deg, linear level)
-    int32_t nsbp, pad0;
+    int32_t nsbp;
+    int32_t arrivals;                // RunType 'A' / 'a': segments carry the receiver angle
     const double *sbp;
 };
 
@@ -85,7 +86,7 @@ struct GroupDev {
     int64_t acc_base;
     int64_t acc_stride_f;    // accumulator elements per frequency field
     int32_t acc_nz;
-    int32_t pad;
+    int32_t field_index;     // index of the group's first field in the launch
 };
 
 // One influence segment (point0 -> point1 of Step_InfluenceGeoCart,
@@ -112,6 +113,33 @@ template<typename R> struct alignas(16) SegRec {
     int32_t job;          // global job (ray) index
     int32_t is;           // step index along the ray
     int32_t ntop, nbot;   // bounce counts of point1
+};
+
+// One arrival (include/bhc/structs.hpp:376-380; 40 bytes, same field order).
+struct ArrivalRec {
+    int32_t NTopBnc, NBotBnc;
+    float SrcDeclAngle, SrcAzimAngle, RcvrDeclAngle, RcvrAzimAngle, a, Phase;
+    float delay_re, delay_im;
+};
+// One eigenray hit (include/bhc/structs.hpp:353-361).
+struct EigenHitRec {
+    int32_t is, itheta, ir, iz, isx, isy, isz, ialpha, ibeta;
+};
+// One beam-receiver contribution of an arrivals / eigen run before ordering:
+// amplitude cnst * w, phase, complex delay (FP64, as AddArr compares them),
+// receiver angle, bounce counts, global job and launch-angle index. Eigen runs
+// reuse ntop / nbot / job for the step, range index and (depth | source << 20).
+struct ArrCand {
+    double amp, phase, delay_re, delay_im;
+    float rcvr_decl;
+    int32_t ntop, nbot, job, aux;
+    int32_t pad;
+};
+// Bit layout of the ordering keys (low to high): arrivals: step | job | cell;
+// eigen: depth | walk position | step | job | field.
+struct ArrKeyBits {
+    int sh_walk, sh_is, sh_job, sh_cell;
+    int total_bits, eigen;
 };
 
 struct RunCounters {

@@ -114,7 +114,8 @@ template<typename R> __device__ __forceinline__ bool infl_prologue(
     rec.tau1r = (R)p1.taur;
     rec.zlo = (R)min(p0.x.y, p1.x.y);
     rec.zhi = (R)max(p0.x.y, p1.x.y);
-    rec.rcvr_decl = (R)0;   // receiver declination: needed by arrivals only
+    // receiver declination (ReceiverAngles, src/influence.hpp:123-133): arrivals only
+    rec.rcvr_decl = e.arrivals ? (R)((180.0 / BHCB_PI) * atan2(rayt.y, rayt.x)) : (R)0;
     rec.ir_lo = min(first, last);
     rec.ir_hi = max(first, last);
     rec.job = job;

@@ -244,7 +244,7 @@ template<bool GAUSS, bool COHERENT> __device__ __forceinline__ bool eval_one(
     return true;
 }
 
-template<bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(32 * MW, 6)
+template<bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(32 * MW, 5)
 influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long long cap,
                        const GroupDev *__restrict__ groups, int ngroups, const double *__restrict__ freqs,
                        float2 *__restrict__ acc, RunCounters *ctr)
@@ -308,7 +308,7 @@ influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long lon
             __syncwarp();
             const int ngrp = 32 / g, gid = lane / g, lig = lane & (g - 1);
             for(int k = gid; k < 32; k += ngrp) {
-                const SegFreqM &P = s_p[w][k];
+                const SegFreqM P = s_p[w][k];   // register copy: the pair loop reads it every iteration
                 if(!P.valid) continue;
                 if(P.npair) {
                     // rectilinear grid: flattened (column, depth pair) units

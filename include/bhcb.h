@@ -102,9 +102,38 @@ int bhcb_field_device(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void **dp
 int bhcb_receivers(bhcb_ctx *ctx, int32_t env_index, double *rr, int32_t nrr, float *rz,
                    int32_t nrz);
 
-/* bhc::writeout (src/api.cpp:465-486) for TL runs: write FileRoot.shd of
-   (env_index, ifreq) in the reference's .shd layout (src/mode/tl.cpp:38-248). */
+/* bhc::writeout (src/api.cpp:465-486): TL runs write FileRoot.shd of
+   (env_index, ifreq) in the reference's .shd layout (src/mode/tl.cpp:38-248);
+   arrivals runs write FileRoot.arr (WriteOutArrivals, src/mode/arr.cpp:88-239:
+   Fortran unformatted records for 'a', list-directed text for 'A'). */
 int bhcb_writeout(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, const char *file_root);
+
+/* Arrivals (RunType 'A' / 'a') and eigenray hits ('E'). Arrivals follow
+   AddArr (src/arrivals.hpp:45-132) in the reference's single-threaded order
+   (ray by ray in job order, step by step), so merging (allow_merging, the
+   reference's AllowMerging, src/mode/arr.hpp:78) is deterministic. */
+typedef struct bhcb_arrival {   /* Arrival, include/bhc/structs.hpp:376-380 */
+    int32_t ntop, nbot;
+    float src_decl, src_azim, rcvr_decl, rcvr_azim, a, phase;   /* degrees; phase in radians */
+    float delay_re, delay_im;                                   /* complex delay (s) */
+} bhcb_arrival;
+typedef struct bhcb_eigen_hit { /* EigenHit, include/bhc/structs.hpp:353-361 */
+    int32_t is, itheta, ir, iz, isx, isy, isz, ialpha, ibeta;
+} bhcb_eigen_hit;
+/* Arrival storage per receiver (ArrInfo::MaxNArr; 0 = sized from max_memory like
+   src/mode/arr.hpp:80-98, at most 1000) and merging; takes effect at the next prepare. */
+int bhcb_set_arrival_options(bhcb_ctx *ctx, int32_t max_narr, int32_t allow_merging);
+/* outputs.arrinfo layout per field: NArr [NSz][NRz_per_range][NRr] int32 and
+   Arr [same][max_narr] bhcb_arrival, amplitudes scaled (PostProcessArrivals,
+   src/mode/arr.cpp:24-74). */
+int bhcb_arrivals_shape(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, int32_t *nsz,
+                        int32_t *nrz_per_range, int32_t *nrr, int32_t *max_narr);
+int bhcb_copy_arrivals(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, int32_t *narr, size_t narr_bytes,
+                       bhcb_arrival *arr, size_t arr_bytes);
+/* outputs.eigen->hits of (env_index, ifreq) in the reference's single-threaded
+   order; *nhits = their number, at most max_hits are copied. */
+int bhcb_eigen_hits(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, bhcb_eigen_hit *hits,
+                    int64_t max_hits, int64_t *nhits);
 
 /* The context's CUDA stream (cudaStream_t), for callers that time or order
    their own work against the tracer's kernels. */
