@@ -142,6 +142,7 @@ struct bhcb_ctx {
     bool gauss = false, coherent = true;
 
     DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
+    unsigned long long job0_h = 0;   // staging for the job counter's start value
 
     // arrivals / eigen runs (RunType 'A', 'a', 'E')
     int mode = MODE_TL;
@@ -431,26 +432,40 @@ void do_prepare(bhcb_ctx *c)
     c->prepared = true;
 }
 
-void do_launch(bhcb_ctx *c)
+// Enqueue trace (+ influence and scale for TL runs) of trace groups [g0, g1):
+// their jobs are [job_base(g0), job_base(g1)), so the job counter starts at
+// job_base(g0). clear: zero the accumulator of those groups first.
+void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear)
 {
     if(!c->prepared) throw StateError("bhcb_launch before bhcb_prepare");
     bool fp64 = c->precision == BHCB_PREC_FP64;
+    const int ngall = (int)c->groups_h.size();
+    const long long job0 = c->groups_h[g0].job_base;
+    const long long job1 = g1 < ngall ? (long long)c->groups_h[g1].job_base : c->njobs;
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(RunCounters) + 64, c->stream));
     RunCounters *ctr = (RunCounters *)c->counters.p;
     unsigned long long init_overflow = 0xffffffffull;
     CK(cudaMemcpyAsync(&ctr->overflow_job, &init_overflow, 4, cudaMemcpyHostToDevice, c->stream));
     unsigned long long *jobc = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
-    CK(cudaMemsetAsync(c->acc.p, 0, (size_t)c->total_acc * sizeof(float2), c->stream));
+    if(job0) {
+        c->job0_h = (unsigned long long)job0;
+        CK(cudaMemcpyAsync(jobc, &c->job0_h, sizeof(unsigned long long), cudaMemcpyHostToDevice, c->stream));
+    }
+    if(clear) {
+        const int64_t a0 = c->groups_h[g0].acc_base;
+        const int64_t a1 = g1 < ngall ? c->groups_h[g1].acc_base : c->total_acc;
+        CK(cudaMemsetAsync((float2 *)c->acc.p + a0, 0, (size_t)(a1 - a0) * sizeof(float2), c->stream));
+    }
     CK(cudaEventRecord(c->ev[0], c->stream));
     int tblock = 32;
-    long long tgrid = std::min<long long>((c->njobs + tblock - 1) / tblock, (long long)c->sm_count * 16);
+    long long tgrid = std::min<long long>((job1 - job0 + tblock - 1) / tblock, (long long)c->sm_count * 16);
     if(tgrid < 1) tgrid = 1;
-    const GroupDev *G = (const GroupDev *)c->groups_d.p;
-    int ng = (int)c->groups_h.size();
+    const GroupDev *G = (const GroupDev *)c->groups_d.p + g0;
+    int ng = g1 - g0;
     if(fp64)
-        CK(launch_trace<double>(G, ng, c->njobs, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
+        CK(launch_trace<double>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
     else
-        CK(launch_trace<float>(G, ng, c->njobs, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
+        CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
     CK(cudaEventRecord(c->ev[1], c->stream));
     if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
     // the influence grid covers the buffer capacity; chunks past the stored
@@ -465,6 +480,11 @@ void do_launch(bhcb_ctx *c)
     CK(cudaEventRecord(c->ev[2], c->stream));
     CK(launch_scale((const float2 *)c->acc.p, (float2 *)c->out.p, G, ng, c->sm_count * 2, c->stream));
     CK(cudaEventRecord(c->ev[3], c->stream));
+}
+
+void do_launch(bhcb_ctx *c)
+{
+    do_launch_range(c, 0, (int)c->groups_h.size(), true);
 }
 
 int do_sync(bhcb_ctx *c)
@@ -577,6 +597,57 @@ void run_arrivals(bhcb_ctx *c)
     c->stats.evals = n;
 }
 
+// TL runs whose segments do not fit in max_memory at once: trace the groups in
+// contiguous waves, halving a wave (by jobs) until its segments fit.
+int run_range(bhcb_ctx *c, int g0, int g1, bhcb_stats &acc)
+{
+    do_launch_range(c, g0, g1, true);
+    do_sync(c);
+    if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
+        if(g1 - g0 <= 1)
+            throw MemError("one environment's segments exceed max_memory; raise bhcb_init.max_memory");
+        const long long j0 = c->groups_h[g0].job_base;
+        const long long j1 = g1 < (int)c->groups_h.size() ? (long long)c->groups_h[g1].job_base : c->njobs;
+        int mid = g0 + 1;
+        while(mid < g1 - 1 && c->groups_h[mid].job_base - j0 < (j1 - j0) / 2) ++mid;
+        int r = run_range(c, g0, mid, acc);
+        if(r) return r;
+        return run_range(c, mid, g1, acc);
+    }
+    if(c->last.err_bits) {
+        char b[96];
+        snprintf(b, sizeof b, "tracer error bits 0x%x", c->last.err_bits);
+        return fail(c, BHCB_ERR_RUN, b);
+    }
+    acc.steps += c->stats.steps;
+    acc.segments += c->stats.segments;
+    acc.evals += c->stats.evals;
+    acc.warn_bits |= c->stats.warn_bits;
+    acc.trace_ms += c->stats.trace_ms;
+    acc.influence_ms += c->stats.influence_ms;
+    acc.total_ms += c->stats.total_ms;
+    acc.groups += 1;   // waves
+    return BHCB_OK;
+}
+
+int run_waves(bhcb_ctx *c)
+{
+    bhcb_stats acc{};
+    int r = run_range(c, 0, (int)c->groups_h.size(), acc);
+    if(r) return r;
+    c->stats.steps = acc.steps;
+    c->stats.segments = acc.segments;
+    c->stats.evals = acc.evals;
+    c->stats.warn_bits = c->warn_bits = acc.warn_bits;
+    c->stats.err_bits = c->err_bits = 0;
+    c->stats.trace_ms = acc.trace_ms;
+    c->stats.influence_ms = acc.influence_ms;
+    c->stats.total_ms = acc.total_ms;
+    c->stats.groups = (int)c->groups_h.size();
+    c->msg("segments exceeded max_memory: traced in " + std::to_string(acc.groups) + " waves");
+    return BHCB_OK;
+}
+
 int run_checked(bhcb_ctx *c)
 {
     for(int attempt = 0; attempt < 8; ++attempt) {
@@ -589,8 +660,10 @@ int run_checked(bhcb_ctx *c)
             size_t abytes = (size_t)c->total_acc * sizeof(float2);
             size_t budget = c->max_memory > 2 * fbytes + abytes ? c->max_memory - 2 * fbytes - abytes : 0;
             unsigned long long maxcap = budget / rec;
-            if(c->seg_cap >= maxcap)
+            if(c->seg_cap >= maxcap) {
+                if(c->mode == MODE_TL && c->groups_h.size() > 1) return run_waves(c);
                 throw MemError("segment buffer exceeds max_memory; raise bhcb_init.max_memory");
+            }
             c->seg_cap = std::min(maxcap, std::max(c->seg_cap * 2, (unsigned long long)(c->last.nseg * 1.25)));
             c->segs.ensure(c->seg_cap * rec);
             continue;

@@ -2,6 +2,7 @@
 
     python -m bellhopcuda_b200.run_workload rd_gauss --nalpha 4001 --all-freqs
     python -m bellhopcuda_b200.run_workload munk_tl --precision fp64
+    python -m bellhopcuda_b200.run_workload batch --count 256 --scale 1.0
 
 Used for profiling captures (ncu) of a chosen size; writes the input files
 under --dir (default: a temporary directory).
@@ -24,18 +25,30 @@ from bellhopcuda_b200.envfile import write_env  # noqa: E402
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["rd_gauss", "munk_tl"])
+    ap.add_argument("workload", choices=["rd_gauss", "munk_tl", "batch"])
     ap.add_argument("--nalpha", type=int, default=0, help="rays (0 = the workload's own)")
     ap.add_argument("--all-freqs", action="store_true", help="rd_gauss: evaluate all 10 frequencies")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--dir", default=None)
+    ap.add_argument("--count", type=int, default=256, help="batch: environments")
+    ap.add_argument("--scale", type=float, default=1.0, help="batch: ray / receiver scale")
     a = ap.parse_args(argv)
+    d = a.dir or tempfile.mkdtemp()
+    prec = B.PREC_FP64 if a.precision == "fp64" else B.PREC_MIXED
+    if a.workload == "batch":
+        roots = [write_env(s, os.path.join(d, "batch_%d" % i))
+                 for i, s in enumerate(W.batch_envs(n=a.count, scale=a.scale))]
+        with B.Tracer(precision=prec) as t:
+            for r in roots:
+                t.add_env(r)
+            for _ in range(a.repeat):
+                t.run()
+                print(json.dumps(t.stats()), flush=True)
+        return 0
     kw = {"nalpha": a.nalpha} if a.nalpha else {}
     spec = W.rd_gauss(**kw) if a.workload == "rd_gauss" else W.munk_tl(**kw)
-    d = a.dir or tempfile.mkdtemp()
     root = write_env(spec, os.path.join(d, a.workload))
-    prec = B.PREC_FP64 if a.precision == "fp64" else B.PREC_MIXED
     with B.Tracer(precision=prec) as t:
         t.setup(root)
         if a.all_freqs and a.workload == "rd_gauss":

@@ -112,6 +112,35 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------------------- ranks
+class RankComm:
+    """Barrier and max-over-ranks around the timed region: NCCL on the GPUs
+    (device "cuda"), gloo on CPU in the multi-rank tests (device "cpu")."""
+
+    def __init__(self, dist=None, device="cuda", sync=None):
+        self.dist, self.device, self.sync = dist, device, sync
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+        if self.sync:
+            self.sync()
+
+    def max_over_ranks(self, x):
+        if not self.dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def aggregate_value(world, fields_per_step, steps, total_s):
+    """Whole-job TL fields/s: every rank computes its own environment (weak
+    scaling); the job time is the slowest rank's."""
+    return world * fields_per_step * steps / total_s
+
+
 # ------------------------------------------------------------- environment
 def make_env(tmp, rank):
     from bellhopcuda_b200 import workloads as W
@@ -308,17 +337,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    comm = RankComm(dist, "cuda", torch.cuda.synchronize)
+    barrier, max_over_ranks = comm.barrier, comm.max_over_ranks
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     fp32_peak, fp64_peak = B.probe_fp_peak(local)
@@ -334,7 +354,7 @@ def main():
         clocks = clk.summary()
         total_s = max_over_ranks(sum(times) / 1000.0)
         ms_per_step = 1000.0 * total_s / args.steps
-        value = world * nf * args.steps / total_s
+        value = aggregate_value(world, nf, args.steps, total_s)
         st = stats[-1]
         t.close()
         # ---- FP64 per-frequency tracer (the plain GPU trace)
