@@ -54,9 +54,9 @@ struct InflState {   // the carried part of InfluenceRayInfo (include/bhc/struct
 
 // Sequential prologue of Step_InfluenceGeoCart (2-D): returns true when the
 // segment has receiver columns to evaluate and fills rec.
-template<typename R> __device__ __forceinline__ bool infl_prologue(
+template<typename R, typename RecR> __device__ __forceinline__ bool infl_prologue(
     const RayPt<R> &p0, const RayPt<R> &p1, InflState &inf, const EnvDev &e, R rcp_q0, R ratio1,
-    int job, int is, SegRec<R> &rec)
+    int job, int is, SegRec<RecR> &rec)
 {
     double rA = inf.x.x, rB = p1.x.x;
     V2<double> d = sub2(p1.x, p0.x);
@@ -96,26 +96,26 @@ template<typename R> __device__ __forceinline__ bool infl_prologue(
     rec.x0r = p0.x.x;
     rec.x0z = p0.x.y;
     rec.tau0r = p0.taur;
-    rec.dtaur = (R)(p1.taur - p0.taur);
-    rec.tau0i = (R)p0.taui;
-    rec.dtaui = (R)(p1.taui - p0.taui);
-    rec.tx = (R)rayt.x;
-    rec.tz = (R)rayt.y;
-    rec.rlen = (R)rlen;
-    rec.q0 = p0.q.x;
-    rec.dq = p1.q.x - p0.q.x;
-    rec.rcp_q0 = rcp_q0;
-    rec.cnst_num = ratio1 * sqrt(p1.c) * p1.Amp;
+    rec.dtaur = (RecR)(p1.taur - p0.taur);
+    rec.tau0i = (RecR)p0.taui;
+    rec.dtaui = (RecR)(p1.taui - p0.taui);
+    rec.tx = (RecR)rayt.x;
+    rec.tz = (RecR)rayt.y;
+    rec.rlen = (RecR)rlen;
+    rec.q0 = (RecR)p0.q.x;
+    rec.dq = (RecR)(p1.q.x - p0.q.x);
+    rec.rcp_q0 = (RecR)rcp_q0;
+    rec.cnst_num = (RecR)(ratio1 * sqrt(p1.c) * p1.Amp);
     const RayPt<R> &pp = e.gaussian ? p1 : p0;
-    rec.phase_a = (R)((double)pp.Phase + inf.phase);
-    rec.phase_b = (R)(inf.phase + BHCB_PI / FLTD(2.0));
-    rec.sigma_seg = max(fabs(p0.q.x), fabs(p1.q.x)) * rcp_q0 / (R)fabs(rayt.x);
-    rec.c0 = p0.c;
-    rec.tau1r = (R)p1.taur;
-    rec.zlo = (R)min(p0.x.y, p1.x.y);
-    rec.zhi = (R)max(p0.x.y, p1.x.y);
+    rec.phase_a = (RecR)((double)pp.Phase + inf.phase);
+    rec.phase_b = (RecR)(inf.phase + BHCB_PI / FLTD(2.0));
+    rec.sigma_seg = (RecR)(max(fabs(p0.q.x), fabs(p1.q.x)) * rcp_q0 / (R)fabs(rayt.x));
+    rec.c0 = (RecR)p0.c;
+    rec.tau1r = (RecR)p1.taur;
+    rec.zlo = (RecR)min(p0.x.y, p1.x.y);
+    rec.zhi = (RecR)max(p0.x.y, p1.x.y);
     // receiver declination (ReceiverAngles, src/influence.hpp:123-133): arrivals only
-    rec.rcvr_decl = e.arrivals ? (R)((180.0 / BHCB_PI) * atan2(rayt.y, rayt.x)) : (R)0;
+    rec.rcvr_decl = e.arrivals ? (RecR)((180.0 / BHCB_PI) * atan2(rayt.y, rayt.x)) : (RecR)0;
     rec.ir_lo = min(first, last);
     rec.ir_hi = max(first, last);
     rec.job = job;

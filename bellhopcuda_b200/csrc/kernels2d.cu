@@ -1,6 +1,7 @@
 // 2-D field-mode kernels for sm_100a.
 //
-//  trace_kernel     one ray per thread (persistent, work-queue driven); runs
+//  trace_kernel     one ray per thread (persistent, work-queue driven), FP64
+//                   ray state, FP32 or FP64 segment records; runs
 //                   RayInit / RayUpdate / RayTerminate (src/trace.hpp:76-589)
 //                   and the sequential part of Step_InfluenceGeoCart
 //                   (src/influence.hpp:1201-1294: duplicate-point skip, caustic
@@ -58,8 +59,9 @@ template<typename R> __device__ __forceinline__ void close_block(SegRec<R> *segs
     for(; cur.next < cur.end; ++cur.next) segs[cur.next].job = -1;
 }
 
-template<typename R> __global__ void __launch_bounds__(64) trace_kernel(
-    const GroupDev *__restrict__ groups, int ngroups, long long njobs, SegRec<R> *segs,
+// R: ray state; RecR: segment record (float for the mixed kernel's FP32 influence).
+template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_kernel(
+    const GroupDev *__restrict__ groups, int ngroups, long long njobs, SegRec<RecR> *segs,
     unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter)
 {
     for(;;) {
@@ -162,7 +164,7 @@ template<typename R> __global__ void __launch_bounds__(64) trace_kernel(
                 reflect2d(p1, p2, tr ? htop : hbot, tr, tI, nI, (R)b0.kappa, e, iSeg, ctr);
                 distances(p2.x, top, bot, dEndTop, dEndBot);
             }
-            SegRec<R> rec;
+            SegRec<RecR> rec;
             if(infl_prologue(p0, p1, inf, e, rcp_q0, ratio1, (int)job, is, rec))
                 emit_seg(rec, segs, cap, ctr, cur, overflow);
             ++is;
@@ -467,7 +469,10 @@ template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroup
                                               unsigned long long *job_counter, int grid, int block,
                                               cudaStream_t st)
 {
-    trace_kernel<R><<<grid, block, 0, st>>>(groups, ngroups, njobs, (SegRec<R> *)segs, cap, ctr,
+    // the ray state is FP64 in both precisions (the mixed precision writes FP32
+    // segment records for its FP32 influence kernel): the trajectory, and with it
+    // every step and reflection decision, is the FP64 one
+    trace_kernel<double, R><<<grid, block, 0, st>>>(groups, ngroups, njobs, (SegRec<R> *)segs, cap, ctr,
                                             job_counter);
     return cudaGetLastError();
 }

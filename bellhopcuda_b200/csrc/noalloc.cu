@@ -136,7 +136,7 @@ template<typename R, bool GAUSS, bool COHERENT> __device__ __forceinline__ void 
 // Variant of trace_kernel (kernels2d.cu) for one trace group and one
 // frequency: same ray physics (src/trace.hpp:76-589), contributions applied
 // inline into the static accumulator.
-template<typename R, bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(64)
+template<typename R, typename RecR, bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(64)
 noalloc_trace_kernel(unsigned char *scratch, double freq)
 {
     NoAllocHeader *H = reinterpret_cast<NoAllocHeader *>(scratch);
@@ -232,13 +232,13 @@ noalloc_trace_kernel(unsigned char *scratch, double freq)
                 reflect2d(p1, p2, tr ? htop : hbot, tr, tI, nI, (R)b0.kappa, e, iSeg, ctr);
                 distances(p2.x, top, bot, dEndTop, dEndBot);
             }
-            SegRec<R> rec;
+            SegRec<RecR> rec;
             if(infl_prologue(p0, p1, inf, e, rcp_q0, ratio1, (int)job, is, rec))
-                eval_segment_inline<R, GAUSS, COHERENT>(rec, e, freq, acc, base, evals);
+                eval_segment_inline<RecR, GAUSS, COHERENT>(rec, e, freq, acc, base, evals);
             ++is;
             if(two) {
                 if(infl_prologue(p1, p2, inf, e, rcp_q0, ratio1, (int)job, is, rec))
-                    eval_segment_inline<R, GAUSS, COHERENT>(rec, e, freq, acc, base, evals);
+                    eval_segment_inline<RecR, GAUSS, COHERENT>(rec, e, freq, acc, base, evals);
                 p0 = p2;
                 ++is;
             } else {
@@ -260,16 +260,18 @@ noalloc_trace_kernel(unsigned char *scratch, double freq)
     if(evals) atomicAdd(&ctr->nevals, evals);
 }
 
+// R: contribution precision; the ray state is FP64 in both precisions, as in
+// the trace kernel
 template<typename R> void launch_fused(const NoAllocJob &J, unsigned char *scratch, int grid)
 {
     if(J.gaussian && J.coherent)
-        noalloc_trace_kernel<R, true, true><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
+        noalloc_trace_kernel<double, R, true, true><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
     else if(J.gaussian)
-        noalloc_trace_kernel<R, true, false><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
+        noalloc_trace_kernel<double, R, true, false><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
     else if(J.coherent)
-        noalloc_trace_kernel<R, false, true><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
+        noalloc_trace_kernel<double, R, false, true><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
     else
-        noalloc_trace_kernel<R, false, false><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
+        noalloc_trace_kernel<double, R, false, false><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
 }
 
 int put_msg(char *msg, size_t n, int code, const char *text)

@@ -33,13 +33,14 @@ def main(argv=None):
     ap.add_argument("--dir", default=None)
     ap.add_argument("--count", type=int, default=256, help="batch: environments")
     ap.add_argument("--scale", type=float, default=1.0, help="batch: ray / receiver scale")
+    ap.add_argument("--max-memory-gb", type=float, default=0.0, help="device budget (0: library default)")
     a = ap.parse_args(argv)
     d = a.dir or tempfile.mkdtemp()
     prec = B.PREC_FP64 if a.precision == "fp64" else B.PREC_MIXED
     if a.workload == "batch":
         roots = [write_env(s, os.path.join(d, "batch_%d" % i))
                  for i, s in enumerate(W.batch_envs(n=a.count, scale=a.scale))]
-        with B.Tracer(precision=prec) as t:
+        with B.Tracer(precision=prec, max_memory=int(a.max_memory_gb * 2**30)) as t:
             for r in roots:
                 t.add_env(r)
             for _ in range(a.repeat):
@@ -49,7 +50,7 @@ def main(argv=None):
     kw = {"nalpha": a.nalpha} if a.nalpha else {}
     spec = W.rd_gauss(**kw) if a.workload == "rd_gauss" else W.munk_tl(**kw)
     root = write_env(spec, os.path.join(d, a.workload))
-    with B.Tracer(precision=prec) as t:
+    with B.Tracer(precision=prec, max_memory=int(a.max_memory_gb * 2**30)) as t:
         t.setup(root)
         if a.all_freqs and a.workload == "rd_gauss":
             t.set_frequencies(0, W.rd_gauss_freqs())

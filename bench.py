@@ -404,7 +404,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 bulk / f64 phase+position", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64 ray trace / f32 beam-receiver contributions", "data": "synthetic",
         "config": {"workload": "rd_gauss: 2-D Gaussian-beam TL, PCHIP SSP 64 nodes, 200-pt bathymetry, "
                                "20001 rays +-30 deg, 501x2001 receivers, 10 freqs 50-500 Hz, "
                                "frequencies share one trajectory",

@@ -64,4 +64,4 @@ def test_batch_in_waves_when_segments_exceed_max_memory(workdir):
     waved, st2 = run(small)
     assert st2["segments"] == st["segments"] and st2["evals"] == st["evals"]
     for a, b in zip(waved, full):
-        np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-12 * np.abs(b).max())
+        np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-12 * np.abs(b).max())
