@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(HERE, "libbhcb.so")
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+FLAG_SERIAL_INFLUENCE = 1   # BHCB_FLAG_SERIAL_INFLUENCE
 
 ERR_NAMES = {
     2: "BHC_ERR_RAYINIT", 3: "BHC_ERR_BOUNDARY_SEG_CONTAINS_NAN",
@@ -42,7 +43,7 @@ class BhcbError(RuntimeError):
 
 class Init(C.Structure):
     _fields_ = [("gpu_index", C.c_int32), ("precision", C.c_int32), ("max_memory", C.c_uint64),
-                ("share_trajectory", C.c_int32), ("reserved", C.c_int32),
+                ("share_trajectory", C.c_int32), ("flags", C.c_int32),
                 ("output_callback", C.c_void_p)]
 
 
@@ -50,7 +51,8 @@ class Stats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("steps", C.c_uint64), ("segments", C.c_uint64),
                 ("evals", C.c_uint64), ("err_bits", C.c_uint32), ("warn_bits", C.c_uint32),
                 ("groups", C.c_int32), ("fields", C.c_int32), ("trace_ms", C.c_double),
-                ("influence_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_uint64)]
+                ("influence_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_uint64),
+                ("influence_span_ms", C.c_double)]
 
 
 class EnvInfo(C.Structure):
@@ -148,9 +150,10 @@ class Tracer:
     """One bhcb context (one GPU, one stream)."""
 
     def __init__(self, gpu: int = 0, precision: int = PREC_MIXED, max_memory: int = 0,
-                 share_trajectory: bool = True):
+                 share_trajectory: bool = True, serial_influence: bool = False):
         self._lib = load_library()
-        init = Init(gpu, precision, max_memory, 1 if share_trajectory else 0, 0, None)
+        flags = FLAG_SERIAL_INFLUENCE if serial_influence else 0
+        init = Init(gpu, precision, max_memory, 1 if share_trajectory else 0, flags, None)
         h = C.c_void_p()
         rc = self._lib.bhcb_open(C.byref(init), C.byref(h))
         if rc != 0:

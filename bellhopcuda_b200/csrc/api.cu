@@ -22,7 +22,10 @@
 namespace bhcb {
 template<typename R> cudaError_t launch_trace(const GroupDev *, int, long long, void *,
                                               unsigned long long, RunCounters *,
-                                              unsigned long long *, int, int, cudaStream_t);
+                                              unsigned long long *, unsigned int *, int, int, cudaStream_t);
+cudaError_t launch_influence_mixed(const void *, unsigned long long, const GroupDev *, int, const double *,
+                                   float2 *, RunCounters *, bool, bool, int, cudaStream_t, unsigned int *,
+                                   unsigned long long *);
 template<typename R> cudaError_t launch_influence(const void *, unsigned long long,
                                                   const GroupDev *, int, const double *, float2 *,
                                                   RunCounters *, bool, bool, int, cudaStream_t);
@@ -124,7 +127,10 @@ struct bhcb_ctx {
     uint64_t max_memory = 16ull << 30;
     void (*output_cb)(const char *) = nullptr;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t stream2 = nullptr;   // influence launches beside the trace
+    bool overlap = true;              // mixed TL runs: influence overlaps the trace
+    // ev: 0 start, 1 trace end, 2 influence end, 3 scale end, 4 first influence launch
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
 
     std::vector<EnvSlot> envs;
@@ -143,6 +149,8 @@ struct bhcb_ctx {
 
     DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
     unsigned long long job0_h = 0;   // staging for the job counter's start value
+    DevBuf blk_state, scan;          // published segment blocks; queue of an overlapped launch
+    bool last_overlapped = false;
 
     // arrivals / eigen runs (RunType 'A', 'a', 'E')
     int mode = MODE_TL;
@@ -435,7 +443,7 @@ void do_prepare(bhcb_ctx *c)
 // Enqueue trace (+ influence and scale for TL runs) of trace groups [g0, g1):
 // their jobs are [job_base(g0), job_base(g1)), so the job counter starts at
 // job_base(g0). clear: zero the accumulator of those groups first.
-void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear)
+void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
 {
     if(!c->prepared) throw StateError("bhcb_launch before bhcb_prepare");
     bool fp64 = c->precision == BHCB_PREC_FP64;
@@ -462,12 +470,54 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear)
     if(tgrid < 1) tgrid = 1;
     const GroupDev *G = (const GroupDev *)c->groups_d.p + g0;
     int ng = g1 - g0;
+    // mixed TL runs driven by the host: influence kernels on stream2 take the
+    // segment blocks the trace publishes while it runs (no kernel waits for
+    // another; the host relaunches them until the trace's end event)
+    const bool ovl = host_driven && c->overlap && !fp64 && c->mode == MODE_TL;
+    c->last_overlapped = ovl;
+    unsigned int *blk = nullptr;
+    if(ovl) {
+        const size_t nblk = (size_t)((c->seg_cap + 31) / 32);   // the influence kernel's chunk count
+        c->blk_state.ensure(nblk * sizeof(unsigned int));
+        c->scan.ensure(64);
+        blk = (unsigned int *)c->blk_state.p;
+        CK(cudaMemsetAsync(blk, 0, nblk * sizeof(unsigned int), c->stream));
+        CK(cudaEventRecord(c->ev[0], c->stream));
+    }
     if(fp64)
-        CK(launch_trace<double>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
+        CK(launch_trace<double>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
+                                c->stream));
     else
-        CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, (int)tgrid, tblock, c->stream));
+        CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
+                               c->stream));
     CK(cudaEventRecord(c->ev[1], c->stream));
     if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
+    if(ovl) {
+        const int igrid = c->sm_count * 8;
+        unsigned long long *scan = (unsigned long long *)c->scan.p;
+        const double *fq = (const double *)c->freqs_d.p;
+        CK(cudaStreamWaitEvent(c->stream2, c->ev[0], 0));
+        CK(cudaEventRecord(c->ev[4], c->stream2));
+        for(;;) {
+            cudaError_t q = cudaEventQuery(c->ev[1]);
+            if(q == cudaSuccess) break;
+            if(q != cudaErrorNotReady) CK(q);
+            CK(cudaMemsetAsync(scan, 0, sizeof(unsigned long long), c->stream2));
+            CK(launch_influence_mixed(c->segs.p, c->seg_cap, G, ng, fq, (float2 *)c->acc.p, ctr, c->gauss,
+                                      c->coherent, igrid, c->stream2, blk, scan));
+            CK(cudaStreamSynchronize(c->stream2));
+        }
+        // the trace has ended: every allocated block is published; take the rest
+        CK(cudaStreamWaitEvent(c->stream2, c->ev[1], 0));
+        CK(cudaMemsetAsync(scan, 0, sizeof(unsigned long long), c->stream2));
+        CK(launch_influence_mixed(c->segs.p, c->seg_cap, G, ng, fq, (float2 *)c->acc.p, ctr, c->gauss,
+                                  c->coherent, igrid, c->stream2, blk, scan));
+        CK(cudaEventRecord(c->ev[2], c->stream2));
+        CK(cudaStreamWaitEvent(c->stream, c->ev[2], 0));
+        CK(launch_scale((const float2 *)c->acc.p, (float2 *)c->out.p, G, ng, c->sm_count * 2, c->stream));
+        CK(cudaEventRecord(c->ev[3], c->stream));
+        return;
+    }
     // the influence grid covers the buffer capacity; chunks past the stored
     // count are skipped by reading the count on the device
     int igrid = c->sm_count * 8;   // persistent warps draining the chunk queue
@@ -482,9 +532,9 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear)
     CK(cudaEventRecord(c->ev[3], c->stream));
 }
 
-void do_launch(bhcb_ctx *c)
+void do_launch(bhcb_ctx *c, bool host_driven)
 {
-    do_launch_range(c, 0, (int)c->groups_h.size(), true);
+    do_launch_range(c, 0, (int)c->groups_h.size(), true, host_driven);
 }
 
 int do_sync(bhcb_ctx *c)
@@ -493,12 +543,16 @@ int do_sync(bhcb_ctx *c)
     CK(cudaMemcpy(&c->last, c->counters.p, sizeof(RunCounters), cudaMemcpyDeviceToHost));
     float t0 = 0, t1 = 0, t2 = 0;
     CK(cudaEventElapsedTime(&t0, c->ev[0], c->ev[1]));
+    float span = 0;
     if(c->mode == MODE_TL) {
         CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
         CK(cudaEventElapsedTime(&t2, c->ev[0], c->ev[3]));
+        if(c->last_overlapped) CK(cudaEventElapsedTime(&span, c->ev[4], c->ev[2]));
+        else span = t1;
     } else {
         t2 = t0;
     }
+    c->stats.influence_span_ms = span;
     c->stats.rays = (uint64_t)c->njobs;
     c->stats.steps = c->last.nsteps;
     c->stats.segments = c->last.nseg;
@@ -601,7 +655,7 @@ void run_arrivals(bhcb_ctx *c)
 // contiguous waves, halving a wave (by jobs) until its segments fit.
 int run_range(bhcb_ctx *c, int g0, int g1, bhcb_stats &acc)
 {
-    do_launch_range(c, g0, g1, true);
+    do_launch_range(c, g0, g1, true, true);
     do_sync(c);
     if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
         if(g1 - g0 <= 1)
@@ -651,7 +705,7 @@ int run_waves(bhcb_ctx *c)
 int run_checked(bhcb_ctx *c)
 {
     for(int attempt = 0; attempt < 8; ++attempt) {
-        do_launch(c);
+        do_launch(c, true);
         do_sync(c);
         if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
             // grow the segment buffer and run again
@@ -836,6 +890,7 @@ int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
         c->precision = init->precision == BHCB_PREC_FP64 ? BHCB_PREC_FP64 : BHCB_PREC_MIXED;
         if(init->max_memory) c->max_memory = init->max_memory;
         c->share = init->share_trajectory != 0;
+        c->overlap = (init->flags & BHCB_FLAG_SERIAL_INFLUENCE) == 0;
         c->output_cb = init->output_callback;
     }
     int ndev = 0;
@@ -847,6 +902,7 @@ int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
     if(cudaSetDevice(c->device) != cudaSuccess) return BHCB_ERR_CUDA;
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
     if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return BHCB_ERR_CUDA;
+    if(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) return BHCB_ERR_CUDA;
     for(auto &e : c->ev)
         if(cudaEventCreate(&e) != cudaSuccess) return BHCB_ERR_CUDA;
     *out = c.release();
@@ -858,13 +914,15 @@ void bhcb_close(bhcb_ctx *c)
     if(!c) return;
     cudaSetDevice(c->device);
     if(c->stream) cudaStreamSynchronize(c->stream);
+    if(c->stream2) cudaStreamSynchronize(c->stream2);
     for(DevBuf *b : {&c->arena, &c->groups_d, &c->freqs_d, &c->acc, &c->out, &c->segs, &c->counters, &c->cand,
                      &c->keys0, &c->keys1, &c->vals0, &c->vals1, &c->hist, &c->narr_d, &c->arr_d, &c->hits_d,
-                     &c->hitfield_d})
+                     &c->hitfield_d, &c->blk_state, &c->scan})
         b->release();
     for(auto &e : c->ev)
         if(e) cudaEventDestroy(e);
     if(c->stream) cudaStreamDestroy(c->stream);
+    if(c->stream2) cudaStreamDestroy(c->stream2);
     delete c;
 }
 
@@ -924,7 +982,7 @@ int bhcb_prepare(bhcb_ctx *c)
 int bhcb_launch(bhcb_ctx *c)
 {
     return guarded(c, [&]() -> int {
-        do_launch(c);
+        do_launch(c, c->overlap);
         return BHCB_OK;
     });
 }

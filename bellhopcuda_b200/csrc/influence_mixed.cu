@@ -7,6 +7,9 @@
 //
 // Work layout. Each warp takes 32 segments from a dynamic queue (heaviest
 // first). For each frequency of the segments' trace group:
+// Beside a running trace (blk_state set), a launch takes only the chunks the
+// tracer has published and exits when the rest are not ready; the host
+// relaunches it until the trace ends (no kernel waits for another).
 //   1. prep: lane k turns segment k into a SegFreqM block (window of receiver
 //      depths, frequency constants, float column / point constants, the
 //      accumulator row pointer) in shared memory;
@@ -247,22 +250,34 @@ template<bool GAUSS, bool COHERENT> __device__ __forceinline__ bool eval_one(
 template<bool GAUSS, bool COHERENT> __global__ void __launch_bounds__(32 * MW, 5)
 influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long long cap,
                        const GroupDev *__restrict__ groups, int ngroups, const double *__restrict__ freqs,
-                       float2 *__restrict__ acc, RunCounters *ctr)
+                       float2 *__restrict__ acc, RunCounters *ctr, unsigned int *blk_state,
+                       unsigned long long *scan)
 {
     // the trace kernel's slot counter may exceed the capacity on overflow
     const unsigned long long nseg = min(__ldcg(&ctr->nseg), cap);
+    unsigned long long *queue = scan ? scan : &ctr->chunk_counter;
     __shared__ SegFreqM s_p[MW][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned long long nchunks = (nseg + 31) / 32;
     unsigned int evals = 0;
     for(;;) {
         unsigned long long ch = 0;
-        if(lane == 0) ch = atomicAdd(&ctr->chunk_counter, 1ull);
+        if(lane == 0) ch = atomicAdd(queue, 1ull);
         ch = __shfl_sync(0xffffffffu, ch, 0);
         if(ch >= nchunks) break;
         // segments are stored in trace order, so the last chunks hold the
         // far-range segments with the widest beams: take the heaviest first
         ch = nchunks - 1 - ch;
+        if(blk_state) {
+            // running beside the trace: take a chunk (a 32-slot block of one
+            // ray) only once the tracer has published it; skipped blocks are
+            // taken by a later launch
+            unsigned int got = 0;
+            if(lane == 0) got = atomicCAS(&blk_state[ch], 1u, 2u);
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if(got != 1u) continue;
+            __threadfence();
+        }
         const unsigned long long k0 = ch * 32 + lane;
         const bool have = k0 < nseg;
         SegRec<float> my;
@@ -270,7 +285,7 @@ influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long lon
             const uint4 *src = reinterpret_cast<const uint4 *>(segs + k0);
             uint4 *dst = reinterpret_cast<uint4 *>(&my);
 #pragma unroll
-            for(int i = 0; i < (int)(sizeof(SegRec<float>) / 16); ++i) dst[i] = __ldcs(src + i);
+            for(int i = 0; i < (int)(sizeof(SegRec<float>) / 16); ++i) dst[i] = __ldcg(src + i);
         } else {
             my.job = -1;
         }
@@ -371,18 +386,23 @@ influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long lon
 
 cudaError_t launch_influence_mixed(const void *segs, unsigned long long cap, const GroupDev *groups, int ngroups,
                                    const double *freqs, float2 *acc, RunCounters *ctr, bool gauss,
-                                   bool coherent, int grid, cudaStream_t st)
+                                   bool coherent, int grid, cudaStream_t st, unsigned int *blk_state,
+                                   unsigned long long *scan)
 {
     const SegRec<float> *s = (const SegRec<float> *)segs;
     const int block = 32 * MW;
     if(gauss && coherent)
-        influence_kernel_mixed<true, true><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr);
+        influence_kernel_mixed<true, true><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr,
+                                                                   blk_state, scan);
     else if(gauss)
-        influence_kernel_mixed<true, false><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr);
+        influence_kernel_mixed<true, false><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr,
+                                                                    blk_state, scan);
     else if(coherent)
-        influence_kernel_mixed<false, true><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr);
+        influence_kernel_mixed<false, true><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr,
+                                                                    blk_state, scan);
     else
-        influence_kernel_mixed<false, false><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr);
+        influence_kernel_mixed<false, false><<<grid, block, 0, st>>>(s, cap, groups, ngroups, freqs, acc, ctr,
+                                                                     blk_state, scan);
     return cudaGetLastError();
 }
 

@@ -33,11 +33,22 @@ struct SlotCursor {
     unsigned long long next = 0, end = 0;   // [next, end) free slots of the current block
 };
 
+// Marks the block that ends at slot `end` as complete for the influence
+// kernels that run while the trace is still going: its records are made
+// visible device-wide before the flag.
+__device__ __forceinline__ void publish_block(unsigned int *blk_state, unsigned long long end)
+{
+    if(!blk_state || end == 0) return;
+    __threadfence();
+    atomicExch(&blk_state[end / SEG_BLOCK - 1], 1u);
+}
+
 template<typename R> __device__ __forceinline__ void emit_seg(
     const SegRec<R> &rec, SegRec<R> *segs, unsigned long long cap, RunCounters *ctr, SlotCursor &cur,
-    bool &overflow)
+    bool &overflow, unsigned int *blk_state)
 {
     if(cur.next == cur.end) {
+        publish_block(blk_state, cur.end);   // the previous block is full
         unsigned long long b = atomicAdd(&ctr->nseg, (unsigned long long)SEG_BLOCK);
         if(b + SEG_BLOCK > cap) {
             overflow = true;
@@ -54,15 +65,17 @@ template<typename R> __device__ __forceinline__ void emit_seg(
 }
 
 // mark the unused tail of the ray's last block as empty
-template<typename R> __device__ __forceinline__ void close_block(SegRec<R> *segs, SlotCursor &cur)
+template<typename R> __device__ __forceinline__ void close_block(SegRec<R> *segs, SlotCursor &cur,
+                                                                unsigned int *blk_state)
 {
     for(; cur.next < cur.end; ++cur.next) segs[cur.next].job = -1;
+    publish_block(blk_state, cur.end);
 }
 
 // R: ray state; RecR: segment record (float for the mixed kernel's FP32 influence).
 template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_kernel(
     const GroupDev *__restrict__ groups, int ngroups, long long njobs, SegRec<RecR> *segs,
-    unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter)
+    unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, unsigned int *blk_state)
 {
     for(;;) {
         long long job = (long long)atomicAdd(job_counter, 1ull);
@@ -166,11 +179,11 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
             }
             SegRec<RecR> rec;
             if(infl_prologue(p0, p1, inf, e, rcp_q0, ratio1, (int)job, is, rec))
-                emit_seg(rec, segs, cap, ctr, cur, overflow);
+                emit_seg(rec, segs, cap, ctr, cur, overflow, blk_state);
             ++is;
             if(two) {
                 if(infl_prologue(p1, p2, inf, e, rcp_q0, ratio1, (int)job, is, rec))
-                    emit_seg(rec, segs, cap, ctr, cur, overflow);
+                    emit_seg(rec, segs, cap, ctr, cur, overflow, blk_state);
                 p0 = p2;
                 ++is;
             } else {
@@ -193,7 +206,7 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
             dBegTop = dEndTop;
             dBegBot = dEndBot;
         }
-        close_block(segs, cur);
+        close_block(segs, cur, blk_state);
         atomicAdd(&ctr->nsteps, nsteps);
     }
 }
@@ -466,20 +479,21 @@ __global__ void scale_kernel(const float2 *__restrict__ acc, float2 *__restrict_
 // ---------------------------------------------------------------- launchers
 template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroups, long long njobs,
                                               void *segs, unsigned long long cap, RunCounters *ctr,
-                                              unsigned long long *job_counter, int grid, int block,
-                                              cudaStream_t st)
+                                              unsigned long long *job_counter, unsigned int *blk_state,
+                                              int grid, int block, cudaStream_t st)
 {
     // the ray state is FP64 in both precisions (the mixed precision writes FP32
     // segment records for its FP32 influence kernel): the trajectory, and with it
     // every step and reflection decision, is the FP64 one
     trace_kernel<double, R><<<grid, block, 0, st>>>(groups, ngroups, njobs, (SegRec<R> *)segs, cap, ctr,
-                                            job_counter);
+                                                    job_counter, blk_state);
     return cudaGetLastError();
 }
 
 cudaError_t launch_influence_mixed(const void *segs, unsigned long long cap, const GroupDev *groups, int ngroups,
                                    const double *freqs, float2 *acc, RunCounters *ctr, bool gauss,
-                                   bool coherent, int grid, cudaStream_t st);
+                                   bool coherent, int grid, cudaStream_t st, unsigned int *blk_state,
+                                   unsigned long long *scan);
 
 template<typename R> cudaError_t launch_influence(const void *segs, unsigned long long nseg,
                                                   const GroupDev *groups, int ngroups,
@@ -488,7 +502,8 @@ template<typename R> cudaError_t launch_influence(const void *segs, unsigned lon
                                                   int grid, cudaStream_t st)
 {
     if constexpr(sizeof(R) == 4) {
-        return launch_influence_mixed(segs, nseg, groups, ngroups, freqs, acc, ctr, gauss, coherent, grid, st);
+        return launch_influence_mixed(segs, nseg, groups, ngroups, freqs, acc, ctr, gauss, coherent, grid, st,
+                                      nullptr, nullptr);
     } else {
         const SegRec<R> *s = (const SegRec<R> *)segs;
         int block = 32 * WARPS_PER_CTA;
@@ -513,9 +528,11 @@ cudaError_t launch_scale(const float2 *acc, float2 *out, const GroupDev *groups,
 }
 
 template cudaError_t launch_trace<float>(const GroupDev *, int, long long, void *, unsigned long long,
-                                         RunCounters *, unsigned long long *, int, int, cudaStream_t);
+                                         RunCounters *, unsigned long long *, unsigned int *, int, int,
+                                         cudaStream_t);
 template cudaError_t launch_trace<double>(const GroupDev *, int, long long, void *, unsigned long long,
-                                          RunCounters *, unsigned long long *, int, int, cudaStream_t);
+                                          RunCounters *, unsigned long long *, unsigned int *, int, int,
+                                          cudaStream_t);
 template cudaError_t launch_influence<float>(const void *, unsigned long long, const GroupDev *, int,
                                              const double *, float2 *, RunCounters *, bool, bool, int,
                                              cudaStream_t);

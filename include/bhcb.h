@@ -37,13 +37,21 @@ enum {
 
 enum { BHCB_PREC_FP64 = 0, BHCB_PREC_MIXED = 1 };
 
+/* Mixed-precision TL runs overlap the influence with the trace: bhcb_run and
+   bhcb_launch relaunch influence kernels on a second stream for the segment
+   blocks the running trace has published, so bhcb_launch returns only once the
+   trace has ended (the final influence and scale kernels are still enqueued,
+   not waited for). This flag keeps the influence after the trace in stream
+   order, for callers that need bhcb_launch not to block (e.g. stream capture). */
+#define BHCB_FLAG_SERIAL_INFLUENCE 1
+
 /* Context options; mirrors bhcInit (include/bhc/structs.hpp:490-546). */
 typedef struct bhcb_init {
     int32_t gpu_index;        /* bhcInit::gpuIndex */
     int32_t precision;        /* BHCB_PREC_FP64 or BHCB_PREC_MIXED */
     uint64_t max_memory;      /* bhcInit::maxMemory (device bytes); 0 = 16 GiB */
     int32_t share_trajectory; /* frequencies share one trace when tables allow (mixed only) */
-    int32_t reserved;
+    int32_t flags;            /* BHCB_FLAG_* */
     void (*output_callback)(const char *message); /* bhcInit::outputCallback */
 } bhcb_init;
 
@@ -52,8 +60,9 @@ typedef struct bhcb_stats {
     uint64_t rays, steps, segments, evals;
     uint32_t err_bits, warn_bits;   /* reference ErrState bit numbering (src/util/errors.hpp:61-93) */
     int32_t groups, fields;         /* trace groups launched, TL fields produced */
-    double trace_ms, influence_ms, total_ms;
+    double trace_ms, influence_ms, total_ms;   /* influence_ms: influence time after the trace ended */
     uint64_t h2d_bytes;             /* table bytes uploaded by the last bhcb_prepare */
+    double influence_span_ms;       /* first influence launch to the last one's end (overlapped runs) */
 } bhcb_stats;
 
 /* Create a context; replaces the bhcInternal construction in bhc::setup
