@@ -375,7 +375,9 @@ def main():
         e2e = {"value": world * nf * len(e2e_times) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
         # ---- roofline of the dominant kernel
-        infl_ms = statistics.mean(s_["influence_ms"] for s_ in stats)
+        # the influence overlaps the trace: its time is the span from its first
+        # launch to the last one's end (includes the part hidden under the trace)
+        infl_ms = statistics.mean(s_["influence_span_ms"] for s_ in stats)
         trace_ms = statistics.mean(s_["trace_ms"] for s_ in stats)
         dom = "influence_kernel" if infl_ms >= trace_ms else "trace_kernel"
         if dom == "influence_kernel":
