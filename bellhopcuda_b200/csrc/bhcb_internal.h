@@ -15,7 +15,7 @@ namespace bhcb {
 
 // SSP interpolation types (reference: src/runtype.hpp:52-75)
 enum SspType : int32_t { SSP_N2LINEAR = 0, SSP_CLINEAR = 1, SSP_CUBIC = 2, SSP_PCHIP = 3,
-                         SSP_ANALYTIC = 4 };
+                         SSP_ANALYTIC = 4, SSP_HEXAHEDRAL = 5 };
 
 // error / warning bits: same numbering as the reference's ErrState
 // (src/util/errors.hpp:61-93); BHCB_ERR_SEG_OVERFLOW is this runtime's own.

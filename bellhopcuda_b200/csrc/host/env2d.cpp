@@ -31,6 +31,18 @@ template<typename T> void read_vector(LdiReader &f, int32_t &n, std::vector<T> &
     for(int i = 0; i < n; ++i) f.read(x[i]);
 }
 
+// SubTab (src/common_setup.hpp:306-334): FMA sub-tabulation
+template<typename T> void subtab(std::vector<T> &x, int n)
+{
+    const T m999 = (T)(sizeof(T) == 4 ? -999.9f : -999.9);
+    const T p01 = (T)(sizeof(T) == 4 ? 0.01f : 0.01);
+    if(n >= 3 && std::fabs(x[2] - m999) < p01) {
+        if(std::fabs(x[1] - m999) < p01) x[1] = x[0];
+        T dx = (x[1] - x[0]) / (T)(n - 1), x0 = x[0];
+        for(int i = 0; i < n; ++i) x[i] = std::fma((T)i, dx, x0);
+    }
+}
+
 void read_bdry_file(const std::string &path, BdryIn &b)
 {
     LdiReader f(path);
@@ -52,6 +64,61 @@ void read_bdry_file(const std::string &path, BdryIn &b)
             for(int k = 0; k < 5; ++k) f.read(b.geo[i][k]);
     }
     b.file = true;
+}
+
+// 3-D boundary grid (src/module/boundary.hpp:103-148): type, Nx + x (km), Ny +
+// y (km), then one record of Nx depths per y
+void read_bdry3_file(const std::string &path, Bdry3In &b)
+{
+    LdiReader f(path);
+    if(!f.good()) env_error("unable to open boundary file " + path);
+    f.record();
+    f.read_chars(b.type, 2);
+    int32_t nx = 0, ny = 0;
+    read_vector(f, nx, b.x_km);
+    subtab(b.x_km, nx);
+    b.x_km.resize(nx);
+    read_vector(f, ny, b.y_km);
+    subtab(b.y_km, ny);
+    b.y_km.resize(ny);
+    if(nx < 2 || ny < 2) env_error("boundary file " + path + ": need at least 2 x 2 points");
+    b.z.assign((size_t)nx * ny, 0.0);
+    for(int iy = 0; iy < ny; ++iy) {
+        f.record();
+        for(int ix = 0; ix < nx; ++ix) f.read(b.z[(size_t)ix * ny + iy]);
+    }
+    if(b.type[1] == 'L') env_error("3-D bottom provinces ('L') are not supported by this build");
+    b.file = true;
+}
+
+// hexahedral SSP file (src/module/ssp.hpp:144-186): Nx + x (km), Ny + y (km),
+// Nz + z (m), then for each z and y one record of Nx sound speeds
+void read_hex_ssp(const std::string &path, EnvInput &in)
+{
+    LdiReader f(path);
+    if(!f.good()) env_error("unable to open hexahedral SSP file " + path);
+    int32_t nx = 0, ny = 0, nz = 0;
+    f.record(); f.read(nx);
+    if(nx < 2) env_error("hexahedral SSP: need at least two points in x, y, z");
+    in.hex_x_km.assign(nx, 0.0);
+    f.record();
+    for(int i = 0; i < nx; ++i) f.read(in.hex_x_km[i]);
+    f.record(); f.read(ny);
+    if(ny < 2) env_error("hexahedral SSP: need at least two points in x, y, z");
+    in.hex_y_km.assign(ny, 0.0);
+    f.record();
+    for(int i = 0; i < ny; ++i) f.read(in.hex_y_km[i]);
+    f.record(); f.read(nz);
+    if(nz < 2) env_error("hexahedral SSP: need at least two points in x, y, z");
+    in.hex_z.assign(nz, 0.0);
+    f.record();
+    for(int i = 0; i < nz; ++i) f.read(in.hex_z[i]);
+    in.hex_c.assign((size_t)nx * ny * nz, 0.0);
+    for(int iz = 0; iz < nz; ++iz)
+        for(int iy = 0; iy < ny; ++iy) {
+            f.record();
+            for(int ix = 0; ix < nx; ++ix) f.read(in.hex_c[((size_t)ix * ny + iy) * nz + iz]);
+        }
 }
 
 // ------------------------------------------------------------- preprocessing
@@ -245,18 +312,6 @@ void pchip(const double *x, const cpxd *y, int n, cpxd *p1, cpxd *p2, cpxd *p3, 
     }
 }
 
-// SubTab (src/common_setup.hpp:306-334): FMA sub-tabulation
-template<typename T> void subtab(std::vector<T> &x, int n)
-{
-    const T m999 = (T)(sizeof(T) == 4 ? -999.9f : -999.9);
-    const T p01 = (T)(sizeof(T) == 4 ? 0.01f : 0.01);
-    if(n >= 3 && std::fabs(x[2] - m999) < p01) {
-        if(std::fabs(x[1] - m999) < p01) x[1] = x[0];
-        T dx = (x[1] - x[0]) / (T)(n - 1), x0 = x[0];
-        for(int i = 0; i < n; ++i) x[i] = std::fma((T)i, dx, x0);
-    }
-}
-
 HsDev make_hs(const EnvInput &in, double freq, double fT, const HsIn &h)
 {
     HsDev d{};
@@ -374,11 +429,12 @@ std::vector<BdryPtDev> build_bdry(const EnvInput &in, double freq, const BdryIn 
 } // namespace
 
 // ---------------------------------------------------------------- read_env
-EnvInput read_env_files(const std::string &root)
+EnvInput read_env_files(const std::string &root, bool o3d)
 {
     EnvInput in;
     LdiReader f(root + ".env");
     if(!f.good()) env_error("unable to open environment file " + root + ".env");
+    in.o3d = o3d;
     f.record(); f.read(in.title);                               // Title
     f.record(); f.read(in.freq0);                               // Freq0
     int32_t nmedia = 1;
@@ -430,6 +486,10 @@ EnvInput read_env_files(const std::string &root)
         } else {
             in.ssp_z = {0.0, in.bot_depth};
         }
+        if(st == 'H') {
+            if(!o3d) env_error("hexahedral SSP ('H') needs a 3-D run");
+            read_hex_ssp(root + ".ssp", in);
+        }
     }
     f.record(); f.read_chars(in.bot_opt, 6);                    // BotOpt
     double bsigma = 0;
@@ -443,9 +503,14 @@ EnvInput read_env_files(const std::string &root)
     } else if(in.bot.bc == 'G') {
         f.record(); f.read(in.bot.zTemp); f.read(in.bot.Mz);
     }
+    if(o3d) {                                                   // SxSy
+        read_vector(f, in.nsx, in.sx_km);
+        read_vector(f, in.nsy, in.sy_km);
+    }
     read_vector(f, in.nsz, in.sz);                              // SzRz
     read_vector(f, in.nrz, in.rz);
     read_vector(f, in.nrr, in.rr_km);                           // RcvrRanges
+    if(o3d) read_vector(f, in.ntheta, in.theta_deg);            // RcvrBearings
     f.record(); f.read_chars(in.run_type, 7);                   // RunType
     {                                                           // RayAnglesElevation
         f.record();
@@ -458,12 +523,32 @@ EnvInput read_env_files(const std::string &root)
         int nread = n == 0 ? 2 : n;
         for(int i = 0; i < nread; ++i) f.read(in.alpha_deg[i]);
     }
+    if(o3d) {                                                   // RayAnglesBearing
+        f.record();
+        f.read(in.nbeta);
+        if(in.top_opt[5] == 'I') f.read(in.isingle_beta);
+        int n = in.nbeta;
+        if(n <= 0) env_error("number of beams in bearing must be positive");
+        in.beta_deg.assign(std::max(3, n), 0.0);
+        if(n > 2) in.beta_deg[2] = FLT(-999.9);
+        f.record();
+        for(int i = 0; i < n; ++i) f.read(in.beta_deg[i]);
+    }
     f.record();                                                 // BeamInfo
-    f.read(in.deltas); f.read(in.box_z); f.read(in.box_r_km);
+    if(o3d) {
+        f.read(in.deltas); f.read(in.box_x_km); f.read(in.box_y_km); f.read(in.box_z);
+    } else {
+        f.read(in.deltas); f.read(in.box_z); f.read(in.box_r_km);
+    }
     if(in.run_type[1] == 'C' || in.run_type[1] == 'R')
         env_error("Cerveny beams are not supported by this build");
-    if(in.top_opt[4] == '~' || in.top_opt[4] == '*') read_bdry_file(root + ".ati", in.ati);
-    if(in.bot_opt[1] == '~' || in.bot_opt[1] == '*') read_bdry_file(root + ".bty", in.bty);
+    if(o3d) {
+        if(in.top_opt[4] == '~' || in.top_opt[4] == '*') read_bdry3_file(root + ".ati", in.ati3);
+        if(in.bot_opt[1] == '~' || in.bot_opt[1] == '*') read_bdry3_file(root + ".bty", in.bty3);
+    } else {
+        if(in.top_opt[4] == '~' || in.top_opt[4] == '*') read_bdry_file(root + ".ati", in.ati);
+        if(in.bot_opt[1] == '~' || in.bot_opt[1] == '*') read_bdry_file(root + ".bty", in.bty);
+    }
     if(in.run_type[2] == '*') {                                 // SBP
         LdiReader s(root + ".sbp");
         if(!s.good()) env_error("unable to open source beam pattern file");
@@ -475,49 +560,13 @@ EnvInput read_env_files(const std::string &root)
     return in;
 }
 
-// -------------------------------------------------------------- preprocess
-EnvTables preprocess(const EnvInput &in, double freq)
+// 1-D SSP tables (src/module/ssp.hpp:453-545, src/curves.hpp:76-372), shared
+// by the 2-D and 3-D preprocessing
+struct Ssp1d {
+    std::vector<double> z, rho, c, cz, n2, n2z, coef;
+};
+void build_ssp1d(const EnvInput &in, double freq, double fT, char st, Ssp1d &t)
 {
-    EnvTables t;
-    t.freq0 = freq;
-    std::memcpy(t.run_type, in.run_type, 7);
-    // RunType validation / normalisation (src/module/runtype.hpp:53-78)
-    switch(t.run_type[0]) {
-    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'V': case 'v': break;
-    case 'R': env_error("ray-trace runs ('R') are not a field mode");
-    default: env_error("unknown RunType");
-    }
-    switch(t.run_type[1]) {
-    case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
-    default: t.run_type[1] = 'G';
-    }
-    if(t.run_type[3] != 'X') t.run_type[3] = 'R';
-    if(t.run_type[4] != 'I') t.run_type[4] = 'R';
-    if(t.run_type[5] != ' ' && t.run_type[5] != '2') env_error("3-D environment given to the 2-D reader");
-    std::memcpy(t.beam_type, "G S ", 4);                       // MoveBeamType (module/beaminfo.hpp:240-244)
-    t.beam_type[0] = t.run_type[1];
-    t.beam_type[3] = t.run_type[6];
-    char bt = t.beam_type[0];
-    if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
-        env_error(std::string("beam type '") + bt + "' is not supported by this build");
-    if(t.beam_type[3] == 'S') env_error("beam shift ('S') is not supported by this build");
-
-    char st = in.top_opt[0];
-    switch(st) {
-    case 'N': t.ssp_type = SSP_N2LINEAR; break;
-    case 'C': t.ssp_type = SSP_CLINEAR; break;
-    case 'S': t.ssp_type = SSP_CUBIC; break;
-    case 'P': t.ssp_type = SSP_PCHIP; break;
-    case 'A': t.ssp_type = SSP_ANALYTIC; break;
-    case 'Q': env_error("quad SSP ('Q') is not supported by this build");
-    default: env_error("unknown SSP type");
-    }
-    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G')
-        env_error("top boundary condition not supported by this build");
-    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G')
-        env_error("bottom boundary condition not supported by this build");
-    // fT: 1000 once an 'A' bottom halfspace has been read (module/boundarycond.hpp:37-58)
-    double fT = in.bot.bc == 'A' ? FLT(1000.0) : 1.0e20;
     int n = (int)in.ssp_z.size();
     if(n < 2) env_error("the SSP must have at least 2 points");
     for(int i = 1; i < n; ++i)
@@ -563,6 +612,55 @@ EnvTables preprocess(const EnvInput &in, double freq)
                 }
         }
     }
+}
+
+// -------------------------------------------------------------- preprocess
+EnvTables preprocess(const EnvInput &in, double freq)
+{
+    EnvTables t;
+    t.freq0 = freq;
+    std::memcpy(t.run_type, in.run_type, 7);
+    // RunType validation / normalisation (src/module/runtype.hpp:53-78)
+    switch(t.run_type[0]) {
+    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'V': case 'v': break;
+    case 'R': env_error("ray-trace runs ('R') are not a field mode");
+    default: env_error("unknown RunType");
+    }
+    switch(t.run_type[1]) {
+    case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
+    default: t.run_type[1] = 'G';
+    }
+    if(t.run_type[3] != 'X') t.run_type[3] = 'R';
+    if(t.run_type[4] != 'I') t.run_type[4] = 'R';
+    if(t.run_type[5] != ' ' && t.run_type[5] != '2') env_error("3-D environment given to the 2-D reader");
+    std::memcpy(t.beam_type, "G S ", 4);                       // MoveBeamType (module/beaminfo.hpp:240-244)
+    t.beam_type[0] = t.run_type[1];
+    t.beam_type[3] = t.run_type[6];
+    char bt = t.beam_type[0];
+    if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
+        env_error(std::string("beam type '") + bt + "' is not supported by this build");
+    if(t.beam_type[3] == 'S') env_error("beam shift ('S') is not supported by this build");
+
+    char st = in.top_opt[0];
+    switch(st) {
+    case 'N': t.ssp_type = SSP_N2LINEAR; break;
+    case 'C': t.ssp_type = SSP_CLINEAR; break;
+    case 'S': t.ssp_type = SSP_CUBIC; break;
+    case 'P': t.ssp_type = SSP_PCHIP; break;
+    case 'A': t.ssp_type = SSP_ANALYTIC; break;
+    case 'Q': env_error("quad SSP ('Q') is not supported by this build");
+    default: env_error("unknown SSP type");
+    }
+    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G')
+        env_error("top boundary condition not supported by this build");
+    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G')
+        env_error("bottom boundary condition not supported by this build");
+    // fT: 1000 once an 'A' bottom halfspace has been read (module/boundarycond.hpp:37-58)
+    double fT = in.bot.bc == 'A' ? FLT(1000.0) : 1.0e20;
+    Ssp1d sp;
+    build_ssp1d(in, freq, fT, st, sp);
+    t.z = sp.z; t.rho = sp.rho; t.c = sp.c; t.cz = sp.cz; t.n2 = sp.n2; t.n2z = sp.n2z; t.coef = sp.coef;
+    const int n = (int)in.ssp_z.size();
     double top_depth = in.ssp_z[0], bot_depth = in.bot_depth;
     if(std::fabs(in.ssp_z[n - 1] - bot_depth) >= FLT(100.0) * FLT_EPSILON)
         t.warnings.push_back("Ocean bottom must be at last SSP depth");
@@ -687,6 +785,212 @@ bool EnvTables::same_trajectory_tables(const EnvTables &o) const
     return vclose(c, o.c) && vclose(cz, o.cz) && vclose(n2, o.n2) && vclose(n2z, o.n2z)
         && vclose(coef, o.coef) && hclose(top, o.top) && hclose(bot, o.bot) && bclose(btop, o.btop)
         && bclose(bbot, o.bbot) && alpha == o.alpha && run_type[0] != 'S';
+}
+
+
+// ------------------------------------------------------------ 3-D preprocess
+namespace {
+
+// grid boundary with the two triangle normals of each cell
+// (src/module/boundary.hpp:56-78 default, 499-523 units, 600-645 normals)
+std::vector<Bdry3Pt> build_bdry3(const Bdry3In &b, bool istop, double depth, int32_t &nx, int32_t &ny)
+{
+    std::vector<Bdry3Pt> bd;
+    const double negtop = istop ? -1.0 : 1.0;
+    if(!b.file) {
+        const double big = 1.0e25;   // BDRYBIG in 3-D (src/boundary.hpp:26-34)
+        nx = ny = 2;
+        bd.resize(4);
+        const double xs[4][2] = {{-big, -big}, {-big, big}, {big, -big}, {big, big}};
+        for(int i = 0; i < 4; ++i) {
+            bd[i].x[0] = xs[i][0]; bd[i].x[1] = xs[i][1]; bd[i].x[2] = depth;
+            bd[i].n1[0] = bd[i].n1[1] = 0.0; bd[i].n1[2] = negtop;
+            bd[i].n2[0] = bd[i].n2[1] = 0.0; bd[i].n2[2] = negtop;
+        }
+        return bd;
+    }
+    nx = (int32_t)b.x_km.size();
+    ny = (int32_t)b.y_km.size();
+    for(int i = 1; i < nx; ++i)
+        if(!(b.x_km[i] > b.x_km[i - 1])) env_error("boundary x-coordinates are not monotonically increasing");
+    for(int i = 1; i < ny; ++i)
+        if(!(b.y_km[i] > b.y_km[i - 1])) env_error("boundary y-coordinates are not monotonically increasing");
+    if(b.type[0] != 'R') env_error("3-D boundary type must be 'R' (rectangular grid)");
+    bd.resize((size_t)nx * ny);
+    for(int ix = 0; ix < nx; ++ix)
+        for(int iy = 0; iy < ny; ++iy) {
+            Bdry3Pt &p = bd[(size_t)ix * ny + iy];
+            p.x[0] = b.x_km[ix] * 1000.0;
+            p.x[1] = b.y_km[iy] * 1000.0;
+            p.x[2] = b.z[(size_t)ix * ny + iy];
+            for(int k = 0; k < 3; ++k) p.n1[k] = p.n2[k] = NAN;
+        }
+    auto sub = [](const double *a, const double *c, double *o) { for(int k = 0; k < 3; ++k) o[k] = a[k] - c[k]; };
+    auto cross = [](const double *u, const double *v, double *o) {
+        o[0] = u[1] * v[2] - u[2] * v[1];
+        o[1] = u[2] * v[0] - u[0] * v[2];
+        o[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    for(int ix = 0; ix < nx - 1; ++ix)
+        for(int iy = 0; iy < ny - 1; ++iy) {
+            const double *p1 = bd[(size_t)ix * ny + iy].x, *p2 = bd[(size_t)(ix + 1) * ny + iy].x;
+            const double *p3 = bd[(size_t)(ix + 1) * ny + iy + 1].x, *p4 = bd[(size_t)ix * ny + iy + 1].x;
+            double u[3], v[3], n[3];
+            Bdry3Pt &q = bd[(size_t)ix * ny + iy];
+            sub(p2, p1, u); sub(p3, p1, v); cross(u, v, n);          // triangle 1
+            if(istop) for(int k = 0; k < 3; ++k) n[k] = -n[k];
+            double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            for(int k = 0; k < 3; ++k) q.n1[k] = n[k] / l;
+            sub(p3, p1, u); sub(p4, p1, v); cross(u, v, n);          // triangle 2
+            if(istop) for(int k = 0; k < 3; ++k) n[k] = -n[k];
+            l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            for(int k = 0; k < 3; ++k) q.n2[k] = n[k] / l;
+        }
+    return bd;
+}
+
+// ReadVector's SubTab + Sort (src/common_setup.hpp:368-381)
+template<typename T> std::vector<T> tab_sort(std::vector<T> v, int n)
+{
+    subtab(v, n);
+    v.resize(n);
+    std::sort(v.begin(), v.end());
+    return v;
+}
+
+// CheckFix360Sweep (src/common_setup.hpp:258-270)
+template<typename T> void fix360(std::vector<T> &a)
+{
+    int n = (int)a.size();
+    if(n > 1 && std::fabs(std::fmod((double)(a[n - 1] - a[0]), FLT(360.0)))
+                    < FLT(10.0) * std::fabs(std::nextafter(360.0, 0.0) - 360.0))
+        a.resize(n - 1);
+}
+
+} // namespace
+
+Env3Tables preprocess3d(const EnvInput &in, double freq)
+{
+    if(!in.o3d) env_error("the environment was not read as a 3-D run");
+    Env3Tables t;
+    t.freq0 = freq;
+    std::memcpy(t.run_type, in.run_type, 7);
+    switch(t.run_type[0]) {   // src/module/runtype.hpp:53-78
+    case 'C': case 'S': case 'I': break;
+    case 'A': case 'a': case 'E': env_error("3-D arrivals / eigenray runs are not supported by this build");
+    case 'R': env_error("ray-trace runs ('R') are not a field mode");
+    default: env_error("unknown RunType");
+    }
+    if(t.run_type[5] != '3') env_error("3-D runs need RunType(6) = '3'");
+    switch(t.run_type[1]) {
+    case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
+    default: t.run_type[1] = 'G';
+    }
+    if(t.run_type[3] != 'X') t.run_type[3] = 'R';
+    if(t.run_type[4] != 'I') t.run_type[4] = 'R';
+    if(t.run_type[4] == 'I') env_error("irregular receiver grids are 2-D only");
+    std::memcpy(t.beam_type, "G S ", 4);
+    t.beam_type[0] = t.run_type[1];
+    t.beam_type[3] = t.run_type[6];
+    char bt = t.beam_type[0];
+    if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
+        env_error(std::string("3-D beam type '") + bt + "' is not supported by this build (Cartesian 'G' / 'B')");
+    if(t.run_type[3] == 'X') env_error("line sources are 2-D only");
+
+    char st = in.top_opt[0];
+    double fT = in.bot.bc == 'A' ? FLT(1000.0) : 1.0e20;
+    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G')
+        env_error("top boundary condition not supported by this build");
+    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G')
+        env_error("bottom boundary condition not supported by this build");
+    double top_depth = in.ssp_z[0], bot_depth = in.bot_depth;
+    if(st == 'H') {
+        t.ssp_type = SSP_HEXAHEDRAL;
+        const int nx = (int)in.hex_x_km.size(), ny = (int)in.hex_y_km.size(), nz = (int)in.hex_z.size();
+        for(int i = 1; i < nx; ++i) if(!(in.hex_x_km[i] > in.hex_x_km[i - 1])) env_error("hexahedral SSP x not monotone");
+        for(int i = 1; i < ny; ++i) if(!(in.hex_y_km[i] > in.hex_y_km[i - 1])) env_error("hexahedral SSP y not monotone");
+        for(int i = 1; i < nz; ++i) if(!(in.hex_z[i] > in.hex_z[i - 1])) env_error("hexahedral SSP z not monotone");
+        for(double v : in.hex_x_km) t.hx.push_back(v * 1000.0);
+        for(double v : in.hex_y_km) t.hy.push_back(v * 1000.0);
+        t.hz = in.hex_z;
+        t.hc = in.hex_c;
+        t.hcz.assign((size_t)nx * ny * (nz - 1), 0.0);
+        for(int ix = 0; ix < nx; ++ix)
+            for(int iy = 0; iy < ny; ++iy)
+                for(int iz = 1; iz < nz; ++iz)
+                    t.hcz[((size_t)ix * ny + iy) * (nz - 1) + iz - 1]
+                        = (t.hc[((size_t)ix * ny + iy) * nz + iz] - t.hc[((size_t)ix * ny + iy) * nz + iz - 1])
+                          / (t.hz[iz] - t.hz[iz - 1]);
+        // SegZToZ (src/module/ssp.hpp:561-585): depths become the grid depths;
+        // the density keeps the .env values, undefined past their count
+        t.z = t.hz;
+        t.rho.assign(nz, NAN);
+        for(int i = 0; i < nz && i < (int)in.ssp_z.size(); ++i) t.rho[i] = in.rho.empty() ? 1.0 : in.rho[i];
+    } else {
+        switch(st) {
+        case 'N': t.ssp_type = SSP_N2LINEAR; break;
+        case 'C': t.ssp_type = SSP_CLINEAR; break;
+        case 'S': t.ssp_type = SSP_CUBIC; break;
+        case 'P': t.ssp_type = SSP_PCHIP; break;
+        case 'A': env_error("analytic SSP is not supported in 3-D by this build");
+        default: env_error("unknown SSP type");
+        }
+        Ssp1d sp;
+        build_ssp1d(in, freq, fT, st, sp);
+        t.z = sp.z; t.rho = sp.rho; t.c = sp.c; t.cz = sp.cz; t.n2 = sp.n2; t.n2z = sp.n2z; t.coef = sp.coef;
+    }
+    t.top = make_hs(in, freq, fT, in.top);
+    t.bot = make_hs(in, freq, fT, in.bot);
+    t.btop = build_bdry3(in.ati3, true, top_depth, t.top_nx, t.top_ny);
+    t.bbot = build_bdry3(in.bty3, false, bot_depth, t.bot_nx, t.bot_ny);
+
+    // sources, receivers, bearings (module/sxsy.hpp, szrz.hpp, rcvrranges.hpp, rcvrbearings.hpp)
+    for(double v : tab_sort(in.sx_km, in.nsx)) t.sx.push_back(v * 1000.0);
+    for(double v : tab_sort(in.sy_km, in.nsy)) t.sy.push_back(v * 1000.0);
+    t.sz = tab_sort(in.sz, in.nsz);
+    t.rz = tab_sort(in.rz, in.nrz);
+    for(auto &v : t.sz) { if(v < top_depth) v = (float)top_depth; if(v > bot_depth) v = (float)bot_depth; }
+    for(auto &v : t.rz) { if(v < top_depth) v = (float)top_depth; if(v > bot_depth) v = (float)bot_depth; }
+    for(double v : tab_sort(in.rr_km, in.nrr)) t.rr.push_back(v * 1000.0);
+    for(size_t i = 1; i < t.rr.size(); ++i)
+        if(!(t.rr[i] > t.rr[i - 1])) env_error("receiver ranges are not monotonically increasing");
+    t.theta = tab_sort(in.theta_deg, in.ntheta);
+    fix360(t.theta);
+
+    // angles (module/rayangles.hpp): elevation and bearing fans
+    if(in.nalpha <= 0) env_error("3-D runs need an explicit number of elevation beams");
+    std::vector<double> al = tab_sort(in.alpha_deg, in.nalpha);
+    fix360(al);
+    std::vector<double> be = tab_sort(in.beta_deg, in.nbeta);
+    fix360(be);
+    for(size_t i = 1; i < al.size(); ++i) if(!(al[i] > al[i - 1])) env_error("elevation angles are not monotonically increasing");
+    for(size_t i = 1; i < be.size(); ++i) if(!(be[i] > be[i - 1])) env_error("bearing angles are not monotonically increasing");
+    for(auto &v : al) v *= kPi / 180.0;
+    for(auto &v : be) v *= kPi / 180.0;
+    t.alpha = al;
+    t.beta = be;
+    t.dalpha = al.size() != 1 ? (al.back() - al.front()) / (double)(al.size() - 1) : FLT(0.0);
+    t.dbeta = be.size() != 1 ? (be.back() - be.front()) / (double)(be.size() - 1) : FLT(0.0);
+    t.isingle_alpha = in.top_opt[5] == 'I' ? in.isingle : 0;
+    t.isingle_beta = in.top_opt[5] == 'I' ? in.isingle_beta : 0;
+
+    // beam box and step (module/beaminfo.hpp:221-237)
+    t.box_x = in.box_x_km * FLT(1000.0);
+    t.box_y = in.box_y_km * FLT(1000.0);
+    t.box_z = in.box_z;
+    if(t.box_x <= 0.0 || t.box_y <= 0.0 || t.box_z <= 0.0) env_error("beam box not set up correctly");
+    t.deltas = in.deltas;
+    if(std::fabs(t.deltas) < DBL_EPSILON) t.deltas = (bot_depth - top_depth) / FLT(10.0);
+
+    if(!in.sbp.empty()) {
+        for(const auto &p : in.sbp) {
+            t.sbp.push_back(p[0]);
+            t.sbp.push_back(std::pow(FLT(10.0), p[1] / FLT(20.0)));
+        }
+    } else {
+        t.sbp = {FLT(-180.0), 1.0, FLT(180.0), 1.0};
+    }
+    return t;
 }
 
 } // namespace bhcb

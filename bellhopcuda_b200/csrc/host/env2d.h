@@ -31,7 +31,16 @@ struct BdryIn {
     std::vector<std::array<double, 5>> geo;   // long format: alphaR betaR rho alphaI betaI
 };
 
+// 3-D boundary grid ('R' .ati/.bty, src/module/boundary.hpp:107-148): depths
+// z[ix * ny + iy] at x[ix] (km), y[iy] (km)
+struct Bdry3In {
+    bool file = false;
+    char type[2] = {'R', ' '};
+    std::vector<double> x_km, y_km, z;
+};
+
 struct EnvInput {
+    bool o3d = false;                          // read with the 3-D module list
     std::string title;
     double freq0 = 50.0;
     char top_opt[6] = {'C', 'V', 'W', ' ', ' ', ' '};
@@ -48,6 +57,13 @@ struct EnvInput {
     std::vector<double> rr_km, alpha_deg;
     char run_type[7] = {'C', 'G', ' ', 'R', 'R', ' ', ' '};
     double deltas = 0, box_z = 0, box_r_km = 0;
+    // 3-D only (src/module/sxsy.hpp, rcvrbearings.hpp, rayangles.hpp, beaminfo.hpp)
+    int32_t nsx = 1, nsy = 1, ntheta = 1, nbeta = 1, isingle_beta = 0;
+    std::vector<double> sx_km, sy_km, theta_deg, beta_deg;
+    double box_x_km = 0, box_y_km = 0;
+    Bdry3In ati3, bty3;
+    // hexahedral SSP (.ssp file, src/module/ssp.hpp:144-190): c[(ix * ny + iy) * nz + iz]
+    std::vector<double> hex_x_km, hex_y_km, hex_z, hex_c;
 };
 
 struct EnvTables {
@@ -68,7 +84,29 @@ struct EnvTables {
     bool same_trajectory_tables(const EnvTables &o) const;
 };
 
-EnvInput read_env_files(const std::string &fileroot);
+// 3-D tables (BELLHOP3D field modes)
+struct Bdry3Pt {                 // grid node (x, y, z) and the normals of its cell's two triangles
+    double x[3], n1[3], n2[3];
+};
+struct Env3Tables {
+    double freq0 = 0;
+    int32_t ssp_type = SSP_CLINEAR;          // SSP_HEXAHEDRAL or a 1-D type
+    std::vector<double> z, rho, c, cz, n2, n2z, coef;   // 1-D tables (complex interleaved), as in 2-D
+    std::vector<double> hx, hy, hz, hc, hcz;             // hexahedral grid (m) and c, dc/dz
+    HsDev top{}, bot{};
+    int32_t top_nx = 2, top_ny = 2, bot_nx = 2, bot_ny = 2;
+    std::vector<Bdry3Pt> btop, bbot;
+    std::vector<double> sx, sy, rr, theta, alpha, beta, sbp;   // m, m, m, deg, rad, rad
+    std::vector<float> sz, rz;
+    double dalpha = 0, dbeta = 0, deltas = 0, box_x = 0, box_y = 0, box_z = 0;
+    int32_t isingle_alpha = 0, isingle_beta = 0;
+    char run_type[7];
+    char beam_type[4];
+    std::vector<std::string> warnings;
+};
+
+EnvInput read_env_files(const std::string &fileroot, bool o3d = false);
 EnvTables preprocess(const EnvInput &in, double freq);
+Env3Tables preprocess3d(const EnvInput &in, double freq);
 
 } // namespace bhcb
