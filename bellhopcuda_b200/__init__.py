@@ -103,6 +103,13 @@ SIGNATURES = [
                                      C.c_size_t]),
     ("bhcb_eigen_hits", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
                                   C.POINTER(C.c_int64)]),
+    ("bhcb_check_env3d", C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.c_char_p,
+                                   C.c_size_t]),
+    ("bhcb_setup3d", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("bhcb_add_env3d", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]),
+    ("bhcb_field_shape3d", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    ("bhcb_grid3d", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p]),
     ("bhcb_version", C.c_char_p, []),
 ]
 
@@ -144,6 +151,18 @@ def check_env(file_root: str) -> dict:
     return dict(nsz=info.nsz, nrz=info.nrz, nrz_per_range=info.nrz_per_range, nrr=info.nrr,
                 nalpha=info.nalpha, ssp_type=info.ssp_type, freq=info.freq, deltas=info.deltas,
                 run_type=info.run_type.decode(), beam_type=info.beam_type.decode())
+
+
+def check_env3d(file_root: str) -> dict:
+    """Validate a 3-D environment on the host (no GPU): field dims and ray count."""
+    lib = load_library()
+    dims = (C.c_int32 * 6)()
+    nrays = C.c_int64()
+    msg = C.create_string_buffer(512)
+    rc = lib.bhcb_check_env3d(file_root.encode(), dims, C.byref(nrays), msg, len(msg))
+    if rc != 0:
+        raise BhcbError(rc, msg.value.decode(errors="replace"))
+    return {"dims": tuple(int(d) for d in dims), "nrays": nrays.value}
 
 
 class Tracer:
@@ -244,6 +263,40 @@ class Tracer:
         self._check(self._lib.bhcb_receivers(self._h, env, rr.ctypes.data_as(C.POINTER(C.c_double)),
                                              nrr, rz.ctypes.data_as(C.POINTER(C.c_float)), rz.size))
         return rr, rz
+
+    # -- 3-D (BELLHOP3D field modes)
+    def setup3d(self, file_root: str):
+        """bhc::setup<true, true>: FileRoot.env read as a 3-D run."""
+        self._check(self._lib.bhcb_setup3d(self._h, file_root.encode()))
+        return self
+
+    def add_env3d(self, file_root: str) -> int:
+        idx = C.c_int32()
+        self._check(self._lib.bhcb_add_env3d(self._h, file_root.encode(), C.byref(idx)))
+        return idx.value
+
+    def field_shape3d(self, env: int = 0):
+        """(NSz, NSx, NSy, Ntheta, NRz, NRr) of a 3-D environment's field."""
+        dims = (C.c_int32 * 6)()
+        self._check(self._lib.bhcb_field_shape3d(self._h, env, dims))
+        return tuple(int(d) for d in dims)
+
+    def field3d(self, env: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """3-D pressure field, shape (NSz, NSx, NSy, Ntheta, NRz, NRr), complex64."""
+        shape = self.field_shape3d(env)
+        if out is None:
+            out = np.empty(shape, np.complex64)
+        self._check(self._lib.bhcb_copy_field(self._h, env, 0, out.ctypes.data, out.nbytes))
+        return out
+
+    def grid3d(self, env: int = 0) -> dict:
+        """Source / receiver coordinates of a 3-D environment (m, m, m, m, m, deg)."""
+        nsz, nsx, nsy, nth, nrz, nrr = self.field_shape3d(env)
+        g = {"sx": np.zeros(nsx), "sy": np.zeros(nsy), "sz": np.zeros(nsz, np.float32),
+             "rr": np.zeros(nrr), "rz": np.zeros(nrz, np.float32), "theta": np.zeros(nth)}
+        self._check(self._lib.bhcb_grid3d(self._h, env, *[g[k].ctypes.data for k in
+                                                            ("sx", "sy", "sz", "rr", "rz", "theta")]))
+        return g
 
     def writeout(self, file_root: str, env: int = 0, ifreq: int = 0):
         self._check(self._lib.bhcb_writeout(self._h, env, ifreq, file_root.encode()))

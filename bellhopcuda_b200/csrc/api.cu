@@ -17,6 +17,8 @@
 #include "../../include/bhcb.h"
 #include "bhcb_internal.h"
 #include "host/env2d.h"
+#include "host/rt.h"
+#include "host/run3d.h"
 #include "noalloc.h"
 
 namespace bhcb {
@@ -48,41 +50,6 @@ cudaError_t launch_eigen_emit(const uint32_t *, const ArrCand *, unsigned long l
 using namespace bhcb;
 
 namespace {
-
-struct CudaError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct StateError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct MemError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-
-#define CK(x)                                                                           \
-    do {                                                                                \
-        cudaError_t e_ = (x);                                                           \
-        if(e_ != cudaSuccess)                                                           \
-            throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));           \
-    } while(0)
-
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    void ensure(size_t n)
-    {
-        if(n <= bytes) return;
-        release();
-        CK(cudaMalloc(&p, n));
-        bytes = n;
-    }
-    void release()
-    {
-        if(p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-};
 
 struct EnvSlot {
     std::string root;
@@ -168,6 +135,11 @@ struct bhcb_ctx {
     std::string last_error;
     uint32_t err_bits = 0, warn_bits = 0;
 
+    // 3-D environments (a context holds either 2-D or 3-D environments)
+    Run3 *r3 = nullptr;
+    int r3_status = BHCB_OK;
+    bool is3d() const { return r3 && run3_count(r3) > 0; }
+
     void msg(const std::string &s) const
     {
         if(output_cb) output_cb(s.c_str());
@@ -200,23 +172,6 @@ template<typename F> int guarded(bhcb_ctx *c, F &&fn)
     } catch(const std::exception &e) {
         return fail(c, BHCB_ERR_INPUT, e.what());
     }
-}
-
-// ------------------------------------------------------------------ arena
-struct Arena {
-    std::vector<uint8_t> bytes;
-    template<typename T> size_t put(const std::vector<T> &v)
-    {
-        size_t off = (bytes.size() + 255) & ~size_t(255);
-        bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 8));
-        if(!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
-        return off;
-    }
-};
-
-template<typename T> T *dptr(void *base, size_t off)
-{
-    return reinterpret_cast<T *>(reinterpret_cast<uint8_t *>(base) + off);
 }
 
 // Key layout and arrival storage of an arrivals / eigen run.
@@ -878,6 +833,25 @@ void write_arrivals(bhcb_ctx *c, const Field &F, const EnvSlot &S, const EnvTabl
 }
 } // namespace
 
+namespace {
+// one complete 3-D run: tables, trace, influence, scale (blocking)
+int run3_checked(bhcb_ctx *c)
+{
+    bhcb_stats st{};
+    uint32_t wb = 0;
+    const uint32_t eb = run3_run(c->r3, c->stream, c->sm_count, c->max_memory, st, wb);
+    c->stats = st;
+    c->err_bits = eb;
+    c->warn_bits = wb;
+    if(eb) {
+        char b[96];
+        snprintf(b, sizeof b, "tracer error bits 0x%x", eb);
+        return fail(c, (eb & (1u << ERR_SEG_OVERFLOW)) ? BHCB_ERR_MEMORY : BHCB_ERR_RUN, b);
+    }
+    return BHCB_OK;
+}
+} // namespace
+
 extern "C" {
 
 int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
@@ -923,6 +897,7 @@ void bhcb_close(bhcb_ctx *c)
         if(e) cudaEventDestroy(e);
     if(c->stream) cudaStreamDestroy(c->stream);
     if(c->stream2) cudaStreamDestroy(c->stream2);
+    run3_free(c->r3);
     delete c;
 }
 
@@ -931,6 +906,7 @@ int bhcb_clear(bhcb_ctx *c)
     return guarded(c, [&]() -> int {
         c->envs.clear();
         c->prepared = false;
+        if(c->r3) run3_clear(c->r3);
         return BHCB_OK;
     });
 }
@@ -939,6 +915,7 @@ int bhcb_add_env(bhcb_ctx *c, const char *root, int32_t *idx)
 {
     return guarded(c, [&]() -> int {
         if(!root) throw std::invalid_argument("file_root is NULL");
+        if(c->is3d()) throw StateError("the context holds 3-D environments: bhcb_clear first");
         EnvSlot S;
         S.root = root;
         S.in = read_env_files(root);
@@ -974,6 +951,7 @@ int bhcb_set_frequencies(bhcb_ctx *c, int32_t env, int32_t n, const double *f)
 int bhcb_prepare(bhcb_ctx *c)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) return BHCB_OK;   // 3-D tables are built by the run itself
         do_prepare(c);
         return BHCB_OK;
     });
@@ -982,6 +960,10 @@ int bhcb_prepare(bhcb_ctx *c)
 int bhcb_launch(bhcb_ctx *c)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) {   // 3-D runs complete inside the launch; bhcb_sync reports the status
+            c->r3_status = run3_checked(c);
+            return BHCB_OK;
+        }
         do_launch(c, c->overlap);
         return BHCB_OK;
     });
@@ -990,6 +972,7 @@ int bhcb_launch(bhcb_ctx *c)
 int bhcb_sync(bhcb_ctx *c)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) return c->r3_status;
         do_sync(c);
         if(c->last.err_bits) {
             char b[96];
@@ -1004,6 +987,7 @@ int bhcb_sync(bhcb_ctx *c)
 int bhcb_run(bhcb_ctx *c)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) return c->r3_status = run3_checked(c);
         if(!c->prepared) do_prepare(c);
         return run_checked(c);
     });
@@ -1012,6 +996,7 @@ int bhcb_run(bhcb_ctx *c)
 int bhcb_field_shape(bhcb_ctx *c, int32_t env, int32_t *nfreq, int32_t *nsz, int32_t *nrzp, int32_t *nrr)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) throw StateError("3-D environment: use bhcb_field_shape3d");
         if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
         const EnvSlot &S = c->envs[env];
         EnvTables T = S.tables.empty() ? preprocess(S.in, S.freqs[0]) : S.tables[0];
@@ -1026,6 +1011,11 @@ int bhcb_field_shape(bhcb_ctx *c, int32_t env, int32_t *nfreq, int32_t *nsz, int
 int bhcb_copy_field(bhcb_ctx *c, int32_t env, int32_t ifreq, void *dst, size_t bytes)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            run3_copy_field(c->r3, env, dst, bytes, c->stream);
+            return BHCB_OK;
+        }
         if(c->mode != MODE_TL) throw StateError("not a TL run: use bhcb_copy_arrivals / bhcb_eigen_hits");
         const Field *F = find_field(c, env, ifreq);
         size_t need = (size_t)F->nsz * F->nrzp * F->nrr * sizeof(float2);
@@ -1039,6 +1029,12 @@ int bhcb_copy_field(bhcb_ctx *c, int32_t env, int32_t ifreq, void *dst, size_t b
 int bhcb_field_device(bhcb_ctx *c, int32_t env, int32_t ifreq, void **dptr_out)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            if(!dptr_out) throw std::invalid_argument("dptr is NULL");
+            *dptr_out = run3_field_device(c->r3, env);
+            return BHCB_OK;
+        }
         const Field *F = find_field(c, env, ifreq);
         if(!dptr_out) throw std::invalid_argument("dptr is NULL");
         *dptr_out = (float2 *)c->out.p + F->base;
@@ -1129,6 +1125,12 @@ int bhcb_eigen_hits(bhcb_ctx *c, int32_t env, int32_t ifreq, bhcb_eigen_hit *hit
 int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
 {
     return guarded(c, [&]() -> int {
+        if(!root) throw std::invalid_argument("file_root is NULL");
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            run3_writeout(c->r3, env, root, c->stream);
+            return BHCB_OK;
+        }
         if(c->mode == MODE_EIGEN)
             throw StateError("eigenray .ray output (re-trace of the hit rays) is not built; use bhcb_eigen_hits");
         if(c->mode == MODE_ARR) {
@@ -1186,6 +1188,53 @@ int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
     });
 }
 
+int bhcb_add_env3d(bhcb_ctx *c, const char *root, int32_t *idx)
+{
+    return guarded(c, [&]() -> int {
+        if(!root) throw std::invalid_argument("file_root is NULL");
+        if(!c->envs.empty()) throw StateError("the context holds 2-D environments: bhcb_clear first");
+        if(!c->r3) c->r3 = run3_new();
+        const int i = run3_add_env(c->r3, root);
+        c->r3_status = BHCB_OK;
+        if(idx) *idx = i;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_setup3d(bhcb_ctx *c, const char *root)
+{
+    int r = bhcb_clear(c);
+    if(r) return r;
+    return bhcb_add_env3d(c, root, nullptr);
+}
+
+int bhcb_field_shape3d(bhcb_ctx *c, int32_t env, int32_t *dims)
+{
+    return guarded(c, [&]() -> int {
+        if(!c->is3d()) throw StateError("not a 3-D context: use bhcb_field_shape");
+        if(!dims) throw std::invalid_argument("dims is NULL");
+        run3_shape(c->r3, env, dims);
+        return BHCB_OK;
+    });
+}
+
+int bhcb_grid3d(bhcb_ctx *c, int32_t env, double *sx, double *sy, float *sz, double *rr, float *rz, double *theta)
+{
+    return guarded(c, [&]() -> int {
+        if(!c->is3d()) throw StateError("not a 3-D context");
+        std::vector<double> vsx, vsy, vrr, vth;
+        std::vector<float> vsz, vrz;
+        run3_grid(c->r3, env, vsx, vsy, vsz, vrr, vrz, vth);
+        if(sx) std::memcpy(sx, vsx.data(), vsx.size() * sizeof(double));
+        if(sy) std::memcpy(sy, vsy.data(), vsy.size() * sizeof(double));
+        if(sz) std::memcpy(sz, vsz.data(), vsz.size() * sizeof(float));
+        if(rr) std::memcpy(rr, vrr.data(), vrr.size() * sizeof(double));
+        if(rz) std::memcpy(rz, vrz.data(), vrz.size() * sizeof(float));
+        if(theta) std::memcpy(theta, vth.data(), vth.size() * sizeof(double));
+        return BHCB_OK;
+    });
+}
+
 int bhcb_stream(bhcb_ctx *c, void **stream)
 {
     if(!c || !stream) return BHCB_ERR_ARG;
@@ -1211,6 +1260,34 @@ int bhcb_last_error(bhcb_ctx *c, char *msg, size_t n, uint32_t *eb, uint32_t *wb
     if(eb) *eb = c->err_bits;
     if(wb) *wb = c->warn_bits;
     return BHCB_OK;
+}
+
+int bhcb_check_env3d(const char *root, int32_t *dims, int64_t *nrays, char *msg, size_t n)
+{
+    try {
+        if(!root) throw std::invalid_argument("file_root is NULL");
+        EnvInput in = read_env_files(root, true);
+        Env3Tables T = preprocess3d(in, in.freq0);
+        if(dims) {
+            dims[0] = (int32_t)T.sz.size(); dims[1] = (int32_t)T.sx.size(); dims[2] = (int32_t)T.sy.size();
+            dims[3] = (int32_t)T.theta.size(); dims[4] = (int32_t)T.rz.size(); dims[5] = (int32_t)T.rr.size();
+        }
+        if(nrays) {
+            int64_t r = (int64_t)T.sz.size() * T.sx.size() * T.sy.size();
+            if(T.isingle_alpha == 0) r *= (int64_t)T.alpha.size();
+            if(T.isingle_beta == 0) r *= (int64_t)T.beta.size();
+            *nrays = r;
+        }
+        if(msg && n) msg[0] = 0;
+        return BHCB_OK;
+    } catch(const std::exception &e) {
+        if(msg && n) {
+            size_t l = std::min(n - 1, std::strlen(e.what()));
+            std::memcpy(msg, e.what(), l);
+            msg[l] = 0;
+        }
+        return BHCB_ERR_INPUT;
+    }
 }
 
 int bhcb_check_env(const char *root, bhcb_env_info *info, char *msg, size_t n)

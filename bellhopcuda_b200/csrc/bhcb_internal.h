@@ -22,11 +22,14 @@ enum SspType : int32_t { SSP_N2LINEAR = 0, SSP_CLINEAR = 1, SSP_CUBIC = 2, SSP_P
 enum : uint32_t {
     ERR_RAYINIT = 2, ERR_BOUNDARY_SEG_NAN = 3, ERR_BOUNDARY_CONDITION_TYPE = 4,
     ERR_INVALID_SSP_TYPE = 5, ERR_OUTSIDE_ALTIMETRY = 6, ERR_OUTSIDE_BATHYMETRY = 7,
+    ERR_OUTSIDE_SSP = 8,
     ERR_SEG_OVERFLOW = 31,
 };
 enum : uint32_t {
     WARN_ONERAY_OUTOFMEMORY = 1, WARN_TOO_FEW_BEAMS = 3, WARN_SOURCE_OUTSIDE_BOUNDARIES = 4,
-    WARN_STEP_NEGATIVE_H = 8, WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17,
+    WARN_OUTSIDE_ALTIMETRY = 6, WARN_OUTSIDE_BATHYMETRY = 7,
+    WARN_STEP_NEGATIVE_H = 8, WARN_TRIDIAG_H_NEGATIVE = 9, WARN_TRIDIAG_H_GROWING = 10,
+    WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17,
 };
 
 struct HsDev {          // halfspace (include/bhc/structs.hpp:93-101)
@@ -72,6 +75,46 @@ struct EnvDev {
     const double *sbp;
 };
 
+// 3-D grid boundary node (x, y, z) with the unit normals of its cell's two
+// triangles (src/module/boundary.hpp:600-645); same layout as the host's.
+struct Bdry3PtDev {
+    double x[3], n1[3], n2[3];
+};
+
+// Preprocessed 3-D environment (BELLHOP3D field modes) for one frequency.
+struct Env3Dev {
+    EnvDev e1d;                      // 1-D SSP tables (ssp_type, nssp, z, rho, c, ...); hexahedral uses z, rho
+    int32_t hex, hnx, hny, hnz;      // hexahedral grid (src/ssp.hpp:220-305)
+    const double *hx, *hy, *hz, *hc, *hcz;
+    HsDev top, bot;
+    int32_t top_nx, top_ny, bot_nx, bot_ny;
+    const Bdry3PtDev *btop, *bbot;
+    int32_t nsx, nsy, nsz, nrr, nrz, ntheta, nalpha, nbeta, isingle_alpha, isingle_beta;
+    const double *sx, *sy, *rr, *tcs;   // tcs: receiver bearing (cos, sin) pairs
+    const double *alpha, *beta;
+    const float *sz, *rz;
+    double dalpha, dbeta, deltas, box_x, box_y, box_z, freq0;
+    int32_t gaussian, coherent, run0, nsbp;
+    const double *sbp;
+};
+
+// One 3-D influence segment (point0 -> point1 of Step_InfluenceGeoCart, 3-D
+// branch, src/influence.hpp:1201-1406) after the receiver-range walk.
+struct alignas(16) SegRec3 {
+    double x0[3];              // point0.x
+    double tau0r, tau0i, dtaur, dtaui;
+    double rayt[3], e1[3], e2[3];   // unit tangent, ray normals (RayNormal_unit at point1.phi)
+    double rlen;
+    double q0[4], dq[4];       // point0.q, point1.q - point0.q, m[col][row] as glm
+    double rcp_q0, rcp_qhat0;  // Dalpha / c0, |cos alpha| Dbeta / c0 of the ray
+    double cnst_num;           // Ratio1 * point1.c * point1.Amp
+    double phase0;             // point0.Phase + inflray.phase
+    double qold;               // det(point0.q): caustic reference of FinalPhase
+    double ldiag;              // L_diag beam radius bound
+    double zlo, zhi;           // min / max depth of the segment
+    int32_t ir_lo, ir_hi, job, is;
+};
+
 struct GroupDev {
     const EnvDev *env;       // device pointer
     int64_t job_base;        // first job index of this group
@@ -87,6 +130,7 @@ struct GroupDev {
     int64_t acc_stride_f;    // accumulator elements per frequency field
     int32_t acc_nz;
     int32_t field_index;     // index of the group's first field in the launch
+    const Env3Dev *env3;     // 3-D groups: the environment (env is then null)
 };
 
 // One influence segment (point0 -> point1 of Step_InfluenceGeoCart,

@@ -945,6 +945,9 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.bbot = build_bdry3(in.bty3, false, bot_depth, t.bot_nx, t.bot_ny);
 
     // sources, receivers, bearings (module/sxsy.hpp, szrz.hpp, rcvrranges.hpp, rcvrbearings.hpp)
+    if(in.nsx <= 0 || in.nsy <= 0 || in.nsz <= 0) env_error("number of sources must be positive");
+    if(in.nrz <= 0 || in.nrr <= 0 || in.ntheta <= 0) env_error("number of receivers / bearings must be positive");
+    if(in.nbeta <= 0) env_error("3-D runs need an explicit number of bearing beams");
     for(double v : tab_sort(in.sx_km, in.nsx)) t.sx.push_back(v * 1000.0);
     for(double v : tab_sort(in.sy_km, in.nsy)) t.sy.push_back(v * 1000.0);
     t.sz = tab_sort(in.sz, in.nsz);

@@ -1,0 +1,68 @@
+// Host runtime pieces shared by the 2-D and 3-D runners behind the C ABI:
+// error classes mapped to bhcb status codes, a growable device buffer and the
+// table arena that packs an environment's arrays into one upload.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace bhcb {
+
+struct CudaError : std::runtime_error {   // -> BHCB_ERR_CUDA
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {  // -> BHCB_ERR_STATE
+    using std::runtime_error::runtime_error;
+};
+struct MemError : std::runtime_error {    // -> BHCB_ERR_MEMORY
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                           \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if(e_ != cudaSuccess)                                                           \
+            throw ::bhcb::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));   \
+    } while(0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t n)
+    {
+        if(n <= bytes) return;
+        release();
+        CK(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    void release()
+    {
+        if(p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+// arrays packed at 256-byte offsets into one host image, uploaded at once
+struct Arena {
+    std::vector<uint8_t> bytes;
+    template<typename T> size_t put(const std::vector<T> &v)
+    {
+        size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 8));
+        if(!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+};
+
+template<typename T> T *dptr(void *base, size_t off)
+{
+    return reinterpret_cast<T *>(reinterpret_cast<uint8_t *>(base) + off);
+}
+
+} // namespace bhcb

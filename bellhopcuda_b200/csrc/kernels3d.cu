@@ -1,0 +1,453 @@
+// 3-D (BELLHOP3D) field-mode kernels for sm_100a, FP64.
+//
+//  trace3d_kernel     one ray per thread (persistent, work-queue driven):
+//                     RayInit / RayUpdate / RayTerminate of the 3-D path
+//                     (src/trace.hpp:76-477) and the sequential part of
+//                     Step_InfluenceGeoCart's 3-D branch (src/influence.hpp:
+//                     1201-1292: duplicate-point skips, caustic phase, beam
+//                     width bound, receiver-range walk); one compact record per
+//                     segment that brackets at least one receiver range.
+//  influence3d_kernel warp-cooperative evaluation of the (segment, range,
+//                     bearing) work of 32 records at a time: a warp prefix sum
+//                     flattens it so lanes stay busy; each lane applies the
+//                     bearing rejections and walks the receiver depths in the
+//                     segment's depth window (src/influence.hpp:1294-1406),
+//                     evaluates InfluenceGeoCore (src/influence.hpp:897-1024)
+//                     and adds the contribution into the field, laid out as
+//                     the reference's [isz][isx][isy][itheta][iz][ir]
+//                     (GetFieldAddr, src/common.hpp:393-405).
+//  sqrt3d_kernel      ScalePressure's intensity-to-pressure conversion for
+//                     incoherent and semi-coherent runs (src/influence.hpp:
+//                     1596-1606); coherent 3-D fields are not scaled.
+#include <cuda_runtime.h>
+
+#include "bhcb_internal.h"
+#include "device_math.cuh"
+#include "trace2d.cuh"
+#include "influence2d.cuh"
+#include "trace3d.cuh"
+
+namespace bhcb {
+
+namespace {
+
+constexpr int SEG_BLOCK3 = 32;
+
+struct Cursor3 {
+    unsigned long long next = 0, end = 0;
+};
+
+__device__ __forceinline__ void emit_seg3(const SegRec3 &rec, SegRec3 *segs, unsigned long long cap,
+                                          RunCounters *ctr, Cursor3 &cur, bool &overflow)
+{
+    if(cur.next == cur.end) {
+        unsigned long long b = atomicAdd(&ctr->nseg, (unsigned long long)SEG_BLOCK3);
+        if(b + SEG_BLOCK3 > cap) {
+            overflow = true;
+            return;
+        }
+        cur.next = b;
+        cur.end = b + SEG_BLOCK3;
+    }
+    static_assert(sizeof(SegRec3) % 16 == 0, "records are written in 16-byte words");
+    const uint4 *src = reinterpret_cast<const uint4 *>(&rec);
+    uint4 *dst = reinterpret_cast<uint4 *>(segs + cur.next++);
+#pragma unroll
+    for(int k = 0; k < (int)(sizeof(SegRec3) / 16); ++k) dst[k] = src[k];
+}
+
+// GetJobIndices, 3-D (src/common.hpp:365-391): ialpha fastest, then ibeta, isy, isx, isz
+struct Job3 {
+    int ialpha, ibeta, isx, isy, isz;
+};
+__device__ __forceinline__ Job3 job_indices3(const Env3Dev &E, int local)
+{
+    Job3 j;
+    if(E.isingle_alpha >= 1) {
+        j.ialpha = E.isingle_alpha - 1;
+    } else {
+        j.ialpha = local % E.nalpha;
+        local /= E.nalpha;
+    }
+    if(E.isingle_beta >= 1) {
+        j.ibeta = E.isingle_beta - 1;
+    } else {
+        j.ibeta = local % E.nbeta;
+        local /= E.nbeta;
+    }
+    j.isy = local % E.nsy;
+    local /= E.nsy;
+    j.isx = local % E.nsx;
+    local /= E.nsx;
+    j.isz = local;
+    return j;
+}
+
+// the carried part of InfluenceRayInfo for the 3-D Cartesian geometric beams
+struct Infl3 {
+    double phase, qOld;
+    double ratio1, rcp_q0, rcp_qhat0;
+    V3 xs;
+    int ir;
+};
+
+__device__ __forceinline__ double row_len(const M2 &q, int row, double s)
+{
+    const double a = q.m[0][row] * s, b = q.m[1][row] * s;
+    return sqrt(a * a + b * b);
+}
+
+// Step_InfluenceGeoCart, 3-D, up to the receiver loop (src/influence.hpp:1201-1292)
+__device__ __forceinline__ bool infl_prologue3(const Ray3 &P0, const Ray3 &P1, Infl3 &inf, const Env3Dev &E,
+                                               int job, int is, SegRec3 &rec)
+{
+    const double ax = P0.x.x - inf.xs.x, ay = P0.x.y - inf.xs.y;
+    const double bx = P1.x.x - inf.xs.x, by = P1.x.y - inf.xs.y;
+    const double rA = sqrt(ax * ax + ay * ay), rB = sqrt(bx * bx + by * by);
+    if(fabs(rA - rB) <= 1.0e3 * spacing_d(rA)) return false;   // IsDuplicatePoint(rB, rA)
+    if(is == 0) inf.ir = rB > rA ? 0 : E.nrr - 1;
+    V3 rayt = sub3(P1.x, P0.x);
+    const double rlen = len3(rayt);
+    if(rlen <= 1.0e3 * spacing_d(P1.x.x)) return false;
+    rayt = v3(rayt.x / rlen, rayt.y / rlen, rayt.z / rlen);
+    V3 e1, e2;
+    ray_normal(rayt, P1.phi, true, 1.0, e1, e2);
+    const double phaseq = m2_det(P0.q);
+    if((phaseq <= 0.0 && inf.qOld > 0.0) || (phaseq >= 0.0 && inf.qOld < 0.0)) inf.phase += BHCB_PI / FLTD(2.0);
+    inf.qOld = phaseq;
+    const double l1 = max(row_len(P0.q, 0, inf.rcp_q0), row_len(P1.q, 0, inf.rcp_q0));
+    const double l2 = max(row_len(P0.q, 1, inf.rcp_qhat0), row_len(P1.q, 1, inf.rcp_qhat0));
+    const double ldiag = sqrt(l1 * l1 + l2 * l2);
+
+    // receiver-range walk (src/influence.hpp:1294-1297, 1386-1399): the
+    // bracketed ranges of one segment are contiguous
+    const double *rr = E.rr;
+    const double rmin = min(rA, rB), rmax = max(rA, rB);
+    int lo = 0x7fffffff, hi = -1;
+    for(;;) {
+        const double r = rr[inf.ir];
+        if(r >= rmin && r < rmax) {
+            lo = min(lo, inf.ir);
+            hi = max(hi, inf.ir);
+        }
+        int irTT;
+        if(rB > r) {
+            if(inf.ir >= E.nrr - 1) break;
+            irTT = inf.ir + 1;
+            if(rr[irTT] >= rB) break;
+        } else {
+            if(inf.ir <= 0) break;
+            irTT = inf.ir - 1;
+            if(rr[irTT] <= rB) break;
+        }
+        inf.ir = irTT;
+    }
+    if(hi < 0) return false;
+    rec.x0[0] = P0.x.x; rec.x0[1] = P0.x.y; rec.x0[2] = P0.x.z;
+    rec.tau0r = P0.taur;
+    rec.tau0i = P0.taui;
+    rec.dtaur = P1.taur - P0.taur;
+    rec.dtaui = P1.taui - P0.taui;
+    rec.rayt[0] = rayt.x; rec.rayt[1] = rayt.y; rec.rayt[2] = rayt.z;
+    rec.e1[0] = e1.x; rec.e1[1] = e1.y; rec.e1[2] = e1.z;
+    rec.e2[0] = e2.x; rec.e2[1] = e2.y; rec.e2[2] = e2.z;
+    rec.rlen = rlen;
+    rec.q0[0] = P0.q.m[0][0]; rec.q0[1] = P0.q.m[0][1]; rec.q0[2] = P0.q.m[1][0]; rec.q0[3] = P0.q.m[1][1];
+    rec.dq[0] = P1.q.m[0][0] - P0.q.m[0][0];
+    rec.dq[1] = P1.q.m[0][1] - P0.q.m[0][1];
+    rec.dq[2] = P1.q.m[1][0] - P0.q.m[1][0];
+    rec.dq[3] = P1.q.m[1][1] - P0.q.m[1][1];
+    rec.rcp_q0 = inf.rcp_q0;
+    rec.rcp_qhat0 = inf.rcp_qhat0;
+    rec.cnst_num = inf.ratio1 * P1.c * P1.Amp;
+    rec.phase0 = P0.Phase + inf.phase;
+    rec.qold = inf.qOld;
+    rec.ldiag = ldiag;
+    rec.zlo = min(P0.x.z, P1.x.z);
+    rec.zhi = max(P0.x.z, P1.x.z);
+    rec.ir_lo = lo;
+    rec.ir_hi = hi;
+    rec.job = job;
+    rec.is = is;
+    return true;
+}
+
+__global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict__ groups, int ngroups,
+                                                     long long job_end, SegRec3 *segs, unsigned long long cap,
+                                                     RunCounters *ctr, unsigned long long *job_counter)
+{
+    for(;;) {
+        const long long job = (long long)atomicAdd(job_counter, 1ull);
+        if(job >= job_end) break;
+        const GroupDev &G = groups[find_group(groups, ngroups, job)];
+        const Env3Dev &E = *G.env3;
+        const Job3 J = job_indices3(E, (int)(job - G.job_base));
+        if(J.isz >= E.nsz) { run_error(ctr, ERR_RAYINIT); continue; }
+
+        // ---- RayInit (src/trace.hpp:76-266), 3-D
+        const double alpha = E.alpha[J.ialpha], beta = E.beta[J.ibeta];
+        const double SrcDecl = (180.0 / BHCB_PI) * alpha;
+        Seg3 iSeg{0, 0, 0};
+        const V3 xs = v3(E.sx[J.isx], E.sy[J.isy], (double)E.sz[J.isz]);
+        SSPOut3 o;
+        eval_ssp3(xs, v3(0.0, 0.0, 1.0), o, E, iSeg, ctr);
+        const double c = o.c;
+        const int ibp = min(bsearch_leq2(E.sbp, E.nsbp, SrcDecl), E.nsbp - 2);
+        const double s = (SrcDecl - E.sbp[2 * ibp]) / (E.sbp[2 * (ibp + 1)] - E.sbp[2 * ibp]);
+        float amp0 = (float)((FLTD(1.0) - s) * E.sbp[2 * ibp + 1] + s * E.sbp[2 * (ibp + 1) + 1]);
+        if(E.run0 == 'S') {
+            const float om = (float)(FLTD(2.0) * BHCB_PI * E.freq0);
+            amp0 = (float)(amp0 * ((double)sqrtf(2.0f) * fabs(sin(om / c * xs.z * sin(alpha)))));
+        }
+        Ray3 p0, p1, p2;
+        const V3 tinit = v3(cos(alpha) * cos(beta), cos(alpha) * sin(beta), sin(alpha));
+        p0.x = xs;
+        p0.c = c;
+        p0.t = v3(tinit.x / c, tinit.y / c, tinit.z / c);
+        p0.taur = p0.taui = 0.0;
+        p0.Amp = (double)amp0;
+        p0.Phase = 0.0;
+        p0.ntop = p0.nbot = 0;
+        p0.p = m2_diag(1.0);
+        p0.q = m2_diag(0.0);
+        p0.phi = 0.0;
+        Bd3 top, bot;
+        top.ix = top.iy = bot.ix = bot.iy = 0;
+        top.justSteppedTo = bot.justSteppedTo = false;
+        top.side = bot.side = false;
+        top.outgoingSide = bot.outgoingSide = false;
+        get_bdry_seg3(xs, p0.t, top, E.btop, E.top_nx, E.top_ny, true, true, ctr);
+        get_bdry_seg3(xs, p0.t, bot, E.bbot, E.bot_nx, E.bot_ny, false, true, ctr);
+        double dTop, dBot;
+        distances3(xs, top, bot, dTop, dBot);
+        if(dTop <= 0.0 || dBot <= 0.0) {
+            run_warn(ctr, WARN_SOURCE_OUTSIDE_BOUNDARIES);
+            continue;
+        }
+        // ---- Init_Influence (src/influence.hpp:525-644), 3-D Cartesian geometric
+        Infl3 inf;
+        inf.ratio1 = sqrt(fabs(cos(alpha)));
+        inf.ratio1 *= sqrt(E.dalpha * E.dbeta) / c;
+        if(E.gaussian) inf.ratio1 /= FLTD(2.0) * BHCB_PI;
+        inf.rcp_q0 = E.dalpha / c;
+        inf.rcp_qhat0 = fabs(cos(alpha)) * E.dbeta / c;
+        inf.phase = 0.0;
+        inf.qOld = m2_det(p0.q);
+        inf.xs = p0.x;
+        inf.ir = bsearch_gt(E.rr, E.nrr, 0.0);
+
+        // beam-box limits of the boundary grids (RayTerminate, src/trace.hpp:400-420)
+        const Bdry3PtDev *bb = E.bbot, *bt = E.btop;
+        const double minx = max(bb[0].x[0], bt[0].x[0]);
+        const double miny = max(bb[0].x[1], bt[0].x[1]);
+        const double maxx = min(bb[(size_t)(E.bot_nx - 1) * E.bot_ny].x[0], bt[(size_t)(E.top_nx - 1) * E.top_ny].x[0]);
+        const double maxy = min(bb[E.bot_ny - 1].x[1], bt[E.top_ny - 1].x[1]);
+
+        int small = 0, is = 0;
+        bool overflow = false;
+        unsigned long long nsteps = 0;
+        Cursor3 cur;
+        for(;;) {
+            if((nsteps & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) break;
+            bool tr = false, br = false;
+            step3d(p0, p1, top, bot, xs, E, iSeg, small, tr, br, ctr);
+            ++nsteps;
+            get_bdry_seg3(p1.x, p1.t, top, E.btop, E.top_nx, E.top_ny, true, false, ctr);
+            get_bdry_seg3(p1.x, p1.t, bot, E.bbot, E.bot_nx, E.bot_ny, false, false, ctr);
+            const bool two = tr || br;
+            if(two) reflect3d(p1, p2, tr ? E.top : E.bot, tr, tr ? top.n : bot.n, E, iSeg, ctr);
+            SegRec3 rec;
+            if(infl_prologue3(p0, p1, inf, E, (int)job, is, rec)) emit_seg3(rec, segs, cap, ctr, cur, overflow);
+            ++is;
+            if(two) {
+                if(infl_prologue3(p1, p2, inf, E, (int)job, is, rec)) emit_seg3(rec, segs, cap, ctr, cur, overflow);
+                p0 = p2;
+                ++is;
+            } else {
+                p0 = p1;
+            }
+            if(overflow) {
+                atomicMin(&ctr->overflow_job, (unsigned int)job);
+                run_error(ctr, ERR_SEG_OVERFLOW);
+                break;
+            }
+            // ---- RayTerminate (src/trace.hpp:391-477), 3-D
+            const V3 x = p0.x, t = p0.t;
+            const bool leftbox = fabs(x.x - xs.x) >= E.box_x || fabs(x.y - xs.y) >= E.box_y || fabs(x.z) >= E.box_z;
+            const bool esc0 = x.x < minx || x.y < miny || (x.x == minx && t.x < 0.0) || (x.y == miny && t.y < 0.0);
+            const bool escN = x.x > maxx || x.y > maxy || (x.x == maxx && t.x > 0.0) || (x.y == maxy && t.y > 0.0);
+            const bool lost = p0.Amp < FLTD(0.005);
+            if(leftbox || lost || esc0 || escN || small > 50) break;
+            if(is >= MAXN_STEPS - 3) {
+                run_warn(ctr, WARN_ONERAY_OUTOFMEMORY);
+                break;
+            }
+        }
+        for(; cur.next < cur.end; ++cur.next) segs[cur.next].job = -1;
+        atomicAdd(&ctr->nsteps, nsteps);
+    }
+}
+
+constexpr int WARPS3 = 4;
+
+// InfluenceGeoCore, 3-D Cartesian (src/influence.hpp:897-1024) and
+// ApplyContribution's TL branch (src/influence.hpp:432-473)
+__device__ __forceinline__ bool core3(const SegRec3 &R, double s, double n1, double n2, bool gauss, bool coherent,
+                                      double omega, float2 &df)
+{
+    double q00 = R.q0[0] + s * R.dq[0], q01 = R.q0[1] + s * R.dq[1];
+    double q10 = R.q0[2] + s * R.dq[2], q11 = R.q0[3] + s * R.dq[3];
+    q00 *= R.rcp_q0;     // row 0 (m[0][0], m[1][0])
+    q10 *= R.rcp_q0;
+    q01 *= R.rcp_qhat0;  // row 1 (m[0][1], m[1][1])
+    q11 *= R.rcp_qhat0;
+    const double qF = q00 * q11 - q10 * q01;
+    const double l1 = sqrt(q00 * q00 + q10 * q10);
+    const double l2 = sqrt(q01 * q01 + q11 * q11);
+    if(nearly_zero(l1) || nearly_zero(l2)) return false;
+    if(nearly_zero(qF)) return false;
+    const double n1p = fabs((-q01 * n2 + q11 * n1) / qF);
+    const double n2p = fabs((q00 * n2 - q10 * n1) / qF);
+    const double bw = gauss ? 4.0 : 1.0;
+    const double dist = gauss ? n1p + n2p : max(n1p, n2p);
+    if(dist > bw * 1.0) return false;
+    const double dr = R.tau0r + s * R.dtaur, di = R.tau0i + s * R.dtaui;
+    const double cnst = R.cnst_num / sqrt(fabs(qF));
+    const double w = gauss ? exp(FLTD(-0.5) * (n1p * n1p + n2p * n2p)) : (FLTD(1.0) - n1p) * (FLTD(1.0) - n2p);
+    double ph = R.phase0;
+    if((qF <= 0.0 && R.qold > 0.0) || (qF >= 0.0 && R.qold < 0.0)) ph += BHCB_PI / FLTD(2.0);
+    if(coherent) {
+        const double a = omega * dr - ph;
+        const double m = exp(omega * di);
+        double sa, ca;
+        sincos(-a, &sa, &ca);
+        const double cw = cnst * w;
+        df = make_float2((float)(cw * (m * ca)), (float)(cw * (m * sa)));
+    } else {
+        double v = cnst * exp(omega * di);
+        v = v * v * w;
+        if(gauss) v *= FLTD(2.0) * BHCB_PI;
+        df = make_float2((float)v, 0.0f);
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
+    const SegRec3 *__restrict__ segs, unsigned long long nseg, const GroupDev *__restrict__ groups, int ngroups,
+    float2 *field, RunCounters *ctr)
+{
+    __shared__ int s_incl[WARPS3][32];
+    __shared__ int s_grp[WARPS3][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned long long nchunk = (nseg + 31) / 32;
+    unsigned long long nevals = 0;
+    for(unsigned long long ch = (unsigned long long)blockIdx.x * WARPS3 + w; ch < nchunk;
+        ch += (unsigned long long)gridDim.x * WARPS3) {
+        const unsigned long long idx = ch * 32 + lane;
+        int n = 0, g = 0;
+        if(idx < nseg) {
+            const int job = __ldg(&segs[idx].job);
+            if(job >= 0) {
+                g = find_group(groups, ngroups, job);
+                const int lo = __ldg(&segs[idx].ir_lo), hi = __ldg(&segs[idx].ir_hi);
+                n = (hi - lo + 1) * groups[g].env3->ntheta;
+            }
+        }
+        int incl = n;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if(lane >= o) incl += v;
+        }
+        __syncwarp();
+        s_incl[w][lane] = incl;
+        s_grp[w][lane] = g;
+        __syncwarp();
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for(int k = lane; k < total; k += 32) {
+            int lo = 0, hi = 31;   // first j with incl[j] > k
+            while(lo < hi) {
+                const int m = (lo + hi) >> 1;
+                if(s_incl[w][m] > k) hi = m; else lo = m + 1;
+            }
+            const int j = lo;
+            const int local = k - (j ? s_incl[w][j - 1] : 0);
+            const SegRec3 &R = segs[ch * 32 + j];
+            const GroupDev &G = groups[s_grp[w][j]];
+            const Env3Dev &E = *G.env3;
+            const int itheta = local % E.ntheta;
+            const int ir = R.ir_lo + local / E.ntheta;
+            const Job3 J = job_indices3(E, (int)(R.job - G.job_base));
+            const double xsx = E.sx[J.isx], xsy = E.sy[J.isy];
+            const double tc = E.tcs[2 * itheta], ts = E.tcs[2 * itheta + 1];
+            const double rr = E.rr[ir];
+            const double xrx = xsx + rr * tc, xry = xsy + rr * ts;
+            const double rtx = R.rayt[0], rty = R.rayt[1], rtz = R.rayt[2];
+            const double dxr = xrx - R.x0[0], dyr = xry - R.x0[1];
+            const bool gauss = E.gaussian != 0;
+            if(!gauss) {
+                const double mprime = fabs(dxr * (-rty) + dyr * rtx);
+                if(mprime > 1.0 * R.ldiag) continue;
+            }
+            if((xrx - xsx) * (R.x0[0] - xsx) + (xry - xsy) * (R.x0[1] - xsy) < 0.0) continue;
+            const double nrz = rtx * tc - rty * (-ts);
+            if(fabs(nrz) < 1e-9) continue;
+            const double Lz = (gauss ? 4.0 : 1.0) * R.ldiag / fabs(nrz);
+            const double zmin = R.zlo - Lz, zmax = R.zhi + Lz;
+            const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
+            const size_t base = ((((size_t)J.isz * E.nsx + J.isx) * E.nsy + J.isy) * E.ntheta + itheta)
+                * (size_t)E.nrz * E.nrr + ir;
+            for(int iz = 0; iz < E.nrz; ++iz) {
+                const double z = (double)E.rz[iz];
+                if(z < zmin || z > zmax) continue;
+                const double dz = z - R.x0[2];
+                const double s = (dxr * rtx + dyr * rty + dz * rtz) / R.rlen;
+                const double n1 = fabs(dxr * R.e1[0] + dyr * R.e1[1] + dz * R.e1[2]);
+                const double n2 = fabs(dxr * R.e2[0] + dyr * R.e2[1] + dz * R.e2[2]);
+                float2 df;
+                if(!core3(R, s, n1, n2, gauss, E.coherent != 0, omega, df)) continue;
+                float2 *dst = field + G.field_base + base + (size_t)iz * E.nrr;
+                atomicAdd(dst, df);
+                ++nevals;
+            }
+        }
+        __syncwarp();
+    }
+    // one counter update per warp
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) nevals += __shfl_down_sync(0xffffffffu, nevals, o);
+    if(lane == 0 && nevals) atomicAdd(&ctr->nevals, nevals);
+}
+
+__global__ void sqrt3d_kernel(float2 *f, long long n)
+{
+    for(long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        f[i] = make_float2(sqrtf(f[i].x), 0.0f);
+}
+
+} // namespace
+
+cudaError_t launch_trace3d(const GroupDev *groups, int ngroups, long long job_end, SegRec3 *segs,
+                           unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, int grid,
+                           cudaStream_t st)
+{
+    trace3d_kernel<<<grid, 64, 0, st>>>(groups, ngroups, job_end, segs, cap, ctr, job_counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_influence3d(const SegRec3 *segs, unsigned long long nseg, const GroupDev *groups, int ngroups,
+                               float2 *field, RunCounters *ctr, int grid, cudaStream_t st)
+{
+    if(nseg == 0) return cudaSuccess;
+    influence3d_kernel<<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, field, ctr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sqrt3d(float2 *f, long long n, int grid, cudaStream_t st)
+{
+    if(n <= 0) return cudaSuccess;
+    sqrt3d_kernel<<<grid, 256, 0, st>>>(f, n);
+    return cudaGetLastError();
+}
+
+} // namespace bhcb

@@ -168,6 +168,9 @@ typedef struct bhcb_env_info {
     char run_type[8], beam_type[8];
 } bhcb_env_info;
 int bhcb_check_env(const char *file_root, bhcb_env_info *info, char *msg, size_t n);
+/* The same check for a 3-D environment: dims as bhcb_field_shape3d, nrays
+   the number of rays (jobs) the run traces. Needs no GPU. */
+int bhcb_check_env3d(const char *file_root, int32_t *dims, int64_t *nrays, char *msg, size_t n);
 
 /* Allocation-free run (no counterpart in the reference). For callers that
    must not allocate device memory once running — work inside a budget owned
@@ -187,6 +190,28 @@ int bhcb_check_env(const char *file_root, bhcb_env_info *info, char *msg, size_t
 #define BHCB_NOALLOC_MAX_FIELD (1 << 21)
 int bhcb_run_noalloc(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void *field_dev, size_t bytes,
                      char *msg, size_t msg_len);
+
+/* BELLHOP3D field modes (bhc::setup / run / writeout with O3D = R3D = true).
+   A context holds either 2-D or 3-D environments (bhcb_clear switches).
+   Supported: RunType 'C' / 'S' / 'I' with RunType(6) = '3', Cartesian
+   geometric hat ('G', '^', ' ') and Gaussian ('B') beams, 1-D profiles
+   ('C', 'N', 'S', 'P') or the hexahedral grid ('H', src/ssp.hpp:215-305),
+   flat or 'R' gridded altimetry / bathymetry (src/boundary.hpp:66-160),
+   boundary conditions 'V', 'R', 'A', 'G'. bhcb_run / bhcb_launch trace and
+   evaluate the whole batch; bhcb_copy_field, bhcb_field_device and
+   bhcb_writeout take ifreq 0. */
+/* bhc::setup<true, true> (src/api.cpp:217-298) on FileRoot.env as a 3-D run. */
+int bhcb_setup3d(bhcb_ctx *ctx, const char *file_root);
+/* Append another 3-D environment to the batch. */
+int bhcb_add_env3d(bhcb_ctx *ctx, const char *file_root, int32_t *env_index);
+/* Field layout [NSz][NSx][NSy][Ntheta][NRz][NRr] complex float (GetFieldAddr,
+   src/common.hpp:393-405); dims = {NSz, NSx, NSy, Ntheta, NRz, NRr}. */
+int bhcb_field_shape3d(bhcb_ctx *ctx, int32_t env_index, int32_t *dims);
+/* Source and receiver coordinates of a 3-D environment (Position,
+   include/bhc/structs.hpp:278-295): Sx, Sy, Rr in m, Sz, Rz in m, theta in
+   degrees; each pointer may be NULL, sizes from bhcb_field_shape3d. */
+int bhcb_grid3d(bhcb_ctx *ctx, int32_t env_index, double *sx, double *sy, float *sz, double *rr, float *rz,
+                double *theta);
 
 /* Library version string. */
 const char *bhcb_version(void);

@@ -1,0 +1,155 @@
+"""3-D (BELLHOP3D) golden cases: small environments written as the reference's
+input files (.env, plus .ssp for the hexahedral grid and .bty / .ati grids).
+
+Each case is a dict of file suffix -> text. The shapes follow the reference's
+own 3-D test environments (Munk slice, hexahedral Munk, seamount and
+paraboloid grids), scaled down so that the reference traces each in seconds.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+MUNK = [(0.0, 1548.52), (200.0, 1530.29), (250.0, 1526.69), (400.0, 1517.78), (600.0, 1509.49),
+        (800.0, 1504.30), (1000.0, 1501.38), (1200.0, 1500.14), (1400.0, 1500.12), (1600.0, 1501.02),
+        (1800.0, 1502.57), (2000.0, 1504.62), (2200.0, 1507.02), (2400.0, 1509.69), (2600.0, 1512.55),
+        (2800.0, 1515.56), (3000.0, 1518.67), (3200.0, 1521.85), (3400.0, 1525.10), (3600.0, 1528.38),
+        (3800.0, 1531.70), (4000.0, 1535.04), (4200.0, 1538.39), (4400.0, 1541.76), (4600.0, 1545.14),
+        (4800.0, 1548.52), (5000.0, 1551.91)]
+
+
+def _vec(vals):
+    return " ".join("%.6f" % v for v in vals) + " /"
+
+
+def env_text(*, title, freq, ssp_opt, depth, ssp, bot, sx, sy, sz, rz, rr_km, theta, run_type, alpha, beta,
+             step, box_km, box_z, nrz_range=None, rr_range=None):
+    """One BELLHOP3D .env file. rz / rr given either as explicit lists or as
+    (n, first, last) ranges that the reader expands (SubTab)."""
+    L = ["'%s'" % title, "%g" % freq, "1", "'%s'" % ssp_opt, "%d 0.0 %g" % (0, depth)]
+    L += ["%g %g /" % (z, c) for z, c in ssp]
+    L += ["'%s' 0.0" % bot[0]]
+    if bot[0] == "A":
+        L += ["%g %g 0.0 %g %g /" % (depth, bot[1], bot[2], bot[3])]
+    L += ["%d" % len(sx), _vec(sx), "%d" % len(sy), _vec(sy), "%d" % len(sz), _vec(sz)]
+    if nrz_range:
+        L += ["%d" % nrz_range[0], "%g %g /" % nrz_range[1:]]
+    else:
+        L += ["%d" % len(rz), _vec(rz)]
+    if rr_range:
+        L += ["%d" % rr_range[0], "%g %g /" % rr_range[1:]]
+    else:
+        L += ["%d" % len(rr_km), _vec(rr_km)]
+    L += ["%d" % len(theta), _vec(theta)]
+    L += ["'%s'" % run_type]
+    L += ["%d" % alpha[0], "%g %g /" % alpha[1:]]
+    L += ["%d" % beta[0], "%g %g /" % beta[1:]]
+    L += ["%g %g %g %g" % (step, box_km[0], box_km[1], box_z)]
+    return "\n".join(L) + "\n"
+
+
+def grid_text(x_km, y_km, z):
+    """'R' altimetry / bathymetry grid: z[ix, iy] in m, one row per y."""
+    L = ["'R'", "%d" % len(x_km), _vec(x_km), "%d" % len(y_km), _vec(y_km)]
+    for iy in range(len(y_km)):
+        L.append(" ".join("%.4f" % z[ix, iy] for ix in range(len(x_km))))
+    return "\n".join(L) + "\n"
+
+
+def hex_ssp_text(x_km, y_km, z, c):
+    """Hexahedral .ssp: c[ix, iy, iz] in m/s, one record per (iz, iy) of Nx values."""
+    L = ["%d" % len(x_km), _vec(x_km)[:-2], "%d" % len(y_km), _vec(y_km)[:-2], "%d" % len(z), _vec(z)[:-2]]
+    for iz in range(len(z)):
+        for iy in range(len(y_km)):
+            L.append(" ".join("%.4f" % c[ix, iy, iz] for ix in range(len(x_km))))
+    return "\n".join(L) + "\n"
+
+
+def _munk_slice(run_type, **kw):
+    args = dict(title="Munk slice 3-D", freq=50.0, ssp_opt="CVW", depth=5000.0, ssp=MUNK,
+                bot=("A", 1600.0, 1.8, 0.8), sx=[0.0], sy=[0.0], sz=[1000.0], rz=None, rr_km=None,
+                theta=[0.0, 2.0, 5.0], run_type=run_type, alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0),
+                step=200.0, box_km=(31.0, 31.0), box_z=5500.0, nrz_range=(51, 0.0, 5000.0),
+                rr_range=(101, 0.0, 30.0))
+    args.update(kw)
+    return {".env": env_text(**args)}
+
+
+def munk3d_gauss():
+    return _munk_slice("CB   3")
+
+
+def munk3d_hat():
+    return _munk_slice("CG   3")
+
+
+def munk3d_hat_incoherent():
+    return _munk_slice("IG   3")
+
+
+def munk3d_gauss_semicoherent():
+    return _munk_slice("SB   3")
+
+
+def munk3d_sources():
+    """Several sources in x, y and z: exercises the job and field layouts."""
+    return _munk_slice("CB   3", sx=[0.0, 1.0], sy=[-0.5, 0.5], sz=[800.0, 1500.0], alpha=(61, -15.0, 15.0),
+                       beta=(11, -6.0, 6.0), theta=[0.0, 3.0], rr_range=(61, 0.0, 20.0), box_km=(25.0, 25.0))
+
+
+def hex3d_gauss():
+    """Hexahedral SSP: a Munk profile whose axis deepens along x and tilts in y."""
+    xs = np.array([-30.0, 0.0, 30.0])
+    ys = np.array([-30.0, 0.0, 30.0])
+    z = np.array([0.0, 500.0, 1000.0, 1500.0, 2500.0, 3500.0, 5000.0])
+    zp, cp = np.array(MUNK).T
+    c = np.zeros((3, 3, len(z)))
+    for ix, x in enumerate(xs):
+        for iy, y in enumerate(ys):
+            shift = 8.0 * x + 4.0 * y          # m of axis depth per km
+            c[ix, iy] = np.interp(z - shift, zp, cp)
+    env = env_text(title="hexahedral Munk", freq=50.0, ssp_opt="HVW", depth=5000.0,
+                   ssp=[(float(zz), 1500.0) for zz in z], bot=("A", 1600.0, 1.8, 0.8), sx=[0.0], sy=[0.0],
+                   sz=[1000.0], rz=None, rr_km=None, theta=[0.0, 3.0, 90.0], run_type="CB   3",
+                   alpha=(101, -18.0, 18.0), beta=(31, -12.0, 12.0), step=200.0, box_km=(25.0, 25.0),
+                   box_z=5500.0, nrz_range=(41, 0.0, 5000.0), rr_range=(81, 0.0, 20.0))
+    return {".env": env, ".ssp": hex_ssp_text(xs, ys, z, c)}
+
+
+def seamount3d_gauss():
+    """Gaussian seamount on an 'R' bathymetry grid, halfspace bottom."""
+    xs = np.linspace(-12.0, 12.0, 25)
+    ys = np.linspace(-12.0, 12.0, 25)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    z = 3000.0 - 2200.0 * np.exp(-((X - 5.0) ** 2 + (Y - 1.0) ** 2) / 4.0)
+    env = env_text(title="seamount 3-D", freq=100.0, ssp_opt="CVW", depth=3000.0,
+                   ssp=[(0.0, 1500.0), (3000.0, 1500.0)], bot=("A", 1650.0, 1.5, 0.5), sx=[0.0], sy=[0.0],
+                   sz=[250.0], rz=[400.0, 1000.0], rr_km=None, theta=[0.0, 10.0, 20.0, 350.0], run_type="CB   3",
+                   alpha=(91, -30.0, 30.0), beta=(73, -180.0, 180.0), step=100.0, box_km=(11.0, 11.0),
+                   box_z=3100.0, rr_range=(101, 0.0, 10.0))
+    return {".env": env.replace("'A' 0.0", "'A~' 0.0"), ".bty": grid_text(xs, ys, z)}
+
+
+def parabot3d_hat():
+    """Paraboloid altimetry-free bottom grid with hat beams and a rigid-free mix."""
+    xs = np.linspace(-6.0, 6.0, 13)
+    ys = np.linspace(-6.0, 6.0, 13)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    z = 600.0 + 12.0 * (X ** 2 + Y ** 2)
+    env = env_text(title="paraboloid bowl", freq=200.0, ssp_opt="CVW", depth=1100.0,
+                   ssp=[(0.0, 1500.0), (1100.0, 1500.0)], bot=("R",), sx=[0.0], sy=[0.0], sz=[100.0],
+                   rz=None, rr_km=None, theta=[0.0, 45.0, 90.0], run_type="CG   3", alpha=(61, -40.0, 40.0),
+                   beta=(37, 0.0, 360.0), step=50.0, box_km=(5.5, 5.5), box_z=1200.0, nrz_range=(21, 0.0, 1000.0),
+                   rr_range=(51, 0.0, 5.0))
+    return {".env": env.replace("'R' 0.0", "'R~' 0.0"), ".bty": grid_text(xs, ys, z)}
+
+
+CASES3D = {
+    "munk3d_gauss": munk3d_gauss,
+    "munk3d_hat": munk3d_hat,
+    "munk3d_hat_incoherent": munk3d_hat_incoherent,
+    "munk3d_gauss_semicoherent": munk3d_gauss_semicoherent,
+    "munk3d_sources": munk3d_sources,
+    "hex3d_gauss": hex3d_gauss,
+    "seamount3d_gauss": seamount3d_gauss,
+    "parabot3d_hat": parabot3d_hat,
+}

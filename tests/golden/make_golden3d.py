@@ -1,0 +1,56 @@
+"""Generate the 3-D golden TL fixtures from the reference itself.
+
+Runs the reference's own bellhopcxx (compiled from its sources by
+oracle/Makefile into oracle/_ref/) as a 3-D run (-3) on every case of
+tests/golden/cases3d.py and stores, per case, the input files' text and the
+scaled complex field as tests/golden/<case>.npz. The GPU tests write the input
+files back from the fixture, so they need neither the reference nor this
+script at run time. Run from the repository root:
+
+    make -C oracle ref && python tests/golden/make_golden3d.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from bellhopcuda_b200.shdfile import read_shd  # noqa: E402
+from cases3d import CASES3D  # noqa: E402
+
+EXE = os.path.join(ROOT, "oracle", "_ref", "bellhopcxx")
+
+
+def main(names=None):
+    with tempfile.TemporaryDirectory() as d:
+        for name, fn in CASES3D.items():
+            if names and name not in names:
+                continue
+            files = fn()
+            root = os.path.join(d, name)
+            for suffix, text in files.items():
+                with open(root + suffix, "w") as f:
+                    f.write(text)
+            t0 = time.time()
+            r = subprocess.run([EXE, "-3", "-1", root], capture_output=True, text=True)
+            if r.returncode != 0:
+                raise SystemExit("reference failed on %s:\n%s%s" % (name, r.stdout[-2000:], r.stderr[-2000:]))
+            shd = read_shd(root + ".shd")
+            texts = {"file_" + suffix[1:]: np.array(text) for suffix, text in files.items()}
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), field=shd["field"],
+                                rr=shd["rr"], rz=shd["rz"], sz=shd["sz"], theta=shd["theta"], **texts)
+            print(name, shd["field"].shape, "%.3g" % float(np.abs(shd["field"]).max()),
+                  "%.1fs" % (time.time() - t0))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -1,0 +1,125 @@
+"""GPU parity of the 3-D (BELLHOP3D) field modes against the reference itself.
+
+The fixtures in tests/golden/*3d*.npz hold each case's input files and the
+field the reference's own bellhopcxx computed as a 3-D run (made by
+tests/golden/make_golden3d.py). The product runs the same files through the C
+ABI. Tolerance: TL = -20 log10|p| within 0.5 dB RMS over receivers where the
+reference's TL < 100 dB (the reference's own FP64 runs differ between
+thread counts by float atomics; the same bound as the 2-D path).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import bellhopcuda_b200 as B
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = sorted(glob.glob(os.path.join(HERE, "golden", "*3d*.npz")))
+TL_MAX = 100.0
+
+
+def write_case(npz, root):
+    for k in npz.files:
+        if k.startswith("file_"):
+            with open(root + "." + k[5:], "w") as f:
+                f.write(str(npz[k]))
+
+
+def tl_err(got, ref):
+    a, b = B.tl_db(got), B.tl_db(ref)
+    m = b < TL_MAX
+    d = np.abs(a[m] - b[m])
+    d = np.where(np.isfinite(d), d, 1e3)
+    return float(np.sqrt(np.mean(d ** 2))), int(m.sum())
+
+
+def to_file_order(u):
+    """product [isz][isx][isy][itheta][iz][ir] -> .shd order [isx][isy][itheta][isz][iz][ir]"""
+    return np.transpose(u, (1, 2, 3, 0, 4, 5))
+
+
+@pytest.mark.parametrize("path", GOLD, ids=[os.path.basename(p)[:-4] for p in GOLD])
+def test_3d_field_matches_reference(path, workdir):
+    g = np.load(path)
+    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.setup3d(root)
+        t.run()
+        u = t.field3d(0)
+        st = t.stats()
+        grid = t.grid3d(0)
+    assert st["err_bits"] == 0
+    assert st["rays"] > 0 and st["segments"] > 0 and st["evals"] > 0
+    np.testing.assert_allclose(grid["rr"], g["rr"])
+    np.testing.assert_array_equal(grid["rz"], g["rz"])
+    np.testing.assert_allclose(grid["theta"], g["theta"])
+    got = to_file_order(u)
+    ref = g["field"]
+    assert got.shape == ref.shape
+    err, n = tl_err(got, ref)
+    assert n > 0
+    assert err < 0.5, "TL RMS %.3f dB over %d receivers" % (err, n)
+
+
+def test_3d_writeout_shd(workdir):
+    from bellhopcuda_b200.shdfile import read_shd
+    path = [p for p in GOLD if "munk3d_sources" in p][0]
+    g = np.load(path)
+    root = os.path.join(workdir, "wr3d")
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.setup3d(root)
+        t.run()
+        u = t.field3d(0)
+        t.writeout(root)
+    shd = read_shd(root + ".shd")
+    np.testing.assert_array_equal(shd["field"], to_file_order(u))
+    np.testing.assert_allclose(shd["theta"], g["theta"])
+    np.testing.assert_array_equal(shd["sz"], g["sz"])
+
+
+def test_3d_batch_equals_single_runs(workdir):
+    """Several 3-D environments in one launch give each one's own field."""
+    names = ["munk3d_hat", "hex3d_gauss", "parabot3d_hat"]
+    roots = []
+    for n in names:
+        g = np.load(os.path.join(HERE, "golden", n + ".npz"))
+        root = os.path.join(workdir, "b3_" + n)
+        write_case(g, root)
+        roots.append(root)
+    singles = []
+    for r in roots:
+        with B.Tracer(precision=B.PREC_FP64) as t:
+            t.setup3d(r)
+            t.run()
+            singles.append(t.field3d(0))
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        for r in roots:
+            t.add_env3d(r)
+        t.run()
+        batch = [t.field3d(i) for i in range(len(roots))]
+        assert t.stats()["groups"] == len(roots)
+    for a, b in zip(batch, singles):
+        np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-6 * np.abs(b).max())
+
+
+def test_3d_small_max_memory_runs_in_waves(workdir):
+    g = np.load(os.path.join(HERE, "golden", "munk3d_gauss.npz"))
+    root = os.path.join(workdir, "w3d")
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.setup3d(root)
+        t.run()
+        full, st = t.field3d(0), t.stats()
+    small = st["segments"] * 288 // 3 + (8 << 20) + full.nbytes + (64 << 20)
+    with B.Tracer(precision=B.PREC_FP64, max_memory=small) as t:
+        t.setup3d(root)
+        t.run()
+        waved, st2 = t.field3d(0), t.stats()
+    assert st2["segments"] == st["segments"]
+    np.testing.assert_allclose(waved, full, rtol=1e-4, atol=1e-6 * np.abs(full).max())

@@ -135,3 +135,65 @@ def test_reader_accepts_reference_inputs(name, workdir):
         B.check_env(os.path.join(workdir, name))
     except B.BhcbError as e:
         assert "not supported" in str(e) or "not a field mode" in str(e), str(e)
+
+
+# ------------------------------------------------------------------ 3-D reader
+GOLD3D = sorted(n[:-4] for n in os.listdir(os.path.join(HERE, "golden")) if "3d" in n and n.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", GOLD3D)
+def test_reader3d_sizes_match_reference_fixture(name, workdir):
+    """The 3-D reader sees the grid the reference wrote in its .shd."""
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    root = os.path.join(workdir, "r3_" + name)
+    for k in g.files:
+        if k.startswith("file_"):
+            with open(root + "." + k[5:], "w") as f:
+                f.write(str(g[k]))
+    info = B.check_env3d(root)
+    nsx, nsy, nth, nsz, nrz, nrr = g["field"].shape
+    assert info["dims"] == (nsz, nsx, nsy, nth, nrz, nrr)
+    assert info["nrays"] > 0
+
+
+def test_reader3d_fixes_360_degree_sweep(workdir):
+    """CheckFix360Sweep drops the duplicate bearing of a full 360-degree fan."""
+    from cases3d import CASES3D
+    root = os.path.join(workdir, "sweep3d")
+    for suffix, text in CASES3D["parabot3d_hat"]().items():
+        with open(root + suffix, "w") as f:
+            f.write(text)
+    info = B.check_env3d(root)
+    assert info["nrays"] == 61 * 36      # 37 bearings 0..360 -> 36
+
+
+def test_reader3d_rejects_2d_runs_and_unsupported_beams(workdir):
+    from cases3d import CASES3D
+    text = CASES3D["munk3d_gauss"]()[".env"]
+    root = os.path.join(workdir, "bad3d")
+    with open(root + ".env", "w") as f:
+        f.write(text.replace("'CB   3'", "'CB    '"))
+    with pytest.raises(B.BhcbError, match="RunType"):
+        B.check_env3d(root)
+    with open(root + ".env", "w") as f:
+        f.write(text.replace("'CB   3'", "'CR   3'"))
+    with pytest.raises(B.BhcbError, match="not supported"):
+        B.check_env3d(root)
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_INPUTS), reason="reference inputs not present")
+@pytest.mark.parametrize("name", ["Munkslice3dGaussian", "Munkslice3dHatCart", "MunkRot3D", "DoubleSeamount3D",
+                                  "PerfectWedge3dHat", "KR3dGaussian"])
+def test_reader3d_accepts_reference_inputs(name, workdir):
+    src = os.path.join(REFERENCE_INPUTS, name)
+    if not os.path.exists(src + ".env"):
+        pytest.skip("no such input")
+    import shutil
+    for ext in (".env", ".bty", ".ati", ".ssp", ".sbp"):
+        if os.path.exists(src + ext):
+            shutil.copy(src + ext, os.path.join(workdir, name + ext))
+    try:
+        info = B.check_env3d(os.path.join(workdir, name))
+        assert info["nrays"] > 0
+    except B.BhcbError as e:
+        assert "not supported" in str(e), str(e)
