@@ -332,12 +332,71 @@ __device__ __forceinline__ bool core3(const SegRec3 &R, double s, double n1, dou
     return true;
 }
 
+// first index with (double)rz >= z (n if none)
+__device__ __forceinline__ int first_depth_at_or_above(const float *rz, int n, double z)
+{
+    int lo = 0, hi = n;
+    while(lo < hi) {
+        const int m = (lo + hi) >> 1;
+        if((double)rz[m] < z) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+// last index with (double)rz <= z (-1 if none)
+__device__ __forceinline__ int last_depth_at_or_below(const float *rz, int n, double z)
+{
+    int lo = 0, hi = n;
+    while(lo < hi) {
+        const int m = (lo + hi) >> 1;
+        if((double)rz[m] <= z) lo = m + 1; else hi = m;
+    }
+    return lo - 1;
+}
+
+// A (range, bearing) pair none of whose depths can pass InfluenceGeoCore's
+// beam-window test. With A the row-scaled interpolated q (2x2), the accepted
+// normal offsets satisfy (n1, n2) = A (+-n1', +-n2'), so their length is at
+// most |A|_F |(n1', n2')| <= |A|_F w (w = 4 for Gaussian n1' + n2' <= 4,
+// sqrt 2 for hat max(n1', n2') <= 1). That length is at least the distance
+// between the receivers' vertical line and the ray line, m' / |t_xy|, and
+// |A(s)|_F is convex in s, so its largest value over the depth window is at
+// one of the window's two ends. The margin keeps rounding from dropping a
+// contribution the per-receiver test would accept.
+__device__ __forceinline__ bool pair_outside_beam(const SegRec3 &R, double dxr, double dyr, double mprime,
+                                                  double z_lo, double z_hi, bool gauss)
+{
+    const double th = sqrt(R.rayt[0] * R.rayt[0] + R.rayt[1] * R.rayt[1]);
+    if(!(th > 0.0)) return false;
+    const double h = dxr * R.rayt[0] + dyr * R.rayt[1];
+    double f = 0.0;
+#pragma unroll
+    for(int e = 0; e < 2; ++e) {
+        const double s = (h + ((e ? z_hi : z_lo) - R.x0[2]) * R.rayt[2]) / R.rlen;
+        const double a0 = (R.q0[0] + s * R.dq[0]) * R.rcp_q0, a2 = (R.q0[2] + s * R.dq[2]) * R.rcp_q0;
+        const double a1 = (R.q0[1] + s * R.dq[1]) * R.rcp_qhat0, a3 = (R.q0[3] + s * R.dq[3]) * R.rcp_qhat0;
+        f = max(f, a0 * a0 + a1 * a1 + a2 * a2 + a3 * a3);
+    }
+    const double w = gauss ? 4.0 : 1.4142135623730951;
+    return mprime > th * w * sqrt(f) * (1.0 + 1e-6) + 1e-9;
+}
+
+// Work is flattened twice per warp: (segment, range, bearing) pairs over the
+// warp's 32 records, then (pair, depth) items over the pairs that survive the
+// bearing rejections, so that every lane evaluates receivers.
 __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     const SegRec3 *__restrict__ segs, unsigned long long nseg, const GroupDev *__restrict__ groups, int ngroups,
     float2 *field, RunCounters *ctr)
 {
+    // per record of the warp's chunk
     __shared__ int s_incl[WARPS3][32];
     __shared__ int s_grp[WARPS3][32];
+    __shared__ long long s_fbase[WARPS3][32];    // field offset of (isz, isx, isy)
+    __shared__ double s_xs[WARPS3][32], s_ys[WARPS3][32];
+    // per surviving pair of a 32-pair batch
+    __shared__ int s_pincl[WARPS3][32];
+    __shared__ int s_prec[WARPS3][32], s_piz0[WARPS3][32];
+    __shared__ double s_pdx[WARPS3][32], s_pdy[WARPS3][32];
+    __shared__ long long s_poff[WARPS3][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned long long nchunk = (nseg + 31) / 32;
     unsigned long long nevals = 0;
@@ -349,8 +408,15 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
             const int job = __ldg(&segs[idx].job);
             if(job >= 0) {
                 g = find_group(groups, ngroups, job);
+                const GroupDev &G = groups[g];
+                const Env3Dev &E = *G.env3;
                 const int lo = __ldg(&segs[idx].ir_lo), hi = __ldg(&segs[idx].ir_hi);
-                n = (hi - lo + 1) * groups[g].env3->ntheta;
+                n = (hi - lo + 1) * E.ntheta;
+                const Job3 J = job_indices3(E, (int)(job - G.job_base));
+                s_fbase[w][lane] = G.field_base
+                    + (long long)(((size_t)J.isz * E.nsx + J.isx) * E.nsy + J.isy) * E.ntheta * E.nrz * E.nrr;
+                s_xs[w][lane] = E.sx[J.isx];
+                s_ys[w][lane] = E.sy[J.isy];
             }
         }
         int incl = n;
@@ -359,57 +425,88 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
             const int v = __shfl_up_sync(0xffffffffu, incl, o);
             if(lane >= o) incl += v;
         }
-        __syncwarp();
         s_incl[w][lane] = incl;
         s_grp[w][lane] = g;
         __syncwarp();
         const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for(int k = lane; k < total; k += 32) {
-            int lo = 0, hi = 31;   // first j with incl[j] > k
-            while(lo < hi) {
-                const int m = (lo + hi) >> 1;
-                if(s_incl[w][m] > k) hi = m; else lo = m + 1;
-            }
-            const int j = lo;
-            const int local = k - (j ? s_incl[w][j - 1] : 0);
-            const SegRec3 &R = segs[ch * 32 + j];
-            const GroupDev &G = groups[s_grp[w][j]];
-            const Env3Dev &E = *G.env3;
-            const int itheta = local % E.ntheta;
-            const int ir = R.ir_lo + local / E.ntheta;
-            const Job3 J = job_indices3(E, (int)(R.job - G.job_base));
-            const double xsx = E.sx[J.isx], xsy = E.sy[J.isy];
-            const double tc = E.tcs[2 * itheta], ts = E.tcs[2 * itheta + 1];
-            const double rr = E.rr[ir];
-            const double xrx = xsx + rr * tc, xry = xsy + rr * ts;
-            const double rtx = R.rayt[0], rty = R.rayt[1], rtz = R.rayt[2];
-            const double dxr = xrx - R.x0[0], dyr = xry - R.x0[1];
-            const bool gauss = E.gaussian != 0;
-            if(!gauss) {
+        for(int kb = 0; kb < total; kb += 32) {
+            // ---- pair stage: bearing rejections and the depth window
+            const int k = kb + lane;
+            int m = 0;
+            if(k < total) {
+                int lo = 0, hi = 31;   // first record j with incl[j] > k
+                while(lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if(s_incl[w][mid] > k) hi = mid; else lo = mid + 1;
+                }
+                const int j = lo;
+                const int local = k - (j ? s_incl[w][j - 1] : 0);
+                const SegRec3 &R = segs[ch * 32 + j];
+                const Env3Dev &E = *groups[s_grp[w][j]].env3;
+                const int itheta = local % E.ntheta;
+                const int ir = R.ir_lo + local / E.ntheta;
+                const double xsx = s_xs[w][j], xsy = s_ys[w][j];
+                const double tc = E.tcs[2 * itheta], ts = E.tcs[2 * itheta + 1];
+                const double rr = E.rr[ir];
+                const double xrx = xsx + rr * tc, xry = xsy + rr * ts;
+                const double rtx = R.rayt[0], rty = R.rayt[1];
+                const double dxr = xrx - R.x0[0], dyr = xry - R.x0[1];
+                const bool gauss = E.gaussian != 0;
                 const double mprime = fabs(dxr * (-rty) + dyr * rtx);
-                if(mprime > 1.0 * R.ldiag) continue;
+                bool keep = gauss || !(mprime > 1.0 * R.ldiag);
+                keep = keep && !((xrx - xsx) * (R.x0[0] - xsx) + (xry - xsy) * (R.x0[1] - xsy) < 0.0);
+                const double nrz = rtx * tc - rty * (-ts);
+                keep = keep && !(fabs(nrz) < 1e-9);
+                if(keep) {
+                    const double Lz = (gauss ? 4.0 : 1.0) * R.ldiag / fabs(nrz);
+                    const double zmin = R.zlo - Lz, zmax = R.zhi + Lz;
+                    // receiver depths are sorted: the window is the index range [iz0, iz1]
+                    const int iz0 = first_depth_at_or_above(E.rz, E.nrz, zmin);
+                    const int iz1 = last_depth_at_or_below(E.rz, E.nrz, zmax);
+                    if(iz0 <= iz1
+                       && !pair_outside_beam(R, dxr, dyr, mprime, (double)E.rz[iz0], (double)E.rz[iz1], gauss)) {
+                        m = iz1 - iz0 + 1;
+                        s_prec[w][lane] = j;
+                        s_piz0[w][lane] = iz0;
+                        s_pdx[w][lane] = dxr;
+                        s_pdy[w][lane] = dyr;
+                        s_poff[w][lane] = s_fbase[w][j] + (long long)itheta * E.nrz * E.nrr + ir;
+                    }
+                }
             }
-            if((xrx - xsx) * (R.x0[0] - xsx) + (xry - xsy) * (R.x0[1] - xsy) < 0.0) continue;
-            const double nrz = rtx * tc - rty * (-ts);
-            if(fabs(nrz) < 1e-9) continue;
-            const double Lz = (gauss ? 4.0 : 1.0) * R.ldiag / fabs(nrz);
-            const double zmin = R.zlo - Lz, zmax = R.zhi + Lz;
-            const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
-            const size_t base = ((((size_t)J.isz * E.nsx + J.isx) * E.nsy + J.isy) * E.ntheta + itheta)
-                * (size_t)E.nrz * E.nrr + ir;
-            for(int iz = 0; iz < E.nrz; ++iz) {
-                const double z = (double)E.rz[iz];
-                if(z < zmin || z > zmax) continue;
-                const double dz = z - R.x0[2];
-                const double s = (dxr * rtx + dyr * rty + dz * rtz) / R.rlen;
+            int pincl = m;
+#pragma unroll
+            for(int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, pincl, o);
+                if(lane >= o) pincl += v;
+            }
+            s_pincl[w][lane] = pincl;
+            __syncwarp();
+            const int ptotal = __shfl_sync(0xffffffffu, pincl, 31);
+            // ---- receiver stage: one (pair, depth) item per lane
+            for(int q = lane; q < ptotal; q += 32) {
+                int lo = 0, hi = 31;
+                while(lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if(s_pincl[w][mid] > q) hi = mid; else lo = mid + 1;
+                }
+                const int pi = lo;
+                const int iz = s_piz0[w][pi] + q - (pi ? s_pincl[w][pi - 1] : 0);
+                const int j = s_prec[w][pi];
+                const SegRec3 &R = segs[ch * 32 + j];
+                const Env3Dev &E = *groups[s_grp[w][j]].env3;
+                const double dxr = s_pdx[w][pi], dyr = s_pdy[w][pi];
+                const double dz = (double)E.rz[iz] - R.x0[2];
+                const double sv = (dxr * R.rayt[0] + dyr * R.rayt[1] + dz * R.rayt[2]) / R.rlen;
                 const double n1 = fabs(dxr * R.e1[0] + dyr * R.e1[1] + dz * R.e1[2]);
                 const double n2 = fabs(dxr * R.e2[0] + dyr * R.e2[1] + dz * R.e2[2]);
+                const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
                 float2 df;
-                if(!core3(R, s, n1, n2, gauss, E.coherent != 0, omega, df)) continue;
-                float2 *dst = field + G.field_base + base + (size_t)iz * E.nrr;
-                atomicAdd(dst, df);
+                if(!core3(R, sv, n1, n2, E.gaussian != 0, E.coherent != 0, omega, df)) continue;
+                atomicAdd(field + s_poff[w][pi] + (long long)iz * E.nrr, df);
                 ++nevals;
             }
+            __syncwarp();
         }
         __syncwarp();
     }

@@ -11,6 +11,11 @@ the reference, the oracle and this library.
                   uniform in 3000-5000 m over 100 km, 10 log-spaced frequencies
                   50-500 Hz, 20001 rays over +-30 deg, 501 x 2001 receivers.
 * ``batch_envs`` — many small uneven spline-SSP environments for batched runs.
+* ``c4_3d``     — 3-D Gaussian-beam TL (or arrivals): hexahedral SSP on a
+                  41 x 41 x 51 grid over 80 x 80 km x 5000 m (Munk plus a seeded
+                  warm-core eddy), 'R' bathymetry on a 101 x 101 grid seeded in
+                  3000-5000 m, source 500 m, 200 Hz, 144 bearings x 361
+                  elevations, receivers 36 bearings x 101 depths x 501 ranges.
 """
 from __future__ import annotations
 
@@ -20,6 +25,7 @@ from typing import List
 import numpy as np
 
 from .envfile import EnvSpec
+from . import envfile3d
 
 
 def munk_c(z, eps=0.00737):
@@ -89,3 +95,47 @@ def batch_envs(n=256, seed=1003, scale=1.0) -> List[EnvSpec]:
             nrr=nrr, rr_km=(0.0, rmax), run_type="CB RR ", nalpha=na, alpha=(-30.0, 30.0),
             deltas=0.0, box_z=depth + 100.0, box_r_km=rmax + 1.0))
     return out
+
+
+def _smooth2d(a, sigma):
+    """Separable Gaussian smoothing with reflecting edges."""
+    r = int(math.ceil(3 * sigma))
+    k = np.exp(-0.5 * (np.arange(-r, r + 1) / sigma) ** 2)
+    k /= k.sum()
+    for ax in (0, 1):
+        pad = [(0, 0), (0, 0)]
+        pad[ax] = (r, r)
+        b = np.pad(a, pad, mode="reflect")
+        a = np.apply_along_axis(lambda v: np.convolve(v, k, mode="valid"), ax, b)
+    return a
+
+
+def c4_3d(seed=1004, run_type="CB   3", scale=1.0, nalpha=361, nbeta=144, ntheta=36, nrz=101, nrr=501,
+          freq=200.0, step=100.0):
+    """The 3-D workload as {suffix: file text}. ``scale`` < 1 shrinks the ray
+    fan and the receiver grid (for parity cases); the environment is the same."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    # hexahedral SSP: Munk + warm-core eddy (+10 m/s, radius 20 km, depth scale 800 m)
+    hx = np.linspace(-40.0, 40.0, 41)
+    hy = np.linspace(-40.0, 40.0, 41)
+    hz = np.linspace(0.0, 5000.0, 51)
+    ex, ey = rng.uniform(-20.0, 20.0, 2)
+    X, Y, Z = np.meshgrid(hx, hy, hz, indexing="ij")
+    r2 = (X - ex) ** 2 + (Y - ey) ** 2
+    c = munk_c(Z) + 10.0 * np.exp(-r2 / (2.0 * 20.0 ** 2)) * np.exp(-Z / 800.0)
+    # bathymetry: U(3000, 5000) smoothed, rescaled back to 3000-5000 m
+    bx = np.linspace(-40.0, 40.0, 101)
+    by = np.linspace(-40.0, 40.0, 101)
+    b = _smooth2d(rng.uniform(3000.0, 5000.0, (101, 101)), 4.0)
+    b = 3000.0 + 2000.0 * (b - b.min()) / (b.max() - b.min())
+    na = max(3, int(round(nalpha * scale)) | 1)
+    nb = max(4, int(round(nbeta * scale)))
+    env = envfile3d.env_text(
+        title="3-D hexahedral Munk + eddy, gridded bathymetry", freq=freq, ssp_opt="HVW", depth=5000.0,
+        ssp=[(float(z), float(munk_c(z))) for z in hz], bot=("A~", 1600.0, 1.8, 0.8), sx=[0.0], sy=[0.0],
+        sz=[500.0], rz=None, rr_km=None, theta=None, run_type=run_type, alpha=(na, -30.0, 30.0),
+        beta=(nb + 1, 0.0, 360.0), step=step, box_km=(39.0, 39.0), box_z=5100.0,
+        nrz_range=(max(2, int(round(nrz * scale))), 0.0, 5000.0),
+        rr_range=(max(2, int(round(nrr * scale))), 0.0, 38.0),
+        theta_range=(max(1, int(round(ntheta * scale))), 0.0, 360.0 - 360.0 / max(1, int(round(ntheta * scale)))))
+    return {".env": env, ".ssp": envfile3d.hex_ssp_text(hx, hy, hz, c), ".bty": envfile3d.grid_text(bx, by, b)}

@@ -7,7 +7,13 @@ paraboloid grids), scaled down so that the reference traces each in seconds.
 """
 from __future__ import annotations
 
+import os
+import sys
+
 import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from bellhopcuda_b200.envfile3d import env_text, grid_text, hex_ssp_text  # noqa: E402
 
 MUNK = [(0.0, 1548.52), (200.0, 1530.29), (250.0, 1526.69), (400.0, 1517.78), (600.0, 1509.49),
         (800.0, 1504.30), (1000.0, 1501.38), (1200.0, 1500.14), (1400.0, 1500.12), (1600.0, 1501.02),
@@ -15,53 +21,6 @@ MUNK = [(0.0, 1548.52), (200.0, 1530.29), (250.0, 1526.69), (400.0, 1517.78), (6
         (2800.0, 1515.56), (3000.0, 1518.67), (3200.0, 1521.85), (3400.0, 1525.10), (3600.0, 1528.38),
         (3800.0, 1531.70), (4000.0, 1535.04), (4200.0, 1538.39), (4400.0, 1541.76), (4600.0, 1545.14),
         (4800.0, 1548.52), (5000.0, 1551.91)]
-
-
-def _vec(vals):
-    return " ".join("%.6f" % v for v in vals) + " /"
-
-
-def env_text(*, title, freq, ssp_opt, depth, ssp, bot, sx, sy, sz, rz, rr_km, theta, run_type, alpha, beta,
-             step, box_km, box_z, nrz_range=None, rr_range=None):
-    """One BELLHOP3D .env file. rz / rr given either as explicit lists or as
-    (n, first, last) ranges that the reader expands (SubTab)."""
-    L = ["'%s'" % title, "%g" % freq, "1", "'%s'" % ssp_opt, "%d 0.0 %g" % (0, depth)]
-    L += ["%g %g /" % (z, c) for z, c in ssp]
-    L += ["'%s' 0.0" % bot[0]]
-    if bot[0] == "A":
-        L += ["%g %g 0.0 %g %g /" % (depth, bot[1], bot[2], bot[3])]
-    L += ["%d" % len(sx), _vec(sx), "%d" % len(sy), _vec(sy), "%d" % len(sz), _vec(sz)]
-    if nrz_range:
-        L += ["%d" % nrz_range[0], "%g %g /" % nrz_range[1:]]
-    else:
-        L += ["%d" % len(rz), _vec(rz)]
-    if rr_range:
-        L += ["%d" % rr_range[0], "%g %g /" % rr_range[1:]]
-    else:
-        L += ["%d" % len(rr_km), _vec(rr_km)]
-    L += ["%d" % len(theta), _vec(theta)]
-    L += ["'%s'" % run_type]
-    L += ["%d" % alpha[0], "%g %g /" % alpha[1:]]
-    L += ["%d" % beta[0], "%g %g /" % beta[1:]]
-    L += ["%g %g %g %g" % (step, box_km[0], box_km[1], box_z)]
-    return "\n".join(L) + "\n"
-
-
-def grid_text(x_km, y_km, z):
-    """'R' altimetry / bathymetry grid: z[ix, iy] in m, one row per y."""
-    L = ["'R'", "%d" % len(x_km), _vec(x_km), "%d" % len(y_km), _vec(y_km)]
-    for iy in range(len(y_km)):
-        L.append(" ".join("%.4f" % z[ix, iy] for ix in range(len(x_km))))
-    return "\n".join(L) + "\n"
-
-
-def hex_ssp_text(x_km, y_km, z, c):
-    """Hexahedral .ssp: c[ix, iy, iz] in m/s, one record per (iz, iy) of Nx values."""
-    L = ["%d" % len(x_km), _vec(x_km)[:-2], "%d" % len(y_km), _vec(y_km)[:-2], "%d" % len(z), _vec(z)[:-2]]
-    for iz in range(len(z)):
-        for iy in range(len(y_km)):
-            L.append(" ".join("%.4f" % c[ix, iy, iz] for ix in range(len(x_km))))
-    return "\n".join(L) + "\n"
 
 
 def _munk_slice(run_type, **kw):
