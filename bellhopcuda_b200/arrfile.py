@@ -21,19 +21,33 @@ def _records(raw: bytes):
 
 
 def read_arr_binary(path: str) -> dict:
+    """2-D or 3-D binary arrivals. 3-D files add source x / y (m), receiver
+    bearings (deg) and per arrival the source and receiver azimuths: records of
+    10 floats (a, phase, delay re / im, src decl, src azim, rcvr decl, rcvr
+    azim, top, bottom bounces) against 8 in 2-D. Receivers are listed per
+    source as (bearing, depth, range), range fastest."""
     recs = _records(open(path, "rb").read())
     dim = next(recs)[:4].decode()
+    is3d = "3" in dim
     freq = float(np.frombuffer(next(recs), "<f4", 1)[0])
+    sx = sy = np.zeros(1)
+    if is3d:
+        r = next(recs); nsx = int(np.frombuffer(r, "<i4", 1)[0]); sx = np.frombuffer(r, "<f8", nsx, 4)
+        r = next(recs); nsy = int(np.frombuffer(r, "<i4", 1)[0]); sy = np.frombuffer(r, "<f8", nsy, 4)
     r = next(recs); nsz = int(np.frombuffer(r, "<i4", 1)[0]); sz = np.frombuffer(r, "<f4", nsz, 4)
     r = next(recs); nrz = int(np.frombuffer(r, "<i4", 1)[0]); rz = np.frombuffer(r, "<f4", nrz, 4)
     r = next(recs); nrr = int(np.frombuffer(r, "<i4", 1)[0]); rr = np.frombuffer(r, "<f8", nrr, 4)
+    theta = np.zeros(1)
+    if is3d:
+        r = next(recs); nth = int(np.frombuffer(r, "<i4", 1)[0]); theta = np.frombuffer(r, "<f8", nth, 4)
+    nf = 10 if is3d else 8
     out = []
-    for _isz in range(nsz):
+    for _src in range(nsz * len(sx) * len(sy)):
         maxn = int(np.frombuffer(next(recs), "<i4", 1)[0])
         src = []
-        for _ in range(nrz * nrr):
+        for _ in range(len(theta) * nrz * nrr):
             narr = int(np.frombuffer(next(recs), "<i4", 1)[0])
-            arrs = [np.frombuffer(next(recs), "<f4", 8).copy() for _ in range(narr)]
-            src.append(np.array(arrs, dtype=np.float32).reshape(narr, 8))
+            arrs = [np.frombuffer(next(recs), "<f4", nf).copy() for _ in range(narr)]
+            src.append(np.array(arrs, dtype=np.float32).reshape(narr, nf))
         out.append(dict(maxn=maxn, arrivals=src))
-    return dict(dim=dim, freq=freq, sz=sz, rz=rz, rr=rr, sources=out)
+    return dict(dim=dim, freq=freq, sx=sx, sy=sy, sz=sz, rz=rz, rr=rr, theta=theta, sources=out)

@@ -42,7 +42,7 @@ cudaError_t radix_sort_pairs(uint64_t *, uint32_t *, uint64_t *, uint32_t *, uns
                              int *, cudaStream_t);
 cudaError_t launch_arr_replay(const uint64_t *, const uint32_t *, const ArrCand *, unsigned long long,
                               const GroupDev *, int, const double *, long long, int, int, int, int32_t *,
-                              ArrivalRec *, int, cudaStream_t);
+                              ArrivalRec *, int, cudaStream_t, bool);
 cudaError_t launch_eigen_emit(const uint32_t *, const ArrCand *, unsigned long long, EigenHitRec *, int32_t *, int,
                               const uint64_t *, int, cudaStream_t);
 } // namespace bhcb
@@ -579,7 +579,7 @@ void run_arrivals(bhcb_ctx *c)
         CK(cudaMemsetAsync(c->arr_d.p, 0, cells * (size_t)c->max_narr * sizeof(ArrivalRec), c->stream));
         CK(launch_arr_replay(c->sorted_keys, c->sorted_vals, (const ArrCand *)c->cand.p, n, G, ng, fq,
                              (long long)cells, c->kb.sh_cell, c->max_narr, c->allow_merging, (int32_t *)c->narr_d.p,
-                             (ArrivalRec *)c->arr_d.p, c->sm_count, c->stream));
+                             (ArrivalRec *)c->arr_d.p, c->sm_count, c->stream, false));
     } else {
         c->hits_d.ensure(nn * sizeof(EigenHitRec));
         c->hitfield_d.ensure(nn * sizeof(int32_t));
@@ -731,30 +731,6 @@ int noalloc_job_from_ctx(bhcb_ctx *c, int32_t env, int32_t ifreq, NoAllocJob *jo
 
 namespace {
 // Fortran sequential unformatted records: [int32 n][n bytes][int32 n]
-struct RecWriter {
-    std::vector<uint8_t> cur;
-    std::ofstream &o;
-    explicit RecWriter(std::ofstream &o_) : o(o_) {}
-    template<typename T> void put(const T &v)
-    {
-        const uint8_t *p = reinterpret_cast<const uint8_t *>(&v);
-        cur.insert(cur.end(), p, p + sizeof(T));
-    }
-    void put_bytes(const void *p, size_t n)
-    {
-        const uint8_t *q = reinterpret_cast<const uint8_t *>(p);
-        cur.insert(cur.end(), q, q + n);
-    }
-    void end()
-    {
-        int32_t n = (int32_t)cur.size();
-        o.write((const char *)&n, 4);
-        o.write((const char *)cur.data(), cur.size());
-        o.write((const char *)&n, 4);
-        cur.clear();
-    }
-};
-
 // WriteOutArrivals (src/mode/arr.cpp:88-239), 2-D: binary for RunType 'a',
 // list-directed text for 'A'.
 void write_arrivals(bhcb_ctx *c, const Field &F, const EnvSlot &S, const EnvTables &T, double freq,
@@ -839,7 +815,8 @@ int run3_checked(bhcb_ctx *c)
 {
     bhcb_stats st{};
     uint32_t wb = 0;
-    const uint32_t eb = run3_run(c->r3, c->stream, c->sm_count, c->max_memory, st, wb);
+    const uint32_t eb = run3_run(c->r3, c->stream, c->sm_count, c->max_memory, c->opt_max_narr, c->allow_merging,
+                                 st, wb);
     c->stats = st;
     c->err_bits = eb;
     c->warn_bits = wb;
@@ -1069,6 +1046,17 @@ int bhcb_arrivals_shape(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *nsz, i
                         int32_t *max_narr)
 {
     return guarded(c, [&]() -> int {
+        if(c->is3d()) {   // 3-D: nsz carries NSz * NSx * NSy * Ntheta, the leading field dimensions
+            if(!run3_is_arrivals(c->r3) || c->r3_status != BHCB_OK) throw StateError("no 3-D arrivals run");
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            int32_t d[6];
+            run3_shape(c->r3, env, d);
+            if(nsz) *nsz = d[0] * d[1] * d[2] * d[3];
+            if(nrzp) *nrzp = d[4];
+            if(nrr) *nrr = d[5];
+            if(max_narr) *max_narr = run3_max_narr(c->r3);
+            return BHCB_OK;
+        }
         if(c->mode != MODE_ARR || !c->prepared) throw StateError("no prepared arrivals run");
         const Field *F = find_field(c, env, ifreq);
         if(nsz) *nsz = F->nsz;
@@ -1084,6 +1072,11 @@ int bhcb_copy_arrivals(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *narr, s
 {
     static_assert(sizeof(bhcb_arrival) == sizeof(ArrivalRec), "arrival record layout");
     return guarded(c, [&]() -> int {
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            run3_copy_arrivals(c->r3, env, narr, narr_bytes, arr, arr_bytes, c->stream);
+            return BHCB_OK;
+        }
         if(c->mode != MODE_ARR || !c->prepared) throw StateError("no arrivals run");
         const Field *F = find_field(c, env, ifreq);
         size_t cells = (size_t)F->nsz * F->nrzp * F->nrr;

@@ -24,6 +24,15 @@ cudaError_t launch_trace3d(const GroupDev *, int, long long, SegRec3 *, unsigned
 cudaError_t launch_influence3d(const SegRec3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
                                int, cudaStream_t);
 cudaError_t launch_sqrt3d(float2 *, long long, int, cudaStream_t);
+cudaError_t launch_arr_gather3d(const SegRec3 *, unsigned long long, const GroupDev *, int, bool, ArrCand *,
+                                uint64_t *, uint32_t *, unsigned long long, unsigned long long *, RunCounters *,
+                                ArrKeyBits, int, cudaStream_t);
+size_t radix_sort_hist_entries(unsigned long long n);
+cudaError_t radix_sort_pairs(uint64_t *, uint32_t *, uint64_t *, uint32_t *, unsigned long long, int, uint32_t *,
+                             int *, cudaStream_t);
+cudaError_t launch_arr_replay(const uint64_t *, const uint32_t *, const ArrCand *, unsigned long long,
+                              const GroupDev *, int, const double *, long long, int, int, int, int32_t *,
+                              ArrivalRec *, int, cudaStream_t, bool);
 
 namespace {
 struct Env3Slot {
@@ -40,8 +49,14 @@ struct Run3 {
     DevBuf arena, groups_d, segs, counters, field;
     long long njobs = 0;
     unsigned long long seg_cap = 0;
-    int64_t total_field = 0;
+    int64_t total_field = 0;   // receiver cells of the batch
     bool ran = false;
+    // arrivals runs (RunType 'A' / 'a')
+    bool arrivals = false;
+    int32_t opt_max_narr = 0, max_narr = 0, allow_merging = 1;
+    uint64_t max_memory = 16ull << 30;
+    ArrKeyBits kb{};
+    DevBuf narr_d, arr_d, cand, keys0, keys1, vals0, vals1, hist;
 };
 
 Run3 *run3_new() { return new Run3(); }
@@ -49,7 +64,9 @@ Run3 *run3_new() { return new Run3(); }
 void run3_free(Run3 *r)
 {
     if(!r) return;
-    for(DevBuf *b : {&r->arena, &r->groups_d, &r->segs, &r->counters, &r->field}) b->release();
+    for(DevBuf *b : {&r->arena, &r->groups_d, &r->segs, &r->counters, &r->field, &r->narr_d, &r->arr_d, &r->cand,
+                     &r->keys0, &r->keys1, &r->vals0, &r->vals1, &r->hist})
+        b->release();
     delete r;
 }
 
@@ -183,8 +200,42 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     r->groups_d.ensure(r->groups_h.size() * sizeof(GroupDev));
     CK(cudaMemcpyAsync(r->groups_d.p, r->groups_h.data(), r->groups_h.size() * sizeof(GroupDev),
                        cudaMemcpyHostToDevice, st));
-    r->field.ensure(std::max<int64_t>(r->total_field, 1) * sizeof(float2));
     r->counters.ensure(sizeof(RunCounters) + 64);
+    // one run type per batch: TL ('C', 'S', 'I') or arrivals ('A', 'a')
+    const char rt0 = r->envs[0].T.run_type[0];
+    r->arrivals = rt0 == 'A' || rt0 == 'a';
+    for(const auto &S : r->envs) {
+        const char t = S.T.run_type[0];
+        if((t == 'A' || t == 'a') != r->arrivals) throw std::runtime_error("a 3-D batch must use one run type");
+    }
+    if(!r->arrivals) {
+        r->field.ensure(std::max<int64_t>(r->total_field, 1) * sizeof(float2));
+        return;
+    }
+    // ordering key (low to high): step | ray | receiver cell
+    int max_njobs = 1;
+    for(const GroupDev &G : r->groups_h) max_njobs = std::max(max_njobs, G.njobs);
+    auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
+    ArrKeyBits kb{};
+    kb.sh_is = 0;
+    kb.sh_job = bits(100000);   // steps per ray (MaxN, include/bhc/structs.hpp:66)
+    kb.sh_cell = kb.sh_job + bits((unsigned long long)max_njobs);
+    kb.total_bits = kb.sh_cell + bits((unsigned long long)r->total_field);
+    if(kb.total_bits > 64) throw MemError("arrival ordering key needs more than 64 bits; split the batch");
+    r->kb = kb;
+    const size_t cells = (size_t)r->total_field;
+    int32_t mx = r->opt_max_narr;
+    if(mx <= 0) {
+        // as the reference (src/mode/arr.hpp:80-98): what a quarter of
+        // max_memory holds per receiver, at most 1000
+        const uint64_t m = (r->max_memory / 4) / (cells * sizeof(ArrivalRec) + 1);
+        mx = (int32_t)std::min<uint64_t>(m, 1000);
+    }
+    if(mx <= 0) throw MemError("insufficient memory to allocate arrivals");
+    r->max_narr = mx;
+    r->narr_d.ensure(cells * sizeof(int32_t));
+    r->arr_d.ensure(cells * (size_t)mx * sizeof(ArrivalRec));
+    CK(cudaMemsetAsync(r->narr_d.p, 0, cells * sizeof(int32_t), st));
     h2d = A.bytes.size() + r->groups_h.size() * sizeof(GroupDev);
 }
 
@@ -193,18 +244,95 @@ struct RangeStats {
     double trace_ms = 0, infl_ms = 0;
 };
 
+// Arrivals of the traced jobs [j0, j1): candidates counted, written with
+// their ordering keys, sorted, then replayed per receiver cell after the
+// arrivals of earlier (lower-numbered) jobs. Returns false, having changed
+// nothing, when the candidates do not fit in max_memory.
+bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg, cudaStream_t st, int sm_count,
+                    RangeStats &acc)
+{
+    (void)j0; (void)j1;
+    RunCounters *ctr = reinterpret_cast<RunCounters *>(r->counters.p);
+    unsigned long long *cursor = reinterpret_cast<unsigned long long *>(
+        reinterpret_cast<uint8_t *>(r->counters.p) + sizeof(RunCounters) + 8);
+    const int igrid = sm_count * 8;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st));
+    CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), st));
+    CK(launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
+                           (int)r->groups_h.size(), true, nullptr, nullptr, nullptr, 0, nullptr, ctr, r->kb, igrid, st));
+    unsigned long long n = 0;
+    CK(cudaMemcpyAsync(&n, &ctr->nevals, sizeof n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const size_t per = sizeof(ArrCand) + 2 * sizeof(uint64_t) + 2 * sizeof(uint32_t);
+    const size_t fixed = r->segs.bytes + r->arr_d.bytes + r->narr_d.bytes + (64u << 20);
+    const size_t avail = r->max_memory > fixed ? r->max_memory - fixed : 0;
+    if((size_t)n * per + radix_sort_hist_entries(n) * 4 > avail && j1 - j0 > 1) {
+        cudaEventDestroy(e0); cudaEventDestroy(e1);
+        return false;
+    }
+    if(n > 0xffffffffull) throw MemError("more than 2^32 arrival candidates in one wave; lower max_memory");
+    if(n) {
+        r->cand.ensure(n * sizeof(ArrCand));
+        r->keys0.ensure(n * sizeof(uint64_t));
+        r->keys1.ensure(n * sizeof(uint64_t));
+        r->vals0.ensure(n * sizeof(uint32_t));
+        r->vals1.ensure(n * sizeof(uint32_t));
+        r->hist.ensure(std::max<size_t>(radix_sort_hist_entries(n), 1) * sizeof(uint32_t));
+        CK(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
+        CK(launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
+                               (int)r->groups_h.size(), false, (ArrCand *)r->cand.p, (uint64_t *)r->keys0.p,
+                               (uint32_t *)r->vals0.p, n, cursor, ctr, r->kb, igrid, st));
+        int in1 = 0;
+        CK(radix_sort_pairs((uint64_t *)r->keys0.p, (uint32_t *)r->vals0.p, (uint64_t *)r->keys1.p,
+                            (uint32_t *)r->vals1.p, n, r->kb.total_bits, (uint32_t *)r->hist.p, &in1, st));
+        const uint64_t *k = (const uint64_t *)(in1 ? r->keys1.p : r->keys0.p);
+        const uint32_t *v = (const uint32_t *)(in1 ? r->vals1.p : r->vals0.p);
+        CK(launch_arr_replay(k, v, (const ArrCand *)r->cand.p, n, (const GroupDev *)r->groups_d.p,
+                             (int)r->groups_h.size(), nullptr, (long long)r->total_field, r->kb.sh_cell,
+                             r->max_narr, r->allow_merging, (int32_t *)r->narr_d.p, (ArrivalRec *)r->arr_d.p,
+                             sm_count, st, true));
+    }
+    CK(cudaEventRecord(e1, st));
+    RunCounters rc{};
+    CK(cudaMemcpyAsync(&rc, ctr, sizeof rc, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    acc.rc.nevals += n;
+    acc.rc.err_bits |= rc.err_bits;
+    acc.rc.warn_bits |= rc.warn_bits;
+    acc.infl_ms += ms;
+    return true;
+}
+
 // trace the jobs [j0, j1) and apply their contributions; on a segment buffer
 // overflow the range is split in halves (waves), which add into the same field
 void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count, uint64_t max_memory,
               RangeStats &acc)
 {
     const size_t rec = sizeof(SegRec3);
-    const size_t fbytes = (size_t)r->total_field * sizeof(float2);
-    const size_t budget = max_memory > fbytes + (64u << 20) ? max_memory - fbytes - (64u << 20) : 0;
+    // TL: the field; arrivals: their storage, and half of the rest is left
+    // for the arrival candidates
+    const size_t fbytes = r->arrivals ? r->arr_d.bytes + r->narr_d.bytes : (size_t)r->total_field * sizeof(float2);
+    size_t budget = max_memory > fbytes + (64u << 20) ? max_memory - fbytes - (64u << 20) : 0;
+    if(r->arrivals) budget /= 2;
     const unsigned long long maxcap = budget / rec;
     if(r->seg_cap == 0) {
-        // a first guess: 64 records per ray, within the budget
-        r->seg_cap = std::min<unsigned long long>(maxcap, std::max<unsigned long long>(1u << 16, 64ull * (j1 - j0)));
+        // a first guess within the budget: a ray emits at most one record per
+        // step that brackets receiver ranges, about one per range it crosses
+        // (plus the unused tail of its last 32-slot block)
+        unsigned long long per_ray = 64;
+        for(const auto &S : r->envs) {
+            const Env3Tables &T = S.T;
+            const double steps = 2.0 * std::max(T.box_x, T.box_y) / std::max(T.deltas, 1e-9);
+            per_ray = std::max<unsigned long long>(
+                per_ray, (unsigned long long)std::min<double>(steps, 1.1 * T.rr.size()) + 32);
+        }
+        r->seg_cap = std::min<unsigned long long>(maxcap, std::max<unsigned long long>(1u << 16, per_ray * (j1 - j0)));
     }
     for(int attempt = 0; attempt < 6; ++attempt) {
         if(r->seg_cap < 1024) throw MemError("max_memory leaves no room for 3-D segment records");
@@ -246,6 +374,22 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
         }
         const unsigned long long nseg = std::min(rc.nseg, r->seg_cap);
         const int igrid = sm_count * 8;
+        if(r->arrivals && rc.err_bits == 0) {
+            cudaEventDestroy(e0); cudaEventDestroy(e2);
+            if(!apply_arrivals(r, j0, j1, nseg, st, sm_count, acc)) {   // candidates exceed the budget
+                cudaEventDestroy(e1);
+                const long long mid = j0 + nj / 2;
+                run_jobs(r, j0, mid, st, sm_count, max_memory, acc);
+                run_jobs(r, mid, j1, st, sm_count, max_memory, acc);
+                return;
+            }
+            cudaEventDestroy(e1);
+            acc.rc.nseg += nseg;
+            acc.rc.nsteps += rc.nsteps;
+            acc.rc.warn_bits |= rc.warn_bits;
+            acc.trace_ms += tms;
+            return;
+        }
         if(rc.err_bits == 0)
             CK(launch_influence3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
                                   (int)r->groups_h.size(), (float2 *)r->field.p, ctr, igrid, st));
@@ -270,15 +414,19 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
 
 } // namespace
 
-uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, bhcb_stats &stats, uint32_t &warn_bits)
+uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, int32_t opt_max_narr,
+                  int32_t allow_merging, bhcb_stats &stats, uint32_t &warn_bits)
 {
     auto t0 = std::chrono::steady_clock::now();
     uint64_t h2d = 0;
+    r->max_memory = max_memory;
+    r->opt_max_narr = opt_max_narr;
+    r->allow_merging = allow_merging;
     prepare3(r, st, h2d);
-    CK(cudaMemsetAsync(r->field.p, 0, std::max<int64_t>(r->total_field, 1) * sizeof(float2), st));
+    if(!r->arrivals) CK(cudaMemsetAsync(r->field.p, 0, std::max<int64_t>(r->total_field, 1) * sizeof(float2), st));
     RangeStats acc;
     run_jobs(r, 0, r->njobs, st, sm_count, max_memory, acc);
-    if(acc.rc.err_bits == 0) {
+    if(acc.rc.err_bits == 0 && !r->arrivals) {
         for(const auto &S : r->envs)
             if(S.T.run_type[0] != 'C')
                 CK(launch_sqrt3d((float2 *)r->field.p + S.field_base, S.field_n, sm_count * 4, st));
@@ -325,6 +473,7 @@ static const Env3Slot &ran_env(const Run3 *r, int env)
 void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
+    if(r->arrivals) throw StateError("not a TL run: use bhcb_copy_arrivals");
     const size_t need = (size_t)S.field_n * sizeof(float2);
     if(!dst || bytes < need) throw std::invalid_argument("destination too small");
     CK(cudaMemcpyAsync(dst, (float2 *)r->field.p + S.field_base, need, cudaMemcpyDeviceToHost, st));
@@ -334,6 +483,7 @@ void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st)
 void *run3_field_device(Run3 *r, int env)
 {
     const Env3Slot &S = ran_env(r, env);
+    if(r->arrivals) throw StateError("not a TL run");
     return (float2 *)r->field.p + S.field_base;
 }
 
@@ -351,10 +501,116 @@ std::vector<std::string> run3_warnings(const Run3 *r, int env)
     return r->envs[env].T.warnings;
 }
 
+bool run3_is_arrivals(const Run3 *r) { return r->arrivals; }
+
+int32_t run3_max_narr(const Run3 *r) { return r->max_narr; }
+
+void run3_copy_arrivals(Run3 *r, int env, int32_t *narr, size_t narr_bytes, void *arr, size_t arr_bytes,
+                        cudaStream_t st)
+{
+    const Env3Slot &S = ran_env(r, env);
+    if(!r->arrivals) throw StateError("not an arrivals run");
+    const size_t cells = (size_t)S.field_n;
+    if(narr) {
+        if(narr_bytes < cells * sizeof(int32_t)) throw std::invalid_argument("narr buffer too small");
+        CK(cudaMemcpyAsync(narr, (int32_t *)r->narr_d.p + S.field_base, cells * sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, st));
+    }
+    if(arr) {
+        const size_t need = cells * (size_t)r->max_narr * sizeof(ArrivalRec);
+        if(arr_bytes < need) throw std::invalid_argument("arrival buffer too small");
+        CK(cudaMemcpyAsync(arr, (ArrivalRec *)r->arr_d.p + (size_t)S.field_base * r->max_narr, need,
+                           cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+}
+
+// WriteOutArrivals, 3-D (src/mode/arr.cpp:88-239): binary for RunType 'a',
+// list-directed text for 'A'
+static void write_arrivals3(Run3 *r, const Env3Slot &S, const std::string &path, cudaStream_t st)
+{
+    const Env3Tables &T = S.T;
+    const size_t cells = (size_t)S.field_n;
+    std::vector<int32_t> narr(cells);
+    std::vector<ArrivalRec> arr(cells * (size_t)r->max_narr);
+    run3_copy_arrivals(r, (int)(&S - r->envs.data()), narr.data(), narr.size() * 4, arr.data(),
+                       arr.size() * sizeof(ArrivalRec), st);
+    const double RadDeg = 180.0 / 3.14159265358979323846;
+    const bool ascii = T.run_type[0] == 'A';
+    std::ofstream o(path, std::ios::binary);
+    if(!o.good()) throw std::runtime_error("cannot open " + path);
+    const int nsx = (int)T.sx.size(), nsy = (int)T.sy.size(), nsz = (int)T.sz.size();
+    const int nth = (int)T.theta.size(), nrz = (int)T.rz.size(), nrr = (int)T.rr.size();
+    char b[256];
+    if(ascii) {
+        o << "3D\n";
+        snprintf(b, sizeof b, "%.9g\n", T.freq0);
+        o << b;
+        o << nsx; for(double v : T.sx) { snprintf(b, sizeof b, " %.17g", v); o << b; } o << "\n";
+        o << nsy; for(double v : T.sy) { snprintf(b, sizeof b, " %.17g", v); o << b; } o << "\n";
+        o << nsz; for(float v : T.sz) { snprintf(b, sizeof b, " %.9g", v); o << b; } o << "\n";
+        o << nrz; for(float v : T.rz) { snprintf(b, sizeof b, " %.9g", v); o << b; } o << "\n";
+        o << nrr; for(double v : T.rr) { snprintf(b, sizeof b, " %.17g", v); o << b; } o << "\n";
+        o << nth; for(double v : T.theta) { snprintf(b, sizeof b, " %.17g", v); o << b; } o << "\n";
+    } else {
+        RecWriter w(o);
+        w.put_bytes("'3D'", 4); w.end();
+        w.put((float)T.freq0); w.end();
+        w.put((int32_t)nsx); w.put_bytes(T.sx.data(), T.sx.size() * 8); w.end();
+        w.put((int32_t)nsy); w.put_bytes(T.sy.data(), T.sy.size() * 8); w.end();
+        w.put((int32_t)nsz); w.put_bytes(T.sz.data(), T.sz.size() * 4); w.end();
+        w.put((int32_t)nrz); w.put_bytes(T.rz.data(), T.rz.size() * 4); w.end();
+        w.put((int32_t)nrr); w.put_bytes(T.rr.data(), T.rr.size() * 8); w.end();
+        w.put((int32_t)nth); w.put_bytes(T.theta.data(), T.theta.size() * 8); w.end();
+    }
+    RecWriter w(o);
+    const size_t per_src = (size_t)nth * nrz * nrr;
+    for(int isz = 0; isz < nsz; ++isz)
+        for(int isx = 0; isx < nsx; ++isx)
+            for(int isy = 0; isy < nsy; ++isy) {
+                const size_t cb = (((size_t)isz * nsx + isx) * nsy + isy) * per_src;
+                int32_t maxn = 0;   // MaxNPerSource (src/mode/arr.cpp:24-74)
+                for(size_t k = 0; k < per_src; ++k) maxn = std::max(maxn, narr[cb + k]);
+                if(ascii) o << maxn << "\n";
+                else { w.put(maxn); w.end(); }
+                for(size_t k = 0; k < per_src; ++k) {
+                    const size_t base = cb + k;
+                    const int32_t n = narr[base];
+                    if(ascii) o << n << "\n";
+                    else { w.put(n); w.end(); }
+                    for(int a = 0; a < n; ++a) {
+                        const ArrivalRec &A = arr[base * r->max_narr + a];
+                        if(ascii) {
+                            snprintf(b, sizeof b, "%.9g %.17g %.9g %.9g %.9g %.9g %.9g %.9g %d %d\n", A.a,
+                                     RadDeg * A.Phase, A.delay_re, A.delay_im, A.SrcDeclAngle, A.SrcAzimAngle,
+                                     A.RcvrDeclAngle, A.RcvrAzimAngle, A.NTopBnc, A.NBotBnc);
+                            o << b;
+                        } else {
+                            w.put(A.a);
+                            w.put((float)(RadDeg * A.Phase));
+                            w.put(A.delay_re);
+                            w.put(A.delay_im);
+                            w.put(A.SrcDeclAngle);
+                            w.put(A.SrcAzimAngle);
+                            w.put(A.RcvrDeclAngle);
+                            w.put(A.RcvrAzimAngle);
+                            w.put((float)A.NTopBnc);
+                            w.put((float)A.NBotBnc);
+                            w.end();
+                        }
+                    }
+                }
+            }
+}
+
 // .shd, 3-D: WriteHeader and WriteOutTL (src/mode/tl.cpp:38-101, 195-248)
 void run3_writeout(Run3 *r, int env, const std::string &root, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
+    if(r->arrivals) {
+        write_arrivals3(r, S, root + ".arr", st);
+        return;
+    }
     const Env3Tables &T = S.T;
     std::vector<float2> u((size_t)S.field_n);
     CK(cudaMemcpyAsync(u.data(), (float2 *)r->field.p + S.field_base, u.size() * sizeof(float2),

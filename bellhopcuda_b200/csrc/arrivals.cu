@@ -30,6 +30,7 @@
 #include "device_math.cuh"
 #include "trace2d.cuh"
 #include "influence2d.cuh"
+#include "trace3d.cuh"
 
 namespace bhcb {
 
@@ -242,6 +243,10 @@ __global__ void __launch_bounds__(32) rs_scatter_kernel(
 // -------------------------------------------------------------- replay
 // AddArr (src/arrivals.hpp:45-132) over one receiver cell's candidates in
 // (ray, step) order, then PostProcessArrivals (src/mode/arr.cpp:24-74).
+// D3: 3-D run (source angles from the 3-D job, receiver azimuth from the
+// candidate, no amplitude scaling); the replay continues from the counts
+// already in narr_out, so job-ordered waves compose.
+template<bool D3>
 __global__ void arr_replay_kernel(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ vals,
                                   const ArrCand *__restrict__ cands, unsigned long long n,
                                   const GroupDev *__restrict__ groups, int ngroups,
@@ -265,14 +270,23 @@ __global__ void arr_replay_kernel(const uint64_t *__restrict__ keys, const uint3
         }
         const unsigned long long end = lo;
         const GroupDev &G = groups[group_of_cell(groups, ngroups, cell)];
-        const EnvDev &e = *G.env;
-        const double omega = 2.0 * BHCB_PI * freqs[G.freq_base];
+        const double omega = D3 ? 2.0 * BHCB_PI * G.env3->freq0 : 2.0 * BHCB_PI * freqs[G.freq_base];
         ArrivalRec *ba = arr_out + (size_t)cell * max_narr;
-        int nt = 0;
+        int nt = D3 ? narr_out[cell] : 0;
         for(unsigned long long k = begin; k < end; ++k) {
             const ArrCand &c = cands[vals[k]];
-            const double src_decl = RAD_DEG * e.alpha[c.aux];
-            const float azim = __int_as_float(0x7fc00000);   // NaN: no azimuth in 2-D
+            double src_decl, src_azim_d = 0.0;
+            float rcvr_azim;
+            if(D3) {
+                const Job3 J = job_indices3(*G.env3, (int)((long long)c.job - G.job_base));
+                src_decl = RAD_DEG * G.env3->alpha[J.ialpha];
+                src_azim_d = RAD_DEG * G.env3->beta[J.ibeta];
+                rcvr_azim = c.rcvr_azim;
+            } else {
+                src_decl = RAD_DEG * G.env->alpha[c.aux];
+                rcvr_azim = __int_as_float(0x7fc00000);   // NaN: no azimuth in 2-D
+            }
+            const float azim = D3 ? (float)src_azim_d : __int_as_float(0x7fc00000);
             if(allow_merging) {
                 const float PhaseTol = 0.05f;
                 bool second = false;
@@ -304,7 +318,7 @@ __global__ void arr_replay_kernel(const uint64_t *__restrict__ keys, const uint3
                     A.SrcDeclAngle = (float)src_decl;
                     A.SrcAzimAngle = azim;
                     A.RcvrDeclAngle = c.rcvr_decl;
-                    A.RcvrAzimAngle = azim;
+                    A.RcvrAzimAngle = rcvr_azim;
                     A.NTopBnc = c.ntop;
                     A.NBotBnc = c.nbot;
                 } else {
@@ -318,7 +332,7 @@ __global__ void arr_replay_kernel(const uint64_t *__restrict__ keys, const uint3
                     A.SrcDeclAngle = __fadd_rn(__fmul_rn(w1, A.SrcDeclAngle), __fmul_rn(w2, (float)src_decl));
                     A.SrcAzimAngle = __fadd_rn(__fmul_rn(w1, A.SrcAzimAngle), __fmul_rn(w2, azim));
                     A.RcvrDeclAngle = __fadd_rn(__fmul_rn(w1, A.RcvrDeclAngle), __fmul_rn(w2, c.rcvr_decl));
-                    A.RcvrAzimAngle = __fadd_rn(__fmul_rn(w1, A.RcvrAzimAngle), __fmul_rn(w2, azim));
+                    A.RcvrAzimAngle = __fadd_rn(__fmul_rn(w1, A.RcvrAzimAngle), __fmul_rn(w2, rcvr_azim));
                 }
             } else {
                 const int j = nt++;
@@ -331,14 +345,17 @@ __global__ void arr_replay_kernel(const uint64_t *__restrict__ keys, const uint3
                 A.SrcDeclAngle = (float)src_decl;
                 A.SrcAzimAngle = azim;
                 A.RcvrDeclAngle = c.rcvr_decl;
-                A.RcvrAzimAngle = azim;
+                A.RcvrAzimAngle = rcvr_azim;
                 A.NTopBnc = c.ntop;
                 A.NBotBnc = c.nbot;
             }
         }
-        // PostProcessArrivals (2-D): clamp the count, scale the amplitudes
+        // PostProcessArrivals (src/mode/arr.cpp:24-74): clamp the count; 2-D
+        // scales the amplitudes (3-D factor 1)
         if(nt > max_narr) nt = max_narr;
         narr_out[cell] = nt;
+        if(D3) continue;
+        const EnvDev &e = *G.env;
         const int ir = (int)((cell - G.field_base) % e.nrr);
         float factor;
         if(e.line_source) factor = (float)(FLTD(4.0) * sqrt(BHCB_PI));
@@ -434,13 +451,17 @@ cudaError_t radix_sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t 
 cudaError_t launch_arr_replay(const uint64_t *keys, const uint32_t *vals, const ArrCand *cands, unsigned long long n,
                               const GroupDev *groups, int ngroups, const double *freqs, long long ncells, int sh_cell,
                               int max_narr, int allow_merging, int32_t *narr, ArrivalRec *arr, int sm_count,
-                              cudaStream_t st)
+                              cudaStream_t st, bool d3)
 {
     long long grid = (ncells + 127) / 128;
     if(grid > (long long)sm_count * 64) grid = (long long)sm_count * 64;
     if(grid < 1) grid = 1;
-    arr_replay_kernel<<<(int)grid, 128, 0, st>>>(keys, vals, cands, n, groups, ngroups, freqs, ncells, sh_cell,
-                                                 max_narr, allow_merging, narr, arr);
+    if(d3)
+        arr_replay_kernel<true><<<(int)grid, 128, 0, st>>>(keys, vals, cands, n, groups, ngroups, freqs, ncells,
+                                                           sh_cell, max_narr, allow_merging, narr, arr);
+    else
+        arr_replay_kernel<false><<<(int)grid, 128, 0, st>>>(keys, vals, cands, n, groups, ngroups, freqs, ncells,
+                                                            sh_cell, max_narr, allow_merging, narr, arr);
     return cudaGetLastError();
 }
 

@@ -113,6 +113,7 @@ struct alignas(16) SegRec3 {
     double ldiag;              // L_diag beam radius bound
     double zlo, zhi;           // min / max depth of the segment
     int32_t ir_lo, ir_hi, job, is;
+    int32_t ntop, nbot;        // point1's bounce counts (arrivals)
 };
 
 struct GroupDev {
@@ -177,7 +178,7 @@ struct ArrCand {
     double amp, phase, delay_re, delay_im;
     float rcvr_decl;
     int32_t ntop, nbot, job, aux;
-    int32_t pad;
+    float rcvr_azim;           // 3-D: receiver azimuth (deg); 2-D: unused
 };
 // Bit layout of the ordering keys (low to high): arrivals: step | job | cell;
 // eigen: depth | walk position | step | job | field.

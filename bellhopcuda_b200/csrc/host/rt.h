@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <fstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -64,5 +65,30 @@ template<typename T> T *dptr(void *base, size_t off)
 {
     return reinterpret_cast<T *>(reinterpret_cast<uint8_t *>(base) + off);
 }
+
+// Fortran sequential unformatted records: [int32 n][n bytes][int32 n]
+struct RecWriter {
+    std::vector<uint8_t> cur;
+    std::ofstream &o;
+    explicit RecWriter(std::ofstream &o_) : o(o_) {}
+    template<typename T> void put(const T &v)
+    {
+        const uint8_t *p = reinterpret_cast<const uint8_t *>(&v);
+        cur.insert(cur.end(), p, p + sizeof(T));
+    }
+    void put_bytes(const void *p, size_t n)
+    {
+        const uint8_t *q = reinterpret_cast<const uint8_t *>(p);
+        cur.insert(cur.end(), q, q + n);
+    }
+    void end()
+    {
+        int32_t n = (int32_t)cur.size();
+        o.write((const char *)&n, 4);
+        o.write((const char *)cur.data(), cur.size());
+        o.write((const char *)&n, 4);
+        cur.clear();
+    }
+};
 
 } // namespace bhcb

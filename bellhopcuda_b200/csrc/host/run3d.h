@@ -22,8 +22,13 @@ int run3_count(const Run3 *r);
 int run3_add_env(Run3 *r, const std::string &root);
 // builds the tables, traces every ray of every environment and evaluates the
 // fields; fills the statistics; returns the tracer's error bits (0 = clean)
-uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, bhcb_stats &stats,
-                  uint32_t &warn_bits);
+uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, int32_t opt_max_narr,
+                  int32_t allow_merging, bhcb_stats &stats, uint32_t &warn_bits);
+// arrivals runs (RunType 'A' / 'a'): storage [cell][max_narr], cells in the field layout
+bool run3_is_arrivals(const Run3 *r);
+int32_t run3_max_narr(const Run3 *r);
+void run3_copy_arrivals(Run3 *r, int env, int32_t *narr, size_t narr_bytes, void *arr, size_t arr_bytes,
+                        cudaStream_t st);
 // dims = {nsz, nsx, nsy, ntheta, nrz, nrr}
 void run3_shape(const Run3 *r, int env, int32_t dims[6]);
 void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st);
@@ -31,7 +36,7 @@ void *run3_field_device(Run3 *r, int env);
 // receiver grid and source positions as the reference's Position (m, deg)
 void run3_grid(const Run3 *r, int env, std::vector<double> &sx, std::vector<double> &sy, std::vector<float> &sz,
                std::vector<double> &rr, std::vector<float> &rz, std::vector<double> &theta);
-// <root>.shd in the reference's 3-D layout
+// <root>.shd (TL) or <root>.arr (arrivals) in the reference's 3-D layouts
 void run3_writeout(Run3 *r, int env, const std::string &root, cudaStream_t st);
 std::vector<std::string> run3_warnings(const Run3 *r, int env);
 

@@ -49,38 +49,11 @@ __device__ __forceinline__ void emit_seg3(const SegRec3 &rec, SegRec3 *segs, uns
         cur.next = b;
         cur.end = b + SEG_BLOCK3;
     }
-    static_assert(sizeof(SegRec3) % 16 == 0, "records are written in 16-byte words");
+    static_assert(sizeof(SegRec3) % 16 == 0 && sizeof(SegRec3) == 288, "records are written in 16-byte words");
     const uint4 *src = reinterpret_cast<const uint4 *>(&rec);
     uint4 *dst = reinterpret_cast<uint4 *>(segs + cur.next++);
 #pragma unroll
     for(int k = 0; k < (int)(sizeof(SegRec3) / 16); ++k) dst[k] = src[k];
-}
-
-// GetJobIndices, 3-D (src/common.hpp:365-391): ialpha fastest, then ibeta, isy, isx, isz
-struct Job3 {
-    int ialpha, ibeta, isx, isy, isz;
-};
-__device__ __forceinline__ Job3 job_indices3(const Env3Dev &E, int local)
-{
-    Job3 j;
-    if(E.isingle_alpha >= 1) {
-        j.ialpha = E.isingle_alpha - 1;
-    } else {
-        j.ialpha = local % E.nalpha;
-        local /= E.nalpha;
-    }
-    if(E.isingle_beta >= 1) {
-        j.ibeta = E.isingle_beta - 1;
-    } else {
-        j.ibeta = local % E.nbeta;
-        local /= E.nbeta;
-    }
-    j.isy = local % E.nsy;
-    local /= E.nsy;
-    j.isx = local % E.nsx;
-    local /= E.nsx;
-    j.isz = local;
-    return j;
 }
 
 // the carried part of InfluenceRayInfo for the 3-D Cartesian geometric beams
@@ -169,6 +142,8 @@ __device__ __forceinline__ bool infl_prologue3(const Ray3 &P0, const Ray3 &P1, I
     rec.ir_hi = hi;
     rec.job = job;
     rec.is = is;
+    rec.ntop = P1.ntop;
+    rec.nbot = P1.nbot;
     return true;
 }
 
@@ -290,10 +265,12 @@ __global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict_
 
 constexpr int WARPS3 = 4;
 
-// InfluenceGeoCore, 3-D Cartesian (src/influence.hpp:897-1024) and
-// ApplyContribution's TL branch (src/influence.hpp:432-473)
-__device__ __forceinline__ bool core3(const SegRec3 &R, double s, double n1, double n2, bool gauss, bool coherent,
-                                      double omega, float2 &df)
+// InfluenceGeoCore, 3-D Cartesian (src/influence.hpp:897-1024): beam-window
+// test, then amplitude cnst, weight w, phase and complex delay of one receiver
+struct Contrib3 {
+    double cnst, w, ph, dr, di;
+};
+__device__ __forceinline__ bool geo_core3(const SegRec3 &R, double s, double n1, double n2, bool gauss, Contrib3 &o)
 {
     double q00 = R.q0[0] + s * R.dq[0], q01 = R.q0[1] + s * R.dq[1];
     double q10 = R.q0[2] + s * R.dq[2], q11 = R.q0[3] + s * R.dq[3];
@@ -311,25 +288,30 @@ __device__ __forceinline__ bool core3(const SegRec3 &R, double s, double n1, dou
     const double bw = gauss ? 4.0 : 1.0;
     const double dist = gauss ? n1p + n2p : max(n1p, n2p);
     if(dist > bw * 1.0) return false;
-    const double dr = R.tau0r + s * R.dtaur, di = R.tau0i + s * R.dtaui;
-    const double cnst = R.cnst_num / sqrt(fabs(qF));
-    const double w = gauss ? exp(FLTD(-0.5) * (n1p * n1p + n2p * n2p)) : (FLTD(1.0) - n1p) * (FLTD(1.0) - n2p);
-    double ph = R.phase0;
-    if((qF <= 0.0 && R.qold > 0.0) || (qF >= 0.0 && R.qold < 0.0)) ph += BHCB_PI / FLTD(2.0);
+    o.dr = R.tau0r + s * R.dtaur;
+    o.di = R.tau0i + s * R.dtaui;
+    o.cnst = R.cnst_num / sqrt(fabs(qF));
+    o.w = gauss ? exp(FLTD(-0.5) * (n1p * n1p + n2p * n2p)) : (FLTD(1.0) - n1p) * (FLTD(1.0) - n2p);
+    o.ph = R.phase0;
+    if((qF <= 0.0 && R.qold > 0.0) || (qF >= 0.0 && R.qold < 0.0)) o.ph += BHCB_PI / FLTD(2.0);
+    return true;
+}
+
+// ApplyContribution's TL branch (src/influence.hpp:448-471)
+__device__ __forceinline__ float2 tl_field3(const Contrib3 &o, bool gauss, bool coherent, double omega)
+{
     if(coherent) {
-        const double a = omega * dr - ph;
-        const double m = exp(omega * di);
+        const double a = omega * o.dr - o.ph;
+        const double m = exp(omega * o.di);
         double sa, ca;
         sincos(-a, &sa, &ca);
-        const double cw = cnst * w;
-        df = make_float2((float)(cw * (m * ca)), (float)(cw * (m * sa)));
-    } else {
-        double v = cnst * exp(omega * di);
-        v = v * v * w;
-        if(gauss) v *= FLTD(2.0) * BHCB_PI;
-        df = make_float2((float)v, 0.0f);
+        const double cw = o.cnst * o.w;
+        return make_float2((float)(cw * (m * ca)), (float)(cw * (m * sa)));
     }
-    return true;
+    double v = o.cnst * exp(omega * o.di);
+    v = v * v * o.w;
+    if(gauss) v *= FLTD(2.0) * BHCB_PI;
+    return make_float2((float)v, 0.0f);
 }
 
 // first index with (double)rz >= z (n if none)
@@ -383,9 +365,15 @@ __device__ __forceinline__ bool pair_outside_beam(const SegRec3 &R, double dxr, 
 // Work is flattened twice per warp: (segment, range, bearing) pairs over the
 // warp's 32 records, then (pair, depth) items over the pairs that survive the
 // bearing rejections, so that every lane evaluates receivers.
+// MODE: INFL_TL adds the field; INFL_ARR_COUNT counts the arrival candidates;
+// INFL_ARR_FILL writes them (AddArr's inputs, src/influence.hpp:444-447) with
+// the key (receiver cell, ray, step) that restores the reference's order.
+enum { INFL_TL = 0, INFL_ARR_COUNT = 1, INFL_ARR_FILL = 2 };
+template<int MODE>
 __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     const SegRec3 *__restrict__ segs, unsigned long long nseg, const GroupDev *__restrict__ groups, int ngroups,
-    float2 *field, RunCounters *ctr)
+    float2 *field, RunCounters *ctr, ArrCand *cands, uint64_t *keys, uint32_t *vals, unsigned long long cand_cap,
+    unsigned long long *cursor, ArrKeyBits kb)
 {
     // per record of the warp's chunk
     __shared__ int s_incl[WARPS3][32];
@@ -429,9 +417,9 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
         s_grp[w][lane] = g;
         __syncwarp();
         const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for(int kb = 0; kb < total; kb += 32) {
+        for(int pb = 0; pb < total; pb += 32) {
             // ---- pair stage: bearing rejections and the depth window
-            const int k = kb + lane;
+            const int k = pb + lane;
             int m = 0;
             if(k < total) {
                 int lo = 0, hi = 31;   // first record j with incl[j] > k
@@ -500,11 +488,33 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
                 const double sv = (dxr * R.rayt[0] + dyr * R.rayt[1] + dz * R.rayt[2]) / R.rlen;
                 const double n1 = fabs(dxr * R.e1[0] + dyr * R.e1[1] + dz * R.e1[2]);
                 const double n2 = fabs(dxr * R.e2[0] + dyr * R.e2[1] + dz * R.e2[2]);
-                const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
-                float2 df;
-                if(!core3(R, sv, n1, n2, E.gaussian != 0, E.coherent != 0, omega, df)) continue;
-                atomicAdd(field + s_poff[w][pi] + (long long)iz * E.nrr, df);
+                Contrib3 o;
+                if(!geo_core3(R, sv, n1, n2, E.gaussian != 0, o)) continue;
                 ++nevals;
+                const long long cell = s_poff[w][pi] + (long long)iz * E.nrr;
+                if(MODE == INFL_TL) {
+                    const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
+                    atomicAdd(field + cell, tl_field3(o, E.gaussian != 0, E.coherent != 0, omega));
+                } else if(MODE == INFL_ARR_FILL) {
+                    const unsigned long long i = atomicAdd(cursor, 1ull);
+                    if(i >= cand_cap) continue;
+                    ArrCand c;
+                    c.amp = o.cnst * o.w;
+                    c.phase = o.ph;
+                    c.delay_re = o.dr;
+                    c.delay_im = o.di;
+                    // ReceiverAngles, 3-D (src/influence.hpp:123-138)
+                    const double rtx = R.rayt[0], rty = R.rayt[1];
+                    c.rcvr_decl = (float)((180.0 / BHCB_PI) * atan2(R.rayt[2], sqrt(rtx * rtx + rty * rty)));
+                    c.rcvr_azim = (float)((180.0 / BHCB_PI) * atan2(rty, rtx));
+                    c.ntop = R.ntop;
+                    c.nbot = R.nbot;
+                    c.job = R.job;
+                    c.aux = 0;
+                    cands[i] = c;
+                    keys[i] = ((uint64_t)cell << kb.sh_cell) | ((uint64_t)R.job << kb.sh_job) | (uint64_t)R.is;
+                    vals[i] = (uint32_t)i;
+                }
             }
             __syncwarp();
         }
@@ -513,7 +523,7 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     // one counter update per warp
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1) nevals += __shfl_down_sync(0xffffffffu, nevals, o);
-    if(lane == 0 && nevals) atomicAdd(&ctr->nevals, nevals);
+    if(MODE != INFL_ARR_FILL && lane == 0 && nevals) atomicAdd(&ctr->nevals, nevals);
 }
 
 __global__ void sqrt3d_kernel(float2 *f, long long n)
@@ -536,7 +546,25 @@ cudaError_t launch_influence3d(const SegRec3 *segs, unsigned long long nseg, con
                                float2 *field, RunCounters *ctr, int grid, cudaStream_t st)
 {
     if(nseg == 0) return cudaSuccess;
-    influence3d_kernel<<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, field, ctr);
+    influence3d_kernel<INFL_TL><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, field, ctr, nullptr,
+                                                               nullptr, nullptr, 0, nullptr, ArrKeyBits{});
+    return cudaGetLastError();
+}
+
+// arrival candidates of a 3-D run: count = true counts them into ctr->nevals;
+// otherwise writes them at cursor (cand_cap slots)
+cudaError_t launch_arr_gather3d(const SegRec3 *segs, unsigned long long nseg, const GroupDev *groups, int ngroups,
+                                bool count, ArrCand *cands, uint64_t *keys, uint32_t *vals,
+                                unsigned long long cand_cap, unsigned long long *cursor, RunCounters *ctr,
+                                ArrKeyBits kb, int grid, cudaStream_t st)
+{
+    if(nseg == 0) return cudaSuccess;
+    if(count)
+        influence3d_kernel<INFL_ARR_COUNT><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, nullptr, ctr,
+                                                                         nullptr, nullptr, nullptr, 0, nullptr, kb);
+    else
+        influence3d_kernel<INFL_ARR_FILL><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, nullptr, ctr,
+                                                                        cands, keys, vals, cand_cap, cursor, kb);
     return cudaGetLastError();
 }
 

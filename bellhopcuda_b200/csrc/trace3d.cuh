@@ -646,4 +646,32 @@ __device__ __forceinline__ void reflect3d(const Ray3 &old, Ray3 &np, const HsDev
     }
 }
 
+
+// GetJobIndices, 3-D (src/common.hpp:365-391): ialpha fastest, then ibeta, isy, isx, isz
+struct Job3 {
+    int ialpha, ibeta, isx, isy, isz;
+};
+__device__ __forceinline__ Job3 job_indices3(const Env3Dev &E, int local)
+{
+    Job3 j;
+    if(E.isingle_alpha >= 1) {
+        j.ialpha = E.isingle_alpha - 1;
+    } else {
+        j.ialpha = local % E.nalpha;
+        local /= E.nalpha;
+    }
+    if(E.isingle_beta >= 1) {
+        j.ibeta = E.isingle_beta - 1;
+    } else {
+        j.ibeta = local % E.nbeta;
+        local /= E.nbeta;
+    }
+    j.isy = local % E.nsy;
+    local /= E.nsy;
+    j.isx = local % E.nsx;
+    local /= E.nsx;
+    j.isz = local;
+    return j;
+}
+
 } // namespace bhcb

@@ -102,6 +102,25 @@ def parabot3d_hat():
     return {".env": env.replace("'R' 0.0", "'R~' 0.0"), ".bty": grid_text(xs, ys, z)}
 
 
+def munk3d_arr_gauss():
+    """Arrivals ('a', binary) on a sparse receiver grid."""
+    return _munk_slice("aB   3", alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0), theta=[0.0, 2.0, 5.0],
+                       nrz_range=(6, 500.0, 3000.0), rr_range=(7, 5.0, 30.0))
+
+
+def munk3d_arr_hat():
+    return _munk_slice("aG   3", alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0), theta=[0.0, 3.0],
+                       nrz_range=(5, 800.0, 2800.0), rr_range=(6, 8.0, 28.0))
+
+
+def parabot3d_arr_hat():
+    """Arrivals with many bottom bounces off a gridded bowl."""
+    f = parabot3d_hat()
+    f[".env"] = f[".env"].replace("'CG   3'", "'aG   3'").replace("21\n0 1000 /", "4\n200 800 /").replace(
+        "51\n0 5 /", "6\n1 5 /")
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -111,4 +130,7 @@ CASES3D = {
     "hex3d_gauss": hex3d_gauss,
     "seamount3d_gauss": seamount3d_gauss,
     "parabot3d_hat": parabot3d_hat,
+    "munk3d_arr_gauss": munk3d_arr_gauss,
+    "munk3d_arr_hat": munk3d_arr_hat,
+    "parabot3d_arr_hat": parabot3d_arr_hat,
 }

@@ -3,7 +3,8 @@
 Runs the reference's own bellhopcxx (compiled from its sources by
 oracle/Makefile into oracle/_ref/) as a 3-D run (-3) on every case of
 tests/golden/cases3d.py and stores, per case, the input files' text and the
-scaled complex field as tests/golden/<case>.npz. The GPU tests write the input
+scaled complex field (TL runs) or the arrivals (RunType 'a') as
+tests/golden/<case>.npz. The GPU tests write the input
 files back from the fixture, so they need neither the reference nor this
 script at run time. Run from the repository root:
 
@@ -24,6 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
+from bellhopcuda_b200.arrfile import read_arr_binary  # noqa: E402
 from bellhopcuda_b200.shdfile import read_shd  # noqa: E402
 from cases3d import CASES3D  # noqa: E402
 
@@ -44,8 +46,20 @@ def main(names=None):
             r = subprocess.run([EXE, "-3", "-1", root], capture_output=True, text=True)
             if r.returncode != 0:
                 raise SystemExit("reference failed on %s:\n%s%s" % (name, r.stdout[-2000:], r.stderr[-2000:]))
-            shd = read_shd(root + ".shd")
             texts = {"file_" + suffix[1:]: np.array(text) for suffix, text in files.items()}
+            if os.path.exists(root + ".arr"):
+                # arrivals: per receiver (source, bearing, depth, range) the
+                # count and the records, flattened with offsets
+                A = read_arr_binary(root + ".arr")
+                narr = np.array([len(a) for src in A["sources"] for a in src["arrivals"]], np.int32)
+                recs = np.concatenate([a for src in A["sources"] for a in src["arrivals"]] or
+                                      [np.zeros((0, 10), np.float32)])
+                np.savez_compressed(os.path.join(HERE, name + ".npz"), narr=narr, arr=recs, rr=A["rr"],
+                                    rz=A["rz"], sz=A["sz"], theta=A["theta"],
+                                    maxn=np.array([s["maxn"] for s in A["sources"]], np.int32), **texts)
+                print(name, "arrivals", int(narr.sum()), "max", int(narr.max()), "%.1fs" % (time.time() - t0))
+                continue
+            shd = read_shd(root + ".shd")
             np.savez_compressed(os.path.join(HERE, name + ".npz"), field=shd["field"],
                                 rr=shd["rr"], rz=shd["rz"], sz=shd["sz"], theta=shd["theta"], **texts)
             print(name, shd["field"].shape, "%.3g" % float(np.abs(shd["field"]).max()),

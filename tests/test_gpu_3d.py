@@ -42,7 +42,8 @@ def to_file_order(u):
     return np.transpose(u, (1, 2, 3, 0, 4, 5))
 
 
-@pytest.mark.parametrize("path", GOLD, ids=[os.path.basename(p)[:-4] for p in GOLD])
+@pytest.mark.parametrize("path", [p for p in GOLD if "_arr_" not in p],
+                         ids=[os.path.basename(p)[:-4] for p in GOLD if "_arr_" not in p])
 def test_3d_field_matches_reference(path, workdir):
     g = np.load(path)
     root = os.path.join(workdir, os.path.basename(path)[:-4])
@@ -123,3 +124,42 @@ def test_3d_small_max_memory_runs_in_waves(workdir):
         waved, st2 = t.field3d(0), t.stats()
     assert st2["segments"] == st["segments"]
     np.testing.assert_allclose(waved, full, rtol=1e-4, atol=1e-6 * np.abs(full).max())
+
+
+ARR3D = sorted(p for p in GOLD if "_arr_" in p)
+TL3D = [p for p in GOLD if "_arr_" not in p]
+
+
+@pytest.mark.parametrize("path", ARR3D, ids=[os.path.basename(p)[:-4] for p in ARR3D])
+def test_3d_arrivals_match_reference(path, workdir):
+    """3-D arrivals (RunType 'a') against the reference's single-threaded run
+    (merging on): counts and bounce counts exact, delays within 1e-6 relative,
+    amplitudes within 1e-4 relative, angles within 1e-3 degrees."""
+    g = np.load(path)
+    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.set_arrival_options(1000, True)
+        t.setup3d(root)
+        t.run()
+        narr, arr = t.arrivals()
+        t.writeout(root + "_gpu")
+    narr = narr.reshape(-1)
+    np.testing.assert_array_equal(narr, g["narr"])
+    assert narr.sum() > 0
+    got = arr.reshape(narr.size, -1)[narr[:, None] > np.arange(arr.shape[-1])]
+    ref = g["arr"]
+    np.testing.assert_array_equal(got["NTopBnc"], ref[:, 8].astype(np.int32))
+    np.testing.assert_array_equal(got["NBotBnc"], ref[:, 9].astype(np.int32))
+    np.testing.assert_allclose(got["delay_re"], ref[:, 2], rtol=1e-6)
+    np.testing.assert_allclose(got["delay_im"], ref[:, 3], rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(got["a"], ref[:, 0], rtol=1e-4)
+    for k, c in (("SrcDeclAngle", 4), ("SrcAzimAngle", 5), ("RcvrDeclAngle", 6), ("RcvrAzimAngle", 7)):
+        np.testing.assert_allclose(got[k], ref[:, c], rtol=0, atol=1e-3, err_msg=k)
+    # the product's own .arr file holds the same records
+    from bellhopcuda_b200.arrfile import read_arr_binary
+    A = read_arr_binary(root + "_gpu.arr")
+    assert A["dim"] == "'3D'"
+    mine = np.concatenate([a for s in A["sources"] for a in s["arrivals"]])
+    np.testing.assert_array_equal(mine[:, 2], got["delay_re"])
+    np.testing.assert_allclose(mine[:, 1], ref[:, 1], rtol=0, atol=1e-3)   # phase in degrees

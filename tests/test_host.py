@@ -151,8 +151,13 @@ def test_reader3d_sizes_match_reference_fixture(name, workdir):
             with open(root + "." + k[5:], "w") as f:
                 f.write(str(g[k]))
     info = B.check_env3d(root)
-    nsx, nsy, nth, nsz, nrz, nrr = g["field"].shape
-    assert info["dims"] == (nsz, nsx, nsy, nth, nrz, nrr)
+    if "field" in g.files:
+        nsx, nsy, nth, nsz, nrz, nrr = g["field"].shape
+        assert info["dims"] == (nsz, nsx, nsy, nth, nrz, nrr)
+    else:   # arrivals fixture: one count per receiver
+        d = info["dims"]
+        assert (d[0], d[3], d[4], d[5]) == (len(g["sz"]), len(g["theta"]), len(g["rz"]), len(g["rr"]))
+        assert int(np.prod(d)) == g["narr"].size
     assert info["nrays"] > 0
 
 
