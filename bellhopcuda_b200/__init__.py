@@ -110,6 +110,11 @@ SIGNATURES = [
     ("bhcb_field_shape3d", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     ("bhcb_grid3d", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p]),
+    ("bhcb_graph_create", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
+                                    C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    ("bhcb_graph_launch", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("bhcb_graph_status", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    ("bhcb_graph_destroy", None, [C.c_void_p]),
     ("bhcb_version", C.c_char_p, []),
 ]
 
@@ -333,6 +338,16 @@ class Tracer:
         if rc != 0:
             raise BhcbError(rc, msg.value.decode(errors="replace"))
 
+    def graph(self, field_dev_ptr: int, nbytes: int, env: int = 0, ifreq: int = 0) -> "FieldGraph":
+        """Capture one field of the prepared context into a CUDA graph writing to field_dev_ptr."""
+        g = C.c_void_p()
+        msg = C.create_string_buffer(512)
+        rc = self._lib.bhcb_graph_create(self._h, env, ifreq, C.c_void_p(field_dev_ptr), nbytes, C.byref(g),
+                                         msg, len(msg))
+        if rc != 0:
+            raise BhcbError(rc, msg.value.decode(errors="replace"))
+        return FieldGraph(self._lib, g)
+
     def stream_ptr(self) -> int:
         p = C.c_void_p()
         self._check(self._lib.bhcb_stream(self._h, C.byref(p)))
@@ -342,6 +357,36 @@ class Tracer:
         s = Stats()
         self._check(self._lib.bhcb_get_stats(self._h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+class FieldGraph:
+    """A captured field run (bhcb_graph_*): launch() replays it, status() waits and checks."""
+
+    def __init__(self, lib, handle):
+        self._lib, self._g = lib, handle
+
+    def launch(self, stream: int = 0):
+        rc = self._lib.bhcb_graph_launch(self._g, C.c_void_p(stream or None))
+        if rc != 0:
+            raise BhcbError(rc, "graph launch failed")
+
+    def status(self, stream: int = 0) -> dict:
+        eb, ev = C.c_uint32(), C.c_uint64()
+        rc = self._lib.bhcb_graph_status(self._g, C.c_void_p(stream or None), C.byref(eb), C.byref(ev))
+        if rc not in (0, 4):
+            raise BhcbError(rc, "graph status failed")
+        return {"err_bits": eb.value, "evals": ev.value}
+
+    def close(self):
+        if self._g:
+            self._lib.bhcb_graph_destroy(self._g)
+            self._g = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def tl_db(p: np.ndarray) -> np.ndarray:

@@ -363,3 +363,120 @@ extern "C" int bhcb_run_noalloc(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq,
     }
     return BHCB_OK;
 }
+
+// ------------------------------------------------------------ CUDA graphs
+// A prepared field captured once into a CUDA graph (header set-up, accumulator
+// clear, fused trace + influence, scale) and replayed with one
+// cudaGraphLaunch per run. The graph owns its scratch (allocated before the
+// capture), so graphs of different fields can be replayed concurrently.
+struct bhcb_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned char *scratch = nullptr;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+};
+
+namespace bhcb {
+namespace {
+__global__ void write_header_kernel(NoAllocHeader h, unsigned char *dst)
+{
+    const unsigned *src = reinterpret_cast<const unsigned *>(&h);
+    unsigned *d = reinterpret_cast<unsigned *>(dst);
+    for(int i = threadIdx.x; i < (int)(sizeof(NoAllocHeader) / 4); i += blockDim.x) d[i] = src[i];
+}
+} // namespace
+} // namespace bhcb
+
+extern "C" void bhcb_graph_destroy(bhcb_graph *g)
+{
+    if(!g) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(g->device);
+    if(g->stream) cudaStreamSynchronize(g->stream);
+    if(g->exec) cudaGraphExecDestroy(g->exec);
+    if(g->graph) cudaGraphDestroy(g->graph);
+    if(g->scratch) cudaFree(g->scratch);
+    if(g->stream) cudaStreamDestroy(g->stream);
+    cudaSetDevice(cur);
+    delete g;
+}
+
+extern "C" int bhcb_graph_create(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void *field_dev, size_t bytes,
+                                 bhcb_graph **out, char *msg, size_t msg_len)
+{
+    if(msg && msg_len) msg[0] = 0;
+    if(!out) return put_msg(msg, msg_len, BHCB_ERR_ARG, "graph output pointer is NULL");
+    *out = nullptr;
+    if(!ctx || !field_dev) return put_msg(msg, msg_len, BHCB_ERR_ARG, "context or output pointer is NULL");
+    NoAllocJob J;
+    const char *why = nullptr;
+    int rc = noalloc_job_from_ctx(ctx, env_index, ifreq, &J, &why);
+    if(rc != BHCB_OK) return put_msg(msg, msg_len, rc, why ? why : "invalid request");
+    const size_t nelem = (size_t)J.nsz * J.nrzp * J.nrr;
+    if(bytes < nelem * sizeof(float2)) return put_msg(msg, msg_len, BHCB_ERR_ARG, "output buffer too small");
+    auto *g = new bhcb_graph();
+    cudaGetDevice(&g->device);
+    auto fail = [&](int code, const char *text) {
+        cudaGetLastError();
+        bhcb_graph_destroy(g);
+        return put_msg(msg, msg_len, code, text);
+    };
+    if(cudaMalloc((void **)&g->scratch, kHeaderBytes + nelem * sizeof(float2)) != cudaSuccess)
+        return fail(BHCB_ERR_MEMORY, "graph scratch allocation failed");
+    if(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(BHCB_ERR_CUDA, "stream creation failed");
+    NoAllocHeader h;
+    memset(&h, 0, sizeof h);
+    h.ctr.overflow_job = 0xffffffffu;
+    h.group = J.group;
+    h.group.job_base = 0;
+    h.group.nfreq = 1;
+    h.group.freq_base = 0;
+    h.group.field_base = 0;
+    h.group.field_stride_f = (int)nelem;
+    h.group.acc_base = 0;
+    h.group.acc_stride_f = (int64_t)nelem;
+    h.group.acc_nz = J.nrzp;
+    J.stream = g->stream;
+    long long grid = (J.group.njobs + 31) / 32;
+    if(grid > (long long)J.sm_count * 16) grid = (long long)J.sm_count * 16;
+    if(grid < 1) grid = 1;
+    if(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(BHCB_ERR_CUDA, "stream capture could not begin");
+    write_header_kernel<<<1, 64, 0, g->stream>>>(h, g->scratch);
+    cudaMemsetAsync(g->scratch + kHeaderBytes, 0, nelem * sizeof(float2), g->stream);
+    if(J.precision == BHCB_PREC_FP64) launch_fused<double>(J, g->scratch, (int)grid);
+    else launch_fused<float>(J, g->scratch, (int)grid);
+    NoAllocHeader *dh = reinterpret_cast<NoAllocHeader *>(g->scratch);
+    launch_scale(reinterpret_cast<const float2 *>(g->scratch + kHeaderBytes), (float2 *)field_dev, &dh->group, 1,
+                 J.sm_count * 2, g->stream);
+    if(cudaStreamEndCapture(g->stream, &g->graph) != cudaSuccess || !g->graph)
+        return fail(BHCB_ERR_CUDA, "stream capture failed");
+    if(cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess)
+        return fail(BHCB_ERR_CUDA, "graph instantiation failed");
+    *out = g;
+    return BHCB_OK;
+}
+
+extern "C" int bhcb_graph_launch(bhcb_graph *g, void *stream)
+{
+    if(!g) return BHCB_ERR_ARG;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    return cudaGraphLaunch(g->exec, s) == cudaSuccess ? BHCB_OK : BHCB_ERR_CUDA;
+}
+
+extern "C" int bhcb_graph_status(bhcb_graph *g, void *stream, uint32_t *err_bits, uint64_t *evals)
+{
+    if(!g) return BHCB_ERR_ARG;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    RunCounters back;
+    const NoAllocHeader *dh = reinterpret_cast<const NoAllocHeader *>(g->scratch);
+    if(cudaMemcpyAsync(&back, &dh->ctr, sizeof back, cudaMemcpyDeviceToHost, s) != cudaSuccess
+       || cudaStreamSynchronize(s) != cudaSuccess)
+        return BHCB_ERR_CUDA;
+    if(err_bits) *err_bits = back.err_bits;
+    if(evals) *evals = back.nevals;
+    return back.err_bits ? BHCB_ERR_RUN : BHCB_OK;
+}

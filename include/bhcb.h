@@ -213,6 +213,21 @@ int bhcb_field_shape3d(bhcb_ctx *ctx, int32_t env_index, int32_t *dims);
 int bhcb_grid3d(bhcb_ctx *ctx, int32_t env_index, double *sx, double *sy, float *sz, double *rr, float *rz,
                 double *theta);
 
+/* CUDA graphs of the hot path (no reference counterpart): one field of a
+   prepared context (bhcb_prepare done, TL run) captured into a graph that
+   writes into field_dev. The graph owns its scratch (allocated here, before
+   the capture); each launch re-clears it, so a graph can be replayed any
+   number of times, and graphs of different fields concurrently. Launch on
+   `stream` (a cudaStream_t; NULL = the graph's own stream). bhcb_graph_status
+   waits for that stream and reports the tracer's error bits and the number
+   of contributions of the last launch. */
+typedef struct bhcb_graph bhcb_graph;
+int bhcb_graph_create(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void *field_dev, size_t bytes,
+                      bhcb_graph **graph, char *msg, size_t msg_len);
+int bhcb_graph_launch(bhcb_graph *graph, void *stream);
+int bhcb_graph_status(bhcb_graph *graph, void *stream, uint32_t *err_bits, uint64_t *evals);
+void bhcb_graph_destroy(bhcb_graph *graph);
+
 /* Library version string. */
 const char *bhcb_version(void);
 
