@@ -115,6 +115,9 @@ SIGNATURES = [
     ("bhcb_graph_launch", C.c_int, [C.c_void_p, C.c_void_p]),
     ("bhcb_graph_status", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     ("bhcb_graph_destroy", None, [C.c_void_p]),
+    ("bhcb_nn_gemm", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("bhcb_nn_status", C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
     ("bhcb_version", C.c_char_p, []),
 ]
 

@@ -228,6 +228,20 @@ int bhcb_graph_launch(bhcb_graph *graph, void *stream);
 int bhcb_graph_status(bhcb_graph *graph, void *stream, uint32_t *err_bits, uint64_t *evals);
 void bhcb_graph_destroy(bhcb_graph *graph);
 
+/* Tensor-core GEMM of the TL surrogate (no reference counterpart):
+   C[M,N] = epi(A[M,K] * B[N,K]^T), A and B row-major bf16 with K a multiple of
+   8 and 16-byte aligned bases, FP32 accumulation in tensor memory (tcgen05).
+   Epilogues: F32 (C float, + bias[N] if bias), BF16 (C bf16, + bias), BF16_GELU
+   (pre = acc + bias stored to aux_out if not NULL, C = gelu(pre), tanh form),
+   BF16_DGELU (C = acc * gelu'(aux_in), aux_in bf16 [M,N]). Enqueued on
+   `stream` (a cudaStream_t, NULL = legacy default). bhcb_nn_status reports
+   (and optionally clears) the sticky error word a kernel sets when one of its
+   bounded waits ran out. */
+enum { BHCB_NN_EPI_F32 = 0, BHCB_NN_EPI_BF16 = 1, BHCB_NN_EPI_BF16_GELU = 2, BHCB_NN_EPI_BF16_DGELU = 3 };
+int bhcb_nn_gemm(const void *A, const void *B, void *C, int32_t M, int32_t N, int32_t K, int32_t epi,
+                 const float *bias, const void *aux_in, void *aux_out, void *stream);
+int bhcb_nn_status(int32_t *error, int32_t clear);
+
 /* Library version string. */
 const char *bhcb_version(void);
 
