@@ -118,6 +118,16 @@ SIGNATURES = [
     ("bhcb_nn_gemm", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bhcb_nn_status", C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
+    ("bhcb_nn_tl_db", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_void_p]),
+    ("bhcb_nn_transpose", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    ("bhcb_nn_mse", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("bhcb_nn_row_rms", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("bhcb_nn_colsum", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("bhcb_nn_adam", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float,
+                               C.c_float, C.c_float, C.c_float, C.c_int32, C.c_float, C.c_void_p, C.c_void_p,
+                               C.c_void_p]),
+    ("bhcb_nn_to_bf16", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    ("bhcb_nn_affine", C.c_int, [C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_void_p]),
     ("bhcb_version", C.c_char_p, []),
 ]
 

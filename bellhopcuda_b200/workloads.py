@@ -11,6 +11,10 @@ the reference, the oracle and this library.
                   uniform in 3000-5000 m over 100 km, 10 log-spaced frequencies
                   50-500 Hz, 20001 rays over +-30 deg, 501 x 2001 receivers.
 * ``batch_envs`` — many small uneven spline-SSP environments for batched runs.
+* ``c5_envs``   — surrogate training / test environments: 2-D coherent hat-beam
+                  TL on a 128 x 256 grid; 64-node SSP = Munk + 8 random smooth
+                  modes N(0, 2 m/s), depth 1000-5000 m, bottom cp 1500-1800
+                  m/s, source 10-500 m, 50-500 Hz (log-uniform).
 * ``c4_3d``     — 3-D Gaussian-beam TL (or arrivals): hexahedral SSP on a
                   41 x 41 x 51 grid over 80 x 80 km x 5000 m (Munk plus a seeded
                   warm-core eddy), 'R' bathymetry on a 101 x 101 grid seeded in
@@ -139,3 +143,49 @@ def c4_3d(seed=1004, run_type="CB   3", scale=1.0, nalpha=361, nbeta=144, ntheta
         rr_range=(max(2, int(round(nrr * scale))), 0.0, 38.0),
         theta_range=(max(1, int(round(ntheta * scale))), 0.0, 360.0 - 360.0 / max(1, int(round(ntheta * scale)))))
     return {".env": env, ".ssp": envfile3d.hex_ssp_text(hx, hy, hz, c), ".bty": envfile3d.grid_text(bx, by, b)}
+
+
+C5_NZ, C5_NR = 128, 256
+C5_RR_KM = (0.08, 20.0)
+
+
+def c5_params(n, seed=1005):
+    """Seeded parameters of n surrogate environments (one row each):
+    depth, bottom cp, source depth, frequency, 8 SSP mode amplitudes."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    depth = rng.uniform(1000.0, 5000.0, n)
+    cp = rng.uniform(1500.0, 1800.0, n)
+    zs = rng.uniform(10.0, 500.0, n)
+    f = np.exp(rng.uniform(math.log(50.0), math.log(500.0), n))
+    a = rng.normal(0.0, 2.0, (n, 8))
+    return dict(depth=depth, cp=cp, zs=zs, f=f, a=a)
+
+
+def c5_ssp(depth, a):
+    """64-node SSP: Munk + sum_k a_k sin(k pi z / D)."""
+    z = np.linspace(0.0, depth, 64)
+    c = munk_c(z) + sum(a[k] * np.sin((k + 1) * np.pi * z / depth) for k in range(8))
+    return z, c
+
+
+def c5_nalpha(depth, freq):
+    """EstimateNumAngles (src/module/rayangles.hpp:212-238) for this grid."""
+    rmax = C5_RR_KM[1] * 1000.0
+    n = max(int(0.3 * rmax * freq / 1500.0), 300)
+    return max(int(np.pi / np.arctan(depth / (10.0 * rmax))), n)
+
+
+def c5_env(P, i) -> EnvSpec:
+    depth, cp, zs, f = float(P["depth"][i]), float(P["cp"][i]), float(P["zs"][i]), float(P["f"][i])
+    z, c = c5_ssp(depth, P["a"][i])
+    return EnvSpec(
+        title="surrogate env %d" % i, freq=f, ssp_type="C", top_bc="V", atten_unit="W",
+        ssp_z=z, ssp_cp=c, bot_bc="A", bot_hs=(depth, cp, 0.0, 1.8, 0.8, 0.0),
+        nsz=1, sz=(zs,), nrz=C5_NZ, rz=(0.0, depth), nrr=C5_NR, rr_km=C5_RR_KM,
+        run_type="CG RR ", nalpha=c5_nalpha(depth, f), alpha=(-60.0, 60.0), deltas=0.0,
+        box_z=depth + 100.0, box_r_km=C5_RR_KM[1] + 1.0)
+
+
+def c5_envs(n=100000, seed=1005) -> List[EnvSpec]:
+    P = c5_params(n, seed)
+    return [c5_env(P, i) for i in range(n)]

@@ -241,6 +241,27 @@ enum { BHCB_NN_EPI_F32 = 0, BHCB_NN_EPI_BF16 = 1, BHCB_NN_EPI_BF16_GELU = 2, BHC
 int bhcb_nn_gemm(const void *A, const void *B, void *C, int32_t M, int32_t N, int32_t K, int32_t epi,
                  const float *bias, const void *aux_in, void *aux_out, void *stream);
 int bhcb_nn_status(int32_t *error, int32_t clear);
+/* Surrogate training / inference helpers (device pointers, enqueued on stream):
+   tl_db: TL = -20 log10|p| of n complex64 pressures, clamped to [lo, hi];
+   transpose: bf16 [rows][cols] -> [cols][rows];
+   mse: grad = bf16(scale * 2 (pred - target)), *loss_dev += sum (pred - target)^2;
+   row_rms: per-row RMS of pred - target (rows x cols float);
+   colsum: db[n] = sum_m dy[m][n] (bf16 in, float out);
+   adam: bias-corrected Adam step `step` (1-based) with decoupled weight decay on
+   FP32 master weights [rows][cols], refreshing the bf16 copy w_bf16 and, if
+   not NULL, its transpose wt_bf16 [cols][rows];
+   to_bf16: float -> bf16. */
+int bhcb_nn_tl_db(const void *field, float *tl, int64_t n, float lo, float hi, void *stream);
+int bhcb_nn_transpose(const void *in, void *out, int32_t rows, int32_t cols, void *stream);
+int bhcb_nn_mse(const float *pred, const float *target, int64_t n, float scale, void *grad, double *loss_dev,
+                void *stream);
+int bhcb_nn_row_rms(const float *pred, const float *target, int32_t rows, int32_t cols, float *rms, void *stream);
+int bhcb_nn_colsum(const void *dy, int32_t M, int32_t N, float *db, void *stream);
+int bhcb_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols, float lr, float beta1,
+                 float beta2, float eps, int32_t step, float weight_decay, void *w_bf16, void *wt_bf16, void *stream);
+int bhcb_nn_to_bf16(const float *x, void *y, int64_t n, void *stream);
+/* x = a * x + b over n floats */
+int bhcb_nn_affine(float *x, int64_t n, float a, float b, void *stream);
 
 /* Library version string. */
 const char *bhcb_version(void);
