@@ -11,7 +11,9 @@
 //                  tcgen05.commit on the stage's "empty" mbarrier frees the slot,
 //                  a final commit signals the epilogue;
 //   all 4 warps    epilogue: tcgen05.ld of their 32 accumulator lanes (rows),
-//                  bias / GELU / GELU' / conversion, stores.
+//                  staged through the (then idle) stage ring so that each store
+//                  instruction writes 32 consecutive columns of one row; bias /
+//                  GELU / GELU' / conversion on the way out.
 // Every mbarrier wait is bounded; a wait that runs out sets the error word,
 // the CTA skips its stores, frees its tensor memory and returns. No TMA load
 // uses cluster multicast.
@@ -208,34 +210,42 @@ __global__ void __launch_bounds__(128, 1) gemm_tc_kernel(const __grid_constant__
     const bool good = ready && s_fail == 0;
     if(!good && threadIdx.x == 0) atomicExch(&g_nn_error, 1);
     if(good) {
-        const int row = m0 + warp * 32 + lane;
+        // every MMA has completed, so the stage ring is free: each warp stages
+        // its 32 rows x 32 columns through shared memory and stores them row by
+        // row, one coalesced 32-column segment per instruction
+        float *stage = reinterpret_cast<float *>(smem) + warp * (32 * 33);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after the ring's async-proxy use
 #pragma unroll 1
         for(int c = 0; c < BN / 32; ++c) {
             float v[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), v);
-            if(row >= M) continue;
-            const int nb = n0 + c * 32;
-            if(nb >= N) continue;
-            const int cnt = min(32, N - nb);
-            const size_t base = (size_t)row * N + nb;
-            if(EPI == BHCB_NN_EPI_F32) {
-                float *out = reinterpret_cast<float *>(C) + base;
-                for(int j = 0; j < cnt; ++j) out[j] = v[j] + (bias ? bias[nb + j] : 0.0f);
-            } else if(EPI == BHCB_NN_EPI_BF16) {
-                __nv_bfloat16 *out = reinterpret_cast<__nv_bfloat16 *>(C) + base;
-                for(int j = 0; j < cnt; ++j) out[j] = __float2bfloat16_rn(v[j] + (bias ? bias[nb + j] : 0.0f));
-            } else if(EPI == BHCB_NN_EPI_BF16_GELU) {
-                __nv_bfloat16 *out = reinterpret_cast<__nv_bfloat16 *>(C) + base;
-                for(int j = 0; j < cnt; ++j) {
-                    const float pre = v[j] + (bias ? bias[nb + j] : 0.0f);
-                    if(aux_out) aux_out[base + j] = __float2bfloat16_rn(pre);
-                    out[j] = __float2bfloat16_rn(gelu_f(pre));
+#pragma unroll
+            for(int j = 0; j < 32; ++j) stage[lane * 33 + j] = v[j];
+            __syncwarp();
+            const int col = n0 + c * 32 + lane;
+            const bool colok = col < N;
+            const float bcol = (bias && colok) ? bias[col] : 0.0f;
+#pragma unroll 4
+            for(int rr = 0; rr < 32; ++rr) {
+                const int row = m0 + warp * 32 + rr;
+                if(row >= M) break;
+                if(!colok) continue;
+                const float acc = stage[rr * 33 + lane];
+                const size_t idx = (size_t)row * N + col;
+                if(EPI == BHCB_NN_EPI_F32) {
+                    reinterpret_cast<float *>(C)[idx] = acc + bcol;
+                } else if(EPI == BHCB_NN_EPI_BF16) {
+                    reinterpret_cast<__nv_bfloat16 *>(C)[idx] = __float2bfloat16_rn(acc + bcol);
+                } else if(EPI == BHCB_NN_EPI_BF16_GELU) {
+                    const float pre = acc + bcol;
+                    if(aux_out) aux_out[idx] = __float2bfloat16_rn(pre);
+                    reinterpret_cast<__nv_bfloat16 *>(C)[idx] = __float2bfloat16_rn(gelu_f(pre));
+                } else {   // BHCB_NN_EPI_BF16_DGELU
+                    reinterpret_cast<__nv_bfloat16 *>(C)[idx]
+                        = __float2bfloat16_rn(acc * dgelu_f(__bfloat162float(aux_in[idx])));
                 }
-            } else {   // BHCB_NN_EPI_BF16_DGELU
-                __nv_bfloat16 *out = reinterpret_cast<__nv_bfloat16 *>(C) + base;
-                for(int j = 0; j < cnt; ++j)
-                    out[j] = __float2bfloat16_rn(v[j] * dgelu_f(__bfloat162float(aux_in[base + j])));
             }
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -7,7 +7,7 @@ A DeepONet-style operator maps an environment to its TL grid:
 * branch net: 128 environment features -> 4 GELU layers of width 1024 -> 512
   coefficients b_k (the SSP sampled at 64 normalised depths, water depth,
   bottom speed, source depth, frequency);
-* trunk net: 64 Fourier features of the normalised receiver coordinates ->
+* trunk net: 128 Fourier features of the normalised receiver coordinates ->
   3 layers of width 512 -> 512 basis values t_k per receiver (the same
   128 x 256 normalised grid for every environment, so one trunk pass serves a
   whole batch);
@@ -39,7 +39,7 @@ from .envfile import write_env
 NZ, NR = W.C5_NZ, W.C5_NR
 NP = NZ * NR
 N_IN = 128
-N_TRUNK_IN = 64
+N_TRUNK_IN = 128
 TL_LO, TL_HI = 30.0, 130.0       # clamp of the training targets (dB)
 TL_MEAN, TL_SCALE = 80.0, 20.0   # normalisation of the network output
 
@@ -72,15 +72,15 @@ def features(P: Dict[str, np.ndarray], idx: Sequence[int]) -> np.ndarray:
 
 
 def trunk_inputs() -> np.ndarray:
-    """(NP, 64) float32 Fourier features of the normalised (depth, range) grid."""
+    """(NP, 128) float32 Fourier features of the normalised (depth, range) grid:
+    geometric frequency ladders up to the grid's Nyquist rate in each axis."""
     u = np.repeat(np.linspace(0.0, 1.0, NZ), NR)
     v = np.tile(np.linspace(0.0, 1.0, NR), NZ)
     f = [u * 2 - 1, v * 2 - 1]
-    for k in range(1, 16):
+    for k in np.geomspace(1.0, NZ / 2.0, 24):
         f += [np.sin(k * math.pi * u), np.cos(k * math.pi * u)]
-    for k in range(1, 16):
+    for k in np.geomspace(1.0, NR / 2.0, 39):
         f += [np.sin(k * math.pi * v), np.cos(k * math.pi * v)]
-    f += [np.zeros_like(u), np.zeros_like(u)]
     return np.stack(f, 1).astype(np.float32)
 
 
@@ -527,6 +527,11 @@ def main(argv=None):
         "returned_within_1db": float((err <= 1.0).mean()),
         "plain_fp64_fields_per_s": a.n / gen["trace_s"],
     }
+    pe = (model.predict_error(X[n_tr + n_va:]) * margin).cpu().numpy()
+    for thr in (2.0, 3.0, 6.0):
+        acc = pe <= thr
+        out["accepted_at_%gdb" % thr] = float(acc.mean())
+        out["accepted_rms_db_mean_at_%gdb" % thr] = float(e0[acc].mean()) if acc.any() else None
     if a.save:
         np.savez_compressed(a.save, **model.state())
     print(json.dumps(out))
