@@ -2,9 +2,11 @@
 //
 //   C[M, N] = epilogue(A[M, K] * B[N, K]^T)      A, B row-major bf16 (K-major)
 //
-// One CTA per 128 x 128 output tile, 128 threads:
+// One CTA per 128 x 128 output tile, 128 threads, three CTAs per SM (64 KiB of
+// shared memory and 128 tensor-memory columns each), so that one CTA's
+// epilogue overlaps the other CTAs' main loops:
 //   warp 0 lane 0  TMA producer: 128 x 64 bf16 tiles of A and B per stage into
-//                  a 4-stage ring (128-byte swizzle), completion on the stage's
+//                  a 2-stage ring (128-byte swizzle), completion on the stage's
 //                  "full" mbarrier (transaction bytes);
 //   warp 1 lane 0  MMA issuer: four tcgen05.mma.kind::f16 (M 128, N 128, K 16)
 //                  per stage into a 128-column FP32 accumulator in tensor memory;
@@ -29,7 +31,7 @@
 namespace bhcb {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 2;
 constexpr int TILE_A = BM * BK * 2;   // 16 KiB
 constexpr int TILE_B = BN * BK * 2;
 constexpr int SMEM_BYTES = STAGES * (TILE_A + TILE_B) + 1024 + 256;
@@ -133,7 +135,7 @@ __device__ __forceinline__ float dgelu_f(float x)
 }
 
 template<int EPI>
-__global__ void __launch_bounds__(128, 1) gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(128, 3) gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB, int M, int N,
                                                          int K, void *C, const float *__restrict__ bias,
                                                          const __nv_bfloat16 *__restrict__ aux_in,
