@@ -41,6 +41,11 @@ class BhcbError(RuntimeError):
         self.err_bits = err_bits
 
 
+class Tuning(C.Structure):
+    _fields_ = [("trace_block", C.c_int32), ("influence_ctas_per_sm", C.c_int32),
+                ("trace_ms", C.c_double), ("influence_ms", C.c_double)]
+
+
 class Init(C.Structure):
     _fields_ = [("gpu_index", C.c_int32), ("precision", C.c_int32), ("max_memory", C.c_uint64),
                 ("share_trajectory", C.c_int32), ("flags", C.c_int32),
@@ -128,6 +133,8 @@ SIGNATURES = [
                                C.c_void_p]),
     ("bhcb_nn_to_bf16", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     ("bhcb_nn_affine", C.c_int, [C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_void_p]),
+    ("bhcb_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),
+    ("bhcb_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("bhcb_version", C.c_char_p, []),
 ]
 
@@ -360,6 +367,17 @@ class Tracer:
         if rc != 0:
             raise BhcbError(rc, msg.value.decode(errors="replace"))
         return FieldGraph(self._lib, g)
+
+    def autotune(self, repeats: int = 2) -> dict:
+        """Time the prepared TL workload with each launch shape; keep the fastest."""
+        t = Tuning()
+        self._check(self._lib.bhcb_autotune(self._h, repeats, C.byref(t)))
+        return {"trace_block": t.trace_block, "influence_ctas_per_sm": t.influence_ctas_per_sm,
+                "trace_ms": t.trace_ms, "influence_ms": t.influence_ms}
+
+    def set_tuning(self, trace_block: int, influence_ctas_per_sm: int):
+        t = Tuning(trace_block, influence_ctas_per_sm, 0.0, 0.0)
+        self._check(self._lib.bhcb_set_tuning(self._h, C.byref(t)))
 
     def stream_ptr(self) -> int:
         p = C.c_void_p()

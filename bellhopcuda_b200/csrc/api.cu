@@ -99,6 +99,9 @@ struct bhcb_ctx {
     // ev: 0 start, 1 trace end, 2 influence end, 3 scale end, 4 first influence launch
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
+    // launch shapes (bhcb_autotune picks them by timing the prepared workload)
+    int trace_block = 32;           // threads per trace CTA (one ray each)
+    int influence_ctas_per_sm = 8;  // persistent influence CTAs per SM
 
     std::vector<EnvSlot> envs;
     bool prepared = false;
@@ -420,7 +423,7 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         CK(cudaMemsetAsync((float2 *)c->acc.p + a0, 0, (size_t)(a1 - a0) * sizeof(float2), c->stream));
     }
     CK(cudaEventRecord(c->ev[0], c->stream));
-    int tblock = 32;
+    int tblock = c->trace_block;
     long long tgrid = std::min<long long>((job1 - job0 + tblock - 1) / tblock, (long long)c->sm_count * 16);
     if(tgrid < 1) tgrid = 1;
     const GroupDev *G = (const GroupDev *)c->groups_d.p + g0;
@@ -448,7 +451,7 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     CK(cudaEventRecord(c->ev[1], c->stream));
     if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
     if(ovl) {
-        const int igrid = c->sm_count * 8;
+        const int igrid = c->sm_count * c->influence_ctas_per_sm;
         unsigned long long *scan = (unsigned long long *)c->scan.p;
         const double *fq = (const double *)c->freqs_d.p;
         CK(cudaStreamWaitEvent(c->stream2, c->ev[0], 0));
@@ -475,7 +478,7 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     }
     // the influence grid covers the buffer capacity; chunks past the stored
     // count are skipped by reading the count on the device
-    int igrid = c->sm_count * 8;   // persistent warps draining the chunk queue
+    int igrid = c->sm_count * c->influence_ctas_per_sm;   // persistent warps draining the chunk queue
     if(fp64)
         CK(launch_influence<double>(c->segs.p, c->seg_cap, G, ng, (const double *)c->freqs_d.p,
                                     (float2 *)c->acc.p, ctr, c->gauss, c->coherent, igrid, c->stream));
@@ -1224,6 +1227,65 @@ int bhcb_grid3d(bhcb_ctx *c, int32_t env, double *sx, double *sy, float *sz, dou
         if(rr) std::memcpy(rr, vrr.data(), vrr.size() * sizeof(double));
         if(rz) std::memcpy(rz, vrz.data(), vrz.size() * sizeof(float));
         if(theta) std::memcpy(theta, vth.data(), vth.size() * sizeof(double));
+        return BHCB_OK;
+    });
+}
+
+int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
+{
+    return guarded(c, [&]() -> int {
+        if(c->is3d()) throw StateError("the autotuner covers the 2-D TL runs");
+        if(!c->prepared) do_prepare(c);
+        if(c->mode != MODE_TL) throw StateError("the autotuner covers TL runs");
+        const int reps = std::max(1, std::min<int>(repeats, 16));
+        const bool overlap = c->overlap;
+        c->overlap = false;   // time the trace and the influence separately
+        auto timed = [&](double &tr, double &inf) {
+            tr = inf = 1e300;
+            for(int r = 0; r < reps; ++r) {
+                if(run_checked(c) != BHCB_OK) throw std::runtime_error("run failed while tuning");
+                tr = std::min(tr, c->stats.trace_ms);
+                inf = std::min(inf, c->stats.influence_ms);
+            }
+        };
+        bhcb_tuning t{};
+        t.trace_block = c->trace_block;
+        t.influence_ctas_per_sm = c->influence_ctas_per_sm;
+        double tr = 0, inf = 0;
+        timed(tr, inf);   // warm-up and the current shape
+        t.trace_ms = tr;
+        t.influence_ms = inf;
+        for(int tb : {32, 64}) {   // the trace kernel is compiled for at most 64 threads per CTA
+            c->trace_block = tb;
+            timed(tr, inf);
+            if(tr < t.trace_ms) { t.trace_ms = tr; t.trace_block = tb; }
+        }
+        c->trace_block = t.trace_block;
+        for(int k : {2, 3, 4, 5, 6, 8, 12}) {
+            c->influence_ctas_per_sm = k;
+            timed(tr, inf);
+            if(inf < t.influence_ms) { t.influence_ms = inf; t.influence_ctas_per_sm = k; }
+        }
+        c->influence_ctas_per_sm = t.influence_ctas_per_sm;
+        c->overlap = overlap;
+        if(out) *out = t;
+        char b[160];
+        snprintf(b, sizeof b, "autotune: trace %d threads/CTA (%.3f ms), influence %d CTAs/SM (%.3f ms)",
+                 t.trace_block, t.trace_ms, t.influence_ctas_per_sm, t.influence_ms);
+        c->msg(b);
+        return BHCB_OK;
+    });
+}
+
+int bhcb_set_tuning(bhcb_ctx *c, const bhcb_tuning *t)
+{
+    return guarded(c, [&]() -> int {
+        if(!t) throw std::invalid_argument("tuning is NULL");
+        if(t->trace_block != 32 && t->trace_block != 64) throw std::invalid_argument("trace_block must be 32 or 64");
+        if(t->influence_ctas_per_sm < 1 || t->influence_ctas_per_sm > 64)
+            throw std::invalid_argument("influence_ctas_per_sm must be in 1..64");
+        c->trace_block = t->trace_block;
+        c->influence_ctas_per_sm = t->influence_ctas_per_sm;
         return BHCB_OK;
     });
 }

@@ -161,12 +161,18 @@ def tl_rms(a, b):
 
 
 # ------------------------------------------------------------- our arm
-def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush):
-    """Device time per step of the prepared run (tables resident in HBM)."""
+def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=None):
+    """Device time per step of the prepared run (tables resident in HBM).
+    tune: None to run the autotuner first (untimed), else a shape to apply."""
     t = B.Tracer(gpu=gpu, precision=precision)
     t.setup(root)
     t.set_frequencies(0, freqs)
     t.prepare()
+    if tune is None:
+        t.tuning = t.autotune(repeats=1)
+    else:
+        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"])
+        t.tuning = tune
     s = torch.cuda.ExternalStream(t.stream_ptr(), device=gpu)
     for _ in range(warmup):
         t.launch()
@@ -187,11 +193,13 @@ def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush):
     return t, times, stats, fields
 
 
-def time_e2e(B, torch, root, freqs, steps, gpu):
+def time_e2e(B, torch, root, freqs, steps, gpu, tune=None):
     """Same metric through the public C ABI with host buffers: setup reads the
     files, prepare uploads the tables, run, and every field copied back to
     pinned host memory, all inside the timed window."""
     t = B.Tracer(gpu=gpu, precision=B.PREC_MIXED)
+    if tune is not None:
+        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"])
     nf = len(freqs)
     t.setup(root)
     t.set_frequencies(0, freqs)
@@ -356,6 +364,7 @@ def main():
         ms_per_step = 1000.0 * total_s / args.steps
         value = aggregate_value(world, nf, args.steps, total_s)
         st = stats[-1]
+        tuning = t.tuning
         t.close()
         # ---- FP64 per-frequency tracer (the plain GPU trace)
         fp64 = None
@@ -370,7 +379,7 @@ def main():
                     "tl_rms_err_db_mixed_vs_fp64_max_over_freqs": max(errs),
                     "trace_ms": stats64[-1]["trace_ms"], "influence_ms": stats64[-1]["influence_ms"]}
         # ---- end to end through the C ABI with host buffers
-        e2e_times, h2d, d2h = time_e2e(B, torch, root, freqs, max(1, args.steps), local)
+        e2e_times, h2d, d2h = time_e2e(B, torch, root, freqs, max(1, args.steps), local, tune=tuning)
         e2e_s = max_over_ranks(sum(e2e_times) / 1000.0)
         e2e = {"value": world * nf * len(e2e_times) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
@@ -412,7 +421,10 @@ def main():
                                "frequencies share one trajectory",
                    "fields_per_step": nf, "rays": int(st["rays"]), "steps_traced": int(st["steps"]),
                    "contributions": int(st["evals"]), "l2": "flushed (256 MiB write) before every timed step",
-                   "parallelism": "replicas per GPU (one environment per rank)"},
+                   "parallelism": "replicas per GPU (one environment per rank)",
+                   "launch_shape": {"trace_block": tuning["trace_block"],
+                                    "influence_ctas_per_sm": tuning["influence_ctas_per_sm"],
+                                    "chosen_by": "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 3 * args.steps, "fp64_trace": fp64,
     }

@@ -263,6 +263,21 @@ int bhcb_nn_to_bf16(const float *x, void *y, int64_t n, void *stream);
 /* x = a * x + b over n floats */
 int bhcb_nn_affine(float *x, int64_t n, float a, float b, void *stream);
 
+/* Autotuner (no reference counterpart): times the prepared 2-D TL workload
+   with each candidate launch shape — trace CTAs of 32 or 64 threads (one ray
+   per thread), 2..12 persistent influence CTAs per SM — `repeats` runs each
+   (best of), keeps the fastest shape in the context and reports it. The
+   trace and the influence are timed apart (serial influence) during tuning.
+   bhcb_set_tuning applies a known shape (e.g. one saved from an earlier
+   process) without timing. The runs leave the context's outputs valid. */
+typedef struct bhcb_tuning {
+    int32_t trace_block;            /* threads per trace CTA */
+    int32_t influence_ctas_per_sm;  /* persistent influence CTAs per SM */
+    double trace_ms, influence_ms;  /* best times measured with the chosen shape */
+} bhcb_tuning;
+int bhcb_autotune(bhcb_ctx *ctx, int32_t repeats, bhcb_tuning *out);
+int bhcb_set_tuning(bhcb_ctx *ctx, const bhcb_tuning *tuning);
+
 /* Library version string. */
 const char *bhcb_version(void);
 
