@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from typing import Optional, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -133,6 +133,9 @@ SIGNATURES = [
                                C.c_void_p]),
     ("bhcb_nn_to_bf16", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     ("bhcb_nn_affine", C.c_int, [C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_void_p]),
+    ("bhcb_rays_shape", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("bhcb_copy_rays", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_size_t]),
     ("bhcb_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),
     ("bhcb_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("bhcb_version", C.c_char_p, []),
@@ -367,6 +370,25 @@ class Tracer:
         if rc != 0:
             raise BhcbError(rc, msg.value.decode(errors="replace"))
         return FieldGraph(self._lib, g)
+
+    def rays(self, env: int = 0, ifreq: int = 0) -> List[dict]:
+        """Ray trajectories of a ray run ('R') or the eigenrays of an eigen run
+        ('E'): one dict per ray with alpha (deg), ntop, nbot and rz (n x 2, m)."""
+        nr, npnt = C.c_int64(), C.c_int64()
+        self._check(self._lib.bhcb_rays_shape(self._h, env, ifreq, C.byref(nr), C.byref(npnt)))
+        n, m = nr.value, npnt.value
+        npts = np.zeros(max(n, 1), np.int32)
+        bnc = np.zeros(2 * max(n, 1), np.int32)
+        alpha = np.zeros(max(n, 1))
+        rz = np.zeros((max(m, 1), 2))
+        self._check(self._lib.bhcb_copy_rays(self._h, env, ifreq, npts.ctypes.data, bnc.ctypes.data,
+                                             alpha.ctypes.data, rz.ctypes.data, rz.nbytes))
+        out, o = [], 0
+        for i in range(n):
+            out.append({"alpha": float(alpha[i]), "ntop": int(bnc[2 * i]), "nbot": int(bnc[2 * i + 1]),
+                        "rz": rz[o:o + npts[i]].copy()})
+            o += int(npts[i])
+        return out
 
     def autotune(self, repeats: int = 2) -> dict:
         """Time the prepared TL workload with each launch shape; keep the fastest."""

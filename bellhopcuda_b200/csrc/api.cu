@@ -43,6 +43,8 @@ cudaError_t radix_sort_pairs(uint64_t *, uint32_t *, uint64_t *, uint32_t *, uns
 cudaError_t launch_arr_replay(const uint64_t *, const uint32_t *, const ArrCand *, unsigned long long,
                               const GroupDev *, int, const double *, long long, int, int, int, int32_t *,
                               ArrivalRec *, int, cudaStream_t, bool);
+cudaError_t launch_rays(const GroupDev *, int, const long long *, const int *, int, const long long *, double2 *, int *,
+                        int *, RunCounters *, bool, int, cudaStream_t);
 cudaError_t launch_eigen_emit(const uint32_t *, const ArrCand *, unsigned long long, EigenHitRec *, int32_t *, int,
                               const uint64_t *, int, cudaStream_t);
 } // namespace bhcb
@@ -66,7 +68,18 @@ struct Field {
     int nsz, nrzp, nrr;
 };
 
-enum { MODE_TL = 0, MODE_ARR = 1, MODE_EIGEN = 2 };
+// Ray trajectories of one field: every ray of a RunType 'R' run, or the rays
+// of its eigen hits re-traced up to the hit; points (r, z) in m, host copies
+struct RaySet {
+    bool valid = false;
+    std::vector<long long> jobs;
+    std::vector<int> limits, npts, bnc;   // bnc: top, bottom bounces of the last point
+    std::vector<long long> off;
+    std::vector<double> alpha_deg;        // take-off angle (SrcDeclAngle)
+    std::vector<double> rz;               // 2 doubles per point
+};
+
+enum { MODE_TL = 0, MODE_ARR = 1, MODE_EIGEN = 2, MODE_RAY = 3 };
 constexpr unsigned long long MAXN_STEPS_HOST = 100000;   // steps per ray (include/bhc/structs.hpp:66)
 
 int run_mode_of(char r0)
@@ -74,8 +87,9 @@ int run_mode_of(char r0)
     if(r0 == 'A' || r0 == 'a') return MODE_ARR;
     if(r0 == 'E') return MODE_EIGEN;
     if(r0 == 'C' || r0 == 'S' || r0 == 'I') return MODE_TL;
+    if(r0 == 'R') return MODE_RAY;
     throw std::runtime_error(std::string("RunType '") + r0 + "' is not supported by this entry point "
-                             "(TL 'C'/'S'/'I', arrivals 'A'/'a', eigen hits 'E')");
+                             "(TL 'C'/'S'/'I', arrivals 'A'/'a', eigen hits 'E', rays 'R')");
 }
 
 int bits_for(unsigned long long n)   // bits to hold values 0..n-1 (at least 1)
@@ -133,6 +147,7 @@ struct bhcb_ctx {
     const uint32_t *sorted_vals = nullptr;
     std::vector<EigenHitRec> hits_h;      // eigen hits of the last run, in reference order
     std::vector<int64_t> hit_begin;       // per field: first hit (size nfields + 1)
+    std::vector<RaySet> rays;             // per field: trajectories (ray runs, eigen re-traces)
     RunCounters last{};
     bhcb_stats stats{};
     std::string last_error;
@@ -386,6 +401,11 @@ void do_prepare(bhcb_ctx *c)
     c->acc.ensure(abytes);
     c->out.ensure(fbytes);
     c->counters.ensure(sizeof(RunCounters) + 64);
+    c->rays.assign(c->fields.size(), RaySet{});
+    if(c->mode == MODE_RAY) {   // trajectories only: no segment records
+        c->prepared = true;
+        return;
+    }
     // segment buffer: grows on overflow
     size_t rec = seg_record_bytes(fp64);
     size_t budget = c->max_memory > 2 * fbytes + abytes ? c->max_memory - 2 * fbytes - abytes : 0;
@@ -525,6 +545,160 @@ int do_sync(bhcb_ctx *c)
     c->err_bits = c->last.err_bits;
     c->warn_bits = c->last.warn_bits;
     return 0;
+}
+
+// index of the trace group that produces field fi
+int group_of_field(const bhcb_ctx *c, int fi)
+{
+    for(size_t g = 0; g < c->groups_h.size(); ++g) {
+        const GroupDev &G = c->groups_h[g];
+        if(fi >= G.field_index && fi < G.field_index + G.nfreq) return (int)g;
+    }
+    throw std::runtime_error("field has no trace group");
+}
+
+// Trajectories of R.jobs (limits as for the ray kernel): a count pass sizes
+// the point buffer exactly, a second pass of the same deterministic trace
+// writes the points; both passes read the context's prepared tables.
+void trace_rays(bhcb_ctx *c, RaySet &R)
+{
+    const int n = (int)R.jobs.size();
+    R.npts.assign(n, 0);
+    R.bnc.assign(2 * (size_t)n, 0);
+    R.off.assign(n, 0);
+    R.rz.clear();
+    R.valid = true;
+    if(n == 0) return;
+    DevBuf jobs_d, lim_d, npts_d, bnc_d, off_d, pts_d;
+    jobs_d.ensure(n * sizeof(long long));
+    lim_d.ensure(n * sizeof(int));
+    npts_d.ensure(n * sizeof(int));
+    bnc_d.ensure(2 * (size_t)n * sizeof(int));
+    off_d.ensure(n * sizeof(long long));
+    auto release = [&]() { for(DevBuf *b : {&jobs_d, &lim_d, &npts_d, &bnc_d, &off_d, &pts_d}) b->release(); };
+    try {
+        CK(cudaMemcpyAsync(jobs_d.p, R.jobs.data(), n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(lim_d.p, R.limits.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->counters.p, 0, sizeof(RunCounters), c->stream));
+        RunCounters *ctr = (RunCounters *)c->counters.p;
+        const GroupDev *G = (const GroupDev *)c->groups_d.p;
+        const int ng = (int)c->groups_h.size();
+        CK(launch_rays(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, nullptr, nullptr,
+                       (int *)npts_d.p, (int *)bnc_d.p, ctr, true, c->sm_count, c->stream));
+        CK(cudaMemcpyAsync(R.npts.data(), npts_d.p, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(R.bnc.data(), bnc_d.p, 2 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        RunCounters rc{};
+        CK(cudaMemcpyAsync(&rc, ctr, sizeof rc, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if(rc.err_bits) {
+            c->err_bits = rc.err_bits;
+            throw std::runtime_error("tracer error while tracing rays");
+        }
+        long long tot = 0;
+        for(int i = 0; i < n; ++i) {
+            R.off[i] = tot;
+            tot += R.npts[i];
+        }
+        if((size_t)tot * sizeof(double2) > c->max_memory) throw MemError("ray points exceed max_memory");
+        pts_d.ensure(std::max<long long>(tot, 1) * sizeof(double2));
+        CK(cudaMemcpyAsync(off_d.p, R.off.data(), n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(launch_rays(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, (const long long *)off_d.p,
+                       (double2 *)pts_d.p, (int *)npts_d.p, (int *)bnc_d.p, ctr, false, c->sm_count, c->stream));
+        R.rz.resize(2 * (size_t)tot);
+        if(tot)
+            CK(cudaMemcpyAsync(R.rz.data(), pts_d.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->warn_bits |= rc.warn_bits;
+    } catch(...) {
+        release();
+        R.valid = false;
+        throw;
+    }
+    release();
+}
+
+// job index and take-off angle of (isz, ialpha) of trace group G
+long long job_of(const bhcb_ctx *c, int g, int isz, int ialpha, double *alpha_deg)
+{
+    const GroupDev &G = c->groups_h[g];
+    const Field &F = c->fields[G.field_index];
+    const EnvTables &T = c->envs[F.env].tables[F.ifreq];
+    const int nal = T.isingle > 0 ? 1 : (int)T.alpha.size();
+    const int local = isz * nal + (T.isingle > 0 ? 0 : ialpha);
+    if(alpha_deg) *alpha_deg = (180.0 / 3.14159265358979323846) * T.alpha[ialpha];
+    return G.job_base + local;
+}
+
+// RunType 'R': every ray of every field (RunRayMode, src/mode/ray.cpp:163-198)
+void run_rays(bhcb_ctx *c)
+{
+    for(size_t fi = 0; fi < c->fields.size(); ++fi) {
+        const int g = group_of_field(c, (int)fi);
+        const GroupDev &G = c->groups_h[g];
+        const Field &F = c->fields[fi];
+        const EnvTables &T = c->envs[F.env].tables[F.ifreq];
+        const int nal = T.isingle > 0 ? 1 : (int)T.alpha.size();
+        RaySet &R = c->rays[fi];
+        R = RaySet{};
+        for(int local = 0; local < G.njobs; ++local) {
+            const int ialpha = T.isingle > 0 ? T.isingle - 1 : local % nal;
+            R.jobs.push_back(G.job_base + local);
+            R.limits.push_back(-1);
+            R.alpha_deg.push_back((180.0 / 3.14159265358979323846) * T.alpha[ialpha]);
+        }
+        trace_rays(c, R);
+    }
+    c->stats = bhcb_stats{};
+    c->stats.rays = (uint64_t)c->njobs;
+    c->stats.fields = (int32_t)c->fields.size();
+    c->stats.groups = (int32_t)c->groups_h.size();
+}
+
+// eigenray re-trace of field fi's hits (EigenModePostWorker, src/mode/eigen.cpp:24-45)
+RaySet &eigen_rays(bhcb_ctx *c, int fi)
+{
+    RaySet &R = c->rays[fi];
+    if(R.valid) return R;
+    if(c->hit_begin.size() != c->fields.size() + 1) throw StateError("no hits: run first");
+    const int g = group_of_field(c, fi);
+    R = RaySet{};
+    for(int64_t k = c->hit_begin[fi]; k < c->hit_begin[fi + 1]; ++k) {
+        const EigenHitRec &h = c->hits_h[k];
+        double a = 0.0;
+        R.jobs.push_back(job_of(c, g, h.isz, h.ialpha, &a));
+        R.limits.push_back(h.is);
+        R.alpha_deg.push_back(a);
+    }
+    trace_rays(c, R);
+    return R;
+}
+
+// .ray file (OpenRAYFile / WriteRay, src/mode/ray.hpp:176-247), 2-D, list-directed text
+void write_rays(const bhcb_ctx *c, const Field &F, const RaySet &R, const std::string &path)
+{
+    const EnvSlot &S = c->envs[F.env];
+    const EnvTables &T = S.tables[F.ifreq];
+    std::ofstream o(path);
+    if(!o.good()) throw std::runtime_error("cannot open " + path);
+    char b[128];
+    o << "'" << S.in.title << "'\n";
+    snprintf(b, sizeof b, "%.17g\n", S.freqs[F.ifreq]);
+    o << b;
+    o << 1 << " " << 1 << " " << T.sz.size() << "\n";
+    o << T.alpha.size() << " " << 1 << "\n";
+    snprintf(b, sizeof b, "%.17g\n%.17g\n", S.in.ssp_z.empty() ? 0.0 : S.in.ssp_z[0], S.in.bot_depth);
+    o << b;
+    o << "'rz'\n";
+    for(size_t i = 0; i < R.jobs.size(); ++i) {
+        if(R.npts[i] <= 0) continue;
+        snprintf(b, sizeof b, "%.17g\n", R.alpha_deg[i]);
+        o << b;
+        o << R.npts[i] << " " << R.bnc[2 * i] << " " << R.bnc[2 * i + 1] << "\n";
+        for(int k = 0; k < R.npts[i]; ++k) {
+            snprintf(b, sizeof b, "%.17g %.17g\n", R.rz[2 * (R.off[i] + k)], R.rz[2 * (R.off[i] + k) + 1]);
+            o << b;
+        }
+    }
 }
 
 // Arrivals / eigen hits of the traced segments: count, gather, order, replay.
@@ -944,6 +1118,12 @@ int bhcb_launch(bhcb_ctx *c)
             c->r3_status = run3_checked(c);
             return BHCB_OK;
         }
+        if(!c->prepared) do_prepare(c);
+        if(c->mode == MODE_RAY) {   // ray runs complete inside the launch
+            run_rays(c);
+            return BHCB_OK;
+        }
+        if(c->mode == MODE_EIGEN) c->rays.assign(c->fields.size(), RaySet{});
         do_launch(c, c->overlap);
         return BHCB_OK;
     });
@@ -953,6 +1133,7 @@ int bhcb_sync(bhcb_ctx *c)
 {
     return guarded(c, [&]() -> int {
         if(c->is3d()) return c->r3_status;
+        if(c->mode == MODE_RAY) return BHCB_OK;
         do_sync(c);
         if(c->last.err_bits) {
             char b[96];
@@ -969,6 +1150,11 @@ int bhcb_run(bhcb_ctx *c)
     return guarded(c, [&]() -> int {
         if(c->is3d()) return c->r3_status = run3_checked(c);
         if(!c->prepared) do_prepare(c);
+        if(c->mode == MODE_RAY) {
+            run_rays(c);
+            return BHCB_OK;
+        }
+        if(c->mode == MODE_EIGEN) c->rays.assign(c->fields.size(), RaySet{});
         return run_checked(c);
     });
 }
@@ -1127,8 +1313,14 @@ int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
             run3_writeout(c->r3, env, root, c->stream);
             return BHCB_OK;
         }
-        if(c->mode == MODE_EIGEN)
-            throw StateError("eigenray .ray output (re-trace of the hit rays) is not built; use bhcb_eigen_hits");
+        if(c->mode == MODE_EIGEN || c->mode == MODE_RAY) {   // .ray: traced rays or re-traced eigenrays
+            const Field *F = find_field(c, env, ifreq);
+            const int fi = (int)(F - c->fields.data());
+            const RaySet &R = c->mode == MODE_EIGEN ? eigen_rays(c, fi) : c->rays[fi];
+            if(!R.valid) throw StateError("no rays: run first");
+            write_rays(c, *F, R, std::string(root) + ".ray");
+            return BHCB_OK;
+        }
         if(c->mode == MODE_ARR) {
             const Field *F = find_field(c, env, ifreq);
             const EnvSlot &S = c->envs[env];
@@ -1227,6 +1419,40 @@ int bhcb_grid3d(bhcb_ctx *c, int32_t env, double *sx, double *sy, float *sz, dou
         if(rr) std::memcpy(rr, vrr.data(), vrr.size() * sizeof(double));
         if(rz) std::memcpy(rz, vrz.data(), vrz.size() * sizeof(float));
         if(theta) std::memcpy(theta, vth.data(), vth.size() * sizeof(double));
+        return BHCB_OK;
+    });
+}
+
+int bhcb_rays_shape(bhcb_ctx *c, int32_t env, int32_t ifreq, int64_t *nrays, int64_t *npoints)
+{
+    return guarded(c, [&]() -> int {
+        if(c->is3d() || (c->mode != MODE_RAY && c->mode != MODE_EIGEN))
+            throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E')");
+        const Field *F = find_field(c, env, ifreq);
+        const int fi = (int)(F - c->fields.data());
+        const RaySet &R = c->mode == MODE_EIGEN ? eigen_rays(c, fi) : c->rays[fi];
+        if(!R.valid) throw StateError("no rays: run first");
+        if(nrays) *nrays = (int64_t)R.jobs.size();
+        if(npoints) *npoints = (int64_t)(R.rz.size() / 2);
+        return BHCB_OK;
+    });
+}
+
+int bhcb_copy_rays(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *npts, int32_t *bounces, double *alpha_deg,
+                   double *rz, size_t rz_bytes)
+{
+    return guarded(c, [&]() -> int {
+        if(c->is3d() || (c->mode != MODE_RAY && c->mode != MODE_EIGEN))
+            throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E')");
+        const Field *F = find_field(c, env, ifreq);
+        const int fi = (int)(F - c->fields.data());
+        const RaySet &R = c->mode == MODE_EIGEN ? eigen_rays(c, fi) : c->rays[fi];
+        if(!R.valid) throw StateError("no rays: run first");
+        if(rz && rz_bytes < R.rz.size() * sizeof(double)) throw std::invalid_argument("rz buffer too small");
+        if(npts) std::memcpy(npts, R.npts.data(), R.npts.size() * sizeof(int32_t));
+        if(bounces) std::memcpy(bounces, R.bnc.data(), R.bnc.size() * sizeof(int32_t));
+        if(alpha_deg) std::memcpy(alpha_deg, R.alpha_deg.data(), R.alpha_deg.size() * sizeof(double));
+        if(rz && !R.rz.empty()) std::memcpy(rz, R.rz.data(), R.rz.size() * sizeof(double));
         return BHCB_OK;
     });
 }

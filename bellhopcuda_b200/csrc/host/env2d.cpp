@@ -622,10 +622,10 @@ EnvTables preprocess(const EnvInput &in, double freq)
     std::memcpy(t.run_type, in.run_type, 7);
     // RunType validation / normalisation (src/module/runtype.hpp:53-78)
     switch(t.run_type[0]) {
-    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'V': case 'v': break;
-    case 'R': env_error("ray-trace runs ('R') are not a field mode");
+    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'V': case 'v': case 'R': break;
     default: env_error("unknown RunType");
     }
+    const bool ray_run = t.run_type[0] == 'R';
     switch(t.run_type[1]) {
     case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
     default: t.run_type[1] = 'G';
@@ -637,9 +637,10 @@ EnvTables preprocess(const EnvInput &in, double freq)
     t.beam_type[0] = t.run_type[1];
     t.beam_type[3] = t.run_type[6];
     char bt = t.beam_type[0];
-    if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
+    // ray runs trace geometric rays whatever the beam type (src/mode/ray.cpp:44-86)
+    if(!ray_run && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
         env_error(std::string("beam type '") + bt + "' is not supported by this build");
-    if(t.beam_type[3] == 'S') env_error("beam shift ('S') is not supported by this build");
+    if(!ray_run && t.beam_type[3] == 'S') env_error("beam shift ('S') is not supported by this build");
 
     char st = in.top_opt[0];
     switch(st) {
@@ -702,11 +703,15 @@ EnvTables preprocess(const EnvInput &in, double freq)
     // angles (module/rayangles.hpp:66-190)
     int na = in.nalpha;
     std::vector<double> al = in.alpha_deg;
-    if(na == 0) {
+    if(na == 0) {   // EstimateNumAngles (src/module/rayangles.hpp:212-238)
         double c0 = FLT(1500.0);
-        na = std::max((int)(FLT(0.3) * rr[in.nrr - 1] * freq / c0), 300);
-        double dth = std::atan((bot_depth - top_depth) / (FLT(10.0) * rr[in.nrr - 1]));
-        na = std::max((int)(kPi / dth), na);
+        if(ray_run) {
+            na = 50;
+        } else {
+            na = std::max((int)(FLT(0.3) * rr[in.nrr - 1] * freq / c0), 300);
+            double dth = std::atan((bot_depth - top_depth) / (FLT(10.0) * rr[in.nrr - 1]));
+            na = std::max((int)(kPi / dth), na);
+        }
         std::vector<double> a(std::max(3, na), 0.0);
         a[0] = al[0];
         a[1] = al[1];

@@ -72,6 +72,114 @@ template<typename R> __device__ __forceinline__ void close_block(SegRec<R> *segs
     publish_block(blk_state, cur.end);
 }
 
+// Per-ray state between steps of the 2-D ray loop.
+template<typename R> struct RayState2 {
+    RayPt<R> p0;
+    BdState top, bot;
+    HsDev htop, hbot;
+    SegState iSeg;
+    double dBegTop, dBegBot;
+    double alpha;
+    R c;
+};
+
+// RayInit (src/trace.hpp:76-266), 2-D: false when the source is on or outside
+// the boundaries (the ray is not traced)
+template<typename R> __device__ __forceinline__ bool ray_init2d(const EnvDev &e, int ialpha, int isz,
+                                                                RayState2<R> &st, RunCounters *ctr)
+{
+    st.iSeg = SegState{0, 0};
+    const double alpha = e.alpha[ialpha];
+    st.alpha = alpha;
+    const double SrcDecl = (180.0 / BHCB_PI) * alpha;
+    const V2<double> xs = mk2(0.0, (double)e.sz[isz]);
+    const V2<R> tinit = mk2((R)cos(alpha), (R)sin(alpha));
+    SSPOut<R> o;
+    eval_ssp(xs, tinit, o, e, st.iSeg, ctr);
+    const R c = o.c;
+    st.c = c;
+    if(e.coherent && ialpha == 0) {
+        double dopt = sqrt((double)c / (FLTD(6.0) * e.freq0 * e.rr[e.nrr - 1]));
+        int nopt = 2 + (int)((e.alpha[e.nalpha - 1] - e.alpha[0]) / dopt);
+        if(e.nalpha < nopt) run_warn(ctr, WARN_TOO_FEW_BEAMS);
+    }
+    int ibp = min(bsearch_leq2(e.sbp, e.nsbp, SrcDecl), e.nsbp - 2);
+    double s = (SrcDecl - e.sbp[2 * ibp]) / (e.sbp[2 * (ibp + 1)] - e.sbp[2 * ibp]);
+    float amp0 = (float)((FLTD(1.0) - s) * e.sbp[2 * ibp + 1] + s * e.sbp[2 * (ibp + 1) + 1]);
+    if(e.run0 == 'S') {
+        float om = (float)(FLTD(2.0) * BHCB_PI * e.freq0);
+        amp0 = (float)(amp0 * ((double)sqrtf(2.0f) * fabs(sin(om / (double)c * xs.y * sin(alpha)))));
+    }
+    RayPt<R> &p0 = st.p0;
+    p0.x = xs;
+    p0.c = c;
+    p0.t = div2(tinit, c);
+    p0.taur = 0.0;
+    p0.taui = 0.0;
+    p0.Amp = (R)amp0;
+    p0.Phase = (R)0;
+    p0.ntop = p0.nbot = 0;
+    p0.p = mk2((R)1, (R)0);
+    p0.q = e.q_zero_init ? mk2((R)0, (R)0) : mk2((R)0, (R)1);
+    st.htop = e.top;
+    st.hbot = e.bot;
+    st.top.Iseg = st.bot.Iseg = 0;
+    st.top.lmin = st.top.lmax = st.bot.lmin = st.bot.lmax = 0.0;
+    get_bdry_seg(xs, (double)p0.t.x, st.top, e.btop, e.ntop, e.top_long, st.htop, true, true, ctr);
+    get_bdry_seg(xs, (double)p0.t.x, st.bot, e.bbot, e.nbot, e.bot_long, st.hbot, false, true, ctr);
+    distances(xs, st.top, st.bot, st.dBegTop, st.dBegBot);
+    if(st.dBegTop <= 0.0 || st.dBegBot <= 0.0) {
+        run_warn(ctr, WARN_SOURCE_OUTSIDE_BOUNDARIES);
+        return false;
+    }
+    return true;
+}
+
+// RayUpdate (src/trace.hpp:274-381), 2-D: one step from st.p0 to p1 and, on a
+// boundary hit, the reflected point p2; returns whether p2 was produced
+template<typename R> __device__ __forceinline__ bool ray_update2d(RayState2<R> &st, RayPt<R> &p1, RayPt<R> &p2,
+                                                                  int &small, double &dEndTop, double &dEndBot,
+                                                                  const EnvDev &e, RunCounters *ctr)
+{
+    bool tr = false, br = false;
+    step2d(st.p0, p1, st.top, st.bot, e, st.iSeg, small, tr, br, ctr);
+    get_bdry_seg(p1.x, (double)p1.t.x, st.top, e.btop, e.ntop, e.top_long, st.htop, true, false, ctr);
+    get_bdry_seg(p1.x, (double)p1.t.x, st.bot, e.bbot, e.nbot, e.bot_long, st.hbot, false, false, ctr);
+    distances(p1.x, st.top, st.bot, dEndTop, dEndBot);
+    const bool two = tr || br;
+    if(two) {
+        const BdryPtDev *bd = tr ? e.btop : e.bbot;
+        const BdState &bs = tr ? st.top : st.bot;
+        const BdryPtDev &b0 = bd[bs.Iseg];
+        const BdryPtDev &b1 = bd[bs.Iseg + 1];
+        V2<R> nI, tI;
+        if(tr ? e.top_curv : e.bot_curv) {
+            double sss = dot2(sub2(p1.x, bs.x), mk2(b0.t[0], b0.t[1])) / b0.Len;
+            nI = mk2((R)((FLTD(1.0) - sss) * b0.Noden[0] + sss * b1.Noden[0]),
+                     (R)((FLTD(1.0) - sss) * b0.Noden[1] + sss * b1.Noden[1]));
+            tI = mk2((R)((FLTD(1.0) - sss) * b0.Nodet[0] + sss * b1.Nodet[0]),
+                     (R)((FLTD(1.0) - sss) * b0.Nodet[1] + sss * b1.Nodet[1]));
+        } else {
+            nI = mk2((R)b0.n[0], (R)b0.n[1]);
+            tI = mk2((R)b0.t[0], (R)b0.t[1]);
+        }
+        reflect2d(p1, p2, tr ? st.htop : st.hbot, tr, tI, nI, (R)b0.kappa, e, st.iSeg, ctr);
+        distances(p2.x, st.top, st.bot, dEndTop, dEndBot);
+    }
+    return two;
+}
+
+// RayTerminate's stop conditions (src/trace.hpp:391-477), 2-D
+template<typename R> __device__ __forceinline__ bool ray_stops2d(const RayState2<R> &st, double dEndTop,
+                                                                 double dEndBot, const EnvDev &e)
+{
+    const RayPt<R> &p0 = st.p0;
+    const bool leftbox = fabs(p0.x.x) >= e.box_x || fabs(p0.x.y) >= e.box_y;
+    const bool escaped = (st.dBegTop < 0.0 && dEndTop < 0.0) || (st.dBegBot < 0.0 && dEndBot < 0.0);
+    const bool lost = (double)p0.Amp < FLTD(0.005);
+    return leftbox || lost || escaped;
+}
+
 // R: ray state; RecR: segment record (float for the mixed kernel's FP32 influence).
 template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_kernel(
     const GroupDev *__restrict__ groups, int ngroups, long long njobs, SegRec<RecR> *segs,
@@ -89,49 +197,13 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
         if(isz >= e.nsz) { run_error(ctr, ERR_RAYINIT); continue; }
 
         // ---- RayInit (src/trace.hpp:76-266)
-        SegState iSeg{0, 0};
-        double alpha = e.alpha[ialpha];
-        double SrcDecl = (180.0 / BHCB_PI) * alpha;
-        V2<double> xs = mk2(0.0, (double)e.sz[isz]);
-        V2<R> tinit = mk2((R)cos(alpha), (R)sin(alpha));
-        SSPOut<R> o;
-        eval_ssp(xs, tinit, o, e, iSeg, ctr);
-        R c = o.c;
-        if(e.coherent && ialpha == 0) {
-            double dopt = sqrt((double)c / (FLTD(6.0) * e.freq0 * e.rr[e.nrr - 1]));
-            int nopt = 2 + (int)((e.alpha[e.nalpha - 1] - e.alpha[0]) / dopt);
-            if(e.nalpha < nopt) run_warn(ctr, WARN_TOO_FEW_BEAMS);
-        }
-        int ibp = min(bsearch_leq2(e.sbp, e.nsbp, SrcDecl), e.nsbp - 2);
-        double s = (SrcDecl - e.sbp[2 * ibp]) / (e.sbp[2 * (ibp + 1)] - e.sbp[2 * ibp]);
-        float amp0 = (float)((FLTD(1.0) - s) * e.sbp[2 * ibp + 1] + s * e.sbp[2 * (ibp + 1) + 1]);
-        if(e.run0 == 'S') {
-            float om = (float)(FLTD(2.0) * BHCB_PI * e.freq0);
-            amp0 = (float)(amp0 * ((double)sqrtf(2.0f) * fabs(sin(om / (double)c * xs.y * sin(alpha)))));
-        }
-        RayPt<R> p0, p1, p2;
-        p0.x = xs;
-        p0.c = c;
-        p0.t = div2(tinit, c);
-        p0.taur = 0.0;
-        p0.taui = 0.0;
-        p0.Amp = (R)amp0;
-        p0.Phase = (R)0;
-        p0.ntop = p0.nbot = 0;
-        p0.p = mk2((R)1, (R)0);
-        p0.q = e.q_zero_init ? mk2((R)0, (R)0) : mk2((R)0, (R)1);
-        HsDev htop = e.top, hbot = e.bot;
-        BdState top, bot;
-        top.Iseg = bot.Iseg = 0;
-        top.lmin = top.lmax = bot.lmin = bot.lmax = 0.0;
-        get_bdry_seg(xs, (double)p0.t.x, top, e.btop, e.ntop, e.top_long, htop, true, true, ctr);
-        get_bdry_seg(xs, (double)p0.t.x, bot, e.bbot, e.nbot, e.bot_long, hbot, false, true, ctr);
-        double dBegTop, dBegBot, dEndTop, dEndBot;
-        distances(xs, top, bot, dBegTop, dBegBot);
-        if(dBegTop <= 0.0 || dBegBot <= 0.0) {
-            run_warn(ctr, WARN_SOURCE_OUTSIDE_BOUNDARIES);
-            continue;
-        }
+        RayState2<R> st;
+        if(!ray_init2d(e, ialpha, isz, st, ctr)) continue;
+        RayPt<R> &p0 = st.p0;
+        RayPt<R> p1, p2;
+        const double alpha = st.alpha;
+        const R c = st.c;
+        double dEndTop, dEndBot;
         // ---- Init_Influence (src/influence.hpp:525-644), Cartesian geometric
         R ratio1 = (R)sqrt(fabs(cos(alpha)));
         if(e.line_source) ratio1 = (R)1;
@@ -151,32 +223,8 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
         for(;;) {
             // another ray's error stops the run (src/trace.hpp:559); polled every 32 steps
             if((nsteps & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) break;
-            bool tr = false, br = false;
-            step2d(p0, p1, top, bot, e, iSeg, small, tr, br, ctr);
+            const bool two = ray_update2d(st, p1, p2, small, dEndTop, dEndBot, e, ctr);
             ++nsteps;
-            get_bdry_seg(p1.x, (double)p1.t.x, top, e.btop, e.ntop, e.top_long, htop, true, false, ctr);
-            get_bdry_seg(p1.x, (double)p1.t.x, bot, e.bbot, e.nbot, e.bot_long, hbot, false, false, ctr);
-            distances(p1.x, top, bot, dEndTop, dEndBot);
-            bool two = tr || br;
-            if(two) {
-                const BdryPtDev *bd = tr ? e.btop : e.bbot;
-                const BdState &bs = tr ? top : bot;
-                const BdryPtDev &b0 = bd[bs.Iseg];
-                const BdryPtDev &b1 = bd[bs.Iseg + 1];
-                V2<R> nI, tI;
-                if(tr ? e.top_curv : e.bot_curv) {
-                    double sss = dot2(sub2(p1.x, bs.x), mk2(b0.t[0], b0.t[1])) / b0.Len;
-                    nI = mk2((R)((FLTD(1.0) - sss) * b0.Noden[0] + sss * b1.Noden[0]),
-                             (R)((FLTD(1.0) - sss) * b0.Noden[1] + sss * b1.Noden[1]));
-                    tI = mk2((R)((FLTD(1.0) - sss) * b0.Nodet[0] + sss * b1.Nodet[0]),
-                             (R)((FLTD(1.0) - sss) * b0.Nodet[1] + sss * b1.Nodet[1]));
-                } else {
-                    nI = mk2((R)b0.n[0], (R)b0.n[1]);
-                    tI = mk2((R)b0.t[0], (R)b0.t[1]);
-                }
-                reflect2d(p1, p2, tr ? htop : hbot, tr, tI, nI, (R)b0.kappa, e, iSeg, ctr);
-                distances(p2.x, top, bot, dEndTop, dEndBot);
-            }
             SegRec<RecR> rec;
             if(infl_prologue(p0, p1, inf, e, rcp_q0, ratio1, (int)job, is, rec))
                 emit_seg(rec, segs, cap, ctr, cur, overflow, blk_state);
@@ -195,19 +243,104 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
                 break;
             }
             // ---- RayTerminate (src/trace.hpp:391-477), 2-D
-            bool leftbox = fabs(p0.x.x) >= e.box_x || fabs(p0.x.y) >= e.box_y;
-            bool escaped = (dBegTop < 0.0 && dEndTop < 0.0) || (dBegBot < 0.0 && dEndBot < 0.0);
-            bool lost = (double)p0.Amp < FLTD(0.005);
-            if(leftbox || lost || escaped) break;
+            if(ray_stops2d(st, dEndTop, dEndBot, e)) break;
             if(is >= MAXN_STEPS - 3) {
                 run_warn(ctr, WARN_ONERAY_OUTOFMEMORY);
                 break;
             }
-            dBegTop = dEndTop;
-            dBegBot = dEndBot;
+            st.dBegTop = dEndTop;
+            st.dBegBot = dEndBot;
         }
         close_block(segs, cur, blk_state);
         atomicAdd(&ctr->nsteps, nsteps);
+    }
+}
+
+// Ray trajectories (MainRayMode, src/trace.hpp:485-519) of listed rays: every
+// ray of a RunType 'R' run, or the rays of eigen hits re-traced up to the hit
+// (EigenModePostWorker, src/mode/eigen.cpp:24-45). One ray per thread, FP64.
+// limits[i] < 0: no limit; else the ray stops two points after step limits[i].
+// COUNT: npts[i] = number of points, bounce counts of the last point in
+// bnc[2i], bnc[2i + 1]; otherwise the points (r, z) go to pts + off[i].
+template<bool COUNT>
+__global__ void __launch_bounds__(64) ray_kernel(const GroupDev *__restrict__ groups, int ngroups,
+                                                 const long long *__restrict__ jobs, const int *__restrict__ limits,
+                                                 int nitems, const long long *__restrict__ off, double2 *pts,
+                                                 int *npts, int *bnc, RunCounters *ctr)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += gridDim.x * blockDim.x) {
+        const long long job = jobs[i];
+        const GroupDev &G = groups[find_group(groups, ngroups, job)];
+        const EnvDev &e = *G.env;
+        const int local = (int)(job - G.job_base);
+        const int nalpha_eff = e.isingle > 0 ? 1 : e.nalpha;
+        const int ialpha = e.isingle > 0 ? e.isingle - 1 : local % nalpha_eff;
+        const int isz = local / nalpha_eff;
+        const int cap = COUNT ? 0x7fffffff : npts[i];   // points the count pass found
+        const long long base = COUNT ? 0 : off[i];
+        auto put = [&](int idx, const RayPt<double> &p) {
+            if(!COUNT && idx < cap) pts[base + idx] = make_double2(p.x.x, p.x.y);
+        };
+        if(isz >= e.nsz) {
+            run_error(ctr, ERR_RAYINIT);
+            if(COUNT) { npts[i] = 0; bnc[2 * i] = bnc[2 * i + 1] = 0; }
+            continue;
+        }
+        RayState2<double> st;
+        int nsteps = -1;
+        int last_top = 0, last_bot = 0;
+        if(!ray_init2d(e, ialpha, isz, st, ctr)) {
+            put(0, st.p0);
+            nsteps = 1;
+        } else {
+            put(0, st.p0);
+            const int limit = limits[i];
+            int is = 0, small = 0;
+            int prev_top = 0, prev_bot = 0;   // bounces of the point before st.p0
+            RayPt<double> p1, p2;
+            double dEndTop, dEndBot;
+            for(;;) {
+                if((is & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) {
+                    nsteps = is + 1;
+                    last_top = st.p0.ntop;
+                    last_bot = st.p0.nbot;
+                    break;
+                }
+                const bool two = ray_update2d(st, p1, p2, small, dEndTop, dEndBot, e, ctr);
+                put(is + 1, p1);
+                if(two) put(is + 2, p2);
+                if(limit >= 0 && is >= limit) {
+                    nsteps = is + 2;
+                    last_top = p1.ntop;
+                    last_bot = p1.nbot;
+                    break;
+                }
+                prev_top = two ? p1.ntop : st.p0.ntop;
+                prev_bot = two ? p1.nbot : st.p0.nbot;
+                is += two ? 2 : 1;
+                st.p0 = two ? p2 : p1;
+                if(ray_stops2d(st, dEndTop, dEndBot, e)) {
+                    nsteps = is + 1;
+                    last_top = st.p0.ntop;
+                    last_bot = st.p0.nbot;
+                    break;
+                }
+                if(is >= MAXN_STEPS - 3) {
+                    run_warn(ctr, WARN_ONERAY_OUTOFMEMORY);
+                    nsteps = is;
+                    last_top = prev_top;
+                    last_bot = prev_bot;
+                    break;
+                }
+                st.dBegTop = dEndTop;
+                st.dBegBot = dEndBot;
+            }
+        }
+        if(COUNT) {
+            npts[i] = nsteps;
+            bnc[2 * i] = last_top;
+            bnc[2 * i + 1] = last_bot;
+        }
     }
 }
 
@@ -541,5 +674,19 @@ template cudaError_t launch_influence<double>(const void *, unsigned long long, 
                                               cudaStream_t);
 
 size_t seg_record_bytes(bool fp64) { return fp64 ? sizeof(SegRec<double>) : sizeof(SegRec<float>); }
+
+cudaError_t launch_rays(const GroupDev *groups, int ngroups, const long long *jobs, const int *limits, int nitems,
+                        const long long *off, double2 *pts, int *npts, int *bnc, RunCounters *ctr, bool count,
+                        int sm_count, cudaStream_t st)
+{
+    if(nitems <= 0) return cudaSuccess;
+    int grid = (nitems + 63) / 64;
+    if(grid > sm_count * 16) grid = sm_count * 16;
+    if(count)
+        ray_kernel<true><<<grid, 64, 0, st>>>(groups, ngroups, jobs, limits, nitems, off, pts, npts, bnc, ctr);
+    else
+        ray_kernel<false><<<grid, 64, 0, st>>>(groups, ngroups, jobs, limits, nitems, off, pts, npts, bnc, ctr);
+    return cudaGetLastError();
+}
 
 } // namespace bhcb
