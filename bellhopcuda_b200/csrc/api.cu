@@ -1290,6 +1290,13 @@ int bhcb_eigen_hits(bhcb_ctx *c, int32_t env, int32_t ifreq, bhcb_eigen_hit *hit
 {
     static_assert(sizeof(bhcb_eigen_hit) == sizeof(EigenHitRec), "eigen hit layout");
     return guarded(c, [&]() -> int {
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            if(c->r3_status != BHCB_OK) throw StateError("no completed 3-D run");
+            const int64_t n = run3_eigen_hits(c->r3, env, hits, hits ? max_hits : 0);
+            if(nhits) *nhits = n;
+            return BHCB_OK;
+        }
         if(c->mode != MODE_EIGEN || !c->prepared) throw StateError("no eigen-hit run");
         if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
         const EnvSlot &S = c->envs[env];

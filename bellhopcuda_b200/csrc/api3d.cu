@@ -30,6 +30,8 @@ cudaError_t launch_arr_gather3d(const SegRec3 *, unsigned long long, const Group
 size_t radix_sort_hist_entries(unsigned long long n);
 cudaError_t radix_sort_pairs(uint64_t *, uint32_t *, uint64_t *, uint32_t *, unsigned long long, int, uint32_t *,
                              int *, cudaStream_t);
+cudaError_t launch_eigen_emit3(const uint32_t *, const ArrCand *, unsigned long long, const GroupDev *, int,
+                               EigenHitRec *, int32_t *, int, cudaStream_t);
 cudaError_t launch_arr_replay(const uint64_t *, const uint32_t *, const ArrCand *, unsigned long long,
                               const GroupDev *, int, const double *, long long, int, int, int, int32_t *,
                               ArrivalRec *, int, cudaStream_t, bool);
@@ -51,8 +53,11 @@ struct Run3 {
     unsigned long long seg_cap = 0;
     int64_t total_field = 0;   // receiver cells of the batch
     bool ran = false;
-    // arrivals runs (RunType 'A' / 'a')
-    bool arrivals = false;
+    // arrivals runs (RunType 'A' / 'a') and eigen-hit runs ('E')
+    bool arrivals = false, eigen = false;
+    std::vector<EigenHitRec> hits_h;   // in the reference's single-threaded order
+    std::vector<int32_t> hit_group;    // environment of each hit
+    DevBuf hits_d, hitgrp_d;
     int32_t opt_max_narr = 0, max_narr = 0, allow_merging = 1;
     uint64_t max_memory = 16ull << 30;
     ArrKeyBits kb{};
@@ -65,7 +70,7 @@ void run3_free(Run3 *r)
 {
     if(!r) return;
     for(DevBuf *b : {&r->arena, &r->groups_d, &r->segs, &r->counters, &r->field, &r->narr_d, &r->arr_d, &r->cand,
-                     &r->keys0, &r->keys1, &r->vals0, &r->vals1, &r->hist})
+                     &r->keys0, &r->keys1, &r->vals0, &r->vals1, &r->hist, &r->hits_d, &r->hitgrp_d})
         b->release();
     delete r;
 }
@@ -201,12 +206,36 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     CK(cudaMemcpyAsync(r->groups_d.p, r->groups_h.data(), r->groups_h.size() * sizeof(GroupDev),
                        cudaMemcpyHostToDevice, st));
     r->counters.ensure(sizeof(RunCounters) + 64);
-    // one run type per batch: TL ('C', 'S', 'I') or arrivals ('A', 'a')
-    const char rt0 = r->envs[0].T.run_type[0];
-    r->arrivals = rt0 == 'A' || rt0 == 'a';
-    for(const auto &S : r->envs) {
-        const char t = S.T.run_type[0];
-        if((t == 'A' || t == 'a') != r->arrivals) throw std::runtime_error("a 3-D batch must use one run type");
+    // one run type per batch: TL ('C', 'S', 'I'), arrivals ('A', 'a') or eigen hits ('E')
+    auto kind = [](char t) { return (t == 'A' || t == 'a') ? 1 : (t == 'E' ? 2 : 0); };
+    const int k0 = kind(r->envs[0].T.run_type[0]);
+    r->arrivals = k0 == 1;
+    r->eigen = k0 == 2;
+    for(const auto &S : r->envs)
+        if(kind(S.T.run_type[0]) != k0) throw std::runtime_error("a 3-D batch must use one run type");
+    auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
+    if(r->eigen) {
+        // ordering key (low to high): depth | bearing | walk position | step | ray | trace group
+        int mz = 1, mt = 1, mr = 1, mj = 1;
+        for(const auto &S : r->envs) {
+            mz = std::max(mz, (int)S.T.rz.size());
+            mt = std::max(mt, (int)S.T.theta.size());
+            mr = std::max(mr, (int)S.T.rr.size());
+        }
+        for(const GroupDev &G : r->groups_h) mj = std::max(mj, G.njobs);
+        ArrKeyBits kb{};
+        kb.eigen = 1;
+        kb.sh_theta = bits((unsigned long long)mz);
+        kb.sh_walk = kb.sh_theta + bits((unsigned long long)mt);
+        kb.sh_is = kb.sh_walk + bits((unsigned long long)mr);
+        kb.sh_job = kb.sh_is + bits(100000);   // steps per ray (MaxN)
+        kb.sh_cell = kb.sh_job + bits((unsigned long long)mj);
+        kb.total_bits = kb.sh_cell + bits((unsigned long long)r->groups_h.size());
+        if(kb.total_bits > 64) throw MemError("eigen-hit ordering key needs more than 64 bits; split the batch");
+        r->kb = kb;
+        r->hits_h.clear();
+        r->hit_group.clear();
+        return;
     }
     if(!r->arrivals) {
         r->field.ensure(std::max<int64_t>(r->total_field, 1) * sizeof(float2));
@@ -215,7 +244,6 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     // ordering key (low to high): step | ray | receiver cell
     int max_njobs = 1;
     for(const GroupDev &G : r->groups_h) max_njobs = std::max(max_njobs, G.njobs);
-    auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
     ArrKeyBits kb{};
     kb.sh_is = 0;
     kb.sh_job = bits(100000);   // steps per ray (MaxN, include/bhc/structs.hpp:66)
@@ -290,10 +318,25 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
                             (uint32_t *)r->vals1.p, n, r->kb.total_bits, (uint32_t *)r->hist.p, &in1, st));
         const uint64_t *k = (const uint64_t *)(in1 ? r->keys1.p : r->keys0.p);
         const uint32_t *v = (const uint32_t *)(in1 ? r->vals1.p : r->vals0.p);
+        if(r->eigen) {
+            r->hits_d.ensure(n * sizeof(EigenHitRec));
+            r->hitgrp_d.ensure(n * sizeof(int32_t));
+            CK(launch_eigen_emit3(v, (const ArrCand *)r->cand.p, n, (const GroupDev *)r->groups_d.p,
+                                  (int)r->groups_h.size(), (EigenHitRec *)r->hits_d.p, (int32_t *)r->hitgrp_d.p,
+                                  sm_count, st));
+            const size_t h0 = r->hits_h.size();
+            r->hits_h.resize(h0 + n);
+            r->hit_group.resize(h0 + n);
+            CK(cudaMemcpyAsync(r->hits_h.data() + h0, r->hits_d.p, n * sizeof(EigenHitRec), cudaMemcpyDeviceToHost,
+                               st));
+            CK(cudaMemcpyAsync(r->hit_group.data() + h0, r->hitgrp_d.p, n * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, st));
+        } else {
         CK(launch_arr_replay(k, v, (const ArrCand *)r->cand.p, n, (const GroupDev *)r->groups_d.p,
                              (int)r->groups_h.size(), nullptr, (long long)r->total_field, r->kb.sh_cell,
                              r->max_narr, r->allow_merging, (int32_t *)r->narr_d.p, (ArrivalRec *)r->arr_d.p,
                              sm_count, st, true));
+        }
     }
     CK(cudaEventRecord(e1, st));
     RunCounters rc{};
@@ -317,9 +360,11 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
     const size_t rec = sizeof(SegRec3);
     // TL: the field; arrivals: their storage, and half of the rest is left
     // for the arrival candidates
-    const size_t fbytes = r->arrivals ? r->arr_d.bytes + r->narr_d.bytes : (size_t)r->total_field * sizeof(float2);
+    const bool cand_mode = r->arrivals || r->eigen;
+    const size_t fbytes = r->arrivals ? r->arr_d.bytes + r->narr_d.bytes
+                                      : (r->eigen ? 0 : (size_t)r->total_field * sizeof(float2));
     size_t budget = max_memory > fbytes + (64u << 20) ? max_memory - fbytes - (64u << 20) : 0;
-    if(r->arrivals) budget /= 2;
+    if(cand_mode) budget /= 2;
     const unsigned long long maxcap = budget / rec;
     if(r->seg_cap == 0) {
         // a first guess within the budget: a ray emits at most one record per
@@ -374,7 +419,7 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
         }
         const unsigned long long nseg = std::min(rc.nseg, r->seg_cap);
         const int igrid = sm_count * 8;
-        if(r->arrivals && rc.err_bits == 0) {
+        if(cand_mode && rc.err_bits == 0) {
             cudaEventDestroy(e0); cudaEventDestroy(e2);
             if(!apply_arrivals(r, j0, j1, nseg, st, sm_count, acc)) {   // candidates exceed the budget
                 cudaEventDestroy(e1);
@@ -423,10 +468,11 @@ uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, i
     r->opt_max_narr = opt_max_narr;
     r->allow_merging = allow_merging;
     prepare3(r, st, h2d);
-    if(!r->arrivals) CK(cudaMemsetAsync(r->field.p, 0, std::max<int64_t>(r->total_field, 1) * sizeof(float2), st));
+    const bool tl = !r->arrivals && !r->eigen;
+    if(tl) CK(cudaMemsetAsync(r->field.p, 0, std::max<int64_t>(r->total_field, 1) * sizeof(float2), st));
     RangeStats acc;
     run_jobs(r, 0, r->njobs, st, sm_count, max_memory, acc);
-    if(acc.rc.err_bits == 0 && !r->arrivals) {
+    if(acc.rc.err_bits == 0 && tl) {
         for(const auto &S : r->envs)
             if(S.T.run_type[0] != 'C')
                 CK(launch_sqrt3d((float2 *)r->field.p + S.field_base, S.field_n, sm_count * 4, st));
@@ -473,7 +519,7 @@ static const Env3Slot &ran_env(const Run3 *r, int env)
 void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
-    if(r->arrivals) throw StateError("not a TL run: use bhcb_copy_arrivals");
+    if(r->arrivals || r->eigen) throw StateError("not a TL run: use bhcb_copy_arrivals / bhcb_eigen_hits");
     const size_t need = (size_t)S.field_n * sizeof(float2);
     if(!dst || bytes < need) throw std::invalid_argument("destination too small");
     CK(cudaMemcpyAsync(dst, (float2 *)r->field.p + S.field_base, need, cudaMemcpyDeviceToHost, st));
@@ -483,7 +529,7 @@ void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st)
 void *run3_field_device(Run3 *r, int env)
 {
     const Env3Slot &S = ran_env(r, env);
-    if(r->arrivals) throw StateError("not a TL run");
+    if(r->arrivals || r->eigen) throw StateError("not a TL run");
     return (float2 *)r->field.p + S.field_base;
 }
 
@@ -502,6 +548,20 @@ std::vector<std::string> run3_warnings(const Run3 *r, int env)
 }
 
 bool run3_is_arrivals(const Run3 *r) { return r->arrivals; }
+
+int64_t run3_eigen_hits(Run3 *r, int env, void *hits, int64_t max_hits)
+{
+    ran_env(r, env);
+    if(!r->eigen) throw StateError("not an eigen-hit run");
+    int64_t n = 0;
+    EigenHitRec *out = reinterpret_cast<EigenHitRec *>(hits);
+    for(size_t k = 0; k < r->hits_h.size(); ++k) {
+        if(r->hit_group[k] != env) continue;
+        if(out && n < max_hits) out[n] = r->hits_h[k];
+        ++n;
+    }
+    return n;
+}
 
 int32_t run3_max_narr(const Run3 *r) { return r->max_narr; }
 
@@ -607,6 +667,7 @@ static void write_arrivals3(Run3 *r, const Env3Slot &S, const std::string &path,
 void run3_writeout(Run3 *r, int env, const std::string &root, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
+    if(r->eigen) throw StateError("3-D eigenray .ray output (re-trace of the hit rays) is not built; use bhcb_eigen_hits");
     if(r->arrivals) {
         write_arrivals3(r, S, root + ".arr", st);
         return;

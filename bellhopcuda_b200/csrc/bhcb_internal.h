@@ -181,10 +181,12 @@ struct ArrCand {
     float rcvr_azim;           // 3-D: receiver azimuth (deg); 2-D: unused
 };
 // Bit layout of the ordering keys (low to high): arrivals: step | job | cell;
-// eigen: depth | walk position | step | job | field.
+// eigen: depth | walk position | step | job | field (3-D: depth | bearing |
+// walk position | step | job | trace group).
 struct ArrKeyBits {
     int sh_walk, sh_is, sh_job, sh_cell;
     int total_bits, eigen;
+    int sh_theta;              // 3-D eigen: bearing index above the depth bits
 };
 
 struct RunCounters {

@@ -881,8 +881,7 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.freq0 = freq;
     std::memcpy(t.run_type, in.run_type, 7);
     switch(t.run_type[0]) {   // src/module/runtype.hpp:53-78
-    case 'C': case 'S': case 'I': case 'A': case 'a': break;
-    case 'E': env_error("3-D eigenray runs are not supported by this build");
+    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': break;
     case 'R': env_error("ray-trace runs ('R') are not a field mode");
     default: env_error("unknown RunType");
     }

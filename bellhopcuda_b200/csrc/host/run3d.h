@@ -26,6 +26,9 @@ uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, i
                   int32_t allow_merging, bhcb_stats &stats, uint32_t &warn_bits);
 // arrivals runs (RunType 'A' / 'a'): storage [cell][max_narr], cells in the field layout
 bool run3_is_arrivals(const Run3 *r);
+// eigen-hit runs ('E'): copies up to max_hits hits of env (reference order) to
+// hits (EigenHitRec records, may be NULL); returns their number
+int64_t run3_eigen_hits(Run3 *r, int env, void *hits, int64_t max_hits);
 int32_t run3_max_narr(const Run3 *r);
 void run3_copy_arrivals(Run3 *r, int env, int32_t *narr, size_t narr_bytes, void *arr, size_t arr_bytes,
                         cudaStream_t st);

@@ -368,7 +368,10 @@ __device__ __forceinline__ bool pair_outside_beam(const SegRec3 &R, double dxr, 
 // MODE: INFL_TL adds the field; INFL_ARR_COUNT counts the arrival candidates;
 // INFL_ARR_FILL writes them (AddArr's inputs, src/influence.hpp:444-447) with
 // the key (receiver cell, ray, step) that restores the reference's order.
-enum { INFL_TL = 0, INFL_ARR_COUNT = 1, INFL_ARR_FILL = 2 };
+// INFL_EIG_COUNT / INFL_EIG_FILL: the same for eigenray hits (RecordEigenHit,
+// src/eigenrays.hpp:24-40), keyed by (trace group, ray, step, position in the
+// receiver-range walk, bearing, depth) — the reference's single-threaded order.
+enum { INFL_TL = 0, INFL_ARR_COUNT = 1, INFL_ARR_FILL = 2, INFL_EIG_COUNT = 3, INFL_EIG_FILL = 4 };
 template<int MODE>
 __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     const SegRec3 *__restrict__ segs, unsigned long long nseg, const GroupDev *__restrict__ groups, int ngroups,
@@ -382,7 +385,7 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     __shared__ double s_xs[WARPS3][32], s_ys[WARPS3][32];
     // per surviving pair of a 32-pair batch
     __shared__ int s_pincl[WARPS3][32];
-    __shared__ int s_prec[WARPS3][32], s_piz0[WARPS3][32];
+    __shared__ int s_prec[WARPS3][32], s_piz0[WARPS3][32], s_pmeta[WARPS3][32];
     __shared__ double s_pdx[WARPS3][32], s_pdy[WARPS3][32];
     __shared__ long long s_poff[WARPS3][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -459,6 +462,7 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
                         s_pdx[w][lane] = dxr;
                         s_pdy[w][lane] = dyr;
                         s_poff[w][lane] = s_fbase[w][j] + (long long)itheta * E.nrz * E.nrr + ir;
+                        s_pmeta[w][lane] = (itheta << 20) | ir;
                     }
                 }
             }
@@ -495,6 +499,29 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
                 if(MODE == INFL_TL) {
                     const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
                     atomicAdd(field + cell, tl_field3(o, E.gaussian != 0, E.coherent != 0, omega));
+                } else if(MODE == INFL_EIG_FILL) {
+                    const unsigned long long i = atomicAdd(cursor, 1ull);
+                    if(i >= cand_cap) continue;
+                    const int itheta = s_pmeta[w][pi] >> 20, ir = s_pmeta[w][pi] & 0xfffff;
+                    // the walk visits the bracketed ranges towards rB: ascending when rB > rA
+                    const double xsx = s_xs[w][j], xsy = s_ys[w][j];
+                    const double ax = R.x0[0] - xsx, ay = R.x0[1] - xsy;
+                    const double bx = ax + R.rayt[0] * R.rlen, by = ay + R.rayt[1] * R.rlen;
+                    const bool up = bx * bx + by * by > ax * ax + ay * ay;
+                    const int walk = up ? ir - R.ir_lo : R.ir_hi - ir;
+                    ArrCand c;
+                    c.amp = c.phase = c.delay_re = c.delay_im = 0.0;
+                    c.rcvr_decl = 0.0f;
+                    c.ntop = R.is;
+                    c.nbot = ir;
+                    c.job = R.job;
+                    c.aux = itheta;
+                    c.rcvr_azim = __int_as_float(iz);
+                    cands[i] = c;
+                    keys[i] = ((uint64_t)s_grp[w][j] << kb.sh_cell) | ((uint64_t)R.job << kb.sh_job)
+                        | ((uint64_t)R.is << kb.sh_is) | ((uint64_t)walk << kb.sh_walk)
+                        | ((uint64_t)itheta << kb.sh_theta) | (uint64_t)iz;
+                    vals[i] = (uint32_t)i;
                 } else if(MODE == INFL_ARR_FILL) {
                     const unsigned long long i = atomicAdd(cursor, 1ull);
                     if(i >= cand_cap) continue;
@@ -523,7 +550,32 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     // one counter update per warp
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1) nevals += __shfl_down_sync(0xffffffffu, nevals, o);
-    if(MODE != INFL_ARR_FILL && lane == 0 && nevals) atomicAdd(&ctr->nevals, nevals);
+    if(MODE != INFL_ARR_FILL && MODE != INFL_EIG_FILL && lane == 0 && nevals) atomicAdd(&ctr->nevals, nevals);
+}
+
+// eigen hits in sorted order (RecordEigenHit layout, include/bhc/structs.hpp:353-361)
+__global__ void eigen_emit3_kernel(const uint32_t *__restrict__ vals, const ArrCand *__restrict__ cands,
+                                   unsigned long long n, const GroupDev *__restrict__ groups, int ngroups,
+                                   EigenHitRec *hits, int32_t *group_of_hit)
+{
+    for(unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < n;
+        k += (unsigned long long)gridDim.x * blockDim.x) {
+        const ArrCand &c = cands[vals[k]];
+        const int g = find_group(groups, ngroups, c.job);
+        const Job3 J = job_indices3(*groups[g].env3, (int)((long long)c.job - groups[g].job_base));
+        EigenHitRec h;
+        h.is = c.ntop;
+        h.itheta = c.aux;
+        h.ir = c.nbot;
+        h.iz = __float_as_int(c.rcvr_azim);
+        h.isx = J.isx;
+        h.isy = J.isy;
+        h.isz = J.isz;
+        h.ialpha = J.ialpha;
+        h.ibeta = J.ibeta;
+        hits[k] = h;
+        group_of_hit[k] = g;
+    }
 }
 
 __global__ void sqrt3d_kernel(float2 *f, long long n)
@@ -559,7 +611,16 @@ cudaError_t launch_arr_gather3d(const SegRec3 *segs, unsigned long long nseg, co
                                 ArrKeyBits kb, int grid, cudaStream_t st)
 {
     if(nseg == 0) return cudaSuccess;
-    if(count)
+    if(kb.eigen) {
+        if(count)
+            influence3d_kernel<INFL_EIG_COUNT><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, nullptr,
+                                                                             ctr, nullptr, nullptr, nullptr, 0, nullptr,
+                                                                             kb);
+        else
+            influence3d_kernel<INFL_EIG_FILL><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, nullptr,
+                                                                            ctr, cands, keys, vals, cand_cap, cursor,
+                                                                            kb);
+    } else if(count)
         influence3d_kernel<INFL_ARR_COUNT><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, nullptr, ctr,
                                                                          nullptr, nullptr, nullptr, 0, nullptr, kb);
     else
@@ -572,6 +633,17 @@ cudaError_t launch_sqrt3d(float2 *f, long long n, int grid, cudaStream_t st)
 {
     if(n <= 0) return cudaSuccess;
     sqrt3d_kernel<<<grid, 256, 0, st>>>(f, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eigen_emit3(const uint32_t *vals, const ArrCand *cands, unsigned long long n,
+                               const GroupDev *groups, int ngroups, EigenHitRec *hits, int32_t *group_of_hit,
+                               int sm_count, cudaStream_t st)
+{
+    if(n == 0) return cudaSuccess;
+    long long grid = (long long)((n + 255) / 256);
+    if(grid > (long long)sm_count * 32) grid = (long long)sm_count * 32;
+    eigen_emit3_kernel<<<(int)grid, 256, 0, st>>>(vals, cands, n, groups, ngroups, hits, group_of_hit);
     return cudaGetLastError();
 }
 

@@ -121,6 +121,18 @@ def parabot3d_arr_hat():
     return f
 
 
+def munk3d_eig_gauss():
+    """Eigenray hits ('E') on a sparse receiver grid."""
+    return _munk_slice("EB   3", alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0), theta=[0.0, 2.0, 5.0],
+                       nrz_range=(3, 800.0, 2800.0), rr_range=(4, 8.0, 26.0))
+
+
+def seamount3d_eig_hat():
+    f = seamount3d_gauss()
+    f[".env"] = f[".env"].replace("'CB   3'", "'EG   3'").replace("101\n0 10 /", "3\n3 9 /")
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -133,4 +145,6 @@ CASES3D = {
     "munk3d_arr_gauss": munk3d_arr_gauss,
     "munk3d_arr_hat": munk3d_arr_hat,
     "parabot3d_arr_hat": parabot3d_arr_hat,
+    "munk3d_eig_gauss": munk3d_eig_gauss,
+    "seamount3d_eig_hat": seamount3d_eig_hat,
 }

@@ -26,6 +26,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
 from bellhopcuda_b200.arrfile import read_arr_binary  # noqa: E402
+from bellhopcuda_b200.rayfile import read_ray  # noqa: E402
 from bellhopcuda_b200.shdfile import read_shd  # noqa: E402
 from cases3d import CASES3D  # noqa: E402
 
@@ -47,6 +48,16 @@ def main(names=None):
             if r.returncode != 0:
                 raise SystemExit("reference failed on %s:\n%s%s" % (name, r.stdout[-2000:], r.stderr[-2000:]))
             texts = {"file_" + suffix[1:]: np.array(text) for suffix, text in files.items()}
+            if files[".env"].count("'E") and os.path.exists(root + ".ray"):
+                # eigen hits: the reference writes the re-traced eigenrays in hit
+                # order; each ray's take-off angle (radians in 3-D) and its point
+                # count (the hit's step + 2) pin the hit list
+                R = read_ray(root + ".ray")
+                np.savez_compressed(os.path.join(HERE, name + ".npz"),
+                                    alpha=np.array([x["alpha"] for x in R["rays"]]),
+                                    npts=np.array([len(x["xy"]) for x in R["rays"]], np.int32), **texts)
+                print(name, "eigenrays", len(R["rays"]), "%.1fs" % (time.time() - t0))
+                continue
             if os.path.exists(root + ".arr"):
                 # arrivals: per receiver (source, bearing, depth, range) the
                 # count and the records, flattened with offsets

@@ -42,8 +42,10 @@ def to_file_order(u):
     return np.transpose(u, (1, 2, 3, 0, 4, 5))
 
 
-@pytest.mark.parametrize("path", [p for p in GOLD if "_arr_" not in p],
-                         ids=[os.path.basename(p)[:-4] for p in GOLD if "_arr_" not in p])
+TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p]
+
+
+@pytest.mark.parametrize("path", TL3D, ids=[os.path.basename(p)[:-4] for p in TL3D])
 def test_3d_field_matches_reference(path, workdir):
     g = np.load(path)
     root = os.path.join(workdir, os.path.basename(path)[:-4])
@@ -127,7 +129,7 @@ def test_3d_small_max_memory_runs_in_waves(workdir):
 
 
 ARR3D = sorted(p for p in GOLD if "_arr_" in p)
-TL3D = [p for p in GOLD if "_arr_" not in p]
+EIG3D = sorted(p for p in GOLD if "_eig_" in p)
 
 
 @pytest.mark.parametrize("path", ARR3D, ids=[os.path.basename(p)[:-4] for p in ARR3D])
@@ -163,3 +165,26 @@ def test_3d_arrivals_match_reference(path, workdir):
     mine = np.concatenate([a for s in A["sources"] for a in s["arrivals"]])
     np.testing.assert_array_equal(mine[:, 2], got["delay_re"])
     np.testing.assert_allclose(mine[:, 1], ref[:, 1], rtol=0, atol=1e-3)   # phase in degrees
+
+
+@pytest.mark.parametrize("path", EIG3D, ids=[os.path.basename(p)[:-4] for p in EIG3D])
+def test_3d_eigen_hits_match_reference(path, workdir):
+    """3-D eigen hits ('E') against the reference's single-threaded run: it
+    writes one re-traced ray per hit, in hit order, whose take-off angle and
+    point count (the hit's step + 2) give each hit's ray and step."""
+    g = np.load(path)
+    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.setup3d(root)
+        t.run()
+        hits = t.eigen_hits(0)
+    assert len(hits) == len(g["alpha"]) > 0
+    np.testing.assert_array_equal(hits["is"] + 2, g["npts"])
+    # the take-off angle of each hit's ray: elevation fan from the .env (alpha1, alpha2, n)
+    txt = str(g["file_env"]).splitlines()
+    k = [i for i, ln in enumerate(txt) if ln.strip().startswith("'E")][0]
+    na = int(txt[k + 1].split()[0])
+    a1, a2 = (float(v) for v in txt[k + 2].replace("/", " ").split()[:2])
+    fan = np.deg2rad(np.linspace(a1, a2, na))
+    np.testing.assert_allclose(fan[hits["ialpha"]], g["alpha"], rtol=1e-9, atol=1e-12)

@@ -154,6 +154,8 @@ def test_reader3d_sizes_match_reference_fixture(name, workdir):
     if "field" in g.files:
         nsx, nsy, nth, nsz, nrz, nrr = g["field"].shape
         assert info["dims"] == (nsz, nsx, nsy, nth, nrz, nrr)
+    elif "npts" in g.files:   # eigen fixture: one re-traced ray per hit
+        assert len(g["npts"]) == len(g["alpha"]) > 0
     else:   # arrivals fixture: one count per receiver
         d = info["dims"]
         assert (d[0], d[3], d[4], d[5]) == (len(g["sz"]), len(g["theta"]), len(g["rz"]), len(g["rr"]))
