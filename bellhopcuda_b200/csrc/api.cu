@@ -290,7 +290,7 @@ void do_prepare(bhcb_ctx *c)
     }
     // --- build device tables
     Arena A;
-    struct EnvOffsets { size_t z, rho, c, cz, n2, n2z, coef, btop, bbot, rr, rz, sz, alpha, sbp; };
+    struct EnvOffsets { size_t z, rho, c, cz, n2, n2z, coef, qr, qc, qcz, trc, brc, btop, bbot, rr, rz, sz, alpha, sbp; };
     std::vector<EnvOffsets> offs;
     std::vector<EnvDev> envdev;
     for(const GroupPlan &gp : plan) {
@@ -299,6 +299,8 @@ void do_prepare(bhcb_ctx *c)
         EnvOffsets o;
         o.z = A.put(T.z); o.rho = A.put(T.rho); o.c = A.put(T.c); o.cz = A.put(T.cz);
         o.n2 = A.put(T.n2); o.n2z = A.put(T.n2z); o.coef = A.put(T.coef);
+        o.qr = A.put(T.qr); o.qc = A.put(T.qc); o.qcz = A.put(T.qcz);
+        o.trc = A.put(T.trc); o.brc = A.put(T.brc);
         o.btop = A.put(T.btop); o.bbot = A.put(T.bbot);
         // depths padded to an even count: the mixed influence kernel reads them in pairs
         std::vector<float> rz_even = T.rz;
@@ -309,6 +311,10 @@ void do_prepare(bhcb_ctx *c)
         EnvDev d{};
         d.ssp_type = T.ssp_type;
         d.nssp = (int)T.z.size();
+        d.nqr = (int)T.qr.size();
+        d.ntrc = (int)(T.trc.size() / 3);
+        d.nbrc = (int)(T.brc.size() / 3);
+        d.beam_shift = T.beam_type[3] == 'S';
         d.top = T.top;
         d.bot = T.bot;
         d.ntop = (int)T.btop.size();
@@ -350,6 +356,8 @@ void do_prepare(bhcb_ctx *c)
         d.c = dptr<double>(ab, o.c); d.cz = dptr<double>(ab, o.cz);
         d.n2 = dptr<double>(ab, o.n2); d.n2z = dptr<double>(ab, o.n2z);
         d.coef = dptr<double>(ab, o.coef);
+        d.qr = dptr<double>(ab, o.qr); d.qc = dptr<double>(ab, o.qc); d.qcz = dptr<double>(ab, o.qcz);
+        d.trc = dptr<double>(ab, o.trc); d.brc = dptr<double>(ab, o.brc);
         d.btop = dptr<BdryPtDev>(ab, o.btop); d.bbot = dptr<BdryPtDev>(ab, o.bbot);
         d.rr = dptr<double>(ab, o.rr); d.rz = dptr<float>(ab, o.rz); d.sz = dptr<float>(ab, o.sz);
         d.alpha = dptr<double>(ab, o.alpha); d.sbp = dptr<double>(ab, o.sbp);

@@ -114,7 +114,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     if(r->envs.empty()) throw StateError("no 3-D environment: call bhcb_setup3d first");
     Arena A;
     struct Offs { size_t z, rho, c, cz, n2, n2z, coef, hx, hy, hz, hc, hcz, btop, bbot, sx, sy, sz, rr, rz, tcs,
-                  alpha, beta, sbp; };
+                  alpha, beta, sbp, trc, brc; };
     std::vector<Offs> offs;
     std::vector<Env3Dev> envdev;
     r->groups_h.clear();
@@ -141,6 +141,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         }
         o.tcs = A.put(tcs);
         o.alpha = A.put(T.alpha); o.beta = A.put(T.beta); o.sbp = A.put(T.sbp);
+        o.trc = A.put(T.trc); o.brc = A.put(T.brc);
         offs.push_back(o);
 
         Env3Dev d{};
@@ -151,6 +152,8 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         e.bot = T.bot;
         e.freq0 = T.freq0;
         e.deltas = T.deltas;
+        e.ntrc = (int)(T.trc.size() / 3);
+        e.nbrc = (int)(T.brc.size() / 3);
         d.hex = T.ssp_type == SSP_HEXAHEDRAL;
         d.hnx = (int)T.hx.size(); d.hny = (int)T.hy.size(); d.hnz = (int)T.hz.size();
         d.top = T.top;
@@ -193,6 +196,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         e.z = dptr<double>(ab, o.z); e.rho = dptr<double>(ab, o.rho);
         e.c = dptr<double>(ab, o.c); e.cz = dptr<double>(ab, o.cz);
         e.n2 = dptr<double>(ab, o.n2); e.n2z = dptr<double>(ab, o.n2z); e.coef = dptr<double>(ab, o.coef);
+        e.trc = dptr<double>(ab, o.trc); e.brc = dptr<double>(ab, o.brc);
         d.hx = dptr<double>(ab, o.hx); d.hy = dptr<double>(ab, o.hy); d.hz = dptr<double>(ab, o.hz);
         d.hc = dptr<double>(ab, o.hc); d.hcz = dptr<double>(ab, o.hcz);
         d.btop = dptr<Bdry3PtDev>(ab, o.btop); d.bbot = dptr<Bdry3PtDev>(ab, o.bbot);

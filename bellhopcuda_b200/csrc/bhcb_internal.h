@@ -15,18 +15,19 @@ namespace bhcb {
 
 // SSP interpolation types (reference: src/runtype.hpp:52-75)
 enum SspType : int32_t { SSP_N2LINEAR = 0, SSP_CLINEAR = 1, SSP_CUBIC = 2, SSP_PCHIP = 3,
-                         SSP_ANALYTIC = 4, SSP_HEXAHEDRAL = 5 };
+                         SSP_ANALYTIC = 4, SSP_HEXAHEDRAL = 5, SSP_QUAD = 6 };
 
 // error / warning bits: same numbering as the reference's ErrState
 // (src/util/errors.hpp:61-93); BHCB_ERR_SEG_OVERFLOW is this runtime's own.
 enum : uint32_t {
     ERR_RAYINIT = 2, ERR_BOUNDARY_SEG_NAN = 3, ERR_BOUNDARY_CONDITION_TYPE = 4,
     ERR_INVALID_SSP_TYPE = 5, ERR_OUTSIDE_ALTIMETRY = 6, ERR_OUTSIDE_BATHYMETRY = 7,
-    ERR_OUTSIDE_SSP = 8,
+    ERR_OUTSIDE_SSP = 8, ERR_QUAD_ISEG = 9,
     ERR_SEG_OVERFLOW = 31,
 };
 enum : uint32_t {
     WARN_ONERAY_OUTOFMEMORY = 1, WARN_TOO_FEW_BEAMS = 3, WARN_SOURCE_OUTSIDE_BOUNDARIES = 4,
+    WARN_OUTSIDE_REFLCOEF = 5,
     WARN_OUTSIDE_ALTIMETRY = 6, WARN_OUTSIDE_BATHYMETRY = 7,
     WARN_STEP_NEGATIVE_H = 8, WARN_TRIDIAG_H_NEGATIVE = 9, WARN_TRIDIAG_H_GROWING = 10,
     WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17,
@@ -51,6 +52,16 @@ struct EnvDev {
     const double *c, *cz;      // complex, interleaved re/im, [nssp]
     const double *n2, *n2z;    // complex [nssp]
     const double *coef;        // complex [4][nssp]: spline (S) or pchip (P) coefficients
+    // quad (range-dependent) SSP (src/ssp.hpp:157-212): profile ranges qr[nqr]
+    // (m), sound speed qc[iz * nqr + ir] and its depth gradient qcz[iz * nqr + ir]
+    int32_t nqr, pad_q;
+    const double *qr, *qc, *qcz;
+    // tabulated reflection coefficients for 'F' boundaries (src/module/reflcoef.hpp):
+    // (theta deg, |R|, phase rad) triples, strictly increasing theta
+    int32_t ntrc, nbrc;
+    const double *trc, *brc;
+    int32_t beam_shift;              // Beam->Type[3] == 'S' (src/reflect.hpp:383-448)
+    int32_t pad_s;
     HsDev top, bot;
     // boundaries
     int32_t ntop, nbot;

@@ -121,6 +121,60 @@ void read_hex_ssp(const std::string &path, EnvInput &in)
         }
 }
 
+// quad SSP file (src/module/ssp.hpp:122-141): Nr, the Nr profile ranges (km),
+// then one record of Nr sound speeds per depth of the .env profile
+void read_quad_ssp(const std::string &path, EnvInput &in)
+{
+    LdiReader f(path);
+    if(!f.good()) env_error("unable to open quad SSP file " + path);
+    int32_t nr = 0;
+    f.record(); f.read(nr);
+    if(nr < 2) env_error("quad SSP: at least two profiles are needed");
+    in.quad_r_km.assign(nr, 0.0);
+    f.record();
+    for(int i = 0; i < nr; ++i) f.read(in.quad_r_km[i]);
+    const size_t nz = in.ssp_z.size();
+    in.quad_c.assign(nz * nr, 0.0);
+    for(size_t iz = 0; iz < nz; ++iz) {
+        f.record();
+        for(int ir = 0; ir < nr; ++ir) f.read(in.quad_c[iz * nr + ir]);
+    }
+    for(int i = 1; i < nr; ++i)
+        if(!(in.quad_r_km[i] > in.quad_r_km[i - 1])) env_error("quad SSP: profile ranges must be monotone increasing");
+}
+
+// reflection coefficient file (src/module/reflcoef.hpp:50-75, 129-145): NPts,
+// then NPts (theta, |R|, phase) triples in one list-directed record
+void read_refl_file(const std::string &path, bool istop, std::vector<std::array<double, 3>> &tab)
+{
+    const std::string which = istop ? "top" : "bottom";
+    LdiReader f(path);
+    if(!f.good()) env_error("unable to open " + which + " reflection coefficient file " + path);
+    int32_t n = 0;
+    f.record(); f.read(n);
+    if(n < 1) env_error(which + " reflection coefficient file: no points");
+    tab.assign(n, {0.0, 0.0, 0.0});
+    f.record();
+    for(int i = 0; i < n; ++i)
+        for(int k = 0; k < 3; ++k) f.read(tab[i][k]);
+    for(int i = 1; i < n; ++i)
+        if(!(tab[i][0] > tab[i - 1][0]))
+            env_error(which + " reflection coefficients must be monotonically increasing");
+}
+
+// the device form: (theta deg, |R|, phase rad) triples (src/module/reflcoef.hpp:155-165)
+std::vector<double> refl_table(const std::vector<std::array<double, 3>> &tab)
+{
+    const double DegRad = kPi / 180.0;
+    std::vector<double> t;
+    for(const auto &r : tab) {
+        t.push_back(r[0]);
+        t.push_back(r[1]);
+        t.push_back(r[2] * DegRad);
+    }
+    return t;
+}
+
 // ------------------------------------------------------------- preprocessing
 double franc_garr(double f, const double fg[4])
 {
@@ -489,6 +543,9 @@ EnvInput read_env_files(const std::string &root, bool o3d)
         if(st == 'H') {
             if(!o3d) env_error("hexahedral SSP ('H') needs a 3-D run");
             read_hex_ssp(root + ".ssp", in);
+        } else if(st == 'Q') {
+            if(o3d) env_error("quad SSP ('Q'): 2-D profile not supported in 3-D or Nx2D mode");
+            read_quad_ssp(root + ".ssp", in);
         }
     }
     f.record(); f.read_chars(in.bot_opt, 6);                    // BotOpt
@@ -549,6 +606,8 @@ EnvInput read_env_files(const std::string &root, bool o3d)
         if(in.top_opt[4] == '~' || in.top_opt[4] == '*') read_bdry_file(root + ".ati", in.ati);
         if(in.bot_opt[1] == '~' || in.bot_opt[1] == '*') read_bdry_file(root + ".bty", in.bty);
     }
+    if(in.bot.bc == 'F') read_refl_file(root + ".brc", false, in.brc);   // BRC
+    if(in.top.bc == 'F') read_refl_file(root + ".trc", true, in.trc);    // TRC
     if(in.run_type[2] == '*') {                                 // SBP
         LdiReader s(root + ".sbp");
         if(!s.good()) env_error("unable to open source beam pattern file");
@@ -640,7 +699,6 @@ EnvTables preprocess(const EnvInput &in, double freq)
     // ray runs trace geometric rays whatever the beam type (src/mode/ray.cpp:44-86)
     if(!ray_run && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
         env_error(std::string("beam type '") + bt + "' is not supported by this build");
-    if(!ray_run && t.beam_type[3] == 'S') env_error("beam shift ('S') is not supported by this build");
 
     char st = in.top_opt[0];
     switch(st) {
@@ -649,19 +707,33 @@ EnvTables preprocess(const EnvInput &in, double freq)
     case 'S': t.ssp_type = SSP_CUBIC; break;
     case 'P': t.ssp_type = SSP_PCHIP; break;
     case 'A': t.ssp_type = SSP_ANALYTIC; break;
-    case 'Q': env_error("quad SSP ('Q') is not supported by this build");
+    case 'Q': t.ssp_type = SSP_QUAD; break;
     default: env_error("unknown SSP type");
     }
-    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G')
+    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G' && in.top.bc != 'F')
         env_error("top boundary condition not supported by this build");
-    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G')
+    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G' && in.bot.bc != 'F')
         env_error("bottom boundary condition not supported by this build");
+    t.brc = refl_table(in.brc);
+    t.trc = refl_table(in.trc);
     // fT: 1000 once an 'A' bottom halfspace has been read (module/boundarycond.hpp:37-58)
     double fT = in.bot.bc == 'A' ? FLT(1000.0) : 1.0e20;
     Ssp1d sp;
     build_ssp1d(in, freq, fT, st, sp);
     t.z = sp.z; t.rho = sp.rho; t.c = sp.c; t.cz = sp.cz; t.n2 = sp.n2; t.n2z = sp.n2z; t.coef = sp.coef;
     const int n = (int)in.ssp_z.size();
+    if(st == 'Q') {
+        // ranges to m and the depth gradient of every profile (src/module/ssp.hpp:456-462,537-545)
+        const int nr = (int)in.quad_r_km.size();
+        if(nr < 2 || in.quad_c.size() != (size_t)n * nr) env_error("quad SSP: the .ssp file was not read");
+        for(double v : in.quad_r_km) t.qr.push_back(v * FLT(1000.0));
+        t.qc = in.quad_c;
+        t.qcz.assign((size_t)n * nr, 0.0);
+        for(int ir = 0; ir < nr; ++ir)
+            for(int iz = 1; iz < n; ++iz)
+                t.qcz[(size_t)(iz - 1) * nr + ir] = (t.qc[(size_t)iz * nr + ir] - t.qc[(size_t)(iz - 1) * nr + ir])
+                    / (in.ssp_z[iz] - in.ssp_z[iz - 1]);
+    }
     double top_depth = in.ssp_z[0], bot_depth = in.bot_depth;
     if(std::fabs(in.ssp_z[n - 1] - bot_depth) >= FLT(100.0) * FLT_EPSILON)
         t.warnings.push_back("Ocean bottom must be at last SSP depth");
@@ -788,7 +860,7 @@ bool EnvTables::same_trajectory_tables(const EnvTables &o) const
     // semi-coherent Lloyd-mirror source amplitude depends on omega
     // (src/trace.hpp:148-152), so 'S' runs never share.
     return vclose(c, o.c) && vclose(cz, o.cz) && vclose(n2, o.n2) && vclose(n2z, o.n2z)
-        && vclose(coef, o.coef) && hclose(top, o.top) && hclose(bot, o.bot) && bclose(btop, o.btop)
+        && vclose(coef, o.coef) && vclose(qc, o.qc) && vclose(qr, o.qr) && hclose(top, o.top) && hclose(bot, o.bot) && bclose(btop, o.btop)
         && bclose(bbot, o.bbot) && alpha == o.alpha && run_type[0] != 'S';
 }
 
@@ -903,10 +975,12 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
 
     char st = in.top_opt[0];
     double fT = in.bot.bc == 'A' ? FLT(1000.0) : 1.0e20;
-    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G')
+    if(in.top.bc != 'V' && in.top.bc != 'R' && in.top.bc != 'A' && in.top.bc != 'G' && in.top.bc != 'F')
         env_error("top boundary condition not supported by this build");
-    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G')
+    if(in.bot.bc != 'V' && in.bot.bc != 'R' && in.bot.bc != 'A' && in.bot.bc != 'G' && in.bot.bc != 'F')
         env_error("bottom boundary condition not supported by this build");
+    t.brc = refl_table(in.brc);
+    t.trc = refl_table(in.trc);
     double top_depth = in.ssp_z[0], bot_depth = in.bot_depth;
     if(st == 'H') {
         t.ssp_type = SSP_HEXAHEDRAL;

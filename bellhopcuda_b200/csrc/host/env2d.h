@@ -64,12 +64,20 @@ struct EnvInput {
     Bdry3In ati3, bty3;
     // hexahedral SSP (.ssp file, src/module/ssp.hpp:144-190): c[(ix * ny + iy) * nz + iz]
     std::vector<double> hex_x_km, hex_y_km, hex_z, hex_c;
+    // quad SSP (.ssp file, src/module/ssp.hpp:122-141): profile ranges (km) and
+    // c[iz * nr + ir] at the .env profile's depths
+    std::vector<double> quad_r_km, quad_c;
+    // tabulated reflection coefficients (.brc / .trc, src/module/reflcoef.hpp:50-75):
+    // angle of incidence (deg), |R|, phase (deg)
+    std::vector<std::array<double, 3>> brc, trc;
 };
 
 struct EnvTables {
     double freq0 = 0;
     int32_t ssp_type = SSP_CLINEAR;
     std::vector<double> z, rho, c, cz, n2, n2z, coef;   // complex tables interleaved
+    std::vector<double> qr, qc, qcz;                    // quad SSP: ranges (m), c and dc/dz [iz * nr + ir]
+    std::vector<double> brc, trc;                       // reflection tables: (theta deg, |R|, phase rad) triples
     HsDev top{}, bot{};
     int32_t top_curv = 0, bot_curv = 0, top_long = 0, bot_long = 0;
     std::vector<BdryPtDev> btop, bbot;
@@ -93,6 +101,7 @@ struct Env3Tables {
     int32_t ssp_type = SSP_CLINEAR;          // SSP_HEXAHEDRAL or a 1-D type
     std::vector<double> z, rho, c, cz, n2, n2z, coef;   // 1-D tables (complex interleaved), as in 2-D
     std::vector<double> hx, hy, hz, hc, hcz;             // hexahedral grid (m) and c, dc/dz
+    std::vector<double> brc, trc;                        // reflection tables as in 2-D
     HsDev top{}, bot{};
     int32_t top_nx = 2, top_ny = 2, bot_nx = 2, bot_ny = 2;
     std::vector<Bdry3Pt> btop, bbot;

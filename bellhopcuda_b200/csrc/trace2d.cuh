@@ -62,6 +62,44 @@ __device__ __forceinline__ void update_seg(double x, bool tpos, const double *a,
     }
 }
 
+// src/ssp.hpp:157-212 — quad (range-dependent) SSP: bilinear in range between
+// two profiles, each linear in depth; the attenuation comes from the .env
+// profile. The density is always interpolated (LinInterpDensity).
+template<typename R> __device__ __forceinline__ void eval_quad(
+    V2<double> x, V2<R> t, SSPOut<R> &o, const EnvDev &e, SegState &s, RunCounters *ctr)
+{
+    const int nr = e.nqr;
+    if(x.x < e.qr[0] || x.x > e.qr[nr - 1]) run_error(ctr, ERR_OUTSIDE_SSP);
+    update_seg(x.y, t.y >= (R)0, e.z, e.nssp, s.z);
+    update_seg(x.x, t.x >= (R)0, e.qr, nr, s.r);
+    {
+        double z0 = e.z[s.z];
+        R w = (R)((x.y - z0) / (e.z[s.z + 1] - z0));
+        o.rho = ((R)1 - w) * (R)e.rho[s.z] + w * (R)e.rho[s.z + 1];
+    }
+    if(s.z >= e.nssp - 1 || s.r >= nr - 1) {
+        run_error(ctr, ERR_QUAD_ISEG);
+        s.z = s.r = 0;
+    }
+    const int iz = s.z, ir = s.r;
+    const R cz1 = (R)e.qcz[iz * nr + ir], cz2 = (R)e.qcz[iz * nr + ir + 1];
+    const double s2d = x.y - e.z[iz];
+    const R s2 = (R)s2d;
+    const R dz = (R)(e.z[iz + 1] - e.z[iz]);
+    const R c1 = (R)e.qc[iz * nr + ir] + s2 * cz1;
+    const R c2 = (R)e.qc[iz * nr + ir + 1] + s2 * cz2;
+    const R dr = (R)(e.qr[ir + 1] - e.qr[ir]);
+    R s1 = (R)(x.x - e.qr[ir]) / dr;
+    s1 = min(s1, (R)1);
+    s1 = max(s1, (R)0);
+    o.c = ((R)1 - s1) * c1 + s1 * c2;
+    const R w2 = s2 / dz;
+    o.ci = ((R)1 - w2) * (R)e.c[2 * iz + 1] + w2 * (R)e.c[2 * iz + 3];
+    const R cz = ((R)1 - s1) * cz1 + s1 * cz2;
+    o.gradc = mk2<R>((c2 - c1) / dr, cz);
+    o.crz = (cz2 - cz1) / dr;
+}
+
 // src/ssp.hpp:53-152,309-375 (1-D profile types evaluated in 2-D). The
 // density (LinInterpDensity) is only used by reflections, so it is evaluated
 // when NEED_RHO is set.
@@ -80,6 +118,10 @@ template<typename R, bool NEED_RHO = false> __device__ __forceinline__ void eval
         o.ci = (R)0;
         o.gradc = mk2<R>((R)0, c0 * u2 * ((R)1 - emxt) * dxt);
         o.czz = c0 * u2 * emxt * dxt * dxt;
+        return;
+    }
+    if(e.ssp_type == SSP_QUAD) {
+        eval_quad(x, t, o, e, s, ctr);
         return;
     }
     update_seg(x.y, t.y >= (R)0, e.z, e.nssp, s.z);
@@ -236,9 +278,13 @@ struct StepGeo {
     }
     __device__ __forceinline__ void seg(bool stepTo, double &h, const BdState &top, const BdState &bot,
                                         V2<double> &x, V2<double> x0, V2<double> u, bool &tr,
-                                        bool &br) const
+                                        bool &br, int ir0) const
     {
         double lmin = max(top.lmin, bot.lmin), lmax = min(top.lmax, bot.lmax);
+        if(e->ssp_type == SSP_QUAD) {          // the quad SSP's range segment bounds the step too
+            lmin = max(lmin, e->qr[ir0]);
+            lmax = min(lmax, e->qr[ir0 + 1]);
+        }
         if(!stepTo) h = 1.7976931348623157e308;
         if(fabs(u.x) > DBL_EPS) {
             if(x.x < lmin) {
@@ -254,18 +300,18 @@ struct StepGeo {
 
 // src/step.hpp:271-342
 __device__ __forceinline__ void reduce_step(
-    const StepGeo &g, V2<double> x0, V2<double> u, int iz0, const BdState &top, const BdState &bot,
+    const StepGeo &g, V2<double> x0, V2<double> u, SegState s0, const BdState &top, const BdState &bot,
     double &h, int &small, RunCounters *ctr)
 {
     double hInt, hB0, hB1, hTop, hBot, hSeg;
     bool dummy;
     V2<double> x = add2(x0, scl2(h, u));
-    g.depth_iface(false, hInt, x, x0, u, iz0);
+    g.depth_iface(false, hInt, x, x0, u, s0.z);
     g.box(false, 0, hB0, x, x0, u);
     g.box(false, 1, hB1, x, x0, u);
     g.topbot(false, hTop, top, x, x0, u, dummy);
     g.topbot(false, hBot, bot, x, x0, u, dummy);
-    g.seg(false, hSeg, top, bot, x, x0, u, dummy, dummy);
+    g.seg(false, hSeg, top, bot, x, x0, u, dummy, dummy, s0.r);
     h = min(min(min(h, hInt), min(min(hB0, hB1), min(hTop, hBot))), hSeg);
     if(h < -1e-4) run_warn(ctr, WARN_STEP_NEGATIVE_H);
     double hmin = INF_STEP * g.e->deltas;
@@ -280,16 +326,16 @@ __device__ __forceinline__ void reduce_step(
 // src/step.hpp:347-424
 __device__ __forceinline__ void step_to_bdry(
     const StepGeo &g, V2<double> x0, V2<double> &x2, V2<double> u, double &h, bool &tr, bool &br,
-    int iz0, const BdState &top, const BdState &bot)
+    SegState s0, const BdState &top, const BdState &bot)
 {
     x2 = add2(x0, scl2(h, u));
-    g.depth_iface(true, h, x2, x0, u, iz0);
+    g.depth_iface(true, h, x2, x0, u, s0.z);
     g.box(true, 0, h, x2, x0, u);
     g.box(true, 1, h, x2, x0, u);
     g.topbot(true, h, top, x2, x0, u, tr);
     g.topbot(true, h, bot, x2, x0, u, br);
     if(br) tr = false;
-    g.seg(true, h, top, bot, x2, x0, u, tr, br);
+    g.seg(true, h, top, bot, x2, x0, u, tr, br, s0.r);
     double hmin = INF_STEP * g.e->deltas;
     if(h < hmin) {
         h = hmin;
@@ -316,7 +362,7 @@ template<typename R> __device__ __forceinline__ void step2d(
     R csq0 = o0.c * o0.c;
     V2<R> u0 = scl2(o0.c, ray0.t);
     double h = e.deltas;
-    reduce_step(g, ray0.x, cvt2<double>(u0), s0.z, top, bot, h, small, ctr);
+    reduce_step(g, ray0.x, cvt2<double>(u0), s0, top, bot, h, small, ctr);
     double halfh = 0.5 * h;
     RayPt<R> ray1;
     ray1.x = add2(ray0.x, scl2(halfh, cvt2<double>(u0)));
@@ -330,11 +376,11 @@ template<typename R> __device__ __forceinline__ void step2d(
     V2<R> pq1p = scl2(-cnn1, ray1.q), pq1q = scl2(o1.c, ray1.p);
     R csq1 = o1.c * o1.c;
     V2<R> u1 = scl2(o1.c, ray1.t);
-    reduce_step(g, ray0.x, cvt2<double>(u1), s0.z, top, bot, h, small, ctr);
+    reduce_step(g, ray0.x, cvt2<double>(u1), s0, top, bot, h, small, ctr);
     double w1 = h / (2.0 * halfh);
     double w0 = 1.0 - w1;
     V2<double> u2 = add2(scl2(w0, cvt2<double>(u0)), scl2(w1, cvt2<double>(u1)));
-    step_to_bdry(g, ray0.x, ray2.x, u2, h, tr, br, s0.z, top, bot);
+    step_to_bdry(g, ray0.x, ray2.x, u2, h, tr, br, s0, top, bot);
     double hw0 = h * w0, hw1 = h * w1;
     ray2.t = sub2(sub2(ray0.t, div2(scl2((R)hw0, o0.gradc), csq0)), div2(scl2((R)hw1, o1.gradc), csq1));
     // travel time in FP64: tau += hw0 / c0 + hw1 / c1 (complex sound speed)
@@ -353,14 +399,82 @@ template<typename R> __device__ __forceinline__ void step2d(
     ray2.nbot = ray0.nbot;
     eval_ssp(ray2.x, ray2.t, o2, e, iSeg, ctr);
     ray2.c = o2.c;
-    if(iSeg.z != s0.z) {
+    if(iSeg.z != s0.z || iSeg.r != s0.r) {
+        // iSeg.r only moves for the quad SSP; a depth crossing takes precedence
         V2<R> gj = sub2(o2.gradc, o0.gradc);
         V2<R> n2 = mk2(-ray2.t.y, ray2.t.x);
         R cnj = dot2(gj, n2), csj = dot2(gj, ray2.t);
-        R rm = ray2.t.x / ray2.t.y;
+        R rm = iSeg.z != s0.z ? ray2.t.x / ray2.t.y : -ray2.t.y / ray2.t.x;
         R rn = rm * ((R)2 * cnj - rm * csj) / ray2.c;
         ray2.p = sub2(ray2.p, scl2(rn, ray2.q));
     }
+}
+
+// InterpolateReflectionCoefficient (src/reflect.hpp:39-92): linear in the
+// angle of incidence theta (deg) between bracketing table rows; zero outside
+// the table (a warning below it). A one-row table matches only its own angle.
+template<typename R> __device__ __forceinline__ void refl_coef(const double *tab, int n, R theta, R &r, R &phi,
+                                                              RunCounters *ctr)
+{
+    if(theta < (R)tab[0]) {
+        r = phi = (R)0;
+        run_warn(ctr, WARN_OUTSIDE_REFLCOEF);
+        return;
+    }
+    if(theta > (R)tab[3 * (n - 1)]) {
+        r = phi = (R)0;
+        return;
+    }
+    if(n < 2) {
+        r = (R)tab[1];
+        phi = (R)tab[2];
+        return;
+    }
+    int il = 0, ir = n - 1;
+    while(ir - il > 1) {
+        int im = (il + ir) >> 1;
+        if((R)tab[3 * im] > theta) ir = im; else il = im;
+    }
+    const R t0 = (R)tab[3 * il], t1 = (R)tab[3 * ir];
+    const R a = (theta - t0) / (t1 - t0);
+    r = ((R)1 - a) * (R)tab[3 * il + 1] + a * (R)tab[3 * ir + 1];
+    phi = ((R)1 - a) * (R)tab[3 * il + 2] + a * (R)tab[3 * ir + 2];
+}
+
+// Beam displacement and width change on a halfspace reflection (RunType(7)
+// 'S'; src/reflect.hpp:383-448, Tindle's formulas as the reference states
+// them): the reflected point moves along the boundary tangent by Re(delta),
+// the travel time grows by Re(delta) cos / c, and q by |d delta| sin c p.
+template<typename R> __device__ __forceinline__ void beam_shift2d(const RayPt<R> &old, RayPt<R> &np,
+                                                                  const HsDev &hs, V2<R> tB, R omega, R c)
+{
+    const Cx<R> cPc = cx<R>((R)hs.cPr, -(R)hs.cPi);                 // conj(cP)
+    const Cx<R> ch = rdivc(old.c, cPc);
+    const R co = old.t.x * old.c, si = old.t.y * old.c;
+    const R ck = omega / old.c;
+    const R rho = (R)hs.rho;
+    const Cx<R> one_m_ch2 = csub(cx<R>((R)1, (R)0), cmul(ch, ch));
+    const Cx<R> a = cscl((R)2 * rho, one_m_ch2);
+    const Cx<R> b = csub(cx<R>(co * co, (R)0), cmul(ch, ch));
+    const Cx<R> d = cadd(cx<R>(rho * rho * si * si, (R)0), b);
+    const Cx<R> sb = csqrt_(b);
+    const R cco = co * co, ssi = si * si;
+    Cx<R> delta = cx<R>((R)0, (R)0);
+    if(fabs(si) >= (R)DBL_EPS)                                     // NotNearlyZero
+        delta = cdiv(cscl(co / si, a), cscl(ck, cmul(sb, d)));
+    const R pdelta = delta.r / (old.c / co);
+    const Cx<R> cksbd = cscl(ck, cmul(sb, d));
+    const Cx<R> t1 = rdivc(cco, cmul(cksbd, b));
+    const Cx<R> t2 = rdivc((R)1 + cco / ssi, cksbd);
+    const Cx<R> t3 = rdivc((R)2 * co * co * (rho * rho - (R)1), cmul(cksbd, d));
+    const Cx<R> dd = cmul(a, csub(csub(t1, t2), t3));
+    const R rdd = -dd.r;
+    const R sdd = rdd / fabs(rdd);
+    const R theta_bot = atan(tB.y / tB.x);
+    np.x.x = np.x.x + (double)(delta.r * cos(theta_bot));
+    np.x.y = np.x.y + (double)(delta.r * sin(theta_bot));
+    np.taur = np.taur + (double)pdelta;
+    np.q = add2(np.q, scl2(sdd * rdd * si * c, old.p));
 }
 
 // src/reflect.hpp:125-452 (2-D branch)
@@ -398,6 +512,14 @@ template<typename R> __device__ __forceinline__ void reflect2d(
     } else if(hs.bc == 'V') {
         np.Amp = old.Amp;
         np.Phase = old.Phase + (R)BHCB_PI;
+    } else if(hs.bc == 'F') {
+        // angle of incidence from the boundary normal, folded about 90 deg
+        R theta = (R)(180.0 / BHCB_PI) * fabs(atan2(Th, Tg));
+        if(theta > (R)90) theta = (R)180 - theta;
+        R rc, ph;
+        refl_coef(istop ? e.trc : e.brc, istop ? e.ntrc : e.nbrc, theta, rc, ph, ctr);
+        np.Amp = old.Amp * rc;
+        np.Phase = old.Phase + ph;
     } else if(hs.bc == 'A' || hs.bc == 'G') {
         R omega = (R)(2.0 * BHCB_PI * e.freq0);
         Cx<R> kx = cx<R>(omega * Tg, (R)0), kz = cx<R>(omega * Th, (R)0);
@@ -434,6 +556,7 @@ template<typename R> __device__ __forceinline__ void reflect2d(
         } else {
             np.Amp = ar * old.Amp;
             np.Phase = old.Phase + atan2(Refl.i, Refl.r);
+            if(e.beam_shift) beam_shift2d(old, np, hs, tB, omega, c);
         }
     } else {
         run_error(ctr, ERR_BOUNDARY_CONDITION_TYPE);

@@ -619,6 +619,13 @@ __device__ __forceinline__ void reflect3d(const Ray3 &old, Ray3 &np, const HsDev
     } else if(hs.bc == 'V') {
         np.Amp = old.Amp;
         np.Phase = old.Phase + BHCB_PI;
+    } else if(hs.bc == 'F') {
+        double theta = (180.0 / BHCB_PI) * fabs(atan2(Th, Tg));
+        if(theta > 90.0) theta = 180.0 - theta;
+        double rc, ph;
+        refl_coef(istop ? E.e1d.trc : E.e1d.brc, istop ? E.e1d.ntrc : E.e1d.nbrc, theta, rc, ph, ctr);
+        np.Amp = old.Amp * rc;
+        np.Phase = old.Phase + ph;
     } else if(hs.bc == 'A' || hs.bc == 'G') {
         const double omega = FLTD(2.0) * BHCB_PI * E.freq0;
         const double gk = omega * Tg;

@@ -133,6 +133,14 @@ def seamount3d_eig_hat():
     return f
 
 
+def munk3d_brc_gauss():
+    """Munk slice over a tabulated bottom reflection coefficient (.brc)."""
+    from cases2d_ext import rayleigh_table
+    f = _munk_slice("CB   3", bot=("F",))
+    f[".brc"] = rayleigh_table(1551.91, 1600.0, 1.8, 0.8, np.arange(0.0, 90.1, 2.0))
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -147,4 +155,5 @@ CASES3D = {
     "parabot3d_arr_hat": parabot3d_arr_hat,
     "munk3d_eig_gauss": munk3d_eig_gauss,
     "seamount3d_eig_hat": seamount3d_eig_hat,
+    "munk3d_brc_gauss": munk3d_brc_gauss,
 }

@@ -1,8 +1,9 @@
 """Generate the ray-trajectory fixtures (.ray) from the reference itself.
 
 Runs the reference's own bellhopcxx (compiled from its sources by
-oracle/Makefile into oracle/_ref/) single-threaded on a ray run ('R') and an
-eigenray run ('E') of the Munk and range-dependent workloads and stores the
+oracle/Makefile into oracle/_ref/) single-threaded on ray runs ('R') and
+eigenray runs ('E') of the Munk and range-dependent workloads, a quad-SSP case
+and a beam-shift case, and stores the
 input files and the trajectories as tests/golden/rays_<case>.npz. Run from the
 repository root:
 
@@ -42,20 +43,39 @@ def cases():
     rd_e.rz = (800.0, 2000.0)
     rd_e.rr_km = (30.0, 60.0)
     rd_e.run_type = "EB RR "
-    return {"munk_ray": munk_r, "rd_ray": rd_r, "munk_eigen": munk_e, "rd_eigen": rd_e}
+    sys.path.insert(0, HERE)
+    from cases2d_ext import CASES2D_EXT
+    quad_r = CASES2D_EXT["x2d_quad_shallow_bty"]()
+    quad_r[".env"] = quad_r[".env"].replace("'CG RR'", "'R'").replace("\n401\n", "\n41\n")
+    shift_r = CASES2D_EXT["x2d_beam_shift_shallow"]()
+    shift_r[".env"] = shift_r[".env"].replace("'CB RR S'", "'RB RR S'").replace("\n301\n", "\n31\n")
+    return {"munk_ray": munk_r, "rd_ray": rd_r, "munk_eigen": munk_e, "rd_eigen": rd_e,
+            "quad_ray": quad_r, "beam_shift_ray": shift_r}
 
 
-def main():
+def write_files(files, root):
+    for suffix, text in files.items():
+        with open(root + suffix, "w") as f:
+            f.write(text)
+    return root
+
+
+def main(names=None):
     with tempfile.TemporaryDirectory() as d:
         for name, spec in cases().items():
-            root = write_env(spec, os.path.join(d, name))
+            if names and name not in names:
+                continue
+            if isinstance(spec, dict):     # input files as text (tests/golden/cases2d_ext.py)
+                root = write_files(spec, os.path.join(d, name))
+            else:
+                root = write_env(spec, os.path.join(d, name))
             r = subprocess.run([EXE, "-2", "-1", root], capture_output=True, text=True)
             if r.returncode != 0:
                 raise SystemExit("reference failed on %s:\n%s" % (name, r.stdout[-2000:]))
             R = read_ray(root + ".ray")
             npts = np.array([len(x["xy"]) for x in R["rays"]], np.int32)
             files = {}
-            for ext in (".env", ".bty", ".ati", ".ssp", ".sbp"):
+            for ext in (".env", ".bty", ".ati", ".ssp", ".sbp", ".brc", ".trc"):
                 if os.path.exists(root + ext):
                     files["file_" + ext[1:]] = np.array(open(root + ext).read())
             np.savez_compressed(os.path.join(HERE, "rays_" + name + ".npz"),
@@ -67,4 +87,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -122,7 +122,8 @@ REFERENCE_INPUTS = "/root/reference/test/in"
 
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INPUTS), reason="reference inputs not present")
-@pytest.mark.parametrize("name", ["Munk", "MunkB_Coh", "MunkB_gb", "DickinsB", "DickinsFlatB", "free"])
+@pytest.mark.parametrize("name", ["Munk", "MunkB_Coh", "MunkB_gb", "DickinsB", "DickinsFlatB", "free",
+                                  "GulfB_rd_gb"])
 def test_reader_accepts_reference_inputs(name, workdir):
     src = os.path.join(REFERENCE_INPUTS, name)
     if not os.path.exists(src + ".env"):
@@ -135,6 +136,48 @@ def test_reader_accepts_reference_inputs(name, workdir):
         B.check_env(os.path.join(workdir, name))
     except B.BhcbError as e:
         assert "not supported" in str(e) or "not a field mode" in str(e), str(e)
+
+
+# ------------------------------------- 2-D options pinned by reference fixtures
+GOLD2D_EXT = sorted(n[:-4] for n in os.listdir(os.path.join(HERE, "golden")) if n.startswith("x2d_")
+                    and n.endswith(".npz"))
+
+
+def write_fixture_files(npz, root):
+    for k in npz.files:
+        if k.startswith("file_"):
+            with open(root + "." + k[5:], "w") as f:
+                f.write(str(npz[k]))
+
+
+@pytest.mark.parametrize("name", GOLD2D_EXT)
+def test_reader2d_ext_sizes_match_reference_fixture(name, workdir):
+    """The reader accepts the option (quad SSP, ...) and sees the grid the
+    reference wrote in its .shd."""
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    root = os.path.join(workdir, name)
+    write_fixture_files(g, root)
+    info = B.check_env(root)
+    nsz, nrz, nrr = g["field"].shape
+    assert (info["nsz"], info["nrz"], info["nrr"]) == (nsz, nrz, nrr)
+    assert info["nalpha"] > 0
+
+
+def test_reader_rejects_bad_quad_ssp(workdir):
+    from cases2d_ext import CASES2D_EXT
+    files = CASES2D_EXT["x2d_quad_munk_gauss"]()
+    root = os.path.join(workdir, "badquad")
+    with open(root + ".env", "w") as f:
+        f.write(files[".env"])
+    with pytest.raises(B.BhcbError, match="quad SSP"):
+        B.check_env(root)                     # no .ssp file
+    lines = files[".ssp"].splitlines()
+    r = lines[1].split()
+    lines[1] = " ".join([r[1], r[0]] + r[2:])
+    with open(root + ".ssp", "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with pytest.raises(B.BhcbError, match="monotone"):
+        B.check_env(root)
 
 
 # ------------------------------------------------------------------ 3-D reader
