@@ -30,7 +30,8 @@ FLAG_SERIAL_INFLUENCE = 1   # BHCB_FLAG_SERIAL_INFLUENCE
 ERR_NAMES = {
     2: "BHC_ERR_RAYINIT", 3: "BHC_ERR_BOUNDARY_SEG_CONTAINS_NAN",
     4: "BHC_ERR_BOUNDARY_CONDITION_TYPE", 5: "BHC_ERR_INVALID_SSP_TYPE",
-    6: "BHC_ERR_OUTSIDE_ALTIMETRY", 7: "BHC_ERR_OUTSIDE_BATHYMETRY", 31: "segment buffer overflow",
+    6: "BHC_ERR_OUTSIDE_ALTIMETRY", 7: "BHC_ERR_OUTSIDE_BATHYMETRY", 8: "BHC_ERR_OUTSIDE_SSP",
+    9: "BHC_ERR_QUAD_ISEG", 31: "segment buffer overflow",
 }
 
 
@@ -371,16 +372,17 @@ class Tracer:
             raise BhcbError(rc, msg.value.decode(errors="replace"))
         return FieldGraph(self._lib, g)
 
-    def rays(self, env: int = 0, ifreq: int = 0) -> List[dict]:
+    def rays(self, env: int = 0, ifreq: int = 0, dim: int = 2) -> List[dict]:
         """Ray trajectories of a ray run ('R') or the eigenrays of an eigen run
-        ('E'): one dict per ray with alpha (deg), ntop, nbot and rz (n x 2, m)."""
+        ('E'): one dict per ray with alpha (deg), ntop, nbot and rz (n x 2,
+        m; dim=3 for 3-D contexts: n x 3 points x, y, z)."""
         nr, npnt = C.c_int64(), C.c_int64()
         self._check(self._lib.bhcb_rays_shape(self._h, env, ifreq, C.byref(nr), C.byref(npnt)))
         n, m = nr.value, npnt.value
         npts = np.zeros(max(n, 1), np.int32)
         bnc = np.zeros(2 * max(n, 1), np.int32)
         alpha = np.zeros(max(n, 1))
-        rz = np.zeros((max(m, 1), 2))
+        rz = np.zeros((max(m, 1), dim))
         self._check(self._lib.bhcb_copy_rays(self._h, env, ifreq, npts.ctypes.data, bnc.ctypes.data,
                                              alpha.ctypes.data, rz.ctypes.data, rz.nbytes))
         out, o = [], 0

@@ -47,6 +47,24 @@ cudaError_t launch_rays(const GroupDev *, int, const long long *, const int *, i
                         int *, RunCounters *, bool, int, cudaStream_t);
 cudaError_t launch_eigen_emit(const uint32_t *, const ArrCand *, unsigned long long, EigenHitRec *, int32_t *, int,
                               const uint64_t *, int, cudaStream_t);
+cudaError_t launch_trace_x(const GroupDev *, int, long long, XSeg *, unsigned long long, RunCounters *,
+                           unsigned long long *, int, int, int, cudaStream_t);
+cudaError_t launch_influence_x(const XSeg *, unsigned long long, const GroupDev *, int, const double *, float2 *,
+                               RunCounters *, int, int, int, cudaStream_t);
+cudaError_t launch_scale_x(const float2 *, float2 *, const GroupDev *, int, const double *, RunCounters *, int,
+                           cudaStream_t);
+
+// influence type of Beam->Type[0] (src/runtype.hpp:150-186)
+int infl_kind_of(char bt)
+{
+    switch(bt) {
+    case 'g': case 'b': return INFL_GEO_RAYCEN;
+    case 'R': return INFL_CERV_RAYCEN;
+    case 'C': return INFL_CERV_CART;
+    case 'S': return INFL_SGB;
+    default: return INFL_GEO_CART;
+    }
+}
 } // namespace bhcb
 
 using namespace bhcb;
@@ -130,6 +148,7 @@ struct bhcb_ctx {
     unsigned long long seg_cap = 0;
     bool any_gauss = false, any_coherent = false, mixed_types = false;
     bool gauss = false, coherent = true;
+    int xkind = INFL_GEO_CART;       // InflKind of the batch
 
     DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
     unsigned long long job0_h = 0;   // staging for the job counter's start value
@@ -282,6 +301,11 @@ void do_prepare(bhcb_ctx *c)
     }
     // one launch handles a single influence flavour; mixed batches are split by the caller
     c->gauss = c->envs[0].tables[0].beam_type[0] == 'B';
+    c->xkind = infl_kind_of(c->envs[0].tables[0].beam_type[0]);
+    for(auto &S : c->envs)
+        if(infl_kind_of(S.tables[0].beam_type[0]) != c->xkind
+           || (c->xkind && S.tables[0].beam_type[0] != c->envs[0].tables[0].beam_type[0]))
+            throw std::runtime_error("a batch must use one beam type");
     c->coherent = c->envs[0].tables[0].run_type[0] == 'C';
     for(auto &S : c->envs) {
         const EnvTables &T0 = S.tables[0];
@@ -315,6 +339,15 @@ void do_prepare(bhcb_ctx *c)
         d.ntrc = (int)(T.trc.size() / 3);
         d.nbrc = (int)(T.brc.size() / 3);
         d.beam_shift = T.beam_type[3] == 'S';
+        d.infl_kind = infl_kind_of(T.beam_type[0]);
+        d.beam1 = T.beam_type[1];
+        d.nimage = T.nimage;
+        d.ibeam_window = T.ibeam_window;
+        d.component = T.component;
+        d.eps_mult = T.eps_mult;
+        d.rloop = T.rloop;
+        d.top_depth = T.top_depth;
+        d.bot_depth = T.bot_depth;
         d.top = T.top;
         d.bot = T.bot;
         d.ntop = (int)T.btop.size();
@@ -336,7 +369,7 @@ void do_prepare(bhcb_ctx *c)
         d.run0 = T.run_type[0];
         d.beam0 = T.beam_type[0];
         d.beam2 = T.beam_type[2];
-        d.gaussian = T.beam_type[0] == 'B';
+        d.gaussian = T.beam_type[0] == 'B' || T.beam_type[0] == 'b';   // IsGaussianGeomInfl
         d.coherent = T.run_type[0] == 'C';
         d.line_source = T.run_type[3] == 'X';
         d.irregular = T.run_type[4] == 'I';
@@ -415,7 +448,7 @@ void do_prepare(bhcb_ctx *c)
         return;
     }
     // segment buffer: grows on overflow
-    size_t rec = seg_record_bytes(fp64);
+    size_t rec = c->xkind ? sizeof(XSeg) : seg_record_bytes(fp64);
     size_t budget = c->max_memory > 2 * fbytes + abytes ? c->max_memory - 2 * fbytes - abytes : 0;
     unsigned long long want = std::max<unsigned long long>(c->seg_cap, (unsigned long long)c->njobs * 1024ull);
     unsigned long long maxcap = budget / rec;
@@ -451,6 +484,26 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         CK(cudaMemsetAsync((float2 *)c->acc.p + a0, 0, (size_t)(a1 - a0) * sizeof(float2), c->stream));
     }
     CK(cudaEventRecord(c->ev[0], c->stream));
+    if(c->xkind) {
+        // ray-centred / Cerveny / simple Gaussian beams: FP64 trace with the
+        // kind's influence prologue, then its influence kernel and scaling
+        const GroupDev *Gx = (const GroupDev *)c->groups_d.p + g0;
+        const int ngx = g1 - g0;
+        long long xgrid = std::min<long long>((job1 - job0 + 63) / 64, (long long)c->sm_count * 16);
+        CK(launch_trace_x(Gx, ngx, job1, (XSeg *)c->segs.p, c->seg_cap, ctr, jobc, c->xkind, (int)std::max(1LL, xgrid),
+                          64, c->stream));
+        CK(cudaEventRecord(c->ev[1], c->stream));
+        c->last_overlapped = false;
+        int nzmax = 1;   // receiver depths per range, the most of the launched groups
+        for(int g = g0; g < g1; ++g) nzmax = std::max(nzmax, c->fields[c->groups_h[g].field_index].nrzp);
+        CK(launch_influence_x((const XSeg *)c->segs.p, c->seg_cap, Gx, ngx, (const double *)c->freqs_d.p,
+                              (float2 *)c->acc.p, ctr, c->xkind, nzmax, c->sm_count * 16, c->stream));
+        CK(cudaEventRecord(c->ev[2], c->stream));
+        CK(launch_scale_x((const float2 *)c->acc.p, (float2 *)c->out.p, Gx, ngx, (const double *)c->freqs_d.p, ctr,
+                          c->sm_count * 2, c->stream));
+        CK(cudaEventRecord(c->ev[3], c->stream));
+        return;
+    }
     int tblock = c->trace_block;
     long long tgrid = std::min<long long>((job1 - job0 + tblock - 1) / tblock, (long long)c->sm_count * 16);
     if(tgrid < 1) tgrid = 1;
@@ -849,7 +902,7 @@ int run_checked(bhcb_ctx *c)
         do_sync(c);
         if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
             // grow the segment buffer and run again
-            size_t rec = seg_record_bytes(c->precision == BHCB_PREC_FP64);
+            size_t rec = c->xkind ? sizeof(XSeg) : seg_record_bytes(c->precision == BHCB_PREC_FP64);
             size_t fbytes = (size_t)c->total_field * sizeof(float2);
             size_t abytes = (size_t)c->total_acc * sizeof(float2);
             size_t budget = c->max_memory > 2 * fbytes + abytes ? c->max_memory - 2 * fbytes - abytes : 0;
@@ -888,6 +941,7 @@ namespace bhcb {
 int noalloc_job_from_ctx(bhcb_ctx *c, int32_t env, int32_t ifreq, NoAllocJob *job, const char **why)
 {
     if(!c->prepared) { *why = "context not prepared: call bhcb_prepare (or bhcb_run) first"; return BHCB_ERR_STATE; }
+    if(c->xkind) { *why = "this entry point covers geometric Cartesian beams ('G', 'B')"; return BHCB_ERR_ARG; }
     if(env < 0 || env >= (int)c->envs.size()) { *why = "env_index out of range"; return BHCB_ERR_ARG; }
     const EnvSlot &S = c->envs[env];
     if(ifreq < 0 || ifreq >= (int)S.field_of_freq.size()) { *why = "ifreq out of range"; return BHCB_ERR_ARG; }
@@ -1441,7 +1495,16 @@ int bhcb_grid3d(bhcb_ctx *c, int32_t env, double *sx, double *sy, float *sz, dou
 int bhcb_rays_shape(bhcb_ctx *c, int32_t env, int32_t ifreq, int64_t *nrays, int64_t *npoints)
 {
     return guarded(c, [&]() -> int {
-        if(c->is3d() || (c->mode != MODE_RAY && c->mode != MODE_EIGEN))
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            if(c->r3_status != BHCB_OK) throw StateError("no 3-D run");
+            int64_t nr = 0, np = 0;
+            run3_rays_shape(c->r3, env, c->stream, nr, np);
+            if(nrays) *nrays = nr;
+            if(npoints) *npoints = np;
+            return BHCB_OK;
+        }
+        if(c->mode != MODE_RAY && c->mode != MODE_EIGEN)
             throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E')");
         const Field *F = find_field(c, env, ifreq);
         const int fi = (int)(F - c->fields.data());
@@ -1457,7 +1520,13 @@ int bhcb_copy_rays(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *npts, int32
                    double *rz, size_t rz_bytes)
 {
     return guarded(c, [&]() -> int {
-        if(c->is3d() || (c->mode != MODE_RAY && c->mode != MODE_EIGEN))
+        if(c->is3d()) {
+            if(ifreq != 0) throw std::invalid_argument("3-D runs have one frequency (ifreq 0)");
+            if(c->r3_status != BHCB_OK) throw StateError("no 3-D run");
+            run3_copy_rays(c->r3, env, c->stream, npts, bounces, alpha_deg, rz, rz_bytes);
+            return BHCB_OK;
+        }
+        if(c->mode != MODE_RAY && c->mode != MODE_EIGEN)
             throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E')");
         const Field *F = find_field(c, env, ifreq);
         const int fi = (int)(F - c->fields.data());
@@ -1478,6 +1547,7 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         if(c->is3d()) throw StateError("the autotuner covers the 2-D TL runs");
         if(!c->prepared) do_prepare(c);
         if(c->mode != MODE_TL) throw StateError("the autotuner covers TL runs");
+        if(c->xkind) throw StateError("the autotuner covers geometric Cartesian beams ('G', 'B')");
         const int reps = std::max(1, std::min<int>(repeats, 16));
         const bool overlap = c->overlap;
         c->overlap = false;   // time the trace and the influence separately

@@ -19,6 +19,8 @@
 
 namespace bhcb {
 
+cudaError_t launch_rays3d(const GroupDev *, int, const long long *, const int *, int, const long long *, double *,
+                          int *, int *, RunCounters *, bool, int, cudaStream_t);
 cudaError_t launch_trace3d(const GroupDev *, int, long long, SegRec3 *, unsigned long long, RunCounters *,
                            unsigned long long *, int, cudaStream_t);
 cudaError_t launch_influence3d(const SegRec3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
@@ -43,6 +45,17 @@ struct Env3Slot {
     Env3Tables T;
     int64_t field_base = 0, field_n = 0;
 };
+
+// Trajectories of listed rays of one environment (RunType 'R': all of them;
+// 'E': the hit rays, each up to its hit step)
+struct RaySet3 {
+    bool valid = false;
+    std::vector<long long> jobs;
+    std::vector<int> limits, npts, bnc;   // bnc: top, bottom bounces of the last point
+    std::vector<long long> off;
+    std::vector<double> alpha_deg;        // take-off declination (SrcDeclAngle)
+    std::vector<double> xyz;              // 3 doubles per point
+};
 } // namespace
 
 struct Run3 {
@@ -62,6 +75,10 @@ struct Run3 {
     uint64_t max_memory = 16ull << 30;
     ArrKeyBits kb{};
     DevBuf narr_d, arr_d, cand, keys0, keys1, vals0, vals1, hist;
+    // ray runs ('R'), and the eigenray re-trace of 'E' runs
+    bool rayrun = false;
+    std::vector<RaySet3> raysets;     // per environment
+    int sm_count = 148;
 };
 
 Run3 *run3_new() { return new Run3(); }
@@ -211,13 +228,16 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
                        cudaMemcpyHostToDevice, st));
     r->counters.ensure(sizeof(RunCounters) + 64);
     // one run type per batch: TL ('C', 'S', 'I'), arrivals ('A', 'a') or eigen hits ('E')
-    auto kind = [](char t) { return (t == 'A' || t == 'a') ? 1 : (t == 'E' ? 2 : 0); };
+    auto kind = [](char t) { return (t == 'A' || t == 'a') ? 1 : (t == 'E' ? 2 : (t == 'R' ? 3 : 0)); };
     const int k0 = kind(r->envs[0].T.run_type[0]);
     r->arrivals = k0 == 1;
     r->eigen = k0 == 2;
+    r->rayrun = k0 == 3;
+    r->raysets.assign(r->envs.size(), RaySet3{});
     for(const auto &S : r->envs)
         if(kind(S.T.run_type[0]) != k0) throw std::runtime_error("a 3-D batch must use one run type");
     auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
+    if(r->rayrun) return;   // trajectories only: no segments, fields or arrivals
     if(r->eigen) {
         // ordering key (low to high): depth | bearing | walk position | step | ray | trace group
         int mz = 1, mt = 1, mr = 1, mj = 1;
@@ -463,6 +483,65 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
 
 } // namespace
 
+namespace {
+// take-off declination (deg) of the local ray index of environment S
+// (GetJobIndices, src/common.hpp:365-391: ialpha fastest)
+double alpha_deg_of(const Env3Tables &T, int local)
+{
+    const int ialpha = T.isingle_alpha >= 1 ? T.isingle_alpha - 1 : local % (int)T.alpha.size();
+    return (180.0 / M_PI) * T.alpha[ialpha];
+}
+
+// Trajectories of R.jobs (limits as for the ray kernel): a count pass sizes the
+// point buffer exactly, a second pass of the same deterministic trace writes
+// the points. Returns the tracer's error bits.
+uint32_t trace_rays3(Run3 *r, RaySet3 &R, cudaStream_t st, uint32_t &warn_bits)
+{
+    const int n = (int)R.jobs.size();
+    R.npts.assign(n, 0);
+    R.bnc.assign(2 * (size_t)n, 0);
+    R.off.assign(n, 0);
+    R.xyz.clear();
+    R.valid = true;
+    if(n == 0) return 0;
+    DevBuf jobs_d, lim_d, npts_d, bnc_d, off_d, pts_d;
+    jobs_d.ensure(n * sizeof(long long));
+    lim_d.ensure(n * sizeof(int));
+    npts_d.ensure(n * sizeof(int));
+    bnc_d.ensure(2 * (size_t)n * sizeof(int));
+    off_d.ensure(n * sizeof(long long));
+    RunCounters *ctr = (RunCounters *)r->counters.p;
+    const GroupDev *G = (const GroupDev *)r->groups_d.p;
+    const int ng = (int)r->groups_h.size();
+    CK(cudaMemcpyAsync(jobs_d.p, R.jobs.data(), n * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(lim_d.p, R.limits.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctr, 0, sizeof(RunCounters), st));
+    CK(launch_rays3d(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, nullptr, nullptr, (int *)npts_d.p,
+                     (int *)bnc_d.p, ctr, true, r->sm_count, st));
+    CK(cudaMemcpyAsync(R.npts.data(), npts_d.p, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(R.bnc.data(), bnc_d.p, 2 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    RunCounters rc{};
+    CK(cudaMemcpyAsync(&rc, ctr, sizeof rc, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    warn_bits |= rc.warn_bits;
+    if(rc.err_bits) return rc.err_bits;
+    long long tot = 0;
+    for(int i = 0; i < n; ++i) {
+        R.off[i] = tot;
+        tot += R.npts[i];
+    }
+    if((uint64_t)tot * 3 * sizeof(double) > r->max_memory) throw MemError("ray points exceed max_memory");
+    pts_d.ensure(std::max<long long>(tot, 1) * 3 * sizeof(double));
+    CK(cudaMemcpyAsync(off_d.p, R.off.data(), n * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(launch_rays3d(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, (const long long *)off_d.p,
+                     (double *)pts_d.p, (int *)npts_d.p, (int *)bnc_d.p, ctr, false, r->sm_count, st));
+    R.xyz.resize(3 * (size_t)tot);
+    if(tot) CK(cudaMemcpyAsync(R.xyz.data(), pts_d.p, tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+} // namespace
+
 uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, int32_t opt_max_narr,
                   int32_t allow_merging, bhcb_stats &stats, uint32_t &warn_bits)
 {
@@ -471,7 +550,32 @@ uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, i
     r->max_memory = max_memory;
     r->opt_max_narr = opt_max_narr;
     r->allow_merging = allow_merging;
+    r->sm_count = sm_count;
     prepare3(r, st, h2d);
+    if(r->rayrun) {   // RunRayMode (src/mode/ray.cpp:163-198): every ray of every environment
+        stats = bhcb_stats{};
+        warn_bits = 0;
+        uint32_t eb = 0;
+        for(size_t i = 0; i < r->envs.size() && !eb; ++i) {
+            const GroupDev &G = r->groups_h[i];
+            RaySet3 &R = r->raysets[i];
+            R = RaySet3{};
+            for(int local = 0; local < G.njobs; ++local) {
+                R.jobs.push_back(G.job_base + local);
+                R.limits.push_back(-1);
+                R.alpha_deg.push_back(alpha_deg_of(r->envs[i].T, local));
+            }
+            eb = trace_rays3(r, R, st, warn_bits);
+        }
+        r->ran = eb == 0;
+        stats.rays = (uint64_t)r->njobs;
+        stats.groups = stats.fields = (int32_t)r->envs.size();
+        stats.err_bits = eb;
+        stats.warn_bits = warn_bits;
+        stats.h2d_bytes = h2d;
+        stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return eb;
+    }
     const bool tl = !r->arrivals && !r->eigen;
     if(tl) CK(cudaMemsetAsync(r->field.p, 0, std::max<int64_t>(r->total_field, 1) * sizeof(float2), st));
     RangeStats acc;
@@ -523,7 +627,8 @@ static const Env3Slot &ran_env(const Run3 *r, int env)
 void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
-    if(r->arrivals || r->eigen) throw StateError("not a TL run: use bhcb_copy_arrivals / bhcb_eigen_hits");
+    if(r->arrivals || r->eigen || r->rayrun)
+        throw StateError("not a TL run: use bhcb_copy_arrivals / bhcb_eigen_hits / bhcb_copy_rays");
     const size_t need = (size_t)S.field_n * sizeof(float2);
     if(!dst || bytes < need) throw std::invalid_argument("destination too small");
     CK(cudaMemcpyAsync(dst, (float2 *)r->field.p + S.field_base, need, cudaMemcpyDeviceToHost, st));
@@ -533,7 +638,7 @@ void run3_copy_field(Run3 *r, int env, void *dst, size_t bytes, cudaStream_t st)
 void *run3_field_device(Run3 *r, int env)
 {
     const Env3Slot &S = ran_env(r, env);
-    if(r->arrivals || r->eigen) throw StateError("not a TL run");
+    if(r->arrivals || r->eigen || r->rayrun) throw StateError("not a TL run");
     return (float2 *)r->field.p + S.field_base;
 }
 
@@ -668,10 +773,99 @@ static void write_arrivals3(Run3 *r, const Env3Slot &S, const std::string &path,
 }
 
 // .shd, 3-D: WriteHeader and WriteOutTL (src/mode/tl.cpp:38-101, 195-248)
+bool run3_has_rays(const Run3 *r) { return r->rayrun || r->eigen; }
+
+// RunType 'R': the traced rays; 'E': the hit rays re-traced up to their hit
+// (EigenModePostWorker, src/mode/eigen.cpp:24-45) on first use, in hit order
+static const RaySet3 &rays_of_env(Run3 *r, int env, cudaStream_t st)
+{
+    const Env3Slot &S = ran_env(r, env);
+    if(!r->rayrun && !r->eigen) throw StateError("rays exist for ray runs ('R') and eigen runs ('E')");
+    RaySet3 &R = r->raysets[env];
+    if(R.valid) return R;
+    if(r->rayrun) throw StateError("no rays: run first");
+    const Env3Tables &T = S.T;
+    const GroupDev &G = r->groups_h[env];
+    const int nal = T.isingle_alpha >= 1 ? 1 : (int)T.alpha.size();
+    const int nbe = T.isingle_beta >= 1 ? 1 : (int)T.beta.size();
+    const int nsx = (int)T.sx.size(), nsy = (int)T.sy.size();
+    for(size_t k = 0; k < r->hits_h.size(); ++k) {
+        if(r->hit_group[k] != env) continue;
+        const EigenHitRec &h = r->hits_h[k];
+        const int ia = T.isingle_alpha >= 1 ? 0 : h.ialpha;
+        const int ib = T.isingle_beta >= 1 ? 0 : h.ibeta;
+        const long long local = ((((long long)h.isz * nsx + h.isx) * nsy + h.isy) * nbe + ib) * nal + ia;
+        R.jobs.push_back(G.job_base + local);
+        R.limits.push_back(h.is);
+        R.alpha_deg.push_back((180.0 / M_PI) * T.alpha[h.ialpha]);
+    }
+    uint32_t wb = 0;
+    const uint32_t eb = trace_rays3(r, R, st, wb);
+    if(eb) {
+        R.valid = false;
+        char b[96];
+        snprintf(b, sizeof b, "tracer error bits 0x%x while re-tracing eigenrays", eb);
+        throw std::runtime_error(b);
+    }
+    return R;
+}
+
+void run3_rays_shape(Run3 *r, int env, cudaStream_t st, int64_t &nrays, int64_t &npoints)
+{
+    const RaySet3 &R = rays_of_env(r, env, st);
+    nrays = (int64_t)R.jobs.size();
+    npoints = (int64_t)(R.xyz.size() / 3);
+}
+
+void run3_copy_rays(Run3 *r, int env, cudaStream_t st, int32_t *npts, int32_t *bounces, double *alpha_deg,
+                    double *xyz, size_t xyz_bytes)
+{
+    const RaySet3 &R = rays_of_env(r, env, st);
+    if(xyz && xyz_bytes < R.xyz.size() * sizeof(double)) throw std::invalid_argument("point buffer too small");
+    if(npts) std::memcpy(npts, R.npts.data(), R.npts.size() * sizeof(int32_t));
+    if(bounces) std::memcpy(bounces, R.bnc.data(), R.bnc.size() * sizeof(int32_t));
+    if(alpha_deg) std::memcpy(alpha_deg, R.alpha_deg.data(), R.alpha_deg.size() * sizeof(double));
+    if(xyz && !R.xyz.empty()) std::memcpy(xyz, R.xyz.data(), R.xyz.size() * sizeof(double));
+}
+
+// .ray file, 3-D (OpenRAYFile / WriteRay, src/mode/ray.hpp:176-247): take-off
+// angles in radians, points (x, y, z)
+static void write_rays3(Run3 *r, int env, const std::string &path, cudaStream_t st)
+{
+    const Env3Slot &S = r->envs[env];
+    const RaySet3 &R = rays_of_env(r, env, st);
+    const Env3Tables &T = S.T;
+    std::ofstream o(path);
+    if(!o.good()) throw std::runtime_error("cannot open " + path);
+    char b[160];
+    o << "'" << S.in.title << "'\n";
+    snprintf(b, sizeof b, "%.17g\n", T.freq0);
+    o << b;
+    o << T.sx.size() << " " << T.sy.size() << " " << T.sz.size() << "\n";
+    o << T.alpha.size() << " " << T.beta.size() << "\n";
+    snprintf(b, sizeof b, "%.17g\n%.17g\n", S.in.ssp_z.empty() ? 0.0 : S.in.ssp_z[0], S.in.bot_depth);
+    o << b;
+    o << "'xyz'\n";
+    for(size_t i = 0; i < R.jobs.size(); ++i) {
+        if(R.npts[i] <= 0) continue;
+        snprintf(b, sizeof b, "%.17g\n", R.alpha_deg[i] * (M_PI / 180.0));
+        o << b;
+        o << R.npts[i] << " " << R.bnc[2 * i] << " " << R.bnc[2 * i + 1] << "\n";
+        for(int k = 0; k < R.npts[i]; ++k) {
+            const double *q = &R.xyz[3 * (R.off[i] + k)];
+            snprintf(b, sizeof b, "%.17g %.17g %.17g\n", q[0], q[1], q[2]);
+            o << b;
+        }
+    }
+}
+
 void run3_writeout(Run3 *r, int env, const std::string &root, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
-    if(r->eigen) throw StateError("3-D eigenray .ray output (re-trace of the hit rays) is not built; use bhcb_eigen_hits");
+    if(r->eigen || r->rayrun) {
+        write_rays3(r, env, root + ".ray", st);
+        return;
+    }
     if(r->arrivals) {
         write_arrivals3(r, S, root + ".arr", st);
         return;

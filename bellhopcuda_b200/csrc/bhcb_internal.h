@@ -27,7 +27,8 @@ enum : uint32_t {
 };
 enum : uint32_t {
     WARN_ONERAY_OUTOFMEMORY = 1, WARN_TOO_FEW_BEAMS = 3, WARN_SOURCE_OUTSIDE_BOUNDARIES = 4,
-    WARN_OUTSIDE_REFLCOEF = 5,
+    WARN_UNBOUNDED_BEAM = 2, WARN_OUTSIDE_REFLCOEF = 5, WARN_CERVENY_WIDTH_BUGGY = 12,
+    WARN_INVALID_WIDTH_BUGGY = 13,
     WARN_OUTSIDE_ALTIMETRY = 6, WARN_OUTSIDE_BATHYMETRY = 7,
     WARN_STEP_NEGATIVE_H = 8, WARN_TRIDIAG_H_NEGATIVE = 9, WARN_TRIDIAG_H_GROWING = 10,
     WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17,
@@ -61,7 +62,13 @@ struct EnvDev {
     int32_t ntrc, nbrc;
     const double *trc, *brc;
     int32_t beam_shift;              // Beam->Type[3] == 'S' (src/reflect.hpp:383-448)
-    int32_t pad_s;
+    // influence type other than geometric Cartesian (INFL_*), and the Cerveny
+    // beam parameters (src/module/beaminfo.hpp:79-90)
+    int32_t infl_kind;
+    int32_t beam1;                   // Beam->Type[1]: width 'F', 'M', 'W' or 'C'
+    int32_t nimage, ibeam_window, component;
+    double eps_mult, rloop;
+    double top_depth, bot_depth;     // Bdry->Top / Bot.hs.Depth (Cerveny images)
     HsDev top, bot;
     // boundaries
     int32_t ntop, nbot;
@@ -191,6 +198,36 @@ struct ArrCand {
     int32_t ntop, nbot, job, aux;
     float rcvr_azim;           // 3-D: receiver azimuth (deg); 2-D: unused
 };
+// Influence types beyond geometric Cartesian (src/influence.hpp:1495-1536):
+// geometric hat / Gaussian in ray-centred coordinates ('g', 'b'), Cerveny
+// paraxial beams in ray-centred ('R') and Cartesian ('C') coordinates, and
+// simple Gaussian beams ('S').
+enum InflKind : int32_t { INFL_GEO_CART = 0, INFL_GEO_RAYCEN = 1, INFL_CERV_RAYCEN = 2, INFL_CERV_CART = 3,
+                          INFL_SGB = 4 };
+
+// One influence record of those types (FP64). Ray-centred kinds store one
+// record per ray segment (point A = the last valid point and its ray normal,
+// point B = point1); the receiver ranges between the two normals depend on the
+// receiver depth and are found per depth by the influence kernel. Cartesian
+// Cerveny and simple Gaussian beams store one record per bracketed receiver
+// range (column), with the ray quantities interpolated to it, because their
+// receiver walk carries state along the ray.
+struct alignas(16) XSeg {
+    double xa, za, nxa, nza;       // ray-centred: point A and its ray normal
+    double xb, zb, nxb, nzb;       // ray-centred: point B and its normal; columns: x, z at the column
+    double tau0r, tau0i, dtaur, dtaui;   // delay at A (columns: at the column), change from A to B
+    double q0r, q0i, dqr, dqi;     // geometric q (real) or Cerveny qB at A, change from A to B
+    double g0r, g0i, dgr, dgi;     // Cerveny gamma at A (columns: at the column), change from A to B
+    double cr, ci;                 // Cartesian Cerveny column: Ratio1 sqrt(c |eps0| / q), KMAH sign
+    double amp, ph_a, ph_b;        // geometric: Ratio1 sqrt(c1) Amp1 and the two FinalPhase values;
+                                   // Cerveny: (Ratio1) Amp1, Phase1; simple Gaussian: Ratio1 cn Amp1, phase
+    double c0, tau1r, rcp_q0, radmax;   // point0.c, point1.tau.real, Dalpha / c0, 50 wavelengths
+    double t1x, t1y, eps_abs;      // point1.t (columns: interpolated rayt), Cerveny |eps1|
+    double sint, sgb_a, drab, dzab; // simple Gaussian: distance along the ray, beam factor, rB - rA, zB - zA
+    double rcvr_decl;              // receiver declination (deg)
+    int32_t job, is, ir, ntop, nbot, kmah0, valid, pad;
+};
+
 // Bit layout of the ordering keys (low to high): arrivals: step | job | cell;
 // eigen: depth | walk position | step | job | field (3-D: depth | bearing |
 // walk position | step | job | trace group).

@@ -597,8 +597,18 @@ EnvInput read_env_files(const std::string &root, bool o3d)
     } else {
         f.read(in.deltas); f.read(in.box_z); f.read(in.box_r_km);
     }
-    if(in.run_type[1] == 'C' || in.run_type[1] == 'R')
-        env_error("Cerveny beams are not supported by this build");
+    if(in.run_type[0] != 'R' && (in.run_type[1] == 'C' || in.run_type[1] == 'R')) {
+        if(o3d) env_error("Cerveny beams are not supported in 3-D (the reference rejects them too)");
+        f.record();
+        f.read_chars(in.cerv_type, 2);
+        f.read(in.eps_mult);
+        f.read(in.rloop);
+        f.record();
+        f.read(in.nimage);
+        f.read(in.ibeam_window);
+        std::string comp;
+        if(f.read(comp) && !comp.empty()) in.component = comp[0];
+    }
     if(o3d) {
         if(in.top_opt[4] == '~' || in.top_opt[4] == '*') read_bdry3_file(root + ".ati", in.ati3);
         if(in.bot_opt[1] == '~' || in.bot_opt[1] == '*') read_bdry3_file(root + ".bty", in.bty3);
@@ -696,9 +706,25 @@ EnvTables preprocess(const EnvInput &in, double freq)
     t.beam_type[0] = t.run_type[1];
     t.beam_type[3] = t.run_type[6];
     char bt = t.beam_type[0];
-    // ray runs trace geometric rays whatever the beam type (src/mode/ray.cpp:44-86)
-    if(!ray_run && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
-        env_error(std::string("beam type '") + bt + "' is not supported by this build");
+    if(bt == 'C' || bt == 'R') {                                 // Cerveny (module/beaminfo.hpp:79-90,130-139)
+        t.beam_type[1] = in.cerv_type[0];
+        t.beam_type[2] = in.cerv_type[1];
+        if(!ray_run && t.beam_type[2] != 'D' && t.beam_type[2] != 'Z' && t.beam_type[2] != 'S')
+            env_error(std::string("unknown curvature condition '") + t.beam_type[2] + "'");
+        if(!ray_run && t.run_type[0] != 'C' && t.run_type[0] != 'S' && t.run_type[0] != 'I')
+            env_error("Cerveny influence does not support eigenrays or arrivals");
+    }
+    t.eps_mult = in.eps_mult;
+    t.rloop = in.rloop;
+    t.nimage = in.nimage;
+    t.ibeam_window = in.ibeam_window;
+    t.component = in.component;
+    if(!ray_run && (bt == 'C' || bt == 'R') && (in.nimage < 1 || in.nimage > 3))
+        env_error("Cerveny beams: the number of images must be 1, 2 or 3");
+    // ray-centred, Cerveny and simple Gaussian beams are TL-only in this build
+    if(!ray_run && (bt == 'g' || bt == 'b' || bt == 'S') && t.run_type[0] != 'C' && t.run_type[0] != 'S'
+       && t.run_type[0] != 'I')
+        env_error(std::string("beam type '") + bt + "' with arrivals or eigenrays is not supported by this build");
 
     char st = in.top_opt[0];
     switch(st) {
@@ -739,6 +765,8 @@ EnvTables preprocess(const EnvInput &in, double freq)
         t.warnings.push_back("Ocean bottom must be at last SSP depth");
     t.top = make_hs(in, freq, fT, in.top);
     t.bot = make_hs(in, freq, fT, in.bot);
+    t.top_depth = top_depth;
+    t.bot_depth = bot_depth;
     t.btop = build_bdry(in, freq, in.ati, true, top_depth, t.top_curv, t.top_long);
     t.bbot = build_bdry(in, freq, in.bty, false, bot_depth, t.bot_curv, t.bot_long);
     for(const auto &p : t.bbot)
@@ -861,7 +889,9 @@ bool EnvTables::same_trajectory_tables(const EnvTables &o) const
     // (src/trace.hpp:148-152), so 'S' runs never share.
     return vclose(c, o.c) && vclose(cz, o.cz) && vclose(n2, o.n2) && vclose(n2z, o.n2z)
         && vclose(coef, o.coef) && vclose(qc, o.qc) && vclose(qr, o.qr) && hclose(top, o.top) && hclose(bot, o.bot) && bclose(btop, o.btop)
-        && bclose(bbot, o.bbot) && alpha == o.alpha && run_type[0] != 'S';
+        && bclose(bbot, o.bbot) && alpha == o.alpha && run_type[0] != 'S'
+        // the other beam types evaluate their beams at the trace frequency
+        && (beam_type[0] == 'G' || beam_type[0] == 'B' || beam_type[0] == '^' || beam_type[0] == ' ');
 }
 
 
@@ -953,10 +983,10 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.freq0 = freq;
     std::memcpy(t.run_type, in.run_type, 7);
     switch(t.run_type[0]) {   // src/module/runtype.hpp:53-78
-    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': break;
-    case 'R': env_error("ray-trace runs ('R') are not a field mode");
+    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'R': break;
     default: env_error("unknown RunType");
     }
+    const bool ray_run3 = t.run_type[0] == 'R';
     if(t.run_type[5] != '3') env_error("3-D runs need RunType(6) = '3'");
     switch(t.run_type[1]) {
     case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
@@ -969,7 +999,8 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.beam_type[0] = t.run_type[1];
     t.beam_type[3] = t.run_type[6];
     char bt = t.beam_type[0];
-    if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
+    // ray runs trace geometric rays whatever the beam type (src/mode/ray.cpp:44-86)
+    if(!ray_run3 && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
         env_error(std::string("3-D beam type '") + bt + "' is not supported by this build (Cartesian 'G' / 'B')");
     if(t.run_type[3] == 'X') env_error("line sources are 2-D only");
 

@@ -57,6 +57,12 @@ struct EnvInput {
     std::vector<double> rr_km, alpha_deg;
     char run_type[7] = {'C', 'G', ' ', 'R', 'R', ' ', ' '};
     double deltas = 0, box_z = 0, box_r_km = 0;
+    // Cerveny beams (src/module/beaminfo.hpp:79-90): width and curvature
+    // options (Beam->Type[1..2]), epsilon multiplier, rLoop, images, window, component
+    char cerv_type[2] = {' ', 'S'};
+    double eps_mult = 1.0, rloop = 1.0;
+    int32_t nimage = 1, ibeam_window = 4;
+    char component = 'P';
     // 3-D only (src/module/sxsy.hpp, rcvrbearings.hpp, rayangles.hpp, beaminfo.hpp)
     int32_t nsx = 1, nsy = 1, ntheta = 1, nbeta = 1, isingle_beta = 0;
     std::vector<double> sx_km, sy_km, theta_deg, beta_deg;
@@ -87,6 +93,9 @@ struct EnvTables {
     char run_type[7];
     char beam_type[4];
     int32_t nrz_per_range = 1, isingle = 0;
+    double eps_mult = 1.0, rloop = 1.0, top_depth = 0.0, bot_depth = 0.0;
+    int32_t nimage = 1, ibeam_window = 4;
+    char component = 'P';
     std::vector<std::string> warnings;
     // true when every frequency-dependent table is identical to other's
     bool same_trajectory_tables(const EnvTables &o) const;

@@ -39,7 +39,14 @@ void *run3_field_device(Run3 *r, int env);
 // receiver grid and source positions as the reference's Position (m, deg)
 void run3_grid(const Run3 *r, int env, std::vector<double> &sx, std::vector<double> &sy, std::vector<float> &sz,
                std::vector<double> &rr, std::vector<float> &rz, std::vector<double> &theta);
-// <root>.shd (TL) or <root>.arr (arrivals) in the reference's 3-D layouts
+// ray runs ('R') and eigen runs ('E'): the traced (resp. re-traced hit) rays of
+// env: per ray the point count, bounces of the last point, take-off
+// declination (deg); the points (x, y, z) ray after ray
+bool run3_has_rays(const Run3 *r);
+void run3_rays_shape(Run3 *r, int env, cudaStream_t st, int64_t &nrays, int64_t &npoints);
+void run3_copy_rays(Run3 *r, int env, cudaStream_t st, int32_t *npts, int32_t *bounces, double *alpha_deg,
+                    double *xyz, size_t xyz_bytes);
+// <root>.shd (TL), <root>.arr (arrivals) or <root>.ray (rays, eigenrays) in the reference's 3-D layouts
 void run3_writeout(Run3 *r, int env, const std::string &root, cudaStream_t st);
 std::vector<std::string> run3_warnings(const Run3 *r, int env);
 

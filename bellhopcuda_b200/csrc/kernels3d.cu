@@ -147,6 +147,95 @@ __device__ __forceinline__ bool infl_prologue3(const Ray3 &P0, const Ray3 &P1, I
     return true;
 }
 
+// Per-ray state of the 3-D ray loop.
+struct RayState3 {
+    Ray3 p0;
+    Bd3 top, bot;
+    Seg3 iSeg;
+    V3 xs;
+    double alpha, beta, c;
+    double minx, miny, maxx, maxy;   // extent of the boundary grids (RayTerminate)
+};
+
+// RayInit (src/trace.hpp:76-266), 3-D: false when the source is on or outside
+// the boundaries (the ray is not traced)
+__device__ __forceinline__ bool ray_init3d(const Env3Dev &E, const Job3 &J, RayState3 &st, RunCounters *ctr)
+{
+    const double alpha = E.alpha[J.ialpha], beta = E.beta[J.ibeta];
+    st.alpha = alpha;
+    st.beta = beta;
+    const double SrcDecl = (180.0 / BHCB_PI) * alpha;
+    st.iSeg = Seg3{0, 0, 0};
+    const V3 xs = v3(E.sx[J.isx], E.sy[J.isy], (double)E.sz[J.isz]);
+    st.xs = xs;
+    SSPOut3 o;
+    eval_ssp3(xs, v3(0.0, 0.0, 1.0), o, E, st.iSeg, ctr);
+    const double c = o.c;
+    st.c = c;
+    const int ibp = min(bsearch_leq2(E.sbp, E.nsbp, SrcDecl), E.nsbp - 2);
+    const double s = (SrcDecl - E.sbp[2 * ibp]) / (E.sbp[2 * (ibp + 1)] - E.sbp[2 * ibp]);
+    float amp0 = (float)((FLTD(1.0) - s) * E.sbp[2 * ibp + 1] + s * E.sbp[2 * (ibp + 1) + 1]);
+    if(E.run0 == 'S') {
+        const float om = (float)(FLTD(2.0) * BHCB_PI * E.freq0);
+        amp0 = (float)(amp0 * ((double)sqrtf(2.0f) * fabs(sin(om / c * xs.z * sin(alpha)))));
+    }
+    Ray3 &p0 = st.p0;
+    const V3 tinit = v3(cos(alpha) * cos(beta), cos(alpha) * sin(beta), sin(alpha));
+    p0.x = xs;
+    p0.c = c;
+    p0.t = v3(tinit.x / c, tinit.y / c, tinit.z / c);
+    p0.taur = p0.taui = 0.0;
+    p0.Amp = (double)amp0;
+    p0.Phase = 0.0;
+    p0.ntop = p0.nbot = 0;
+    p0.p = m2_diag(1.0);
+    p0.q = m2_diag(0.0);
+    p0.phi = 0.0;
+    st.top.ix = st.top.iy = st.bot.ix = st.bot.iy = 0;
+    st.top.justSteppedTo = st.bot.justSteppedTo = false;
+    st.top.side = st.bot.side = false;
+    st.top.outgoingSide = st.bot.outgoingSide = false;
+    get_bdry_seg3(xs, p0.t, st.top, E.btop, E.top_nx, E.top_ny, true, true, ctr);
+    get_bdry_seg3(xs, p0.t, st.bot, E.bbot, E.bot_nx, E.bot_ny, false, true, ctr);
+    double dTop, dBot;
+    distances3(xs, st.top, st.bot, dTop, dBot);
+    if(dTop <= 0.0 || dBot <= 0.0) {
+        run_warn(ctr, WARN_SOURCE_OUTSIDE_BOUNDARIES);
+        return false;
+    }
+    const Bdry3PtDev *bb = E.bbot, *bt = E.btop;
+    st.minx = max(bb[0].x[0], bt[0].x[0]);
+    st.miny = max(bb[0].x[1], bt[0].x[1]);
+    st.maxx = min(bb[(size_t)(E.bot_nx - 1) * E.bot_ny].x[0], bt[(size_t)(E.top_nx - 1) * E.top_ny].x[0]);
+    st.maxy = min(bb[E.bot_ny - 1].x[1], bt[E.top_ny - 1].x[1]);
+    return true;
+}
+
+// RayUpdate (src/trace.hpp:274-381), 3-D: one step from st.p0 to p1 and, on a
+// boundary hit, the reflected point p2; returns whether p2 was produced
+__device__ __forceinline__ bool ray_update3d(RayState3 &st, Ray3 &p1, Ray3 &p2, int &small, const Env3Dev &E,
+                                             RunCounters *ctr)
+{
+    bool tr = false, br = false;
+    step3d(st.p0, p1, st.top, st.bot, st.xs, E, st.iSeg, small, tr, br, ctr);
+    get_bdry_seg3(p1.x, p1.t, st.top, E.btop, E.top_nx, E.top_ny, true, false, ctr);
+    get_bdry_seg3(p1.x, p1.t, st.bot, E.bbot, E.bot_nx, E.bot_ny, false, false, ctr);
+    const bool two = tr || br;
+    if(two) reflect3d(p1, p2, tr ? E.top : E.bot, tr, tr ? st.top.n : st.bot.n, E, st.iSeg, ctr);
+    return two;
+}
+
+// RayTerminate's stop conditions (src/trace.hpp:391-477), 3-D
+__device__ __forceinline__ bool ray_stops3d(const RayState3 &st, int small, const Env3Dev &E)
+{
+    const V3 x = st.p0.x, t = st.p0.t;
+    const bool leftbox = fabs(x.x - st.xs.x) >= E.box_x || fabs(x.y - st.xs.y) >= E.box_y || fabs(x.z) >= E.box_z;
+    const bool esc0 = x.x < st.minx || x.y < st.miny || (x.x == st.minx && t.x < 0.0) || (x.y == st.miny && t.y < 0.0);
+    const bool escN = x.x > st.maxx || x.y > st.maxy || (x.x == st.maxx && t.x > 0.0) || (x.y == st.maxy && t.y > 0.0);
+    const bool lost = st.p0.Amp < FLTD(0.005);
+    return leftbox || lost || esc0 || escN || small > 50;
+}
+
 __global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict__ groups, int ngroups,
                                                      long long job_end, SegRec3 *segs, unsigned long long cap,
                                                      RunCounters *ctr, unsigned long long *job_counter)
@@ -158,47 +247,11 @@ __global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict_
         const Env3Dev &E = *G.env3;
         const Job3 J = job_indices3(E, (int)(job - G.job_base));
         if(J.isz >= E.nsz) { run_error(ctr, ERR_RAYINIT); continue; }
-
-        // ---- RayInit (src/trace.hpp:76-266), 3-D
-        const double alpha = E.alpha[J.ialpha], beta = E.beta[J.ibeta];
-        const double SrcDecl = (180.0 / BHCB_PI) * alpha;
-        Seg3 iSeg{0, 0, 0};
-        const V3 xs = v3(E.sx[J.isx], E.sy[J.isy], (double)E.sz[J.isz]);
-        SSPOut3 o;
-        eval_ssp3(xs, v3(0.0, 0.0, 1.0), o, E, iSeg, ctr);
-        const double c = o.c;
-        const int ibp = min(bsearch_leq2(E.sbp, E.nsbp, SrcDecl), E.nsbp - 2);
-        const double s = (SrcDecl - E.sbp[2 * ibp]) / (E.sbp[2 * (ibp + 1)] - E.sbp[2 * ibp]);
-        float amp0 = (float)((FLTD(1.0) - s) * E.sbp[2 * ibp + 1] + s * E.sbp[2 * (ibp + 1) + 1]);
-        if(E.run0 == 'S') {
-            const float om = (float)(FLTD(2.0) * BHCB_PI * E.freq0);
-            amp0 = (float)(amp0 * ((double)sqrtf(2.0f) * fabs(sin(om / c * xs.z * sin(alpha)))));
-        }
-        Ray3 p0, p1, p2;
-        const V3 tinit = v3(cos(alpha) * cos(beta), cos(alpha) * sin(beta), sin(alpha));
-        p0.x = xs;
-        p0.c = c;
-        p0.t = v3(tinit.x / c, tinit.y / c, tinit.z / c);
-        p0.taur = p0.taui = 0.0;
-        p0.Amp = (double)amp0;
-        p0.Phase = 0.0;
-        p0.ntop = p0.nbot = 0;
-        p0.p = m2_diag(1.0);
-        p0.q = m2_diag(0.0);
-        p0.phi = 0.0;
-        Bd3 top, bot;
-        top.ix = top.iy = bot.ix = bot.iy = 0;
-        top.justSteppedTo = bot.justSteppedTo = false;
-        top.side = bot.side = false;
-        top.outgoingSide = bot.outgoingSide = false;
-        get_bdry_seg3(xs, p0.t, top, E.btop, E.top_nx, E.top_ny, true, true, ctr);
-        get_bdry_seg3(xs, p0.t, bot, E.bbot, E.bot_nx, E.bot_ny, false, true, ctr);
-        double dTop, dBot;
-        distances3(xs, top, bot, dTop, dBot);
-        if(dTop <= 0.0 || dBot <= 0.0) {
-            run_warn(ctr, WARN_SOURCE_OUTSIDE_BOUNDARIES);
-            continue;
-        }
+        RayState3 st;
+        if(!ray_init3d(E, J, st, ctr)) continue;
+        Ray3 &p0 = st.p0;
+        Ray3 p1, p2;
+        const double alpha = st.alpha, c = st.c;
         // ---- Init_Influence (src/influence.hpp:525-644), 3-D Cartesian geometric
         Infl3 inf;
         inf.ratio1 = sqrt(fabs(cos(alpha)));
@@ -211,26 +264,14 @@ __global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict_
         inf.xs = p0.x;
         inf.ir = bsearch_gt(E.rr, E.nrr, 0.0);
 
-        // beam-box limits of the boundary grids (RayTerminate, src/trace.hpp:400-420)
-        const Bdry3PtDev *bb = E.bbot, *bt = E.btop;
-        const double minx = max(bb[0].x[0], bt[0].x[0]);
-        const double miny = max(bb[0].x[1], bt[0].x[1]);
-        const double maxx = min(bb[(size_t)(E.bot_nx - 1) * E.bot_ny].x[0], bt[(size_t)(E.top_nx - 1) * E.top_ny].x[0]);
-        const double maxy = min(bb[E.bot_ny - 1].x[1], bt[E.top_ny - 1].x[1]);
-
         int small = 0, is = 0;
         bool overflow = false;
         unsigned long long nsteps = 0;
         Cursor3 cur;
         for(;;) {
             if((nsteps & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) break;
-            bool tr = false, br = false;
-            step3d(p0, p1, top, bot, xs, E, iSeg, small, tr, br, ctr);
+            const bool two = ray_update3d(st, p1, p2, small, E, ctr);
             ++nsteps;
-            get_bdry_seg3(p1.x, p1.t, top, E.btop, E.top_nx, E.top_ny, true, false, ctr);
-            get_bdry_seg3(p1.x, p1.t, bot, E.bbot, E.bot_nx, E.bot_ny, false, false, ctr);
-            const bool two = tr || br;
-            if(two) reflect3d(p1, p2, tr ? E.top : E.bot, tr, tr ? top.n : bot.n, E, iSeg, ctr);
             SegRec3 rec;
             if(infl_prologue3(p0, p1, inf, E, (int)job, is, rec)) emit_seg3(rec, segs, cap, ctr, cur, overflow);
             ++is;
@@ -247,12 +288,7 @@ __global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict_
                 break;
             }
             // ---- RayTerminate (src/trace.hpp:391-477), 3-D
-            const V3 x = p0.x, t = p0.t;
-            const bool leftbox = fabs(x.x - xs.x) >= E.box_x || fabs(x.y - xs.y) >= E.box_y || fabs(x.z) >= E.box_z;
-            const bool esc0 = x.x < minx || x.y < miny || (x.x == minx && t.x < 0.0) || (x.y == miny && t.y < 0.0);
-            const bool escN = x.x > maxx || x.y > maxy || (x.x == maxx && t.x > 0.0) || (x.y == maxy && t.y > 0.0);
-            const bool lost = p0.Amp < FLTD(0.005);
-            if(leftbox || lost || esc0 || escN || small > 50) break;
+            if(ray_stops3d(st, small, E)) break;
             if(is >= MAXN_STEPS - 3) {
                 run_warn(ctr, WARN_ONERAY_OUTOFMEMORY);
                 break;
@@ -260,6 +296,91 @@ __global__ void __launch_bounds__(64) trace3d_kernel(const GroupDev *__restrict_
         }
         for(; cur.next < cur.end; ++cur.next) segs[cur.next].job = -1;
         atomicAdd(&ctr->nsteps, nsteps);
+    }
+}
+
+// Ray trajectories, 3-D (MainRayMode, src/trace.hpp:485-519) of listed rays:
+// every ray of a RunType 'R' run, or the rays of eigen hits re-traced up to the
+// hit (EigenModePostWorker, src/mode/eigen.cpp:24-45). One ray per thread.
+// limits[i] < 0: no limit; else the ray stops two points after step limits[i].
+// COUNT: npts[i] = number of points, bounce counts of the last point in
+// bnc[2i], bnc[2i + 1]; otherwise the points (x, y, z) go to pts + 3 off[i].
+template<bool COUNT>
+__global__ void __launch_bounds__(64) ray3d_kernel(const GroupDev *__restrict__ groups, int ngroups,
+                                                   const long long *__restrict__ jobs, const int *__restrict__ limits,
+                                                   int nitems, const long long *__restrict__ off, double *pts,
+                                                   int *npts, int *bnc, RunCounters *ctr)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += gridDim.x * blockDim.x) {
+        const long long job = jobs[i];
+        const GroupDev &G = groups[find_group(groups, ngroups, job)];
+        const Env3Dev &E = *G.env3;
+        const Job3 J = job_indices3(E, (int)(job - G.job_base));
+        const int cap = COUNT ? 0x7fffffff : npts[i];
+        const long long base = COUNT ? 0 : off[i];
+        auto put = [&](int idx, const Ray3 &p) {
+            if(!COUNT && idx < cap) {
+                double *q = pts + 3 * (base + idx);
+                q[0] = p.x.x;
+                q[1] = p.x.y;
+                q[2] = p.x.z;
+            }
+        };
+        if(J.isz >= E.nsz) {
+            run_error(ctr, ERR_RAYINIT);
+            if(COUNT) { npts[i] = 0; bnc[2 * i] = bnc[2 * i + 1] = 0; }
+            continue;
+        }
+        RayState3 st;
+        int nsteps = -1, last_top = 0, last_bot = 0;
+        if(!ray_init3d(E, J, st, ctr)) {
+            put(0, st.p0);
+            nsteps = 1;
+        } else {
+            put(0, st.p0);
+            const int limit = limits[i];
+            int is = 0, small = 0, prev_top = 0, prev_bot = 0;
+            Ray3 p1, p2;
+            for(;;) {
+                if((is & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) {
+                    nsteps = is + 1;
+                    last_top = st.p0.ntop;
+                    last_bot = st.p0.nbot;
+                    break;
+                }
+                const bool two = ray_update3d(st, p1, p2, small, E, ctr);
+                put(is + 1, p1);
+                if(two) put(is + 2, p2);
+                if(limit >= 0 && is >= limit) {
+                    nsteps = is + 2;
+                    last_top = p1.ntop;
+                    last_bot = p1.nbot;
+                    break;
+                }
+                prev_top = two ? p1.ntop : st.p0.ntop;
+                prev_bot = two ? p1.nbot : st.p0.nbot;
+                is += two ? 2 : 1;
+                st.p0 = two ? p2 : p1;
+                if(ray_stops3d(st, small, E)) {
+                    nsteps = is + 1;
+                    last_top = st.p0.ntop;
+                    last_bot = st.p0.nbot;
+                    break;
+                }
+                if(is >= MAXN_STEPS - 3) {
+                    run_warn(ctr, WARN_ONERAY_OUTOFMEMORY);
+                    nsteps = is;
+                    last_top = prev_top;
+                    last_bot = prev_bot;
+                    break;
+                }
+            }
+        }
+        if(COUNT) {
+            npts[i] = nsteps;
+            bnc[2 * i] = last_top;
+            bnc[2 * i + 1] = last_bot;
+        }
     }
 }
 
@@ -585,6 +706,20 @@ __global__ void sqrt3d_kernel(float2 *f, long long n)
 }
 
 } // namespace
+
+cudaError_t launch_rays3d(const GroupDev *groups, int ngroups, const long long *jobs, const int *limits, int nitems,
+                          const long long *off, double *pts, int *npts, int *bnc, RunCounters *ctr, bool count,
+                          int sm_count, cudaStream_t st)
+{
+    if(nitems <= 0) return cudaSuccess;
+    int grid = (nitems + 63) / 64;
+    if(grid > sm_count * 16) grid = sm_count * 16;
+    if(count)
+        ray3d_kernel<true><<<grid, 64, 0, st>>>(groups, ngroups, jobs, limits, nitems, off, pts, npts, bnc, ctr);
+    else
+        ray3d_kernel<false><<<grid, 64, 0, st>>>(groups, ngroups, jobs, limits, nitems, off, pts, npts, bnc, ctr);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_trace3d(const GroupDev *groups, int ngroups, long long job_end, SegRec3 *segs,
                            unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, int grid,

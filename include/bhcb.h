@@ -263,14 +263,16 @@ int bhcb_nn_to_bf16(const float *x, void *y, int64_t n, void *stream);
 /* x = a * x + b over n floats */
 int bhcb_nn_affine(float *x, int64_t n, float a, float b, void *stream);
 
-/* Ray trajectories (2-D): RunType 'R' traces every ray (RunRayMode,
+/* Ray trajectories (2-D and 3-D): RunType 'R' traces every ray (RunRayMode,
    src/mode/ray.cpp:163-198); for eigen runs ('E') the rays of the hits of
    (env_index, ifreq) are re-traced up to their hit (PostProcessEigenrays,
    src/mode/eigen.cpp:63-92) on the first call. bhcb_writeout writes them as
    FileRoot.ray (OpenRAYFile / WriteRay, src/mode/ray.hpp:176-247).
    bhcb_copy_rays: npts[nrays] points per ray, bounces[2 nrays] top / bottom
-   bounce counts of the last point, alpha_deg[nrays] take-off angles, rz the
-   points (r, z) in m, ray after ray (2 doubles each, npoints in total). */
+   bounce counts of the last point, alpha_deg[nrays] take-off declinations
+   (degrees), rz the points ray after ray, npoints in total: (r, z) in m,
+   2 doubles each, for 2-D contexts; (x, y, z) in m, 3 doubles each, for 3-D
+   contexts (ifreq 0). */
 int bhcb_rays_shape(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, int64_t *nrays, int64_t *npoints);
 int bhcb_copy_rays(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, int32_t *npts, int32_t *bounces,
                    double *alpha_deg, double *rz, size_t rz_bytes);

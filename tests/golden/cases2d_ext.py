@@ -151,6 +151,35 @@ def beam_shift_munk_hat():
     return {".env": env_text(spec)}
 
 
+def _with_beam_lines(files, width_curv="MS", eps_mult=1.0, rloop=10.0, nimage=1, ibwin=5, comp="P"):
+    """Append the Cerveny beam records (src/module/beaminfo.hpp:79-90): width /
+    curvature options, epsilon multiplier, rLoop (km), then the number of
+    images, beam window and field component."""
+    files[".env"] = files[".env"] + "'%s' %r %r\n%d %d '%s'\n" % (width_curv, float(eps_mult), float(rloop), nimage,
+                                                                 ibwin, comp)
+    return files
+
+
+def _munk_small(run_type, **kw):
+    spec = _munk_spec(bot_bc="A", bot_hs=(5000.0, 1600.0, 0.0, 1.8, 0.8, 0.0), run_type=run_type, nalpha=301,
+                      alpha=(-20.0, 20.0), rr_km=(0.0, 50.0), nrr=201, nrz=51)
+    for k, v in kw.items():
+        setattr(spec, k, v)
+    return {".env": env_text(spec)}
+
+
+def _shallow_small(run_type, **kw):
+    z = np.array([0.0, 30.0, 60.0, 100.0])
+    c = np.array([1520.0, 1515.0, 1495.0, 1490.0])
+    spec = EnvSpec(title="shallow beams", freq=200.0, ssp_type="C", top_bc="V", atten_unit="W", ssp_z=z,
+                   ssp_cp=c, bot_bc="A", bot_hs=(100.0, 1700.0, 0.0, 1.9, 0.5, 0.0), nsz=2, sz=(20.0, 70.0), nrz=41,
+                   rz=(0.0, 100.0), nrr=161, rr_km=(0.0, 8.0), run_type=run_type, nalpha=301, alpha=(-60.0, 60.0),
+                   deltas=0.0, box_z=110.0, box_r_km=8.1)
+    for k, v in kw.items():
+        setattr(spec, k, v)
+    return {".env": env_text(spec)}
+
+
 CASES2D_EXT = {
     "x2d_quad_munk_gauss": quad_munk_gauss,
     "x2d_quad_munk_hat": quad_munk_hat,
@@ -161,4 +190,19 @@ CASES2D_EXT = {
     "x2d_trc_brc_shallow_incoherent": trc_brc_shallow_incoherent,
     "x2d_beam_shift_shallow": beam_shift_shallow,
     "x2d_beam_shift_munk_hat": beam_shift_munk_hat,
+    # geometric beams in ray-centred coordinates ('g' hat, 'b' Gaussian)
+    "x2d_raycen_hat_munk": lambda: _munk_small("Cg RR "),
+    "x2d_raycen_gauss_munk": lambda: _munk_small("Cb RR "),
+    "x2d_raycen_hat_shallow_incoherent": lambda: _shallow_small("Ig RR "),
+    "x2d_raycen_gauss_shallow_semicoherent": lambda: _shallow_small("Sb RR "),
+    # Cerveny paraxial beams: ray-centred ('R') and Cartesian ('C')
+    "x2d_cerveny_raycen_munk": lambda: _with_beam_lines(_munk_small("CR RR ")),
+    "x2d_cerveny_cart_munk": lambda: _with_beam_lines(_munk_small("CC RR ")),
+    "x2d_cerveny_raycen_shallow_images": lambda: _with_beam_lines(_shallow_small("CR RR "), "FS", 1.0, 1.0, 3, 4),
+    "x2d_cerveny_cart_shallow_images_incoherent": lambda: _with_beam_lines(_shallow_small("IC RR "), "FD", 0.5, 1.0,
+                                                                           2, 4),
+    "x2d_cerveny_raycen_wkb_vertical": lambda: _with_beam_lines(_munk_small("CR RR "), "WS", 1.0, 10.0, 1, 5, "V"),
+    # simple Gaussian beams ('S')
+    "x2d_sgb_munk": lambda: _munk_small("CS RR "),
+    "x2d_sgb_shallow_incoherent": lambda: _shallow_small("IS RR "),
 }

@@ -141,6 +141,20 @@ def munk3d_brc_gauss():
     return f
 
 
+def munk3d_ray():
+    """Ray trajectories ('R'), 3-D: a small fan in elevation and bearing."""
+    return _munk_slice("R    3", alpha=(11, -12.0, 12.0), beta=(5, -6.0, 6.0), theta=[0.0])
+
+
+def seamount3d_ray():
+    """Ray trajectories over the seamount grid (bottom reflections off the
+    triangulated bathymetry)."""
+    f = seamount3d_gauss()
+    f[".env"] = f[".env"].replace("'CB   3'", "'R    3'").replace("91\n-30 30 /", "9\n-30 30 /").replace(
+        "73\n-180 180 /", "12\n-180 180 /")
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -156,4 +170,6 @@ CASES3D = {
     "munk3d_eig_gauss": munk3d_eig_gauss,
     "seamount3d_eig_hat": seamount3d_eig_hat,
     "munk3d_brc_gauss": munk3d_brc_gauss,
+    "munk3d_ray": munk3d_ray,
+    "seamount3d_ray": seamount3d_ray,
 }

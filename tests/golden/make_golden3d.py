@@ -48,15 +48,21 @@ def main(names=None):
             if r.returncode != 0:
                 raise SystemExit("reference failed on %s:\n%s%s" % (name, r.stdout[-2000:], r.stderr[-2000:]))
             texts = {"file_" + suffix[1:]: np.array(text) for suffix, text in files.items()}
-            if files[".env"].count("'E") and os.path.exists(root + ".ray"):
-                # eigen hits: the reference writes the re-traced eigenrays in hit
-                # order; each ray's take-off angle (radians in 3-D) and its point
-                # count (the hit's step + 2) pin the hit list
+            if os.path.exists(root + ".ray"):
+                # ray runs ('R') and eigen hits ('E'): the reference writes the
+                # traced rays (eigen: the hit rays re-traced, in hit order, so each
+                # ray's take-off angle in radians and point count, the hit's step +
+                # 2, pin the hit list) with their points (x, y, z)
                 R = read_ray(root + ".ray")
+                npts = np.array([len(x["xy"]) for x in R["rays"]], np.int32)
+                # points of the first (at most) 64 rays keep the fixture small
+                nkeep = min(len(npts), 64)
                 np.savez_compressed(os.path.join(HERE, name + ".npz"),
-                                    alpha=np.array([x["alpha"] for x in R["rays"]]),
-                                    npts=np.array([len(x["xy"]) for x in R["rays"]], np.int32), **texts)
-                print(name, "eigenrays", len(R["rays"]), "%.1fs" % (time.time() - t0))
+                                    alpha=np.array([x["alpha"] for x in R["rays"]]), npts=npts,
+                                    bnc=np.array([[x["ntop"], x["nbot"]] for x in R["rays"]], np.int32).reshape(-1, 2),
+                                    xyz=np.concatenate([x["xy"] for x in R["rays"][:nkeep]]) if nkeep
+                                    else np.zeros((0, 3)), xyz_rays=np.int32(nkeep), **texts)
+                print(name, "rays", len(R["rays"]), "points", int(npts.sum()), "%.1fs" % (time.time() - t0))
                 continue
             if os.path.exists(root + ".arr"):
                 # arrivals: per receiver (source, bearing, depth, range) the

@@ -42,7 +42,7 @@ def to_file_order(u):
     return np.transpose(u, (1, 2, 3, 0, 4, 5))
 
 
-TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p]
+TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p and "_ray" not in p]
 
 
 @pytest.mark.parametrize("path", TL3D, ids=[os.path.basename(p)[:-4] for p in TL3D])
@@ -188,3 +188,65 @@ def test_3d_eigen_hits_match_reference(path, workdir):
     a1, a2 = (float(v) for v in txt[k + 2].replace("/", " ").split()[:2])
     fan = np.deg2rad(np.linspace(a1, a2, na))
     np.testing.assert_allclose(fan[hits["ialpha"]], g["alpha"], rtol=1e-9, atol=1e-12)
+
+
+RAY3D = sorted(p for p in GOLD if "_ray" in p)
+
+
+def compare_rays3d(rays, g, frac=0.97):
+    """Same rays in the same order (take-off angle, point count, bounce
+    counts); on at least frac of the rays whose points the fixture keeps,
+    every point within 1 mm (a boundary decision may fall differently at the
+    last floating-point digit: FP64 on both sides, different contraction)."""
+    assert len(rays) == len(g["npts"]) > 0
+    np.testing.assert_allclose(np.deg2rad([r["alpha"] for r in rays]), g["alpha"], rtol=1e-9, atol=1e-12)
+    same_n = sum(len(r["rz"]) == n for r, n in zip(rays, g["npts"]))
+    assert same_n >= frac * len(rays), "%d of %d point counts equal" % (same_n, len(rays))
+    nkeep = int(g["xyz_rays"])
+    offs = np.concatenate([[0], np.cumsum(g["npts"][:nkeep])])
+    good = 0
+    for i in range(nkeep):
+        ref = g["xyz"][offs[i]:offs[i + 1]]
+        r = rays[i]
+        if len(r["rz"]) == len(ref) and (r["ntop"], r["nbot"]) == tuple(g["bnc"][i]) and \
+                np.max(np.abs(r["rz"] - ref)) <= 1e-3:
+            good += 1
+    assert good >= frac * nkeep, "%d of %d rays equal" % (good, nkeep)
+
+
+@pytest.mark.parametrize("path", RAY3D, ids=[os.path.basename(p)[:-4] for p in RAY3D])
+def test_3d_rays_match_reference(path, workdir):
+    """3-D ray runs ('R') against the reference's single-threaded .ray output,
+    and the product's own .ray file read back."""
+    from bellhopcuda_b200.rayfile import read_ray
+    g = np.load(path)
+    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.setup3d(root)
+        t.run()
+        rays = t.rays(dim=3)
+        t.writeout(root + "_gpu")
+    compare_rays3d(rays, g)
+    R = read_ray(root + "_gpu.ray")
+    assert R["kind"] == "xyz" and len(R["rays"]) == len(rays)
+    for a, b in zip(R["rays"], rays):
+        np.testing.assert_array_equal(a["xy"], b["rz"])
+        assert (a["ntop"], a["nbot"]) == (b["ntop"], b["nbot"])
+
+
+@pytest.mark.parametrize("path", EIG3D, ids=[os.path.basename(p)[:-4] for p in EIG3D])
+def test_3d_eigenrays_match_reference(path, workdir):
+    """The hit rays re-traced up to their hit (PostProcessEigenrays) against
+    the reference's .ray output of the same 3-D eigen run."""
+    g = np.load(path)
+    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.setup3d(root)
+        t.run()
+        rays = t.rays(dim=3)
+        t.writeout(root + "_gpu")
+    compare_rays3d(rays, g)
+    from bellhopcuda_b200.rayfile import read_ray
+    assert len(read_ray(root + "_gpu.ray")["rays"]) == len(rays)

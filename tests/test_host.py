@@ -100,7 +100,12 @@ def test_reader_rejects_bad_box(workdir):
 
 
 def test_reader_rejects_unsupported_beam(workdir):
-    root = _write(workdir, "cerveny", run_type="CC RR ")
+    """Cerveny beams are TL-only (as in the reference); ray-centred and simple
+    Gaussian beams with arrivals are outside this build."""
+    root = _write(workdir, "cerveny", run_type="AC RR ")
+    with pytest.raises(B.BhcbError, match="does not support eigenrays or arrivals"):
+        B.check_env(root)
+    root = _write(workdir, "raycen_arr", run_type="Ag RR ")
     with pytest.raises(B.BhcbError, match="not supported"):
         B.check_env(root)
 
