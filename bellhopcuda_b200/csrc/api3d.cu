@@ -21,6 +21,10 @@ namespace bhcb {
 
 cudaError_t launch_rays3d(const GroupDev *, int, const long long *, const int *, int, const long long *, double *,
                           int *, int *, RunCounters *, bool, int, cudaStream_t);
+cudaError_t launch_trace3d_rc(const GroupDev *, int, long long, XSeg3 *, unsigned long long, RunCounters *,
+                              unsigned long long *, int, cudaStream_t);
+cudaError_t launch_influence3d_rc(const XSeg3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
+                                  int, int, cudaStream_t);
 cudaError_t launch_trace3d(const GroupDev *, int, long long, SegRec3 *, unsigned long long, RunCounters *,
                            unsigned long long *, int, cudaStream_t);
 cudaError_t launch_influence3d(const SegRec3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
@@ -78,6 +82,7 @@ struct Run3 {
     // ray runs ('R'), and the eigenray re-trace of 'E' runs
     bool rayrun = false;
     std::vector<RaySet3> raysets;     // per environment
+    bool raycen = false;              // geometric beams in ray-centred coordinates ('g', 'b')
     int sm_count = 148;
 };
 
@@ -182,7 +187,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         d.isingle_alpha = T.isingle_alpha; d.isingle_beta = T.isingle_beta;
         d.dalpha = T.dalpha; d.dbeta = T.dbeta; d.deltas = T.deltas;
         d.box_x = T.box_x; d.box_y = T.box_y; d.box_z = T.box_z; d.freq0 = T.freq0;
-        d.gaussian = T.beam_type[0] == 'B';
+        d.gaussian = T.beam_type[0] == 'B' || T.beam_type[0] == 'b';   // IsGaussianGeomInfl
         d.coherent = T.run_type[0] == 'C';
         d.run0 = T.run_type[0];
         d.nsbp = (int)(T.sbp.size() / 2);
@@ -234,6 +239,11 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     r->eigen = k0 == 2;
     r->rayrun = k0 == 3;
     r->raysets.assign(r->envs.size(), RaySet3{});
+    auto rc = [](char b) { return b == 'g' || b == 'b'; };
+    r->raycen = !r->rayrun && rc(r->envs[0].T.beam_type[0]);
+    for(const auto &S : r->envs)
+        if(!r->rayrun && rc(S.T.beam_type[0]) != r->raycen)
+            throw std::runtime_error("a 3-D batch must use Cartesian or ray-centred beams throughout");
     for(const auto &S : r->envs)
         if(kind(S.T.run_type[0]) != k0) throw std::runtime_error("a 3-D batch must use one run type");
     auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
@@ -381,7 +391,7 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
 void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count, uint64_t max_memory,
               RangeStats &acc)
 {
-    const size_t rec = sizeof(SegRec3);
+    const size_t rec = r->raycen ? sizeof(XSeg3) : sizeof(SegRec3);
     // TL: the field; arrivals: their storage, and half of the rest is left
     // for the arrival candidates
     const bool cand_mode = r->arrivals || r->eigen;
@@ -421,8 +431,12 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
         CK(cudaEventRecord(e0, st));
         const long long nj = j1 - j0;
         const int tgrid = (int)std::max<long long>(1, std::min<long long>((nj + 63) / 64, (long long)sm_count * 16));
-        CK(launch_trace3d((const GroupDev *)r->groups_d.p, (int)r->groups_h.size(), j1, (SegRec3 *)r->segs.p,
-                          r->seg_cap, ctr, jc, tgrid, st));
+        if(r->raycen)
+            CK(launch_trace3d_rc((const GroupDev *)r->groups_d.p, (int)r->groups_h.size(), j1, (XSeg3 *)r->segs.p,
+                                 r->seg_cap, ctr, jc, tgrid, st));
+        else
+            CK(launch_trace3d((const GroupDev *)r->groups_d.p, (int)r->groups_h.size(), j1, (SegRec3 *)r->segs.p,
+                              r->seg_cap, ctr, jc, tgrid, st));
         CK(cudaEventRecord(e1, st));
         RunCounters rc{};
         CK(cudaMemcpyAsync(&rc, ctr, sizeof rc, cudaMemcpyDeviceToHost, st));
@@ -459,9 +473,15 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
             acc.trace_ms += tms;
             return;
         }
-        if(rc.err_bits == 0)
+        if(rc.err_bits == 0 && r->raycen) {
+            int nzt = 1;   // (depth, bearing) pairs per record, the most of the batch
+            for(const auto &S : r->envs) nzt = std::max(nzt, (int)(S.T.rz.size() * S.T.theta.size()));
+            CK(launch_influence3d_rc((const XSeg3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
+                                     (int)r->groups_h.size(), (float2 *)r->field.p, ctr, nzt, sm_count * 16, st));
+        } else if(rc.err_bits == 0) {
             CK(launch_influence3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
                                   (int)r->groups_h.size(), (float2 *)r->field.p, ctr, igrid, st));
+        }
         CK(cudaEventRecord(e2, st));
         RunCounters rc2{};
         CK(cudaMemcpyAsync(&rc2, ctr, sizeof rc2, cudaMemcpyDeviceToHost, st));

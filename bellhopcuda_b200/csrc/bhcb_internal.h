@@ -228,6 +228,22 @@ struct alignas(16) XSeg {
     int32_t job, is, ir, ntop, nbot, kmah0, valid, pad;
 };
 
+// One 3-D segment of geometric beams in ray-centred coordinates ('g', 'b';
+// Step_InfluenceGeoRayCen, 3-D branch, src/influence.hpp:1030-1194): point0
+// with the ray normals of the last valid point, point1 with its own normals,
+// and what InfluenceGeoCore interpolates between them.
+struct alignas(16) XSeg3 {
+    double x0[3], n1a[3], n2a[3], ta[3];   // point0.x, inflray.rayn1 / rayn2, point0.c point0.t
+    double x1[3], n1b[3], n2b[3], tb[3];   // point1.x, its ray normals, point1.c point1.t
+    double q0[4], dq[4];                   // point0.q, point1.q - point0.q (m[col][row] as glm)
+    double tau0r, tau0i, dtaur, dtaui;
+    double rcp_q0, rcp_qhat0, cnst_num;    // Dalpha / c0, |cos alpha| Dbeta / c0, Ratio1 point1.c point1.Amp
+    double phase0, qold;                   // point0.Phase + inflray.phase; det(point0.q) (caustic reference)
+    double maxr_m, maxr_n;                 // Gaussian: largest beam radii along the two normals
+    double xs, ys;                         // source position
+    int32_t job, is, ntop, nbot;
+};
+
 // Bit layout of the ordering keys (low to high): arrivals: step | job | cell;
 // eigen: depth | walk position | step | job | field (3-D: depth | bearing |
 // walk position | step | job | trace group).

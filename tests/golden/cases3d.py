@@ -155,6 +155,28 @@ def seamount3d_ray():
     return f
 
 
+def munk3d_raycen_hat():
+    """Geometric hat beams in ray-centred coordinates ('g')."""
+    return _munk_slice("Cg   3")
+
+
+def munk3d_raycen_gauss():
+    """Geometric Gaussian beams in ray-centred coordinates ('b')."""
+    return _munk_slice("Cb   3")
+
+
+def seamount3d_raycen_hat():
+    f = seamount3d_gauss()
+    f[".env"] = f[".env"].replace("'CB   3'", "'Cg   3'")
+    return f
+
+
+def parabot3d_raycen_incoherent():
+    f = parabot3d_hat()
+    f[".env"] = f[".env"].replace("'CG   3'", "'Ig   3'")
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -172,4 +194,8 @@ CASES3D = {
     "munk3d_brc_gauss": munk3d_brc_gauss,
     "munk3d_ray": munk3d_ray,
     "seamount3d_ray": seamount3d_ray,
+    "munk3d_raycen_hat": munk3d_raycen_hat,
+    "munk3d_raycen_gauss": munk3d_raycen_gauss,
+    "seamount3d_raycen_hat": seamount3d_raycen_hat,
+    "parabot3d_raycen_incoherent": parabot3d_raycen_incoherent,
 }

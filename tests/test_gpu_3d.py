@@ -42,7 +42,7 @@ def to_file_order(u):
     return np.transpose(u, (1, 2, 3, 0, 4, 5))
 
 
-TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p and "_ray" not in p]
+TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p and not p.endswith("_ray.npz")]
 
 
 @pytest.mark.parametrize("path", TL3D, ids=[os.path.basename(p)[:-4] for p in TL3D])
@@ -190,7 +190,7 @@ def test_3d_eigen_hits_match_reference(path, workdir):
     np.testing.assert_allclose(fan[hits["ialpha"]], g["alpha"], rtol=1e-9, atol=1e-12)
 
 
-RAY3D = sorted(p for p in GOLD if "_ray" in p)
+RAY3D = sorted(p for p in GOLD if p.endswith("_ray.npz"))
 
 
 def compare_rays3d(rays, g, frac=0.97):
