@@ -43,7 +43,7 @@ class BhcbError(RuntimeError):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("trace_block", C.c_int32), ("influence_ctas_per_sm", C.c_int32),
+    _fields_ = [("trace_block", C.c_int32), ("influence_ctas_per_sm", C.c_int32), ("stage_kb", C.c_int32),
                 ("trace_ms", C.c_double), ("influence_ms", C.c_double)]
 
 
@@ -397,10 +397,10 @@ class Tracer:
         t = Tuning()
         self._check(self._lib.bhcb_autotune(self._h, repeats, C.byref(t)))
         return {"trace_block": t.trace_block, "influence_ctas_per_sm": t.influence_ctas_per_sm,
-                "trace_ms": t.trace_ms, "influence_ms": t.influence_ms}
+                "stage_kb": t.stage_kb, "trace_ms": t.trace_ms, "influence_ms": t.influence_ms}
 
-    def set_tuning(self, trace_block: int, influence_ctas_per_sm: int):
-        t = Tuning(trace_block, influence_ctas_per_sm, 0.0, 0.0)
+    def set_tuning(self, trace_block: int, influence_ctas_per_sm: int, stage_kb: int = 32):
+        t = Tuning(trace_block, influence_ctas_per_sm, stage_kb, 0.0, 0.0)
         self._check(self._lib.bhcb_set_tuning(self._h, C.byref(t)))
 
     def stream_ptr(self) -> int:

@@ -20,11 +20,13 @@
 #include "host/rt.h"
 #include "host/run3d.h"
 #include "noalloc.h"
+#include "tabstage.cuh"
 
 namespace bhcb {
 template<typename R> cudaError_t launch_trace(const GroupDev *, int, long long, void *,
                                               unsigned long long, RunCounters *,
-                                              unsigned long long *, unsigned int *, int, int, cudaStream_t);
+                                              unsigned long long *, unsigned int *, int, int, cudaStream_t,
+                                              unsigned int);
 cudaError_t launch_influence_mixed(const void *, unsigned long long, const GroupDev *, int, const double *,
                                    float2 *, RunCounters *, bool, bool, int, cudaStream_t, unsigned int *,
                                    unsigned long long *);
@@ -149,6 +151,8 @@ struct bhcb_ctx {
     bool any_gauss = false, any_coherent = false, mixed_types = false;
     bool gauss = false, coherent = true;
     int xkind = INFL_GEO_CART;       // InflKind of the batch
+    unsigned int stage_cap = STAGE_DEFAULT_BYTES;   // staging budget per trace CTA (bhcb_tuning.stage_kb)
+    std::vector<EnvDev> envdev_h;    // the prepared environments (counts; plans the staging)
 
     DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
     unsigned long long job0_h = 0;   // staging for the job counter's start value
@@ -378,6 +382,7 @@ void do_prepare(bhcb_ctx *c)
         d.arrivals = c->mode == MODE_ARR;
         envdev.push_back(d);
     }
+    c->envdev_h = envdev;
     size_t env_off = A.put(envdev);
     c->arena.ensure(A.bytes.size());
     void *ab = c->arena.p;
@@ -505,6 +510,11 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         return;
     }
     int tblock = c->trace_block;
+    unsigned int stage_bytes = 0;   // tables of the launched groups that fit the staging budget
+    for(int g = g0; g < g1; ++g) {
+        size_t off[ST_COUNT];
+        stage_bytes = std::max<unsigned int>(stage_bytes, (unsigned int)stage_plan(c->envdev_h[g], c->stage_cap, off));
+    }
     long long tgrid = std::min<long long>((job1 - job0 + tblock - 1) / tblock, (long long)c->sm_count * 16);
     if(tgrid < 1) tgrid = 1;
     const GroupDev *G = (const GroupDev *)c->groups_d.p + g0;
@@ -525,10 +535,10 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     }
     if(fp64)
         CK(launch_trace<double>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
-                                c->stream));
+                                c->stream, stage_bytes));
     else
         CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
-                               c->stream));
+                               c->stream, stage_bytes));
     CK(cudaEventRecord(c->ev[1], c->stream));
     if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
     if(ovl) {
@@ -1572,6 +1582,13 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
             if(tr < t.trace_ms) { t.trace_ms = tr; t.trace_block = tb; }
         }
         c->trace_block = t.trace_block;
+        t.stage_kb = (int32_t)(c->stage_cap / 1024);
+        for(int kb : {0, 32, 64}) {   // shared-memory table staging
+            c->stage_cap = (unsigned int)kb * 1024u;
+            timed(tr, inf);
+            if(tr < t.trace_ms) { t.trace_ms = tr; t.stage_kb = kb; }
+        }
+        c->stage_cap = (unsigned int)t.stage_kb * 1024u;
         for(int k : {2, 3, 4, 5, 6, 8, 12}) {
             c->influence_ctas_per_sm = k;
             timed(tr, inf);
@@ -1581,8 +1598,8 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         c->overlap = overlap;
         if(out) *out = t;
         char b[160];
-        snprintf(b, sizeof b, "autotune: trace %d threads/CTA (%.3f ms), influence %d CTAs/SM (%.3f ms)",
-                 t.trace_block, t.trace_ms, t.influence_ctas_per_sm, t.influence_ms);
+        snprintf(b, sizeof b, "autotune: trace %d threads/CTA, %d KB staged (%.3f ms), influence %d CTAs/SM (%.3f ms)",
+                 t.trace_block, t.stage_kb, t.trace_ms, t.influence_ctas_per_sm, t.influence_ms);
         c->msg(b);
         return BHCB_OK;
     });
@@ -1595,8 +1612,11 @@ int bhcb_set_tuning(bhcb_ctx *c, const bhcb_tuning *t)
         if(t->trace_block != 32 && t->trace_block != 64) throw std::invalid_argument("trace_block must be 32 or 64");
         if(t->influence_ctas_per_sm < 1 || t->influence_ctas_per_sm > 64)
             throw std::invalid_argument("influence_ctas_per_sm must be in 1..64");
+        if(t->stage_kb < 0 || t->stage_kb > (int32_t)(STAGE_MAX_BYTES / 1024))
+            throw std::invalid_argument("stage_kb must be in 0..64");
         c->trace_block = t->trace_block;
         c->influence_ctas_per_sm = t->influence_ctas_per_sm;
+        c->stage_cap = (unsigned int)t->stage_kb * 1024u;
         return BHCB_OK;
     });
 }

@@ -23,6 +23,7 @@ enum : uint32_t {
     ERR_RAYINIT = 2, ERR_BOUNDARY_SEG_NAN = 3, ERR_BOUNDARY_CONDITION_TYPE = 4,
     ERR_INVALID_SSP_TYPE = 5, ERR_OUTSIDE_ALTIMETRY = 6, ERR_OUTSIDE_BATHYMETRY = 7,
     ERR_OUTSIDE_SSP = 8, ERR_QUAD_ISEG = 9,
+    ERR_STAGE_WAIT = 30,             // a shared-memory table staging wait ran out (this runtime's own)
     ERR_SEG_OVERFLOW = 31,
 };
 enum : uint32_t {

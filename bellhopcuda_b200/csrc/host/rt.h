@@ -49,13 +49,15 @@ struct DevBuf {
     }
 };
 
-// arrays packed at 256-byte offsets into one host image, uploaded at once
+// arrays packed at 256-byte offsets into one host image, uploaded at once;
+// each array's space is padded to a multiple of 16 bytes (bulk copies move
+// whole 16-byte words)
 struct Arena {
     std::vector<uint8_t> bytes;
     template<typename T> size_t put(const std::vector<T> &v)
     {
         size_t off = (bytes.size() + 255) & ~size_t(255);
-        bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 8));
+        bytes.resize(off + std::max<size_t>((v.size() * sizeof(T) + 15) & ~size_t(15), 16));
         if(!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
         return off;
     }

@@ -23,19 +23,29 @@
 #include "trace2d.cuh"
 #include "influence2d.cuh"
 #include "ray2d.cuh"
+#include "tabstage.cuh"
 
 namespace bhcb {
 
 // R: ray state; RecR: segment record (float for the mixed kernel's FP32 influence).
 template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_kernel(
     const GroupDev *__restrict__ groups, int ngroups, long long njobs, SegRec<RecR> *segs,
-    unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, unsigned int *blk_state)
+    unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, unsigned int *blk_state,
+    unsigned int stage_budget)
 {
+    // tables of the group this CTA's first rays belong to, staged in shared memory
+    extern __shared__ __align__(16) unsigned char s_tab[];
+    __shared__ EnvDev s_env;
+    __shared__ __align__(8) uint64_t s_bar;
+    const long long hint = min(njobs - 1, groups[0].job_base + (long long)blockIdx.x * blockDim.x);
+    const int gs = find_group(groups, ngroups, hint);
+    const bool staged = stage_budget > 0 && stage_env_tables(groups[gs].env, s_env, s_tab, stage_budget, &s_bar, ctr);
     for(;;) {
         long long job = (long long)atomicAdd(job_counter, 1ull);
         if(job >= njobs) break;
-        const GroupDev &G = groups[find_group(groups, ngroups, job)];
-        const EnvDev &e = *G.env;
+        const int gi = find_group(groups, ngroups, job);
+        const GroupDev &G = groups[gi];
+        const EnvDev &e = (staged && gi == gs) ? s_env : *G.env;
         int local = (int)(job - G.job_base);
         int nalpha_eff = e.isingle > 0 ? 1 : e.nalpha;
         int ialpha = e.isingle > 0 ? e.isingle - 1 : local % nalpha_eff;
@@ -100,6 +110,7 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
         close_block(segs, cur, blk_state);
         atomicAdd(&ctr->nsteps, nsteps);
     }
+    if(stage_budget > 0 && !staged) stage_drain(&s_bar);
 }
 
 // Ray trajectories (MainRayMode, src/trace.hpp:485-519) of listed rays: every
@@ -459,13 +470,21 @@ __global__ void scale_kernel(const float2 *__restrict__ acc, float2 *__restrict_
 template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroups, long long njobs,
                                               void *segs, unsigned long long cap, RunCounters *ctr,
                                               unsigned long long *job_counter, unsigned int *blk_state,
-                                              int grid, int block, cudaStream_t st)
+                                              int grid, int block, cudaStream_t st, unsigned int stage_bytes)
 {
     // the ray state is FP64 in both precisions (the mixed precision writes FP32
     // segment records for its FP32 influence kernel): the trajectory, and with it
     // every step and reflection decision, is the FP64 one
-    trace_kernel<double, R><<<grid, block, 0, st>>>(groups, ngroups, njobs, (SegRec<R> *)segs, cap, ctr,
-                                                    job_counter, blk_state);
+    static bool attr_set = false;
+    if(!attr_set) {   // dynamic shared memory above the 48 KB default
+        cudaError_t e = cudaFuncSetAttribute(trace_kernel<double, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)STAGE_MAX_BYTES);
+        if(e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if(stage_bytes > STAGE_MAX_BYTES) stage_bytes = STAGE_MAX_BYTES;
+    trace_kernel<double, R><<<grid, block, stage_bytes, st>>>(groups, ngroups, njobs, (SegRec<R> *)segs, cap, ctr,
+                                                              job_counter, blk_state, stage_bytes);
     return cudaGetLastError();
 }
 
@@ -508,10 +527,10 @@ cudaError_t launch_scale(const float2 *acc, float2 *out, const GroupDev *groups,
 
 template cudaError_t launch_trace<float>(const GroupDev *, int, long long, void *, unsigned long long,
                                          RunCounters *, unsigned long long *, unsigned int *, int, int,
-                                         cudaStream_t);
+                                         cudaStream_t, unsigned int);
 template cudaError_t launch_trace<double>(const GroupDev *, int, long long, void *, unsigned long long,
                                           RunCounters *, unsigned long long *, unsigned int *, int, int,
-                                          cudaStream_t);
+                                          cudaStream_t, unsigned int);
 template cudaError_t launch_influence<float>(const void *, unsigned long long, const GroupDev *, int,
                                              const double *, float2 *, RunCounters *, bool, bool, int,
                                              cudaStream_t);

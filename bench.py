@@ -171,7 +171,7 @@ def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=N
     if tune is None:
         t.tuning = t.autotune(repeats=1)
     else:
-        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"])
+        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"])
         t.tuning = tune
     s = torch.cuda.ExternalStream(t.stream_ptr(), device=gpu)
     for _ in range(warmup):
@@ -199,7 +199,7 @@ def time_e2e(B, torch, root, freqs, steps, gpu, tune=None):
     pinned host memory, all inside the timed window."""
     t = B.Tracer(gpu=gpu, precision=B.PREC_MIXED)
     if tune is not None:
-        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"])
+        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"])
     nf = len(freqs)
     t.setup(root)
     t.set_frequencies(0, freqs)
@@ -424,6 +424,7 @@ def main():
                    "parallelism": "replicas per GPU (one environment per rank)",
                    "launch_shape": {"trace_block": tuning["trace_block"],
                                     "influence_ctas_per_sm": tuning["influence_ctas_per_sm"],
+                                    "stage_kb": tuning["stage_kb"],
                                     "chosen_by": "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 3 * args.steps, "fp64_trace": fp64,

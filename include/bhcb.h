@@ -279,7 +279,8 @@ int bhcb_copy_rays(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, int32_t *npt
 
 /* Autotuner (no reference counterpart): times the prepared 2-D TL workload
    with each candidate launch shape — trace CTAs of 32 or 64 threads (one ray
-   per thread), 2..12 persistent influence CTAs per SM — `repeats` runs each
+   per thread), 0, 32 or 64 KB of environment tables staged in each trace
+   CTA's shared memory, 2..12 persistent influence CTAs per SM — `repeats` runs each
    (best of), keeps the fastest shape in the context and reports it. The
    trace and the influence are timed apart (serial influence) during tuning.
    bhcb_set_tuning applies a known shape (e.g. one saved from an earlier
@@ -287,6 +288,7 @@ int bhcb_copy_rays(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, int32_t *npt
 typedef struct bhcb_tuning {
     int32_t trace_block;            /* threads per trace CTA */
     int32_t influence_ctas_per_sm;  /* persistent influence CTAs per SM */
+    int32_t stage_kb;               /* shared memory (KB, 0..64) a trace CTA stages environment tables into */
     double trace_ms, influence_ms;  /* best times measured with the chosen shape */
 } bhcb_tuning;
 int bhcb_autotune(bhcb_ctx *ctx, int32_t repeats, bhcb_tuning *out);

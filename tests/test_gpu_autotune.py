@@ -24,6 +24,7 @@ def test_autotune_keeps_results(precision, tmp_path):
         tune = t.autotune(repeats=1)
         assert tune["trace_block"] in (32, 64)
         assert tune["influence_ctas_per_sm"] in (2, 3, 4, 5, 6, 8, 12)
+        assert tune["stage_kb"] in (0, 32, 64)
         assert 0 < tune["trace_ms"] < 1e4 and 0 < tune["influence_ms"] < 1e4
         t.run()
         got = [t.field(0, i) for i in range(2)]
@@ -31,6 +32,9 @@ def test_autotune_keeps_results(precision, tmp_path):
             np.testing.assert_allclose(a, b, rtol=1e-3, atol=1e-6 * np.abs(b).max())
         with pytest.raises(B.BhcbError):
             t.set_tuning(48, 4)
-        t.set_tuning(64, 3)
-        t.run()
-        np.testing.assert_allclose(t.field(0, 0), ref[0], rtol=1e-3, atol=1e-6 * np.abs(ref[0]).max())
+        with pytest.raises(B.BhcbError):
+            t.set_tuning(64, 3, 65)
+        for stage_kb in (0, 64):   # tables from global memory, all tables staged
+            t.set_tuning(64, 3, stage_kb)
+            t.run()
+            np.testing.assert_allclose(t.field(0, 0), ref[0], rtol=1e-3, atol=1e-6 * np.abs(ref[0]).max())
