@@ -51,20 +51,23 @@ def build(verbose: bool = False, force: bool = False, ptxas_v: bool = False) -> 
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
-    objs = []
+    objs, cmds = [], []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
     for src in CU_SOURCES:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         cmd = [cc, *ARCH, "-lineinfo", *common, "--expt-relaxed-constexpr", "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_v:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd, verbose)
+        cmds.append(cmd)
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-        cmd = [cc, *common, "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj]
-        _run(cmd, verbose)
+        cmds.append([cc, *common, "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    # translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(lambda c: _run(c, verbose), cmds))
     tmp = LIB + ".tmp"
     _run([cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], verbose)
     os.replace(tmp, LIB)
