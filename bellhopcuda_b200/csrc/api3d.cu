@@ -25,6 +25,12 @@ cudaError_t launch_trace3d_rc(const GroupDev *, int, long long, XSeg3 *, unsigne
                               unsigned long long *, int, cudaStream_t);
 cudaError_t launch_influence3d_rc(const XSeg3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
                                   int, int, cudaStream_t);
+cudaError_t launch_trace_nx(const GroupDev *, int, long long, void *, unsigned long long, RunCounters *,
+                            unsigned long long *, int, cudaStream_t);
+cudaError_t launch_influence_nx(const void *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *, int,
+                                int, cudaStream_t);
+cudaError_t launch_scale_nx(float2 *, const GroupDev *, int, int, cudaStream_t);
+size_t nx_record_bytes();
 cudaError_t launch_trace3d(const GroupDev *, int, long long, SegRec3 *, unsigned long long, RunCounters *,
                            unsigned long long *, int, cudaStream_t);
 cudaError_t launch_influence3d(const SegRec3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
@@ -83,6 +89,7 @@ struct Run3 {
     bool rayrun = false;
     std::vector<RaySet3> raysets;     // per environment
     bool raycen = false;              // geometric beams in ray-centred coordinates ('g', 'b')
+    bool nx2d = false;                // N x 2-D rays (RunType(6) '2')
     int sm_count = 148;
 };
 
@@ -176,6 +183,13 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         e.deltas = T.deltas;
         e.ntrc = (int)(T.trc.size() / 3);
         e.nbrc = (int)(T.brc.size() / 3);
+        // the plane's receiver ranges and beam flags for the 2-D influence of Nx2D rays
+        e.nrr = (int)T.rr.size();
+        e.gaussian = T.beam_type[0] == 'B';
+        e.coherent = T.run_type[0] == 'C';
+        e.beam2 = T.beam_type[2];
+        e.run0 = T.run_type[0];
+        e.arrivals = 0;
         d.hex = T.ssp_type == SSP_HEXAHEDRAL;
         d.hnx = (int)T.hx.size(); d.hny = (int)T.hy.size(); d.hnz = (int)T.hz.size();
         d.top = T.top;
@@ -219,6 +233,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         e.c = dptr<double>(ab, o.c); e.cz = dptr<double>(ab, o.cz);
         e.n2 = dptr<double>(ab, o.n2); e.n2z = dptr<double>(ab, o.n2z); e.coef = dptr<double>(ab, o.coef);
         e.trc = dptr<double>(ab, o.trc); e.brc = dptr<double>(ab, o.brc);
+        e.rr = dptr<double>(ab, o.rr);
         d.hx = dptr<double>(ab, o.hx); d.hy = dptr<double>(ab, o.hy); d.hz = dptr<double>(ab, o.hz);
         d.hc = dptr<double>(ab, o.hc); d.hcz = dptr<double>(ab, o.hcz);
         d.btop = dptr<Bdry3PtDev>(ab, o.btop); d.bbot = dptr<Bdry3PtDev>(ab, o.bbot);
@@ -239,6 +254,9 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     r->eigen = k0 == 2;
     r->rayrun = k0 == 3;
     r->raysets.assign(r->envs.size(), RaySet3{});
+    r->nx2d = r->envs[0].T.nx2d;
+    for(const auto &S : r->envs)
+        if(S.T.nx2d != r->nx2d) throw std::runtime_error("a 3-D batch must be all 3-D or all Nx2D");
     auto rc = [](char b) { return b == 'g' || b == 'b'; };
     r->raycen = !r->rayrun && rc(r->envs[0].T.beam_type[0]);
     for(const auto &S : r->envs)
@@ -391,7 +409,7 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
 void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count, uint64_t max_memory,
               RangeStats &acc)
 {
-    const size_t rec = r->raycen ? sizeof(XSeg3) : sizeof(SegRec3);
+    const size_t rec = r->nx2d ? nx_record_bytes() : (r->raycen ? sizeof(XSeg3) : sizeof(SegRec3));
     // TL: the field; arrivals: their storage, and half of the rest is left
     // for the arrival candidates
     const bool cand_mode = r->arrivals || r->eigen;
@@ -431,7 +449,10 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
         CK(cudaEventRecord(e0, st));
         const long long nj = j1 - j0;
         const int tgrid = (int)std::max<long long>(1, std::min<long long>((nj + 63) / 64, (long long)sm_count * 16));
-        if(r->raycen)
+        if(r->nx2d)
+            CK(launch_trace_nx((const GroupDev *)r->groups_d.p, (int)r->groups_h.size(), j1, r->segs.p, r->seg_cap,
+                               ctr, jc, tgrid, st));
+        else if(r->raycen)
             CK(launch_trace3d_rc((const GroupDev *)r->groups_d.p, (int)r->groups_h.size(), j1, (XSeg3 *)r->segs.p,
                                  r->seg_cap, ctr, jc, tgrid, st));
         else
@@ -473,7 +494,12 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
             acc.trace_ms += tms;
             return;
         }
-        if(rc.err_bits == 0 && r->raycen) {
+        if(rc.err_bits == 0 && r->nx2d) {
+            int nz = 1;
+            for(const auto &S : r->envs) nz = std::max(nz, (int)S.T.rz.size());
+            CK(launch_influence_nx(r->segs.p, nseg, (const GroupDev *)r->groups_d.p, (int)r->groups_h.size(),
+                                   (float2 *)r->field.p, ctr, nz, sm_count * 16, st));
+        } else if(rc.err_bits == 0 && r->raycen) {
             int nzt = 1;   // (depth, bearing) pairs per record, the most of the batch
             for(const auto &S : r->envs) nzt = std::max(nzt, (int)(S.T.rz.size() * S.T.theta.size()));
             CK(launch_influence3d_rc((const XSeg3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
@@ -601,9 +627,13 @@ uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, i
     RangeStats acc;
     run_jobs(r, 0, r->njobs, st, sm_count, max_memory, acc);
     if(acc.rc.err_bits == 0 && tl) {
-        for(const auto &S : r->envs)
-            if(S.T.run_type[0] != 'C')
+        for(size_t i = 0; i < r->envs.size(); ++i) {
+            const auto &S = r->envs[i];
+            if(r->nx2d)   // 2-D pressure scaling along each plane's ranges
+                CK(launch_scale_nx((float2 *)r->field.p, (const GroupDev *)r->groups_d.p, (int)i, sm_count * 4, st));
+            else if(S.T.run_type[0] != 'C')
                 CK(launch_sqrt3d((float2 *)r->field.p + S.field_base, S.field_n, sm_count * 4, st));
+        }
         CK(cudaStreamSynchronize(st));
     }
     r->ran = acc.rc.err_bits == 0;

@@ -32,7 +32,7 @@ enum : uint32_t {
     WARN_INVALID_WIDTH_BUGGY = 13,
     WARN_OUTSIDE_ALTIMETRY = 6, WARN_OUTSIDE_BATHYMETRY = 7,
     WARN_STEP_NEGATIVE_H = 8, WARN_TRIDIAG_H_NEGATIVE = 9, WARN_TRIDIAG_H_GROWING = 10,
-    WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17,
+    WARN_CPCHIP_INVALIDXT = 16, WARN_CPCHIP_INVALIDCCOEF = 17, WARN_OCEANTORAYX_GAVEUP = 18,
 };
 
 struct HsDev {          // halfspace (include/bhc/structs.hpp:93-101)

@@ -987,7 +987,9 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     default: env_error("unknown RunType");
     }
     const bool ray_run3 = t.run_type[0] == 'R';
-    if(t.run_type[5] != '3') env_error("3-D runs need RunType(6) = '3'");
+    if(t.run_type[5] != '3' && t.run_type[5] != '2')
+        env_error("3-D runs need RunType(6) = '3' (3-D rays) or '2' (Nx2D)");
+    t.nx2d = t.run_type[5] == '2';
     switch(t.run_type[1]) {
     case 'C': case 'R': case 'S': case 'b': case 'B': case 'g': break;
     default: t.run_type[1] = 'G';
@@ -1004,6 +1006,13 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
         env_error(std::string("3-D beam type '") + bt + "' is not supported by this build (geometric 'G', 'B', 'g', 'b')");
     if(!ray_run3 && (bt == 'g' || bt == 'b') && t.run_type[0] != 'C' && t.run_type[0] != 'S' && t.run_type[0] != 'I')
         env_error("3-D ray-centred beams with arrivals or eigenrays are not supported by this build");
+    if(t.nx2d) {   // Nx2D: TL runs with Cartesian geometric beams
+        if(ray_run3 || (t.run_type[0] != 'C' && t.run_type[0] != 'S' && t.run_type[0] != 'I'))
+            env_error("Nx2D ray, arrival and eigenray runs are not supported by this build (TL runs are)");
+        if(!(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
+            env_error(std::string("Nx2D beam type '") + bt + "' is not supported by this build (Cartesian 'G' / 'B')");
+        if(t.beam_type[3] == 'S') env_error("Nx2D beam shift is not supported by this build");
+    }
     if(t.run_type[3] == 'X') env_error("line sources are 2-D only");
 
     char st = in.top_opt[0];
@@ -1077,6 +1086,7 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     fix360(al);
     std::vector<double> be = tab_sort(in.beta_deg, in.nbeta);
     fix360(be);
+    if(t.nx2d && !ray_run3) be = t.theta;   // beams on the receiver radials (src/module/rayangles.hpp:163-179)
     for(size_t i = 1; i < al.size(); ++i) if(!(al[i] > al[i - 1])) env_error("elevation angles are not monotonically increasing");
     for(size_t i = 1; i < be.size(); ++i) if(!(be[i] > be[i - 1])) env_error("bearing angles are not monotonically increasing");
     for(auto &v : al) v *= kPi / 180.0;

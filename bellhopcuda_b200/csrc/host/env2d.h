@@ -120,6 +120,7 @@ struct Env3Tables {
     int32_t isingle_alpha = 0, isingle_beta = 0;
     char run_type[7];
     char beam_type[4];
+    bool nx2d = false;                       // RunType(6) '2': N x 2-D rays in the 3-D ocean
     std::vector<std::string> warnings;
 };
 

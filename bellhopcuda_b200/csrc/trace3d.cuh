@@ -244,7 +244,8 @@ __device__ __forceinline__ void tangent_normals(const Ray3 &r, double c, V3 nB, 
 
 // ------------------------------------------------------------ step geometry
 // src/step.hpp:41-79 (depth interfaces; none past the first / last layer in 3-D)
-__device__ __forceinline__ void depth_iface3(bool stepTo, double &h, V3 &x, V3 x0, V3 u, int iz0, const Env3Dev &E)
+__device__ __forceinline__ void depth_iface3(bool stepTo, double &h, V3 &x, V3 x0, V3 u, int iz0, const Env3Dev &E,
+                                             int &snap)
 {
     if(!stepTo) h = 1.7976931348623157e308;
     if(fabs(u.z) > DBL_EPS) {
@@ -252,10 +253,10 @@ __device__ __forceinline__ void depth_iface3(bool stepTo, double &h, V3 &x, V3 x
         const int nz = E.e1d.nssp;
         if(z[iz0] > x.z && iz0 > 0) {
             h = (z[iz0] - x0.z) / u.z;
-            if(stepTo) { x = add3(x0, scl3(h, u)); x.z = z[iz0]; }
+            if(stepTo) { x = add3(x0, scl3(h, u)); x.z = z[iz0]; snap = 2; }
         } else if(z[iz0 + 1] < x.z && iz0 + 1 < nz - 1) {
             h = (z[iz0 + 1] - x0.z) / u.z;
-            if(stepTo) { x = add3(x0, scl3(h, u)); x.z = z[iz0 + 1]; }
+            if(stepTo) { x = add3(x0, scl3(h, u)); x.z = z[iz0 + 1]; snap = 2; }
         }
     }
 }
@@ -267,7 +268,8 @@ __device__ __forceinline__ void setc3(V3 &v, int d, double a)
 }
 
 // BeamBoxCrossing (src/step.hpp:84-108): box centred at (source x, y, 0)
-__device__ __forceinline__ void box3(bool stepTo, int d, double &h, V3 &x, V3 x0, V3 u, V3 xs, const Env3Dev &E)
+__device__ __forceinline__ void box3(bool stepTo, int d, double &h, V3 &x, V3 x0, V3 u, V3 xs, const Env3Dev &E,
+                                     int &snap)
 {
     if(!stepTo) h = 1.7976931348623157e308;
     const double bx = d == 0 ? E.box_x : (d == 1 ? E.box_y : E.box_z);
@@ -278,12 +280,14 @@ __device__ __forceinline__ void box3(bool stepTo, int d, double &h, V3 &x, V3 x0
         if(stepTo) {
             x = add3(x0, scl3(h, u));
             setc3(x, d, ctr + copysign(bx, d0));
+            snap = d;
         }
     }
 }
 
 // TopBotCrossing (src/step.hpp:113-147)
-__device__ __forceinline__ void topbot3(bool stepTo, double &h, const Bd3 &bd, V3 &x, V3 x0, V3 u, bool &refl)
+__device__ __forceinline__ void topbot3(bool stepTo, double &h, const Bd3 &bd, V3 &x, V3 x0, V3 u, bool &refl,
+                                        int &snap)
 {
     if(!stepTo) h = 1.7976931348623157e308;
     const V3 d = sub3(x, bd.x), d0 = sub3(x0, bd.x);
@@ -293,6 +297,7 @@ __device__ __forceinline__ void topbot3(bool stepTo, double &h, const Bd3 &bd, V
         if(stepTo) {
             x = add3(x0, scl3(h, u));
             if(fabs(bd.n.x) < DBL_EPS && fabs(bd.n.y) < DBL_EPS) x.z = bd.x.z;
+            snap = 2;   // exactness in depth matters most, flat or not
         }
         refl = true;
     } else {
@@ -302,7 +307,7 @@ __device__ __forceinline__ void topbot3(bool stepTo, double &h, const Bd3 &bd, V
 
 // TopBotSegCrossing in x or y (src/step.hpp:153-205), with the hexahedral cell limits
 __device__ __forceinline__ void cellseg3(bool stepTo, bool isY, double &h, const Bd3 &top, const Bd3 &bot, V3 &x,
-                                         V3 x0, V3 u, const Env3Dev &E, const Seg3 &s0, bool &tr, bool &br)
+                                         V3 x0, V3 u, const Env3Dev &E, const Seg3 &s0, bool &tr, bool &br, int &snap)
 {
     double lmin = isY ? max(top.ymin, bot.ymin) : max(top.xmin, bot.xmin);
     double lmax = isY ? min(top.ymax, bot.ymax) : min(top.xmax, bot.xmax);
@@ -320,6 +325,7 @@ __device__ __forceinline__ void cellseg3(bool stepTo, bool isY, double &h, const
             if(stepTo) {
                 x = add3(x0, scl3(h, u));
                 if(isY) x.y = lmin; else x.x = lmin;
+                snap = isY ? 1 : 0;
                 tr = br = false;
             }
         } else if(xw > lmax) {
@@ -327,6 +333,7 @@ __device__ __forceinline__ void cellseg3(bool stepTo, bool isY, double &h, const
             if(stepTo) {
                 x = add3(x0, scl3(h, u));
                 if(isY) x.y = lmax; else x.x = lmax;
+                snap = isY ? 1 : 0;
                 tr = br = false;
             }
         }
@@ -335,7 +342,7 @@ __device__ __forceinline__ void cellseg3(bool stepTo, bool isY, double &h, const
 
 // TriDiagCrossing (src/step.hpp:210-256)
 __device__ __forceinline__ void tridiag3(bool stepTo, double &h, Bd3 &bd, V3 &x, V3 x0, V3 u, bool &tr, bool &br,
-                                         RunCounters *ctr)
+                                         RunCounters *ctr, int &snap)
 {
     if(!stepTo) h = 1.7976931348623157e308;
     if(bd.onEdge) return;
@@ -358,6 +365,7 @@ __device__ __forceinline__ void tridiag3(bool stepTo, double &h, Bd3 &bd, V3 &x,
         x = add3(x0, scl3(h, u));
         bd.justSteppedTo = true;
         bd.outgoingSide = newSide;
+        snap = -2;   // x or y, unspecified
         tr = br = false;
     }
 }
@@ -368,17 +376,18 @@ __device__ __forceinline__ void reduce_step3(V3 x0, V3 u, const Seg3 &s0, Bd3 &t
 {
     double hInt, hB0, hB1, hB2, hTop, hBot, hX, hY, hTD, hBD;
     bool dummy = false, d2 = false;
+    int sn = -1;
     V3 x = add3(x0, scl3(h, u));
-    depth_iface3(false, hInt, x, x0, u, s0.z, E);
-    box3(false, 0, hB0, x, x0, u, xs, E);
-    box3(false, 1, hB1, x, x0, u, xs, E);
-    box3(false, 2, hB2, x, x0, u, xs, E);
-    topbot3(false, hTop, top, x, x0, u, dummy);
-    topbot3(false, hBot, bot, x, x0, u, dummy);
-    cellseg3(false, false, hX, top, bot, x, x0, u, E, s0, dummy, d2);
-    cellseg3(false, true, hY, top, bot, x, x0, u, E, s0, dummy, d2);
-    tridiag3(false, hTD, top, x, x0, u, dummy, d2, ctr);
-    tridiag3(false, hBD, bot, x, x0, u, dummy, d2, ctr);
+    depth_iface3(false, hInt, x, x0, u, s0.z, E, sn);
+    box3(false, 0, hB0, x, x0, u, xs, E, sn);
+    box3(false, 1, hB1, x, x0, u, xs, E, sn);
+    box3(false, 2, hB2, x, x0, u, xs, E, sn);
+    topbot3(false, hTop, top, x, x0, u, dummy, sn);
+    topbot3(false, hBot, bot, x, x0, u, dummy, sn);
+    cellseg3(false, false, hX, top, bot, x, x0, u, E, s0, dummy, d2, sn);
+    cellseg3(false, true, hY, top, bot, x, x0, u, E, s0, dummy, d2, sn);
+    tridiag3(false, hTD, top, x, x0, u, dummy, d2, ctr, sn);
+    tridiag3(false, hBD, bot, x, x0, u, dummy, d2, ctr, sn);
     h = min(min(min(h, hInt), min(min(min(hB0, hB1), hB2), min(hTop, hBot))), min(min(hX, hY), min(hTD, hBD)));
     if(h < -1e-4) run_warn(ctr, WARN_STEP_NEGATIVE_H);
     const double hmin = INF_STEP * E.deltas;
@@ -390,30 +399,35 @@ __device__ __forceinline__ void reduce_step3(V3 x0, V3 u, const Seg3 &s0, Bd3 &t
     }
 }
 
-// StepToBdry, 3-D (src/step.hpp:345-422)
+// StepToBdry, 3-D (src/step.hpp:345-422); snap: the coordinate the landing
+// point was put on exactly (OceanToRayX's snapDim: -1 none, 0 x, 1 y, 2 z,
+// -2 x or y)
 __device__ __forceinline__ void step_to_bdry3(V3 x0, V3 &x2, V3 u, double &h, bool &tr, bool &br, const Seg3 &s0,
-                                              Bd3 &top, Bd3 &bot, V3 xs, const Env3Dev &E, RunCounters *ctr)
+                                              Bd3 &top, Bd3 &bot, V3 xs, const Env3Dev &E, RunCounters *ctr, int &snap)
 {
     x2 = add3(x0, scl3(h, u));
-    depth_iface3(true, h, x2, x0, u, s0.z, E);
-    box3(true, 0, h, x2, x0, u, xs, E);
-    box3(true, 1, h, x2, x0, u, xs, E);
-    box3(true, 2, h, x2, x0, u, xs, E);
-    topbot3(true, h, top, x2, x0, u, tr);
-    topbot3(true, h, bot, x2, x0, u, br);
+    snap = -1;
+    depth_iface3(true, h, x2, x0, u, s0.z, E, snap);
+    box3(true, 0, h, x2, x0, u, xs, E, snap);
+    box3(true, 1, h, x2, x0, u, xs, E, snap);
+    box3(true, 2, h, x2, x0, u, xs, E, snap);
+    topbot3(true, h, top, x2, x0, u, tr, snap);
+    topbot3(true, h, bot, x2, x0, u, br, snap);
     if(br) tr = false;
-    cellseg3(true, false, h, top, bot, x2, x0, u, E, s0, tr, br);
-    cellseg3(true, true, h, top, bot, x2, x0, u, E, s0, tr, br);
-    tridiag3(true, h, top, x2, x0, u, tr, br, ctr);
-    tridiag3(true, h, bot, x2, x0, u, tr, br, ctr);
+    cellseg3(true, false, h, top, bot, x2, x0, u, E, s0, tr, br, snap);
+    cellseg3(true, true, h, top, bot, x2, x0, u, E, s0, tr, br, snap);
+    tridiag3(true, h, top, x2, x0, u, tr, br, ctr, snap);
+    tridiag3(true, h, bot, x2, x0, u, tr, br, ctr, snap);
     const double hmin = INF_STEP * E.deltas;
     if(h < hmin) {
         h = hmin;
         x2 = add3(x0, scl3(h, u));
+        snap = -1;
         if(dot3(top.n, sub3(x2, top.x)) > DBL_EPS) {
             tr = true;
             top.justSteppedTo = false;
             bot.justSteppedTo = false;
+            snap = 2;
         } else {
             tr = false;
         }
@@ -422,6 +436,7 @@ __device__ __forceinline__ void step_to_bdry3(V3 x0, V3 &x2, V3 u, double &h, bo
             tr = false;
             top.justSteppedTo = false;
             bot.justSteppedTo = false;
+            snap = 2;
         } else {
             br = false;
         }
@@ -551,7 +566,8 @@ __device__ __forceinline__ void step3d(const Ray3 &r0, Ray3 &r2, Bd3 &top, Bd3 &
     const double w1 = h / (2.0 * halfh);
     const double w0 = 1.0 - w1;
     const V3 u2 = add3(scl3(w0, u0), scl3(w1, u1));
-    step_to_bdry3(r0.x, r2.x, u2, h, tr, br, s0, top, bot, xs, E, ctr);
+    int snap;
+    step_to_bdry3(r0.x, r2.x, u2, h, tr, br, s0, top, bot, xs, E, ctr, snap);
     const double hw0 = h * w0, hw1 = h * w1;
     r2.t = v3(r0.t.x - hw0 * o0.gradc.x / csq0 - hw1 * o1.gradc.x / csq1,
               r0.t.y - hw0 * o0.gradc.y / csq0 - hw1 * o1.gradc.y / csq1,

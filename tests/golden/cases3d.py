@@ -177,6 +177,33 @@ def parabot3d_raycen_incoherent():
     return f
 
 
+def munk3d_nx2d_gauss():
+    """Nx2D (RunType(6) '2'): 2-D Gaussian beams along each receiver bearing of
+    the Munk slice."""
+    return _munk_slice("CB   2")
+
+
+def hex3d_nx2d_hat():
+    """Nx2D through the hexahedral SSP (range- and bearing-dependent channel)."""
+    f = hex3d_gauss()
+    f[".env"] = f[".env"].replace("'CB   3'", "'CG   2'")
+    return f
+
+
+def seamount3d_nx2d_gauss():
+    """Nx2D over the seamount grid: bottom reflections off the triangles
+    projected on each bearing's plane."""
+    f = seamount3d_gauss()
+    f[".env"] = f[".env"].replace("'CB   3'", "'CB   2'")
+    return f
+
+
+def parabot3d_nx2d_incoherent():
+    f = parabot3d_hat()
+    f[".env"] = f[".env"].replace("'CG   3'", "'IG   2'")
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -198,4 +225,8 @@ CASES3D = {
     "munk3d_raycen_gauss": munk3d_raycen_gauss,
     "seamount3d_raycen_hat": seamount3d_raycen_hat,
     "parabot3d_raycen_incoherent": parabot3d_raycen_incoherent,
+    "munk3d_nx2d_gauss": munk3d_nx2d_gauss,
+    "hex3d_nx2d_hat": hex3d_nx2d_hat,
+    "seamount3d_nx2d_gauss": seamount3d_nx2d_gauss,
+    "parabot3d_nx2d_incoherent": parabot3d_nx2d_incoherent,
 }

@@ -1,7 +1,8 @@
 """Generate the 3-D golden TL fixtures from the reference itself.
 
 Runs the reference's own bellhopcxx (compiled from its sources by
-oracle/Makefile into oracle/_ref/) as a 3-D run (-3) on every case of
+oracle/Makefile into oracle/_ref/) as a 3-D run (-3), or an Nx2D run (-4) for
+cases whose RunType(6) is '2', on every case of
 tests/golden/cases3d.py and stores, per case, the input files' text and the
 scaled complex field (TL runs) or the arrivals (RunType 'a') as
 tests/golden/<case>.npz. The GPU tests write the input
@@ -44,7 +45,11 @@ def main(names=None):
                 with open(root + suffix, "w") as f:
                     f.write(text)
             t0 = time.time()
-            r = subprocess.run([EXE, "-3", "-1", root], capture_output=True, text=True)
+            # RunType(6) '2' selects the reference's Nx2D mode (-4), '3' its 3-D mode
+            run_line = [ln for ln in files[".env"].splitlines() if ln.startswith("'") and ln.rstrip().endswith(
+                ("3'", "2'"))]
+            dim = "-4" if run_line and run_line[-1].rstrip().endswith("2'") else "-3"
+            r = subprocess.run([EXE, dim, "-1", root], capture_output=True, text=True)
             if r.returncode != 0:
                 raise SystemExit("reference failed on %s:\n%s%s" % (name, r.stdout[-2000:], r.stderr[-2000:]))
             texts = {"file_" + suffix[1:]: np.array(text) for suffix, text in files.items()}
