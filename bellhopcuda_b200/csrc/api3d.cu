@@ -195,6 +195,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         d.top = T.top;
         d.bot = T.bot;
         d.top_nx = T.top_nx; d.top_ny = T.top_ny; d.bot_nx = T.bot_nx; d.bot_ny = T.bot_ny;
+        d.top_curv = T.top_curv; d.bot_curv = T.bot_curv;
         d.nsx = (int)T.sx.size(); d.nsy = (int)T.sy.size(); d.nsz = (int)T.sz.size();
         d.nrr = (int)T.rr.size(); d.nrz = (int)T.rz.size(); d.ntheta = (int)T.theta.size();
         d.nalpha = (int)T.alpha.size(); d.nbeta = (int)T.beta.size();

@@ -98,6 +98,9 @@ struct EnvDev {
 // triangles (src/module/boundary.hpp:600-645); same layout as the host's.
 struct Bdry3PtDev {
     double x[3], n1[3], n2[3];
+    double noden[3];                 // node normal (curvilinear 'C' grids)
+    double zxx, zxy, zyy;            // depth curvatures of the cell ('C'; 0 otherwise)
+    double kxx, kxy, kyy;            // angle curvatures of the cell ('C'; 0 otherwise)
 };
 
 // Preprocessed 3-D environment (BELLHOP3D field modes) for one frequency.
@@ -107,6 +110,7 @@ struct Env3Dev {
     const double *hx, *hy, *hz, *hc, *hcz;
     HsDev top, bot;
     int32_t top_nx, top_ny, bot_nx, bot_ny;
+    int32_t top_curv, bot_curv;      // 'C' grids: normals and curvature interpolated at reflections
     const Bdry3PtDev *btop, *bbot;
     int32_t nsx, nsy, nsz, nrr, nrz, ntheta, nalpha, nbeta, isingle_alpha, isingle_beta;
     const double *sx, *sy, *rr, *tcs;   // tcs: receiver bearing (cos, sin) pairs

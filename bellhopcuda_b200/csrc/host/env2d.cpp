@@ -898,6 +898,62 @@ bool EnvTables::same_trajectory_tables(const EnvTables &o) const
 // ------------------------------------------------------------ 3-D preprocess
 namespace {
 
+// Node normals of a grid boundary, from one-sided differences at the edges and
+// centred ones inside, and for a curvilinear ('C') grid the curvatures of each
+// cell: depth curvatures from the change of the unscaled node normal across
+// the cell, scaled by its length, and angle curvatures from the change of the
+// normal's angle in the x-z plane (src/module/boundary.hpp:643-823); zero for
+// flat-triangle grids (src/module/boundary.hpp:866-887). The last row and
+// column hold no cell and get NaN, never read.
+void curvatures3(std::vector<Bdry3Pt> &bd, int nx, int ny, bool curvilinear)
+{
+    auto P = [&](int ix, int iy) -> Bdry3Pt & { return bd[(size_t)ix * ny + iy]; };
+    std::vector<double> nu((size_t)nx * ny * 3), phi((size_t)nx * ny);
+    for(int ix = 0; ix < nx; ++ix)
+        for(int iy = 0; iy < ny; ++iy) {
+            const int x0 = ix == 0 ? 0 : ix - 1, x1 = ix == nx - 1 ? ix : ix + 1;
+            const int y0 = iy == 0 ? 0 : iy - 1, y1 = iy == ny - 1 ? iy : iy + 1;
+            const double mx = (P(x1, iy).x[2] - P(x0, iy).x[2]) / (P(x1, iy).x[0] - P(x0, iy).x[0]);
+            const double my = (P(ix, y1).x[2] - P(ix, y0).x[2]) / (P(ix, y1).x[1] - P(ix, y0).x[1]);
+            const double n[3] = {-mx, -my, 1.0};
+            const double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            double *u = &nu[((size_t)ix * ny + iy) * 3];
+            for(int k = 0; k < 3; ++k) {
+                u[k] = n[k];
+                P(ix, iy).noden[k] = n[k] / l;
+            }
+            phi[(size_t)ix * ny + iy] = std::atan2(n[2], n[0]);
+        }
+    for(int ix = 0; ix < nx; ++ix)
+        for(int iy = 0; iy < ny; ++iy) {
+            Bdry3Pt &q = P(ix, iy);
+            if(ix == nx - 1 || iy == ny - 1) {
+                q.zxx = q.zxy = q.zyy = q.kxx = q.kxy = q.kyy = NAN;
+                continue;
+            }
+            if(!curvilinear) {
+                q.zxx = q.zxy = q.zyy = q.kxx = q.kxy = q.kyy = 0.0;
+                continue;
+            }
+            const double *u00 = &nu[((size_t)ix * ny + iy) * 3];
+            const double *u10 = &nu[((size_t)(ix + 1) * ny + iy) * 3];
+            const double *u01 = &nu[((size_t)ix * ny + iy + 1) * 3];
+            const Bdry3Pt &a = P(ix, iy), &bx = P(ix + 1, iy), &by = P(ix, iy + 1);
+            q.zxx = -(u10[0] - u00[0]) / (bx.x[0] - a.x[0]);
+            const double lx = std::sqrt((bx.x[0] - a.x[0]) * (bx.x[0] - a.x[0]) + (bx.x[2] - a.x[2]) * (bx.x[2] - a.x[2]));
+            q.kxx = (phi[(size_t)(ix + 1) * ny + iy] - phi[(size_t)ix * ny + iy]) / lx;
+            q.zxy = -(u01[0] - u00[0]) / (by.x[1] - a.x[1]);
+            const double ly = std::sqrt((by.x[1] - a.x[1]) * (by.x[1] - a.x[1]) + (by.x[2] - a.x[2]) * (by.x[2] - a.x[2]));
+            q.kxy = (phi[(size_t)ix * ny + iy + 1] - phi[(size_t)ix * ny + iy]) / ly;
+            q.zyy = -(u01[1] - u00[1]) / (by.x[1] - a.x[1]);
+            q.kyy = (phi[(size_t)ix * ny + iy + 1] - phi[(size_t)ix * ny + iy]) / ly;
+            const double ln = std::sqrt(u00[0] * u00[0] + u00[1] * u00[1] + u00[2] * u00[2]);
+            q.zxx /= ln;
+            q.zxy /= ln;
+            q.zyy /= ln;
+        }
+}
+
 // grid boundary with the two triangle normals of each cell
 // (src/module/boundary.hpp:56-78 default, 499-523 units, 600-645 normals)
 std::vector<Bdry3Pt> build_bdry3(const Bdry3In &b, bool istop, double depth, int32_t &nx, int32_t &ny)
@@ -914,6 +970,7 @@ std::vector<Bdry3Pt> build_bdry3(const Bdry3In &b, bool istop, double depth, int
             bd[i].n1[0] = bd[i].n1[1] = 0.0; bd[i].n1[2] = negtop;
             bd[i].n2[0] = bd[i].n2[1] = 0.0; bd[i].n2[2] = negtop;
         }
+        curvatures3(bd, nx, ny, false);
         return bd;
     }
     nx = (int32_t)b.x_km.size();
@@ -922,7 +979,8 @@ std::vector<Bdry3Pt> build_bdry3(const Bdry3In &b, bool istop, double depth, int
         if(!(b.x_km[i] > b.x_km[i - 1])) env_error("boundary x-coordinates are not monotonically increasing");
     for(int i = 1; i < ny; ++i)
         if(!(b.y_km[i] > b.y_km[i - 1])) env_error("boundary y-coordinates are not monotonically increasing");
-    if(b.type[0] != 'R') env_error("3-D boundary type must be 'R' (rectangular grid)");
+    if(b.type[0] != 'R' && b.type[0] != 'C')
+        env_error("3-D boundary type must be 'R' (flat triangles) or 'C' (curvilinear)");
     bd.resize((size_t)nx * ny);
     for(int ix = 0; ix < nx; ++ix)
         for(int iy = 0; iy < ny; ++iy) {
@@ -953,6 +1011,7 @@ std::vector<Bdry3Pt> build_bdry3(const Bdry3In &b, bool istop, double depth, int
             l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
             for(int k = 0; k < 3; ++k) q.n2[k] = n[k] / l;
         }
+    curvatures3(bd, nx, ny, b.type[0] == 'C');
     return bd;
 }
 
@@ -1063,6 +1122,8 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.bot = make_hs(in, freq, fT, in.bot);
     t.btop = build_bdry3(in.ati3, true, top_depth, t.top_nx, t.top_ny);
     t.bbot = build_bdry3(in.bty3, false, bot_depth, t.bot_nx, t.bot_ny);
+    t.top_curv = in.ati3.file && in.ati3.type[0] == 'C';
+    t.bot_curv = in.bty3.file && in.bty3.type[0] == 'C';
 
     // sources, receivers, bearings (module/sxsy.hpp, szrz.hpp, rcvrranges.hpp, rcvrbearings.hpp)
     if(in.nsx <= 0 || in.nsy <= 0 || in.nsz <= 0) env_error("number of sources must be positive");

@@ -102,8 +102,10 @@ struct EnvTables {
 };
 
 // 3-D tables (BELLHOP3D field modes)
-struct Bdry3Pt {                 // grid node (x, y, z) and the normals of its cell's two triangles
-    double x[3], n1[3], n2[3];
+struct Bdry3Pt {                 // grid node (x, y, z), the normals of its cell's two triangles, and for
+    double x[3], n1[3], n2[3];   // curvilinear grids the node normal and the cell's curvatures
+    double noden[3];
+    double zxx, zxy, zyy, kxx, kxy, kyy;
 };
 struct Env3Tables {
     double freq0 = 0;
@@ -113,6 +115,7 @@ struct Env3Tables {
     std::vector<double> brc, trc;                        // reflection tables as in 2-D
     HsDev top{}, bot{};
     int32_t top_nx = 2, top_ny = 2, bot_nx = 2, bot_ny = 2;
+    int32_t top_curv = 0, bot_curv = 0;
     std::vector<Bdry3Pt> btop, bbot;
     std::vector<double> sx, sy, rr, theta, alpha, beta, sbp;   // m, m, m, deg, rad, rad
     std::vector<float> sz, rz;

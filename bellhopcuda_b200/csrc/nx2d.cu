@@ -152,10 +152,11 @@ __device__ void step_nx(const RayN &ray0, RayN &ray2, Bd3 &top, Bd3 &bot, const 
     }
 }
 
-// Reflect, Nx2D (src/reflect.hpp:125-452, O3D && !R3D): the 3-D triangle
-// normal projected on the plane; flat triangles carry no curvature
-__device__ void reflect_nx(const RayN &old, RayN &np, const HsDev &hs, bool istop, V3 nB3, const Env3Dev &E,
-                           const OrgN &org, Seg3 &iSeg, RunCounters *ctr)
+// Reflect, Nx2D (src/reflect.hpp:125-452, O3D && !R3D): the 3-D boundary
+// normal projected on the plane; kappa the boundary curvature along the plane
+// (OceanToRayCurvature, src/reflect.hpp:94-121; 0 for flat triangles)
+__device__ void reflect_nx(const RayN &old, RayN &np, const HsDev &hs, bool istop, V3 nB3, double kappa,
+                           const Env3Dev &E, const OrgN &org, Seg3 &iSeg, RunCounters *ctr)
 {
     V2<double> nB = to_ray_t(nB3, org);
     nB = scl2(1.0 / sqrt(dot2(nB, nB)), nB);
@@ -175,7 +176,7 @@ __device__ void reflect_nx(const RayN &old, RayN &np, const HsDev &hs, bool isto
     np.taui = old.taui;
     const V2<double> rayt = scl2(c, old.t), rayn = mk2(-rayt.y, rayt.x);
     const V2<double> rayt_t = scl2(c, np.t), rayn_t = mk2(rayt_t.y, -rayt_t.x);
-    double rn = 0.0;   // 2 kappa / c^2 / Th with kappa = 0
+    double rn = FLTD(2.0) * kappa / (c * c) / Th;
     double cnjump = -dot2(o.gradc, sub2(rayn_t, rayn));
     const double csjump = -dot2(o.gradc, sub2(rayt_t, rayt));
     if(istop) { cnjump = -cnjump; rn = -rn; }
@@ -296,7 +297,26 @@ __device__ bool ray_update_nx(RayStateN &st, RayN &p1, RayN &p2, int &small, con
     get_bdry_seg3(x_o, t_o, st.top, E.btop, E.top_nx, E.top_ny, true, false, ctr);
     get_bdry_seg3(x_o, t_o, st.bot, E.bbot, E.bot_nx, E.bot_ny, false, false, ctr);
     const bool two = tr || br;
-    if(two) reflect_nx(p1, p2, tr ? E.top : E.bot, tr, tr ? st.top.n : st.bot.n, E, st.org, st.iSeg, ctr);
+    if(two) {
+        const Bd3 &b = tr ? st.top : st.bot;
+        V3 nI = b.n;
+        double kappa = 0.0;
+        if(tr ? E.top_curv : E.bot_curv) {   // curvilinear grid (src/trace.hpp:318-341)
+            const Bdry3PtDev *bd = tr ? E.btop : E.bbot;
+            const int ny = tr ? E.top_ny : E.bot_ny;
+            const double s1 = (x_o.x - b.x.x) / (b.xmax - b.xmin), s2 = (x_o.y - b.x.y) / (b.ymax - b.ymin);
+            const double m1 = 1.0 - s1, m2 = 1.0 - s2;
+            const Bdry3PtDev &d00 = bd[(size_t)b.ix * ny + b.iy], &d01 = bd[(size_t)b.ix * ny + b.iy + 1];
+            const Bdry3PtDev &d10 = bd[(size_t)(b.ix + 1) * ny + b.iy], &d11 = bd[(size_t)(b.ix + 1) * ny + b.iy + 1];
+            nI = v3(d00.noden[0] * m1 * m2 + d10.noden[0] * s1 * m2 + d11.noden[0] * s1 * s2 + d01.noden[0] * m1 * s2,
+                    d00.noden[1] * m1 * m2 + d10.noden[1] * s1 * m2 + d11.noden[1] * s1 * s2 + d01.noden[1] * m1 * s2,
+                    d00.noden[2] * m1 * m2 + d10.noden[2] * s1 * m2 + d11.noden[2] * s1 * s2 + d01.noden[2] * m1 * s2);
+            const double tx = st.org.tx, ty = st.org.ty;
+            kappa = d00.kxx * tx * tx + FLTD(2.0) * d00.kxy * tx * ty + d00.kyy * ty * ty;
+            if(tr) kappa = -kappa;
+        }
+        reflect_nx(p1, p2, tr ? E.top : E.bot, tr, nI, kappa, E, st.org, st.iSeg, ctr);
+    }
     return two;
 }
 

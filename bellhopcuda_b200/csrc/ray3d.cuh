@@ -83,7 +83,28 @@ __device__ __forceinline__ bool ray_update3d(RayState3 &st, Ray3 &p1, Ray3 &p2, 
     get_bdry_seg3(p1.x, p1.t, st.top, E.btop, E.top_nx, E.top_ny, true, false, ctr);
     get_bdry_seg3(p1.x, p1.t, st.bot, E.bbot, E.bot_nx, E.bot_ny, false, false, ctr);
     const bool two = tr || br;
-    if(two) reflect3d(p1, p2, tr ? E.top : E.bot, tr, tr ? st.top.n : st.bot.n, E, st.iSeg, ctr);
+    if(two) {
+        const Bd3 &b = tr ? st.top : st.bot;
+        V3 nI = b.n;
+        double zxx = 0.0, zxy = 0.0, zyy = 0.0;
+        if(tr ? E.top_curv : E.bot_curv) {
+            // curvilinear grid: normal interpolated between the cell's node
+            // normals, curvature of the cell (src/trace.hpp:318-341)
+            const Bdry3PtDev *bd = tr ? E.btop : E.bbot;
+            const int ny = tr ? E.top_ny : E.bot_ny;
+            const double s1 = (p1.x.x - b.x.x) / (b.xmax - b.xmin), s2 = (p1.x.y - b.x.y) / (b.ymax - b.ymin);
+            const double m1 = 1.0 - s1, m2 = 1.0 - s2;
+            const Bdry3PtDev &d00 = bd[(size_t)b.ix * ny + b.iy], &d01 = bd[(size_t)b.ix * ny + b.iy + 1];
+            const Bdry3PtDev &d10 = bd[(size_t)(b.ix + 1) * ny + b.iy], &d11 = bd[(size_t)(b.ix + 1) * ny + b.iy + 1];
+            nI = v3(d00.noden[0] * m1 * m2 + d10.noden[0] * s1 * m2 + d11.noden[0] * s1 * s2 + d01.noden[0] * m1 * s2,
+                    d00.noden[1] * m1 * m2 + d10.noden[1] * s1 * m2 + d11.noden[1] * s1 * s2 + d01.noden[1] * m1 * s2,
+                    d00.noden[2] * m1 * m2 + d10.noden[2] * s1 * m2 + d11.noden[2] * s1 * s2 + d01.noden[2] * m1 * s2);
+            zxx = d00.zxx;
+            zxy = d00.zxy;
+            zyy = d00.zyy;
+        }
+        reflect3d(p1, p2, tr ? E.top : E.bot, tr, nI, zxx, zxy, zyy, E, st.iSeg, ctr);
+    }
     return two;
 }
 

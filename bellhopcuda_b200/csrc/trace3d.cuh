@@ -588,10 +588,13 @@ __device__ __forceinline__ void step3d(const Ray3 &r0, Ray3 &r2, Bd3 &top, Bd3 &
         interface_corr3(r2, sub3(o2.gradc, o0.gradc), iSeg, s0);
 }
 
-// Reflect, 3-D (src/reflect.hpp:125-452) on a flat-triangle boundary: the
-// boundary curvature matrix is zero, the halfspace uses the gamma form
+// Reflect, 3-D (src/reflect.hpp:125-452): nB the boundary normal (a
+// triangle's, or interpolated between the node normals of a curvilinear
+// grid), zxx, zxy, zyy the cell's depth curvatures (0 for flat triangles);
+// the halfspace uses the gamma form
 __device__ __forceinline__ void reflect3d(const Ray3 &old, Ray3 &np, const HsDev &hs, bool istop, V3 nB,
-                                          const Env3Dev &E, Seg3 &iSeg, RunCounters *ctr)
+                                          double zxx, double zxy, double zyy, const Env3Dev &E, Seg3 &iSeg,
+                                          RunCounters *ctr)
 {
     const double Th = dot3(old.t, nB);
     V3 tB = sub3(old.t, scl3(Th, nB));
@@ -609,8 +612,7 @@ __device__ __forceinline__ void reflect3d(const Ray3 &old, Ray3 &np, const HsDev
     V3 rayt, rayn1, rayn2, rayt_t, rayn1_t, rayn2_t;
     tangent_normals(old, o.c, nB, rayt, rayn1, rayn2, -1.0);
     tangent_normals(np, o.c, nB, rayt_t, rayn1_t, rayn2_t, -1.0);
-    // DMat = Rot^T (2 kappa) Rot with kappa = 0 (kept for its NaN behaviour on
-    // a ray normal to the boundary)
+    // DMat = Rot^T (2 kappa) Rot, kappa = [[zxx, zxy], [zxy, zyy]] / 2
     double tx = rayt.x, ty = rayt.y;
     double tl = sqrt(tx * tx + ty * ty);
     tx /= tl; ty /= tl;
@@ -618,7 +620,9 @@ __device__ __forceinline__ void reflect3d(const Ray3 &old, Ray3 &np, const HsDev
     double nl = sqrt(nx * nx + ny * ny);
     nx /= nl; ny /= nl;
     const M2 Rot = m2_cols(tx, ty, nx, ny);
-    const M2 D = m2_mul(m2_T(Rot), m2_mul(m2_diag(0.0), Rot));
+    const M2 K2 = m2_cols(FLTD(2.0) * (zxx / FLTD(2.0)), FLTD(2.0) * (zxy / FLTD(2.0)), FLTD(2.0) * (zxy / FLTD(2.0)),
+                          FLTD(2.0) * (zyy / FLTD(2.0)));
+    const M2 D = m2_mul(m2_T(Rot), m2_mul(K2, Rot));
     const double cn1j = dot3(o.gradc, sub3(scl3(-1.0, rayn1_t), rayn1));
     const double cn2j = dot3(o.gradc, sub3(scl3(-1.0, rayn2_t), rayn2));
     const double csj = -dot3(o.gradc, sub3(rayt_t, rayt));

@@ -51,9 +51,10 @@ def env_text(*, title: str, freq: float, ssp_opt: str, depth: float, ssp: Sequen
     return "\n".join(L) + "\n"
 
 
-def grid_text(x_km, y_km, z) -> str:
-    """'R' altimetry / bathymetry grid: z[ix, iy] in m, one row per y."""
-    L = ["'R'", "%d" % len(x_km), _vec(x_km), "%d" % len(y_km), _vec(y_km)]
+def grid_text(x_km, y_km, z, kind="R") -> str:
+    """Altimetry / bathymetry grid ('R' flat triangles, 'C' curvilinear):
+    z[ix, iy] in m, one row per y."""
+    L = ["'%s'" % kind, "%d" % len(x_km), _vec(x_km), "%d" % len(y_km), _vec(y_km)]
     for iy in range(len(y_km)):
         L.append(" ".join("%.4f" % z[ix, iy] for ix in range(len(x_km))))
     return "\n".join(L) + "\n"

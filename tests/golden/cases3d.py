@@ -204,6 +204,25 @@ def parabot3d_nx2d_incoherent():
     return f
 
 
+def _curvilinear(files):
+    """The same boundary grid read as curvilinear ('C'): reflections use the
+    normal interpolated between the node normals and the cell's curvature."""
+    files[".bty"] = files[".bty"].replace("'R'", "'C'", 1)
+    return files
+
+
+def parabot3d_curv_hat():
+    return _curvilinear(parabot3d_hat())
+
+
+def seamount3d_curv_gauss():
+    return _curvilinear(seamount3d_gauss())
+
+
+def parabot3d_curv_nx2d():
+    return _curvilinear(parabot3d_nx2d_incoherent())
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -229,4 +248,7 @@ CASES3D = {
     "hex3d_nx2d_hat": hex3d_nx2d_hat,
     "seamount3d_nx2d_gauss": seamount3d_nx2d_gauss,
     "parabot3d_nx2d_incoherent": parabot3d_nx2d_incoherent,
+    "parabot3d_curv_hat": parabot3d_curv_hat,
+    "seamount3d_curv_gauss": seamount3d_curv_gauss,
+    "parabot3d_curv_nx2d": parabot3d_curv_nx2d,
 }
