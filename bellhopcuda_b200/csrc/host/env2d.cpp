@@ -585,11 +585,12 @@ EnvInput read_env_files(const std::string &root, bool o3d)
         f.read(in.nbeta);
         if(in.top_opt[5] == 'I') f.read(in.isingle_beta);
         int n = in.nbeta;
-        if(n <= 0) env_error("number of beams in bearing must be positive");
+        if(n < 0) env_error("number of beams in bearing must not be negative");
         in.beta_deg.assign(std::max(3, n), 0.0);
         if(n > 2) in.beta_deg[2] = FLT(-999.9);
         f.record();
-        for(int i = 0; i < n; ++i) f.read(in.beta_deg[i]);
+        const int nread = n == 0 ? 2 : n;   // 0: the count is chosen in preprocessing
+        for(int i = 0; i < nread; ++i) f.read(in.beta_deg[i]);
     }
     f.record();                                                 // BeamInfo
     if(o3d) {
@@ -1128,7 +1129,7 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     // sources, receivers, bearings (module/sxsy.hpp, szrz.hpp, rcvrranges.hpp, rcvrbearings.hpp)
     if(in.nsx <= 0 || in.nsy <= 0 || in.nsz <= 0) env_error("number of sources must be positive");
     if(in.nrz <= 0 || in.nrr <= 0 || in.ntheta <= 0) env_error("number of receivers / bearings must be positive");
-    if(in.nbeta <= 0) env_error("3-D runs need an explicit number of bearing beams");
+
     for(double v : tab_sort(in.sx_km, in.nsx)) t.sx.push_back(v * 1000.0);
     for(double v : tab_sort(in.sy_km, in.nsy)) t.sy.push_back(v * 1000.0);
     t.sz = tab_sort(in.sz, in.nsz);
@@ -1141,11 +1142,31 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.theta = tab_sort(in.theta_deg, in.ntheta);
     fix360(t.theta);
 
-    // angles (module/rayangles.hpp): elevation and bearing fans
-    if(in.nalpha <= 0) env_error("3-D runs need an explicit number of elevation beams");
-    std::vector<double> al = tab_sort(in.alpha_deg, in.nalpha);
+    // angles (module/rayangles.hpp): elevation and bearing fans; a count of 0
+    // is chosen as EstimateNumAngles does (src/module/rayangles.hpp:212-238):
+    // 50 for ray runs, else from the phase of adjacent beams at the last range
+    // (and, in elevation, beams thin against the water depth)
+    auto estimate = [&](std::vector<double> v, int n, bool bearing) {
+        if(n > 0) return tab_sort(v, n);
+        const double rmax = t.rr.back();
+        if(ray_run3) {
+            n = 50;
+        } else {
+            n = std::max((int)((bearing ? FLT(0.1) : FLT(0.3)) * rmax * freq / FLT(1500.0)), 300);
+            if(!bearing) {
+                const double dth = std::atan((bot_depth - top_depth) / (FLT(10.0) * rmax));
+                n = std::max((int)(kPi / dth), n);
+            }
+        }
+        std::vector<double> a(std::max(3, n), 0.0);
+        a[0] = v[0];
+        a[1] = v[1];
+        if(n > 2) a[2] = FLT(-999.9);
+        return tab_sort(a, n);
+    };
+    std::vector<double> al = estimate(in.alpha_deg, in.nalpha, false);
     fix360(al);
-    std::vector<double> be = tab_sort(in.beta_deg, in.nbeta);
+    std::vector<double> be = estimate(in.beta_deg, in.nbeta, true);
     fix360(be);
     if(t.nx2d && !ray_run3) be = t.theta;   // beams on the receiver radials (src/module/rayangles.hpp:163-179)
     for(size_t i = 1; i < al.size(); ++i) if(!(al[i] > al[i - 1])) env_error("elevation angles are not monotonically increasing");

@@ -128,7 +128,8 @@ REFERENCE_INPUTS = "/root/reference/test/in"
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INPUTS), reason="reference inputs not present")
 @pytest.mark.parametrize("name", ["Munk", "MunkB_Coh", "MunkB_gb", "DickinsB", "DickinsFlatB", "free",
-                                  "GulfB_rd_gb"])
+                                  "GulfB_rd_gb", "GulfB_ri_Cerveny", "MunkB_Coh_CervenyR", "MunkB_Coh_CervenyC",
+                                  "DickinsCervenyB", "Gulf_ray_rd"])
 def test_reader_accepts_reference_inputs(name, workdir):
     src = os.path.join(REFERENCE_INPUTS, name)
     if not os.path.exists(src + ".env"):
@@ -238,7 +239,8 @@ def test_reader3d_rejects_2d_runs_and_unsupported_beams(workdir):
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INPUTS), reason="reference inputs not present")
 @pytest.mark.parametrize("name", ["Munkslice3dGaussian", "Munkslice3dHatCart", "MunkRot3D", "DoubleSeamount3D",
-                                  "PerfectWedge3dHat", "KR3dGaussian"])
+                                  "PerfectWedge3dHat", "KR3dGaussian", "HyperBot3DHatCart", "KR3d_ray",
+                                  "DoubleSeamount3D_ray", "Munkslice2dGaussian"])
 def test_reader3d_accepts_reference_inputs(name, workdir):
     src = os.path.join(REFERENCE_INPUTS, name)
     if not os.path.exists(src + ".env"):
