@@ -1589,7 +1589,7 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
             if(tr < t.trace_ms) { t.trace_ms = tr; t.stage_kb = kb; }
         }
         c->stage_cap = (unsigned int)t.stage_kb * 1024u;
-        for(int k : {2, 3, 4, 5, 6, 8, 12}) {
+        for(int k : {2, 3, 4, 5, 6, 8, 10, 12}) {
             c->influence_ctas_per_sm = k;
             timed(tr, inf);
             if(inf < t.influence_ms) { t.influence_ms = inf; t.influence_ctas_per_sm = k; }
