@@ -19,6 +19,8 @@
 
 namespace bhcb {
 
+cudaError_t launch_rays_nx(const GroupDev *, int, const long long *, const int *, int, const long long *, double *,
+                           int *, int *, RunCounters *, bool, int, cudaStream_t);
 cudaError_t launch_rays3d(const GroupDev *, int, const long long *, const int *, int, const long long *, double *,
                           int *, int *, RunCounters *, bool, int, cudaStream_t);
 cudaError_t launch_trace3d_rc(const GroupDev *, int, long long, XSeg3 *, unsigned long long, RunCounters *,
@@ -563,7 +565,8 @@ uint32_t trace_rays3(Run3 *r, RaySet3 &R, cudaStream_t st, uint32_t &warn_bits)
     CK(cudaMemcpyAsync(jobs_d.p, R.jobs.data(), n * sizeof(long long), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(lim_d.p, R.limits.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctr, 0, sizeof(RunCounters), st));
-    CK(launch_rays3d(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, nullptr, nullptr, (int *)npts_d.p,
+    auto rays = r->nx2d ? launch_rays_nx : launch_rays3d;   // Nx2D: 2-D rays, points in ocean coordinates
+    CK(rays(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, nullptr, nullptr, (int *)npts_d.p,
                      (int *)bnc_d.p, ctr, true, r->sm_count, st));
     CK(cudaMemcpyAsync(R.npts.data(), npts_d.p, n * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(R.bnc.data(), bnc_d.p, 2 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -580,7 +583,7 @@ uint32_t trace_rays3(Run3 *r, RaySet3 &R, cudaStream_t st, uint32_t &warn_bits)
     if((uint64_t)tot * 3 * sizeof(double) > r->max_memory) throw MemError("ray points exceed max_memory");
     pts_d.ensure(std::max<long long>(tot, 1) * 3 * sizeof(double));
     CK(cudaMemcpyAsync(off_d.p, R.off.data(), n * sizeof(long long), cudaMemcpyHostToDevice, st));
-    CK(launch_rays3d(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, (const long long *)off_d.p,
+    CK(rays(G, ng, (const long long *)jobs_d.p, (const int *)lim_d.p, n, (const long long *)off_d.p,
                      (double *)pts_d.p, (int *)npts_d.p, (int *)bnc_d.p, ctr, false, r->sm_count, st));
     R.xyz.resize(3 * (size_t)tot);
     if(tot) CK(cudaMemcpyAsync(R.xyz.data(), pts_d.p, tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));

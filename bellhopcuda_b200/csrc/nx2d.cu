@@ -506,7 +506,104 @@ __global__ void scale_nx_kernel(float2 *field, const GroupDev *__restrict__ grou
     }
 }
 
+// Ray trajectories, Nx2D (MainRayMode, src/trace.hpp:485-519, with the
+// points written in ocean coordinates as WriteRay does, src/mode/ray.hpp:
+// 240-247): COUNT pass then fill pass as for the 2-D and 3-D rays.
+template<bool COUNT>
+__global__ void __launch_bounds__(64) ray_nx_kernel(const GroupDev *__restrict__ groups, int ngroups,
+                                                    const long long *__restrict__ jobs, const int *__restrict__ limits,
+                                                    int nitems, const long long *__restrict__ off, double *pts,
+                                                    int *npts, int *bnc, RunCounters *ctr)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += gridDim.x * blockDim.x) {
+        const long long job = jobs[i];
+        const GroupDev &G = groups[find_group(groups, ngroups, job)];
+        const Env3Dev &E = *G.env3;
+        const Job3 J = job_indices3(E, (int)(job - G.job_base));
+        const int cap = COUNT ? 0x7fffffff : npts[i];
+        const long long base = COUNT ? 0 : off[i];
+        RayStateN st;
+        auto put = [&](int idx, const RayN &p) {
+            if(!COUNT && idx < cap) {
+                const V3 x = to_ocean_x(p.x, st.org);
+                double *q = pts + 3 * (base + idx);
+                q[0] = x.x;
+                q[1] = x.y;
+                q[2] = x.z;
+            }
+        };
+        if(J.isz >= E.nsz) {
+            run_error(ctr, ERR_RAYINIT);
+            if(COUNT) { npts[i] = 0; bnc[2 * i] = bnc[2 * i + 1] = 0; }
+            continue;
+        }
+        int nsteps = -1, last_top = 0, last_bot = 0;
+        if(!ray_init_nx(E, J, st, ctr)) {
+            put(0, st.p0);
+            nsteps = 1;
+        } else {
+            put(0, st.p0);
+            const int limit = limits[i];
+            int is = 0, small = 0, prev_top = 0, prev_bot = 0;
+            RayN p1, p2;
+            for(;;) {
+                if((is & 31) == 0 && __ldcg(&ctr->err_bits) != 0u) {
+                    nsteps = is + 1;
+                    last_top = st.p0.ntop;
+                    last_bot = st.p0.nbot;
+                    break;
+                }
+                const bool two = ray_update_nx(st, p1, p2, small, E, ctr);
+                put(is + 1, p1);
+                if(two) put(is + 2, p2);
+                if(limit >= 0 && is >= limit) {
+                    nsteps = is + 2;
+                    last_top = p1.ntop;
+                    last_bot = p1.nbot;
+                    break;
+                }
+                prev_top = two ? p1.ntop : st.p0.ntop;
+                prev_bot = two ? p1.nbot : st.p0.nbot;
+                is += two ? 2 : 1;
+                st.p0 = two ? p2 : p1;
+                if(ray_stops_nx(st, small, E)) {
+                    nsteps = is + 1;
+                    last_top = st.p0.ntop;
+                    last_bot = st.p0.nbot;
+                    break;
+                }
+                if(is >= MAXN_STEPS - 3) {
+                    run_warn(ctr, WARN_ONERAY_OUTOFMEMORY);
+                    nsteps = is;
+                    last_top = prev_top;
+                    last_bot = prev_bot;
+                    break;
+                }
+            }
+        }
+        if(COUNT) {
+            npts[i] = nsteps;
+            bnc[2 * i] = last_top;
+            bnc[2 * i + 1] = last_bot;
+        }
+    }
+}
+
 } // namespace
+
+cudaError_t launch_rays_nx(const GroupDev *groups, int ngroups, const long long *jobs, const int *limits, int nitems,
+                           const long long *off, double *pts, int *npts, int *bnc, RunCounters *ctr, bool count,
+                           int sm_count, cudaStream_t st)
+{
+    if(nitems <= 0) return cudaSuccess;
+    int grid = (nitems + 63) / 64;
+    if(grid > sm_count * 16) grid = sm_count * 16;
+    if(count)
+        ray_nx_kernel<true><<<grid, 64, 0, st>>>(groups, ngroups, jobs, limits, nitems, off, pts, npts, bnc, ctr);
+    else
+        ray_nx_kernel<false><<<grid, 64, 0, st>>>(groups, ngroups, jobs, limits, nitems, off, pts, npts, bnc, ctr);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_trace_nx(const GroupDev *groups, int ngroups, long long job_end, void *segs,
                             unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, int grid,

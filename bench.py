@@ -48,8 +48,8 @@ ORACLE_STEPS_PER_TRACE = 20993289
 ORACLE_EVALS_ALL_FREQS = 6440570521
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one full-size
 # influence launch (10 frequencies), from the ncu capture summarised in
-# profiles/influence_kernel_rd_gauss.md: 786.03 MB read + 129.76 MB written.
-INFLUENCE_DRAM_BYTES = 915.79e6
+# profiles/influence_kernel_rd_gauss.md: 863.87 MB read + 343.98 MB written.
+INFLUENCE_DRAM_BYTES = 1207.85e6
 
 
 def log(*a):

@@ -223,6 +223,18 @@ def parabot3d_curv_nx2d():
     return _curvilinear(parabot3d_nx2d_incoherent())
 
 
+def munk3d_nx2d_ray():
+    """Nx2D ray run: 2-D rays in the planes of the bearing fan (not replaced by
+    the receiver bearings for ray runs), points written in (x, y, z)."""
+    return _munk_slice("R    2", alpha=(11, -12.0, 12.0), beta=(5, -6.0, 6.0), theta=[0.0])
+
+
+def seamount3d_nx2d_ray():
+    f = seamount3d_ray()
+    f[".env"] = f[".env"].replace("'R    3'", "'R    2'")
+    return f
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -251,4 +263,6 @@ CASES3D = {
     "parabot3d_curv_hat": parabot3d_curv_hat,
     "seamount3d_curv_gauss": seamount3d_curv_gauss,
     "parabot3d_curv_nx2d": parabot3d_curv_nx2d,
+    "munk3d_nx2d_ray": munk3d_nx2d_ray,
+    "seamount3d_nx2d_ray": seamount3d_nx2d_ray,
 }
