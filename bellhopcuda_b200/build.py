@@ -21,6 +21,10 @@ CU_SOURCES = ["kernels2d.cu", "influence_mixed.cu", "arrivals.cu", "kernels3d.cu
               "noalloc.cu", "nn_gemm.cu", "nn_ops.cu", "influence_x.cu", "influence3d_x.cu", "nx2d.cu"]
 CPP_SOURCES = ["host/ldi.cpp", "host/env2d.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Nx2D tracer: products and sums rounded separately, as the reference's host
+# build computes them (its landing decisions on boundary grid lines follow the
+# last bits of the position)
+EXTRA = {"nx2d.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -55,7 +59,8 @@ def build(verbose: bool = False, force: bool = False, ptxas_v: bool = False) -> 
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
     for src in CU_SOURCES:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-        cmd = [cc, *ARCH, "-lineinfo", *common, "--expt-relaxed-constexpr", "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [cc, *ARCH, "-lineinfo", *common, "--expt-relaxed-constexpr", *EXTRA.get(src, []), "-c",
+               os.path.join(CSRC, src), "-o", obj]
         if ptxas_v:
             cmd.insert(1, "-Xptxas=-v")
         cmds.append(cmd)

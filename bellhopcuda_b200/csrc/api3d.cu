@@ -145,7 +145,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     if(r->envs.empty()) throw StateError("no 3-D environment: call bhcb_setup3d first");
     Arena A;
     struct Offs { size_t z, rho, c, cz, n2, n2z, coef, hx, hy, hz, hc, hcz, btop, bbot, sx, sy, sz, rr, rz, tcs,
-                  alpha, beta, sbp, trc, brc; };
+                  alpha, beta, acs, bcs, sbp, trc, brc; };
     std::vector<Offs> offs;
     std::vector<Env3Dev> envdev;
     r->groups_h.clear();
@@ -172,6 +172,12 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         }
         o.tcs = A.put(tcs);
         o.alpha = A.put(T.alpha); o.beta = A.put(T.beta); o.sbp = A.put(T.sbp);
+        // launch directions as the host's libm gives them, so that the Nx2D
+        // planes (cos beta, sin beta) are the same doubles as the reference's
+        std::vector<double> acs, bcs;
+        for(double a : T.alpha) { acs.push_back(std::cos(a)); acs.push_back(std::sin(a)); }
+        for(double b : T.beta) { bcs.push_back(std::cos(b)); bcs.push_back(std::sin(b)); }
+        o.acs = A.put(acs); o.bcs = A.put(bcs);
         o.trc = A.put(T.trc); o.brc = A.put(T.brc);
         offs.push_back(o);
 
@@ -243,6 +249,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         d.sx = dptr<double>(ab, o.sx); d.sy = dptr<double>(ab, o.sy); d.sz = dptr<float>(ab, o.sz);
         d.rr = dptr<double>(ab, o.rr); d.rz = dptr<float>(ab, o.rz); d.tcs = dptr<double>(ab, o.tcs);
         d.alpha = dptr<double>(ab, o.alpha); d.beta = dptr<double>(ab, o.beta); d.sbp = dptr<double>(ab, o.sbp);
+        d.acs = dptr<double>(ab, o.acs); d.bcs = dptr<double>(ab, o.bcs);
         r->groups_h[i].env3 = dptr<Env3Dev>(ab, env_off + i * sizeof(Env3Dev));
     }
     CK(cudaMemcpyAsync(ab, A.bytes.data(), A.bytes.size(), cudaMemcpyHostToDevice, st));

@@ -115,6 +115,7 @@ struct Env3Dev {
     int32_t nsx, nsy, nsz, nrr, nrz, ntheta, nalpha, nbeta, isingle_alpha, isingle_beta;
     const double *sx, *sy, *rr, *tcs;   // tcs: receiver bearing (cos, sin) pairs
     const double *alpha, *beta;
+    const double *acs, *bcs;            // (cos, sin) pairs of alpha and beta, from the host's libm
     const float *sz, *rz;
     double dalpha, dbeta, deltas, box_x, box_y, box_z, freq0;
     int32_t gaussian, coherent, run0, nsbp;

@@ -20,6 +20,15 @@
 //  influence_nx_kernel  one thread per (record, receiver depth); contributions
 //                       added into the [isz][isx][isy][itheta][iz][ir] field.
 //  scale_nx_kernel      ScalePressure, 2-D form (src/influence.hpp:1556-1627).
+//
+// This file is compiled without multiply-add contraction (-fmad=false) and
+// takes the plane's (cos beta, sin beta) and the launch (cos alpha, sin alpha)
+// from host tables: the landing on an x or y grid line of the boundary
+// (OceanToRayX's ulp nudges towards the forward side, at most four) decides
+// whether the next step starts in the new cell or first takes a forced small
+// step, and that decision follows the last bits of the ocean position. With
+// separately rounded products and sums and the same direction doubles, those
+// bits follow the reference's own arithmetic.
 #include <cuda_runtime.h>
 
 #include "bhcb_internal.h"
@@ -238,7 +247,7 @@ struct RayStateN {
 // RayInit, Nx2D (src/trace.hpp:76-266)
 __device__ bool ray_init_nx(const Env3Dev &E, const Job3 &J, RayStateN &st, RunCounters *ctr)
 {
-    const double alpha = E.alpha[J.ialpha], beta = E.beta[J.ibeta];
+    const double alpha = E.alpha[J.ialpha];
     st.alpha = alpha;
     const double SrcDecl = (180.0 / BHCB_PI) * alpha;
     st.iSeg = Seg3{0, 0, 0};
@@ -248,8 +257,8 @@ __device__ bool ray_init_nx(const Env3Dev &E, const Job3 &J, RayStateN &st, RunC
     const double c = o.c;
     st.c = c;
     st.org.xs = xs;
-    st.org.tx = cos(beta);
-    st.org.ty = sin(beta);
+    st.org.tx = E.bcs[2 * J.ibeta];
+    st.org.ty = E.bcs[2 * J.ibeta + 1];
     const int ibp = min(bsearch_leq2(E.sbp, E.nsbp, SrcDecl), E.nsbp - 2);
     const double s = (SrcDecl - E.sbp[2 * ibp]) / (E.sbp[2 * (ibp + 1)] - E.sbp[2 * ibp]);
     float amp0 = (float)((FLTD(1.0) - s) * E.sbp[2 * ibp + 1] + s * E.sbp[2 * (ibp + 1) + 1]);
@@ -260,7 +269,7 @@ __device__ bool ray_init_nx(const Env3Dev &E, const Job3 &J, RayStateN &st, RunC
     RayN &p0 = st.p0;
     p0.x = mk2(0.0, xs.z);
     p0.c = c;
-    p0.t = mk2(cos(alpha) / c, sin(alpha) / c);
+    p0.t = mk2(E.acs[2 * J.ialpha] / c, E.acs[2 * J.ialpha + 1] / c);
     p0.taur = p0.taui = 0.0;
     p0.Amp = (double)amp0;
     p0.Phase = 0.0;
