@@ -29,6 +29,9 @@ cudaError_t launch_influence3d_rc(const XSeg3 *, unsigned long long, const Group
                                   int, int, cudaStream_t);
 cudaError_t launch_trace_nx(const GroupDev *, int, long long, void *, unsigned long long, RunCounters *,
                             unsigned long long *, int, cudaStream_t);
+cudaError_t launch_arr_gather_nx(const void *, unsigned long long, const GroupDev *, int, bool, ArrCand *,
+                                 uint64_t *, uint32_t *, unsigned long long, unsigned long long *, RunCounters *,
+                                 ArrKeyBits, int, cudaStream_t);
 cudaError_t launch_influence_nx(const void *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *, int,
                                 int, cudaStream_t);
 cudaError_t launch_scale_nx(float2 *, const GroupDev *, int, int, cudaStream_t);
@@ -182,6 +185,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         offs.push_back(o);
 
         Env3Dev d{};
+        d.nx2d = T.nx2d ? 1 : 0;
         EnvDev &e = d.e1d;
         e.ssp_type = T.ssp_type == SSP_HEXAHEDRAL ? SSP_CLINEAR : T.ssp_type;
         e.nssp = (int)T.z.size();
@@ -197,7 +201,7 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         e.coherent = T.run_type[0] == 'C';
         e.beam2 = T.beam_type[2];
         e.run0 = T.run_type[0];
-        e.arrivals = 0;
+        e.arrivals = T.nx2d && (T.run_type[0] == 'A' || T.run_type[0] == 'a');   // records carry the receiver angle
         d.hex = T.ssp_type == SSP_HEXAHEDRAL;
         d.hnx = (int)T.hx.size(); d.hny = (int)T.hy.size(); d.hnz = (int)T.hz.size();
         d.top = T.top;
@@ -351,8 +355,15 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, st));
     CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), st));
-    CK(launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
-                           (int)r->groups_h.size(), true, nullptr, nullptr, nullptr, 0, nullptr, ctr, r->kb, igrid, st));
+    // Nx2D: 2-D records on the bearing planes; 3-D: SegRec3
+    auto gather = [&](bool count, ArrCand *c, uint64_t *k, uint32_t *v, unsigned long long cap,
+                      unsigned long long *cur) {
+        return r->nx2d ? launch_arr_gather_nx(r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
+                                              (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, igrid, st)
+                       : launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
+                                             (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, igrid, st);
+    };
+    CK(gather(true, nullptr, nullptr, nullptr, 0, nullptr));
     unsigned long long n = 0;
     CK(cudaMemcpyAsync(&n, &ctr->nevals, sizeof n, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -372,9 +383,7 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
         r->vals1.ensure(n * sizeof(uint32_t));
         r->hist.ensure(std::max<size_t>(radix_sort_hist_entries(n), 1) * sizeof(uint32_t));
         CK(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
-        CK(launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
-                               (int)r->groups_h.size(), false, (ArrCand *)r->cand.p, (uint64_t *)r->keys0.p,
-                               (uint32_t *)r->vals0.p, n, cursor, ctr, r->kb, igrid, st));
+        CK(gather(false, (ArrCand *)r->cand.p, (uint64_t *)r->keys0.p, (uint32_t *)r->vals0.p, n, cursor));
         int in1 = 0;
         CK(radix_sort_pairs((uint64_t *)r->keys0.p, (uint32_t *)r->vals0.p, (uint64_t *)r->keys1.p,
                             (uint32_t *)r->vals1.p, n, r->kb.total_bits, (uint32_t *)r->hist.p, &in1, st));

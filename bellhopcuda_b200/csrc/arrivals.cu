@@ -351,16 +351,19 @@ __global__ void arr_replay_kernel(const uint64_t *__restrict__ keys, const uint3
             }
         }
         // PostProcessArrivals (src/mode/arr.cpp:24-74): clamp the count; 2-D
-        // scales the amplitudes (3-D factor 1)
+        // and Nx2D scale the amplitudes (3-D factor 1)
         if(nt > max_narr) nt = max_narr;
         narr_out[cell] = nt;
-        if(D3) continue;
-        const EnvDev &e = *G.env;
-        const int ir = (int)((cell - G.field_base) % e.nrr);
+        if(D3 && !G.env3->nx2d) continue;
+        // 2-D rays (2-D and Nx2D): cylindrical spreading per receiver range,
+        // the last index of both field layouts
+        const double *rr = D3 ? G.env3->rr : G.env->rr;
+        const int nrr = D3 ? G.env3->nrr : G.env->nrr;
+        const int ir = (int)((cell - G.field_base) % nrr);
         float factor;
-        if(e.line_source) factor = (float)(FLTD(4.0) * sqrt(BHCB_PI));
-        else if(fabs(e.rr[ir]) < DBL_EPS) factor = 1e5f;
-        else factor = (float)(FLTD(1.0) / sqrt(e.rr[ir]));
+        if(!D3 && G.env->line_source) factor = (float)(FLTD(4.0) * sqrt(BHCB_PI));
+        else if(fabs(rr[ir]) < DBL_EPS) factor = 1e5f;
+        else factor = (float)(FLTD(1.0) / sqrt(rr[ir]));
         for(int j = 0; j < nt; ++j) ba[j].a = __fmul_rn(ba[j].a, factor);
     }
 }

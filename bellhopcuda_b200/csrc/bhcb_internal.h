@@ -116,6 +116,7 @@ struct Env3Dev {
     const double *sx, *sy, *rr, *tcs;   // tcs: receiver bearing (cos, sin) pairs
     const double *alpha, *beta;
     const double *acs, *bcs;            // (cos, sin) pairs of alpha and beta, from the host's libm
+    int32_t nx2d;                       // RunType(6) '2': 2-D rays in the bearing planes
     const float *sz, *rz;
     double dalpha, dbeta, deltas, box_x, box_y, box_z, freq0;
     int32_t gaussian, coherent, run0, nsbp;

@@ -498,6 +498,85 @@ __global__ void __launch_bounds__(128) influence_nx_kernel(const SegRec<double> 
     if((threadIdx.x & 31) == 0 && evals) atomicAdd(&ctr->nevals, (unsigned long long)evals);
 }
 
+// Arrivals, Nx2D: the contributions of influence_nx_kernel as arrival
+// candidates (ApplyContribution with itheta = ibeta and AddArr,
+// src/influence.hpp:434-451; ReceiverAngles 2-D form, src/influence.hpp:
+// 123-136: receiver azimuth = the source azimuth) keyed (receiver cell, ray,
+// step) for the shared radix sort and per-cell replay. One thread per record.
+// COUNT: counts into ctr->nevals; otherwise candidate i at atomicAdd(cursor).
+template<bool COUNT>
+__global__ void __launch_bounds__(128) arr_gather_nx_kernel(const SegRec<double> *__restrict__ segs,
+                                                            unsigned long long cap,
+                                                            const GroupDev *__restrict__ groups, int ngroups,
+                                                            ArrCand *cands, uint64_t *keys, uint32_t *vals,
+                                                            unsigned long long cand_cap, unsigned long long *cursor,
+                                                            RunCounters *ctr, ArrKeyBits kb)
+{
+    const unsigned long long nseg = min(__ldcg(&ctr->nseg), cap);
+    unsigned long long count = 0;
+    for(unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < nseg;
+        k += (unsigned long long)gridDim.x * blockDim.x) {
+        const SegRec<double> &S = segs[k];
+        if(S.job < 0) continue;
+        const GroupDev &G = groups[find_group(groups, ngroups, S.job)];
+        const Env3Dev &E = *G.env3;
+        const bool gauss = E.gaussian != 0;
+        const double freq = E.freq0;
+        double sig = S.sigma_seg, fl = 0.0;
+        if(gauss) {   // AdjustSigma (src/influence.hpp:91-100)
+            fl = min(FLTD(0.2) * freq * S.tau1r, BHCB_PI * (S.c0 / freq));
+            sig = max(sig, fl);
+        }
+        const double rmax = (gauss ? 4.0 : 1.0) * sig;
+        const bool window = fabs(S.tx) > FLTD(0.50001);
+        const int local = (int)((long long)S.job - G.job_base);
+        const Job3 J = job_indices3(E, local);
+        const long long plane = G.field_base
+            + ((((long long)J.isz * E.nsx + J.isx) * E.nsy + J.isy) * E.ntheta + J.ibeta) * E.nrz * E.nrr;
+        const float azim = (float)((180.0 / BHCB_PI) * E.beta[J.ibeta]);
+        for(int iz = 0; iz < E.nrz; ++iz) {
+            const double zr = (double)E.rz[iz];
+            if(window && (zr < S.zlo - rmax || zr > S.zhi + rmax)) continue;
+            const double dz = zr - S.x0z;
+            for(int ir = S.ir_lo; ir <= S.ir_hi; ++ir) {
+                const double dr = E.rr[ir] - S.x0r;
+                const double s = (dr * S.tx + dz * S.tz) / S.rlen;
+                const double n1 = fabs(dz * S.tx - dr * S.tz);
+                const double qF = S.q0 + s * S.dq;
+                double sigma = fabs(qF * S.rcp_q0);
+                const double sig0 = sigma;
+                if(gauss) sigma = max(sigma, fl);
+                if(n1 >= (gauss ? 4.0 : 1.0) * sigma) continue;
+                if(COUNT) {
+                    ++count;
+                    continue;
+                }
+                const unsigned long long i = atomicAdd(cursor, 1ull);
+                if(i >= cand_cap) continue;
+                const double w = gauss ? exp(FLTD(-0.5) * (n1 / sigma) * (n1 / sigma)) * (sig0 / sigma)
+                                       : (sigma - n1) / sigma;
+                const bool caustic = (qF <= 0.0 && S.q0 > 0.0) || (qF >= 0.0 && S.q0 < 0.0);
+                const long long cell = plane + (long long)iz * E.nrr + ir;
+                ArrCand c;
+                c.amp = S.cnst_num / sqrt(fabs(qF)) * w;
+                c.phase = caustic ? S.phase_b : S.phase_a;
+                c.delay_re = S.tau0r + s * S.dtaur;
+                c.delay_im = S.tau0i + s * S.dtaui;
+                c.rcvr_decl = (float)S.rcvr_decl;
+                c.rcvr_azim = azim;
+                c.ntop = S.ntop;
+                c.nbot = S.nbot;
+                c.job = S.job;
+                c.aux = J.ialpha;
+                cands[i] = c;
+                keys[i] = ((uint64_t)cell << kb.sh_cell) | ((uint64_t)local << kb.sh_job) | (uint64_t)S.is;
+                vals[i] = (uint32_t)i;
+            }
+        }
+    }
+    if(COUNT && count) atomicAdd(&ctr->nevals, count);
+}
+
 // ScalePressure, 2-D form (src/influence.hpp:1556-1627): intensity to
 // pressure for incoherent runs, then -1 / sqrt(r)
 __global__ void scale_nx_kernel(float2 *field, const GroupDev *__restrict__ groups, int g)
@@ -619,6 +698,22 @@ cudaError_t launch_trace_nx(const GroupDev *groups, int ngroups, long long job_e
                             cudaStream_t st)
 {
     trace_nx_kernel<<<grid, 64, 0, st>>>(groups, ngroups, job_end, (SegRec<double> *)segs, cap, ctr, job_counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_arr_gather_nx(const void *segs, unsigned long long nseg, const GroupDev *groups, int ngroups,
+                                 bool count, ArrCand *cands, uint64_t *keys, uint32_t *vals,
+                                 unsigned long long cand_cap, unsigned long long *cursor, RunCounters *ctr,
+                                 ArrKeyBits kb, int grid, cudaStream_t st)
+{
+    if(nseg == 0) return cudaSuccess;
+    const SegRec<double> *S = (const SegRec<double> *)segs;
+    if(count)
+        arr_gather_nx_kernel<true><<<grid, 128, 0, st>>>(S, nseg, groups, ngroups, nullptr, nullptr, nullptr, 0,
+                                                         nullptr, ctr, kb);
+    else
+        arr_gather_nx_kernel<false><<<grid, 128, 0, st>>>(S, nseg, groups, ngroups, cands, keys, vals, cand_cap,
+                                                          cursor, ctr, kb);
     return cudaGetLastError();
 }
 

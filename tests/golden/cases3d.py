@@ -229,6 +229,13 @@ def munk3d_nx2d_ray():
     return _munk_slice("R    2", alpha=(11, -12.0, 12.0), beta=(5, -6.0, 6.0), theta=[0.0])
 
 
+def munk3d_nx2d_arr_gauss():
+    """Nx2D arrivals ('a', binary): the 2-D Gaussian beams of each receiver
+    bearing's plane as arrivals, cylindrical spreading per range."""
+    return _munk_slice("aB   2", alpha=(121, -20.3, 20.3), theta=[0.0, 2.0, 5.0], nrz_range=(6, 500.0, 3000.0),
+                       rr_range=(7, 5.0, 30.0))
+
+
 def seamount3d_nx2d_ray():
     f = seamount3d_ray()
     f[".env"] = f[".env"].replace("'R    3'", "'R    2'")
@@ -265,4 +272,5 @@ CASES3D = {
     "parabot3d_curv_nx2d": parabot3d_curv_nx2d,
     "munk3d_nx2d_ray": munk3d_nx2d_ray,
     "seamount3d_nx2d_ray": seamount3d_nx2d_ray,
+    "munk3d_nx2d_arr_gauss": munk3d_nx2d_arr_gauss,
 }
