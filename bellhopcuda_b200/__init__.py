@@ -99,7 +99,6 @@ SIGNATURES = [
     ("bhcb_last_error", C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_uint32)]),
     ("bhcb_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
-    ("bhcb_probe_fp_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("bhcb_run_noalloc", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
                                    C.c_char_p, C.c_size_t]),
     ("bhcb_check_env", C.c_int, [C.c_char_p, C.POINTER(EnvInfo), C.c_char_p, C.c_size_t]),
@@ -157,16 +156,6 @@ def load_library():
             fn.argtypes = args
         _lib = lib
     return _lib
-
-
-def probe_fp_peak(gpu: int = 0):
-    """Measured (FP32, FP64) FMA throughput in TFLOP/s."""
-    lib = load_library()
-    a, b = C.c_double(), C.c_double()
-    rc = lib.bhcb_probe_fp_peak(gpu, C.byref(a), C.byref(b))
-    if rc != 0:
-        raise BhcbError(rc, "peak probe failed")
-    return a.value, b.value
 
 
 def check_env(file_root: str) -> dict:

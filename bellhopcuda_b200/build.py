@@ -17,14 +17,19 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libbhcb.so")
 BUILD = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["kernels2d.cu", "influence_mixed.cu", "arrivals.cu", "kernels3d.cu", "api.cu", "api3d.cu", "probe.cu",
+CU_SOURCES = ["kernels2d.cu", "influence_mixed.cu", "arrivals.cu", "kernels3d.cu", "api.cu", "api3d.cu",
               "noalloc.cu", "nn_gemm.cu", "nn_ops.cu", "influence_x.cu", "influence3d_x.cu", "nx2d.cu"]
 CPP_SOURCES = ["host/ldi.cpp", "host/env2d.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# Nx2D tracer: products and sums rounded separately, as the reference's host
-# build computes them (its landing decisions on boundary grid lines follow the
-# last bits of the position)
-EXTRA = {"nx2d.cu": ["-fmad=false"]}
+# FP64 ray tracers (2-D, 3-D, Nx2D, the ray-centred / Cerveny / SGB prologues,
+# the allocation-free fused kernel) and the FP64 influence / arrival gathers:
+# products and sums rounded separately, as the reference's x86 host build
+# computes them. Step-size reductions, boundary snaps and arrival merges are
+# decided at tolerance edges, so a contracted multiply-add changes step counts
+# and arrival counts of a few rays. The FP32 influence kernel keeps contraction.
+NO_FMAD = ("kernels2d.cu", "kernels3d.cu", "nx2d.cu", "influence_x.cu", "influence3d_x.cu", "noalloc.cu",
+           "arrivals.cu")
+EXTRA = {src: ["-fmad=false"] for src in NO_FMAD}
 
 
 def nvcc() -> str:

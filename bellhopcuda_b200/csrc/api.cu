@@ -318,7 +318,7 @@ void do_prepare(bhcb_ctx *c)
     }
     // --- build device tables
     Arena A;
-    struct EnvOffsets { size_t z, rho, c, cz, n2, n2z, coef, qr, qc, qcz, trc, brc, btop, bbot, rr, rz, sz, alpha, sbp; };
+    struct EnvOffsets { size_t z, rho, c, cz, n2, n2z, coef, qr, qc, qcz, trc, brc, btop, bbot, rr, rz, sz, alpha, acs, sbp; };
     std::vector<EnvOffsets> offs;
     std::vector<EnvDev> envdev;
     for(const GroupPlan &gp : plan) {
@@ -334,6 +334,11 @@ void do_prepare(bhcb_ctx *c)
         std::vector<float> rz_even = T.rz;
         if(rz_even.size() & 1) rz_even.push_back(rz_even.back());
         o.rr = A.put(T.rr); o.rz = A.put(rz_even); o.sz = A.put(T.sz); o.alpha = A.put(T.alpha);
+        // launch directions from the host's libm, the same doubles as the
+        // reference's RayInit (src/trace.hpp:61) computes on the CPU
+        std::vector<double> acs;
+        for(double a : T.alpha) { acs.push_back(std::cos(a)); acs.push_back(std::sin(a)); }
+        o.acs = A.put(acs);
         o.sbp = A.put(T.sbp);
         offs.push_back(o);
         EnvDev d{};
@@ -398,7 +403,7 @@ void do_prepare(bhcb_ctx *c)
         d.trc = dptr<double>(ab, o.trc); d.brc = dptr<double>(ab, o.brc);
         d.btop = dptr<BdryPtDev>(ab, o.btop); d.bbot = dptr<BdryPtDev>(ab, o.bbot);
         d.rr = dptr<double>(ab, o.rr); d.rz = dptr<float>(ab, o.rz); d.sz = dptr<float>(ab, o.sz);
-        d.alpha = dptr<double>(ab, o.alpha); d.sbp = dptr<double>(ab, o.sbp);
+        d.alpha = dptr<double>(ab, o.alpha); d.acs = dptr<double>(ab, o.acs); d.sbp = dptr<double>(ab, o.sbp);
     }
     CK(cudaMemcpyAsync(ab, A.bytes.data(), A.bytes.size(), cudaMemcpyHostToDevice, c->stream));
     c->stats.h2d_bytes = A.bytes.size();
@@ -951,6 +956,7 @@ namespace bhcb {
 int noalloc_job_from_ctx(bhcb_ctx *c, int32_t env, int32_t ifreq, NoAllocJob *job, const char **why)
 {
     if(!c->prepared) { *why = "context not prepared: call bhcb_prepare (or bhcb_run) first"; return BHCB_ERR_STATE; }
+    if(c->mode != MODE_TL) { *why = "the context was prepared for arrivals, eigenrays or rays, not a TL field"; return BHCB_ERR_STATE; }
     if(c->xkind) { *why = "this entry point covers geometric Cartesian beams ('G', 'B')"; return BHCB_ERR_ARG; }
     if(env < 0 || env >= (int)c->envs.size()) { *why = "env_index out of range"; return BHCB_ERR_ARG; }
     const EnvSlot &S = c->envs[env];
@@ -969,6 +975,7 @@ int noalloc_job_from_ctx(bhcb_ctx *c, int32_t env, int32_t ifreq, NoAllocJob *jo
             job->nrzp = F.nrzp;
             job->nrr = F.nrr;
             job->sm_count = c->sm_count;
+            job->device = c->device;
             job->stream = c->stream;
             return BHCB_OK;
         }

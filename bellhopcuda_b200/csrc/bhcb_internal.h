@@ -81,6 +81,7 @@ struct EnvDev {
     const double *rr;
     const float *rz, *sz;
     const double *alpha;
+    const double *acs;               // (cos, sin) pairs of alpha from the host's libm, as the reference's RayInit has them
     double dalpha, delta_r;
     // beam (include/bhc/structs.hpp:331-341)
     double deltas, box_x, box_y, freq0;

@@ -4,11 +4,12 @@
 // Who needs this: callers that must not allocate once they are running — code
 // that works inside a fixed device-memory budget owned by another allocator
 // (a framework's caching allocator that holds the free memory), real-time
-// loops with an allocation-free policy after initialisation, and code that
-// issues work while a CUDA stream is being captured into a graph (cudaMalloc
-// is not allowed there). They prepare a context once (bhcb_open / bhcb_setup /
-// bhcb_prepare, which do allocate), then call this entry point as often as
-// they like.
+// loops with an allocation-free policy after initialisation. They prepare a
+// context once (bhcb_open / bhcb_setup / bhcb_prepare, which do allocate),
+// then call this entry point as often as they like. The call is synchronous
+// (it copies the run header in and the counters out and waits for the
+// context stream); work that is to be captured into a CUDA graph uses the
+// bhcb_graph_* entry points below instead.
 //
 // How: it runs a variant of the trace kernel that evaluates each segment's
 // beam-receiver contributions inline instead of storing segment records, so
@@ -18,8 +19,9 @@
 // (16 MiB + 256 B) that every GPU which loads the library holds until the
 // process exits. Host code cannot use the
 // array's name as a device address, so the first call on each device, with
-// that device current, looks the address up with cudaGetSymbolAddress and
-// keeps it. That first call should therefore come before any stream capture.
+// that device (the context's GPU) made current, looks the address up with
+// cudaGetSymbolAddress and keeps it. Every call runs on the context's GPU and
+// restores the caller's current device before it returns.
 //
 // All calls on a device share the array: each call clears the counters and
 // the accumulator before use, and two calls whose GPU work overlaps (two
@@ -158,7 +160,7 @@ noalloc_trace_kernel(unsigned char *scratch, double freq)
         double alpha = e.alpha[ialpha];
         double SrcDecl = (180.0 / BHCB_PI) * alpha;
         V2<double> xs = mk2(0.0, (double)e.sz[isz]);
-        V2<R> tinit = mk2((R)cos(alpha), (R)sin(alpha));
+        V2<R> tinit = mk2((R)e.acs[2 * ialpha], (R)e.acs[2 * ialpha + 1]);
         SSPOut<R> o;
         eval_ssp(xs, tinit, o, e, iSeg, ctr);
         R c = o.c;
@@ -274,6 +276,22 @@ template<typename R> void launch_fused(const NoAllocJob &J, unsigned char *scrat
         noalloc_trace_kernel<double, R, false, false><<<grid, 32, 0, J.stream>>>(scratch, J.freq);
 }
 
+// Makes the context's GPU current for the lifetime of the guard and gives the
+// caller's current device back afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev)
+    {
+        if(cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if(prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 int put_msg(char *msg, size_t n, int code, const char *text)
 {
     if(msg && n) {
@@ -307,9 +325,12 @@ extern "C" int bhcb_run_noalloc(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq,
         return put_msg(msg, msg_len, BHCB_ERR_ARG, b);
     }
     if(bytes < nelem * sizeof(float2)) return put_msg(msg, msg_len, BHCB_ERR_ARG, "output buffer too small");
-    int dev = 0;
-    if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return put_msg(msg, msg_len, BHCB_ERR_CUDA, "no current CUDA device");
+    const int dev = J.device;
+    if(dev < 0 || dev >= kMaxDevices) return put_msg(msg, msg_len, BHCB_ERR_CUDA, "context device out of range");
+    // the context's stream, tables and the caller's buffer live on the
+    // context's GPU: run there whatever device the caller has current
+    DeviceGuard guard(dev);
+    if(!guard.ok) return put_msg(msg, msg_len, BHCB_ERR_CUDA, "cannot make the context's device current");
     void *scratch = nullptr;
     {
         // one-time set-up per device, with that device current
@@ -416,8 +437,11 @@ extern "C" int bhcb_graph_create(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq
     if(rc != BHCB_OK) return put_msg(msg, msg_len, rc, why ? why : "invalid request");
     const size_t nelem = (size_t)J.nsz * J.nrzp * J.nrr;
     if(bytes < nelem * sizeof(float2)) return put_msg(msg, msg_len, BHCB_ERR_ARG, "output buffer too small");
+    // graph scratch, stream and capture on the context's GPU
+    DeviceGuard guard(J.device);
+    if(!guard.ok) return put_msg(msg, msg_len, BHCB_ERR_CUDA, "cannot make the context's device current");
     auto *g = new bhcb_graph();
-    cudaGetDevice(&g->device);
+    g->device = J.device;
     auto fail = [&](int code, const char *text) {
         cudaGetLastError();
         bhcb_graph_destroy(g);

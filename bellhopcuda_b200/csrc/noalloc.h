@@ -13,6 +13,7 @@ struct NoAllocJob {   // one field of a prepared context
     double freq;
     int precision, gaussian, coherent;
     int nsz, nrzp, nrr, sm_count;
+    int device;       // the context's GPU: its stream, tables and buffers live there
     cudaStream_t stream;
 };
 

@@ -77,7 +77,7 @@ template<typename R> __device__ __forceinline__ bool ray_init2d(const EnvDev &e,
     st.alpha = alpha;
     const double SrcDecl = (180.0 / BHCB_PI) * alpha;
     const V2<double> xs = mk2(0.0, (double)e.sz[isz]);
-    const V2<R> tinit = mk2((R)cos(alpha), (R)sin(alpha));
+    const V2<R> tinit = mk2((R)e.acs[2 * ialpha], (R)e.acs[2 * ialpha + 1]);
     SSPOut<R> o;
     eval_ssp(xs, tinit, o, e, st.iSeg, ctr);
     const R c = o.c;

@@ -42,7 +42,9 @@ __device__ __forceinline__ bool ray_init3d(const Env3Dev &E, const Job3 &J, RayS
         amp0 = (float)(amp0 * ((double)sqrtf(2.0f) * fabs(sin(om / c * xs.z * sin(alpha)))));
     }
     Ray3 &p0 = st.p0;
-    const V3 tinit = v3(cos(alpha) * cos(beta), cos(alpha) * sin(beta), sin(alpha));
+    // launch direction from the host's cos / sin of the angles (the reference's RayInit computes them on the CPU)
+    const double ca = E.acs[2 * J.ialpha], sa = E.acs[2 * J.ialpha + 1];
+    const V3 tinit = v3(ca * E.bcs[2 * J.ibeta], ca * E.bcs[2 * J.ibeta + 1], sa);
     p0.x = xs;
     p0.c = c;
     p0.t = v3(tinit.x / c, tinit.y / c, tinit.z / c);

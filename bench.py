@@ -35,6 +35,10 @@ sys.path.insert(0, ROOT)
 METRIC = "TL fields/s on 1 B200: mixed vs FP64 trace, surrogate vs plain, <=0.5 dB TL err"
 UNIT = "TL fields/s"
 WORKLOAD = "rd_gauss"
+# the workload both arms run (identical in both JSON lines)
+CONFIG = {"workload": "rd_gauss: 2-D Gaussian-beam TL, PCHIP SSP 64 nodes, 200-pt bathymetry, 20001 rays "
+                      "+-30 deg, 501x2001 receivers, 10 freqs 50-500 Hz (log-spaced)",
+          "fields": 10, "rays": 20001, "receivers": 501 * 2001}
 
 # Algorithmic work per unit, frozen before the first GPU timing: one 2-D
 # oracle ray step (Step + RayUpdate + RayTerminate for a 1-D SSP) and one
@@ -141,6 +145,19 @@ def aggregate_value(world, fields_per_step, steps, total_s):
     return world * fields_per_step * steps / total_s
 
 
+# ------------------------------------------------------------- FP pipe peaks
+def probe_fp_peak(gpu):
+    """Measured (FP32, FP64) FMA throughput in TFLOP/s from bench_probe.so
+    (bench_probe.cu, built by __graft_entry__.build())."""
+    lib = ctypes.CDLL(os.path.join(ROOT, "bench_probe.so"))
+    lib.bench_probe_fp_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double)]
+    a, b = ctypes.c_double(), ctypes.c_double()
+    if lib.bench_probe_fp_peak(gpu, ctypes.byref(a), ctypes.byref(b)) != 0:
+        raise RuntimeError("FP peak probe failed")
+    return a.value, b.value
+
+
 # ------------------------------------------------------------- environment
 def make_env(tmp, rank):
     from bellhopcuda_b200 import workloads as W
@@ -228,86 +245,79 @@ def time_e2e(B, torch, root, freqs, steps, gpu, tune=None):
 
 
 # ------------------------------------------------------- reference CPU arm
-_libc = ctypes.CDLL(None)
-_libc.fma.restype = ctypes.c_double
-_libc.fma.argtypes = [ctypes.c_double] * 3
-
-
-def sampled_angles(n, a0, a1, first, m):
-    """The reference's sub-tabulated launch angles (SubTab, FMA form) first..first+m-1."""
-    dx = (a1 - a0) / (n - 1)
-    return [_libc.fma(float(i), dx, a0) for i in range(first, first + m)]
-
-
-def reference_sample(spec, freqs, m, tmp):
-    """Run the reference's own bellhopcxx (all host cores) on m consecutive rays
-    of every frequency; returns (estimated seconds per full step, detail)."""
+def reference_field(spec, freq, tmp, tag):
+    """One whole TL field of the workload (all 20001 rays at one frequency)
+    by the reference's own bellhopcxx on all host threads; returns the run's
+    own 'Run:' time in seconds (bhc::run only, file reading and writing
+    excluded) and the process's wall time."""
     import copy
     from bellhopcuda_b200.envfile import write_env
     exe = os.path.join(ROOT, "oracle", "_ref", "bellhopcxx")
     if not os.path.exists(exe):
-        return None, "oracle/_ref/bellhopcxx not built"
-    n = spec.nalpha
-    total_ms, detail = 0.0, []
-    for k, f in enumerate(freqs):
-        first = int((k + 0.5) * (n - m) / len(freqs))
-        s2 = copy.deepcopy(spec)
-        s2.freq = f
-        s2.nalpha = m
-        s2.alpha = sampled_angles(n, spec.alpha[0], spec.alpha[1], first, m)
-        root = write_env(s2, os.path.join(tmp, "refsample_%d" % k))
-        out = subprocess.run([exe, "-2", root], capture_output=True, text=True, timeout=600)
-        mm = re.search(r"Run:\s*([0-9.eE+-]+)\s*ms", out.stdout)
-        if out.returncode != 0 or not mm:
-            return None, "bellhopcxx failed: " + (out.stdout + out.stderr)[-200:]
-        ms = float(mm.group(1))
-        total_ms += ms
-        detail.append(ms)
-    est_s = total_ms * (n / m) / 1000.0
-    return est_s, detail
+        raise FileNotFoundError("oracle/_ref/bellhopcxx not built")
+    s2 = copy.deepcopy(spec)
+    s2.freq = freq
+    root = write_env(s2, os.path.join(tmp, "ref_%s" % tag))
+    t0 = time.perf_counter()
+    out = subprocess.run([exe, "-2", root], capture_output=True, text=True, timeout=1200)
+    wall = time.perf_counter() - t0
+    mm = re.search(r"Run:\s*([0-9.eE+-]+)\s*ms", out.stdout)
+    if out.returncode != 0 or not mm:
+        raise RuntimeError("bellhopcxx failed: " + (out.stdout + out.stderr)[-200:])
+    return float(mm.group(1)) / 1000.0, wall
 
 
-def cpu_baseline(spec, freqs, tmp, m=300):
-    est_s, detail = reference_sample(spec, freqs, m, tmp)
-    if est_s is None:
-        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                "sample": detail}
-    return {"value": len(freqs) / est_s, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-            "sample": "reference bellhopcxx (unmodified sources, all %d host threads), %d consecutive "
-                      "rays of the %d-ray fan for each of the %d frequencies, Run time scaled by "
-                      "%d/%d" % (os.cpu_count(), m, spec.nalpha, len(freqs), spec.nalpha, m),
-            "sample_run_ms": detail}
+def cpu_baseline(spec, freqs, tmp):
+    """Bounded sample for the main line: five whole fields (every other
+    frequency of the ten), each the full ray fan and receiver grid."""
+    idx = list(range(0, len(freqs), 2))
+    try:
+        runs = [reference_field(spec, freqs[i], tmp, "cb%d" % i)[0] for i in idx]
+    except Exception as e:   # noqa: BLE001 - reported, not fatal to the GPU line
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": str(e)}
+    return {"value": len(idx) / sum(runs), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": "reference bellhopcxx (unmodified sources, %d host threads): %d whole TL fields of the "
+                      "workload (20001 rays, 501x2001 receivers) at %s Hz; value = fields / sum of the "
+                      "runs' own Run: times" % (os.cpu_count(), len(idx),
+                                                ", ".join("%.1f" % freqs[i] for i in idx)),
+            "run_s": runs}
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's CPU implementation on the same workload: each step is
+    one whole TL field (the full 20001-ray fan over the 501 x 2001 grid) at
+    one of the ten frequencies, the frequencies taken in turn, so K steps
+    cover the ten fields K / 10 times. Measured, not extrapolated."""
     if rank != 0:
         return 0
     from bellhopcuda_b200 import workloads as W
     with tempfile.TemporaryDirectory() as tmp:
         spec = W.rd_gauss()
         freqs = W.rd_gauss_freqs()
-        vals = []
-        for _ in range(max(args.warmup, 0)):
-            reference_sample(spec, freqs, args.ref_rays, tmp)
-        for _ in range(args.steps):
-            est_s, detail = reference_sample(spec, freqs, args.ref_rays, tmp)
-            if est_s is None:
-                print(json.dumps({"impl": "reference", "unavailable": str(detail)}))
-                return 0
-            vals.append(len(freqs) / est_s)
-        v = statistics.mean(vals)
+        try:
+            for i in range(max(args.warmup, 0)):
+                reference_field(spec, freqs[i % len(freqs)], tmp, "w%d" % i)
+            runs, walls = [], []
+            for i in range(args.steps):
+                r, w = reference_field(spec, freqs[i % len(freqs)], tmp, "s%d" % i)
+                runs.append(r)
+                walls.append(w)
+        except Exception as e:   # noqa: BLE001 - the arm reports why it cannot run
+            print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+            return 0
+        v = args.steps / sum(runs)
         line = {
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * len(freqs) / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(runs) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "rd_gauss: 2-D Gaussian-beam TL, PCHIP SSP 64 nodes, 200-pt bathymetry, "
-                                   "20001 rays +-30 deg, 501x2001 receivers, 10 freqs 50-500 Hz",
-                       "sample": "%d rays per frequency" % args.ref_rays},
+            "data": "synthetic", "config": dict(CONFIG),
+            "step": "one whole TL field per step (frequencies in turn: %s)" % ", ".join(
+                "%.1f" % freqs[i % len(freqs)] for i in range(args.steps)),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                             "sample": "%d consecutive rays per frequency of the %d-ray fan, scaled"
-                                       % (args.ref_rays, spec.nalpha)},
+                             "sample": "%d whole fields of the workload, the reference's Run: time per field"
+                                       % args.steps},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s_per_field": statistics.mean(walls),
         }
         print(json.dumps(line))
     return 0
@@ -320,7 +330,6 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-rays", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     args = ap.parse_args()
@@ -349,7 +358,7 @@ def main():
     barrier, max_over_ranks = comm.barrier, comm.max_over_ranks
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    fp32_peak, fp64_peak = B.probe_fp_peak(local)
+    fp32_peak, fp64_peak = probe_fp_peak(local)
     with tempfile.TemporaryDirectory() as tmp:
         spec, root, freqs = make_env(tmp, rank)
         nf = len(freqs)
@@ -399,7 +408,7 @@ def main():
         roofline = {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": fp32_peak,
                     "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
                     "traffic": INFLUENCE_DRAM_BYTES if dom == "influence_kernel" else None,
-                    "peak_source": "bhcb_probe_fp_peak FP32 FMA probe measured in this run "
+                    "peak_source": "FP32 FMA probe (bench_probe.cu) measured in this run "
                                    "(MEASURED_PEAKS.json has no FP32 figure)",
                     "work": "%s x %d oracle units per launch" % (
                         ("F_infl=%g flop" % F_INFL, ORACLE_EVALS_ALL_FREQS) if dom == "influence_kernel"
@@ -411,16 +420,15 @@ def main():
                     "fp64_peak_tflops": fp64_peak}
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(spec, freqs, tmp, m=args.ref_rays)
+            cpu = cpu_baseline(spec, freqs, tmp)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 ray trace / f32 beam-receiver contributions", "data": "synthetic",
-        "config": {"workload": "rd_gauss: 2-D Gaussian-beam TL, PCHIP SSP 64 nodes, 200-pt bathymetry, "
-                               "20001 rays +-30 deg, 501x2001 receivers, 10 freqs 50-500 Hz, "
-                               "frequencies share one trajectory",
-                   "fields_per_step": nf, "rays": int(st["rays"]), "steps_traced": int(st["steps"]),
-                   "contributions": int(st["evals"]), "l2": "flushed (256 MiB write) before every timed step",
+        "config": dict(CONFIG),
+        "detail": {"frequencies_share_one_trajectory": True, "fields_per_step": nf, "rays": int(st["rays"]),
+                   "steps_traced": int(st["steps"]), "contributions": int(st["evals"]),
+                   "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": "replicas per GPU (one environment per rank)",
                    "launch_shape": {"trace_block": tuning["trace_block"],
                                     "influence_ctas_per_sm": tuning["influence_ctas_per_sm"],

@@ -1,10 +1,10 @@
-// Floating-point pipe peak probe: the roofline denominator for the tracer's
-// kernels, which are bound by the FP32/FP64 pipes rather than by HBM or the
-// tensor cores. Each thread runs independent FMA chains; every SM gets many
-// resident warps so the pipes, not latency, set the rate.
+// Floating-point pipe peak probe used by bench.py (not part of the library):
+// the roofline denominator for the tracer's kernels, which are bound by the
+// FP32/FP64 pipes rather than by HBM or the tensor cores. Each thread runs
+// independent FMA chains; every SM gets many resident warps so the pipes, not
+// latency, set the rate. Built by __graft_entry__.build() into bench_probe.so.
 #include <cuda_runtime.h>
-
-#include "../../include/bhcb.h"
+#include <stdint.h>
 
 namespace {
 
@@ -52,12 +52,13 @@ template<typename T> double run_probe(int sms)
 
 } // namespace
 
-extern "C" int bhcb_probe_fp_peak(int32_t gpu_index, double *fp32_tflops, double *fp64_tflops)
+// returns 0 on success, 3 (a CUDA error) otherwise
+extern "C" int bench_probe_fp_peak(int32_t gpu_index, double *fp32_tflops, double *fp64_tflops)
 {
-    if(cudaSetDevice(gpu_index) != cudaSuccess) return BHCB_ERR_CUDA;
+    if(cudaSetDevice(gpu_index) != cudaSuccess) return 3;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu_index);
     if(fp32_tflops) *fp32_tflops = run_probe<float>(sms);
     if(fp64_tflops) *fp64_tflops = run_probe<double>(sms);
-    return cudaGetLastError() == cudaSuccess ? BHCB_OK : BHCB_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }

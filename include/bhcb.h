@@ -148,10 +148,6 @@ int bhcb_eigen_hits(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, bhcb_eigen_
    their own work against the tracer's kernels. */
 int bhcb_stream(bhcb_ctx *ctx, void **stream);
 
-/* Measured FP32 / FP64 FMA throughput of the device (TFLOP/s), the roofline
-   denominators of the tracer's pipe-bound kernels. */
-int bhcb_probe_fp_peak(int32_t gpu_index, double *fp32_tflops, double *fp64_tflops);
-
 /* Counters of the last run. */
 int bhcb_get_stats(bhcb_ctx *ctx, bhcb_stats *stats);
 
@@ -174,19 +170,21 @@ int bhcb_check_env3d(const char *file_root, int32_t *dims, int64_t *nrays, char 
 
 /* Allocation-free run (no counterpart in the reference). For callers that
    must not allocate device memory once running — work inside a budget owned
-   by another allocator, allocation-free real-time loops, issuing work while a
-   stream is being captured. Computes field (env_index, ifreq) of a context
-   prepared earlier (bhcb_prepare / bhcb_run, which allocate) into the
+   by another allocator, allocation-free real-time loops. Computes TL field
+   (env_index, ifreq) of a context prepared earlier for a TL run (bhcb_prepare
+   / bhcb_run, which allocate; other run types give BHCB_ERR_STATE) into the
    caller's device buffer field_dev ([NSz][NRz_per_range][NRr] complex float,
-   bytes >= its size) on the context stream, then synchronises. It calls no
-   cudaMalloc / cudaFree: its scratch (accumulator, counters, field
-   descriptor) is a static device array the library reserves on every GPU
-   that loads it, limited to BHCB_NOALLOC_MAX_FIELD receivers per field; larger
-   fields are rejected with BHCB_ERR_ARG. The first call on a device looks up
-   the array's address (cudaGetSymbolAddress) and should come before any
-   stream capture. All calls on a device share the array: calls whose GPU
-   work overlaps race and must be serialised. msg (may be NULL) receives the
-   reason of a failure. */
+   bytes >= its size, on the context's GPU) on the context stream, then
+   synchronises; it is not meant for stream capture (bhcb_graph_* is). It
+   runs on the context's GPU whatever device is current and restores the
+   current device. It calls no cudaMalloc / cudaFree: its scratch
+   (accumulator, counters, field descriptor) is a static device array the
+   library reserves on every GPU that loads it, limited to
+   BHCB_NOALLOC_MAX_FIELD receivers per field; larger fields are rejected with
+   BHCB_ERR_ARG. The first call on a device looks up the array's address
+   (cudaGetSymbolAddress). All calls on a device share the array: calls whose
+   GPU work overlaps race and must be serialised. msg (may be NULL) receives
+   the reason of a failure. */
 #define BHCB_NOALLOC_MAX_FIELD (1 << 21)
 int bhcb_run_noalloc(bhcb_ctx *ctx, int32_t env_index, int32_t ifreq, void *field_dev, size_t bytes,
                      char *msg, size_t msg_len);

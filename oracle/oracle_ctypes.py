@@ -239,3 +239,55 @@ def run(spec, max_narr=20, allow_merging=1, eigen_memsize=100000, rays=None):
     res.update(rr=rr, rz=rz, nsteps=out.nsteps, nevals=out.nevals,
                err_bits=out.err_bits, warn_bits=out.warn_bits, rc=rc)
     return res
+
+
+def run_threaded(spec, nthreads=None, chunk=None):
+    """Coherent TL of the whole fan, traced in ray ranges on host threads.
+
+    The C restatement holds no global state and ctypes releases the GIL for
+    the call, so ray ranges run side by side; ScalePressure is linear for
+    coherent runs, so the range fields add up to the field of the whole fan
+    (float additions in another order: equal to within float rounding).
+    Returns the summed field and the summed step and contribution counts."""
+    from concurrent.futures import ThreadPoolExecutor
+    if spec.run_type[0] != "C":
+        raise ValueError("run_threaded: coherent TL runs only (incoherent fields are not additive)")
+    n = sizes(spec)["Nalpha"]
+    nthreads = nthreads or os.cpu_count() or 1
+    chunk = chunk or max(1, -(-n // (4 * nthreads)))
+    ranges = [(a, min(chunk, n - a)) for a in range(0, n, chunk)]
+    with ThreadPoolExecutor(max_workers=nthreads) as ex:
+        parts = list(ex.map(lambda r: run(spec, rays=r), ranges))
+    out = dict(parts[0])
+    out["field"] = sum(p["field"] for p in parts)
+    out["nsteps"] = sum(p["nsteps"] for p in parts)
+    out["nevals"] = sum(p["nevals"] for p in parts)
+    out["err_bits"] = 0
+    for p in parts:
+        out["err_bits"] |= p["err_bits"]
+    return out
+
+
+def sizes(spec):
+    """NSz, NRz, NRr and Nalpha as the oracle's preprocessing gives them."""
+    lib = load()
+    env, keep = make_env(spec)
+    out = O2Out()
+    if lib.oracle2d_sizes(C.byref(env), C.byref(out)) != 0:
+        raise RuntimeError("oracle: invalid environment")
+    del keep
+    return {"NSz": out.NSz, "NRz": out.NRz, "NRz_per_range": out.NRz_per_range, "NRr": out.NRr,
+            "Nalpha": out.Nalpha}
+
+
+def reference_dir() -> str:
+    """The reference source tree: $BHCB_REFERENCE, else oracle/Makefile's REF
+    default (the one place that names it)."""
+    env = os.environ.get("BHCB_REFERENCE")
+    if env:
+        return env
+    try:
+        return subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True,
+                              check=True).stdout.strip()
+    except (OSError, subprocess.CalledProcessError):
+        return ""

@@ -123,7 +123,9 @@ def test_open_without_gpu_fails_loudly():
         B.Tracer()
 
 
-REFERENCE_INPUTS = "/root/reference/test/in"
+import oracle_ctypes  # noqa: E402  (test infrastructure: locates the reference tree)
+
+REFERENCE_INPUTS = os.path.join(oracle_ctypes.reference_dir(), "test", "in")
 
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INPUTS), reason="reference inputs not present")
