@@ -39,7 +39,7 @@ from bellhopcuda_b200.shdfile import read_shd  # noqa: E402
 
 EXE = os.path.join(ROOT, "oracle", "_ref", "bellhopcxx")
 NTHETA_SUBSET = 2          # bearings 0 and 180 degrees of the 36-bearing grid
-SAMPLE_EVERY = 97          # arrival records kept for every 97th receiver
+SAMPLE_EVERY = 997         # arrival records kept for every 997th receiver
 
 
 def c4_files(run_type: str, ntheta: int = NTHETA_SUBSET) -> dict:
