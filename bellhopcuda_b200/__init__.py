@@ -26,7 +26,6 @@ LIB_PATH = os.path.join(HERE, "libbhcb.so")
 PREC_FP64 = 0
 PREC_MIXED = 1
 FLAG_SERIAL_INFLUENCE = 1   # BHCB_FLAG_SERIAL_INFLUENCE
-FLAG_SEGMENT_INFLUENCE = 2  # BHCB_FLAG_SEGMENT_INFLUENCE
 
 ERR_NAMES = {
     2: "BHC_ERR_RAYINIT", 3: "BHC_ERR_BOUNDARY_SEG_CONTAINS_NAN",
@@ -188,11 +187,9 @@ class Tracer:
     """One bhcb context (one GPU, one stream)."""
 
     def __init__(self, gpu: int = 0, precision: int = PREC_MIXED, max_memory: int = 0,
-                 share_trajectory: bool = True, serial_influence: bool = False,
-                 segment_influence: bool = False):
+                 share_trajectory: bool = True, serial_influence: bool = False):
         self._lib = load_library()
-        flags = (FLAG_SERIAL_INFLUENCE if serial_influence else 0) | \
-            (FLAG_SEGMENT_INFLUENCE if segment_influence else 0)
+        flags = FLAG_SERIAL_INFLUENCE if serial_influence else 0
         init = Init(gpu, precision, max_memory, 1 if share_trajectory else 0, flags, None)
         h = C.c_void_p()
         rc = self._lib.bhcb_open(C.byref(init), C.byref(h))

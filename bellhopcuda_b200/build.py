@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libbhcb.so")
 BUILD = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["kernels2d.cu", "influence_mixed.cu", "influence_tile.cu", "arrivals.cu", "kernels3d.cu", "api.cu", "api3d.cu",
+CU_SOURCES = ["kernels2d.cu", "influence_mixed.cu", "arrivals.cu", "kernels3d.cu", "api.cu", "api3d.cu",
               "noalloc.cu", "nn_gemm.cu", "nn_ops.cu", "influence_x.cu", "influence3d_x.cu", "nx2d.cu"]
 CPP_SOURCES = ["host/ldi.cpp", "host/env2d.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

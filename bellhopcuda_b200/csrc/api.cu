@@ -34,14 +34,6 @@ template<typename R> cudaError_t launch_influence(const void *, unsigned long lo
                                                   const GroupDev *, int, const double *, float2 *,
                                                   RunCounters *, bool, bool, int, cudaStream_t);
 cudaError_t launch_scale(const float2 *, float2 *, const GroupDev *, int, int, cudaStream_t);
-cudaError_t launch_tile_binning(const void *, unsigned long long, const RunCounters *, RunCounters *,
-                                const GroupDev *, int, const TileGroupDev *, unsigned int *, float *, unsigned int *,
-                                unsigned int *, long long, long long, int, unsigned int *, unsigned long long, int,
-                                cudaStream_t);
-cudaError_t launch_tiles(const void *, const GroupDev *, int, const TileGroupDev *, const double *,
-                         const unsigned int *, const unsigned int *, const unsigned int *, unsigned long long, int,
-                         int, unsigned long long, float2 *, RunCounters *, bool, bool, int, cudaStream_t);
-int tile_ctas_per_sm(int nfreq_max, bool gauss, bool coherent);
 size_t seg_record_bytes(bool fp64);
 template<typename R> cudaError_t launch_arr_gather(const void *, unsigned long long, const GroupDev *, int,
                                                    const double *, bool, bool, ArrCand *, uint64_t *, uint32_t *,
@@ -166,15 +158,6 @@ struct bhcb_ctx {
     unsigned long long job0_h = 0;   // staging for the job counter's start value
     DevBuf blk_state, scan;          // published segment blocks; queue of an overlapped launch
     bool last_overlapped = false;
-    // tiled influence (mixed-precision TL on rectilinear grids): per-group
-    // tile layout, bin counts / work estimates / offsets, tile order, bin lists
-    bool tiled_opt = true;           // BHCB_FLAG_SEGMENT_INFLUENCE turns it off
-    bool tiles = false;              // the prepared batch takes the tiled path
-    std::vector<TileGroupDev> tg_h;
-    DevBuf tg_d, tcnt, twork, toff, torder, tlist;
-    long long nbins = 0;
-    int ndb_max = 1, nfreq_max = 1;
-    unsigned long long list_cap = 0;
 
     // arrivals / eigen runs (RunType 'A', 'a', 'E')
     int mode = MODE_TL;
@@ -275,59 +258,6 @@ void prepare_arrivals(bhcb_ctx *c)
         c->narr_d.ensure(cells * sizeof(int32_t));
         c->arr_d.ensure(cells * (size_t)mx * sizeof(ArrivalRec));
     }
-}
-
-// Tile layout of the tiled influence: bins [isz][column block] per group,
-// depth blocks of TILE_DEPTHS; taken by mixed-precision TL batches of
-// geometric Cartesian beams on rectilinear grids.
-void prepare_tiles(bhcb_ctx *c)
-{
-    c->tiles = false;
-    if(!c->tiled_opt || c->precision == BHCB_PREC_FP64 || c->mode != MODE_TL || c->xkind) return;
-    for(const EnvDev &d : c->envdev_h)
-        if(d.irregular) return;
-    std::vector<TileGroupDev> tg;
-    long long nbins = 0;
-    int ndb_max = 1, nfreq_max = 1;
-    for(size_t g = 0; g < c->groups_h.size(); ++g) {
-        const GroupDev &G = c->groups_h[g];
-        const EnvSlot &S = c->envs[c->fields[G.field_index].env];
-        const EnvTables &T = S.tables[c->fields[G.field_index].ifreq];
-        TileGroupDev t{};
-        t.bin_base = nbins;
-        t.ncb = ((int)T.rr.size() + TILE_COLS - 1) / TILE_COLS;
-        t.ndb = (T.nrz_per_range + TILE_DEPTHS - 1) / TILE_DEPTHS;
-        const size_t nr = T.rr.size();
-        t.rstep = nr > 1 ? T.rr[1] - T.rr[0] : 0.0;
-        bool uni = nr > 1;
-        for(size_t i = 1; i < nr && uni; ++i) {
-            const double want = T.rr[0] + (double)i * t.rstep;
-            uni = std::fabs(T.rr[i] - want) <= 1e-9 * std::max(1.0, std::fabs(T.rr[i]));
-        }
-        t.uniform_r = uni ? 1 : 0;
-        const size_t nz = T.rz.size();
-        t.dz_mean = nz > 1 ? std::max(1e-3f, (float)((T.rz.back() - T.rz.front()) / (double)(nz - 1))) : 1.f;
-        nbins += (long long)T.sz.size() * t.ncb;
-        ndb_max = std::max(ndb_max, t.ndb);
-        nfreq_max = std::max(nfreq_max, (int)G.nfreq);
-        tg.push_back(t);
-    }
-    if(ndb_max > 255 || (unsigned long long)nbins * (unsigned long long)ndb_max >= 0xffffffffull) return;
-    c->tg_h = tg;
-    c->nbins = nbins;
-    c->ndb_max = ndb_max;
-    c->nfreq_max = nfreq_max;
-    c->tg_d.ensure(tg.size() * sizeof(TileGroupDev));
-    CK(cudaMemcpyAsync(c->tg_d.p, tg.data(), tg.size() * sizeof(TileGroupDev), cudaMemcpyHostToDevice, c->stream));
-    c->tcnt.ensure((size_t)(nbins + 1) * sizeof(unsigned int));
-    c->twork.ensure((size_t)(nbins + 1) * sizeof(float));
-    c->toff.ensure((size_t)(nbins + 1) * sizeof(unsigned int));
-    c->torder.ensure((size_t)nbins * ndb_max * sizeof(unsigned int));
-    // a segment is listed once per column block it touches: most touch one or two
-    c->list_cap = std::max<unsigned long long>(c->list_cap, c->seg_cap * 3);
-    c->tlist.ensure(c->list_cap * sizeof(unsigned int));
-    c->stats.h2d_bytes += tg.size() * sizeof(TileGroupDev);
-    c->tiles = true;
 }
 
 void do_prepare(bhcb_ctx *c)
@@ -536,7 +466,6 @@ void do_prepare(bhcb_ctx *c)
     c->seg_cap = std::min(want, maxcap);
     c->segs.ensure(c->seg_cap * rec);
     if(c->mode != MODE_TL) prepare_arrivals(c);
-    prepare_tiles(c);
     c->prepared = true;
 }
 
@@ -559,7 +488,7 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         c->job0_h = (unsigned long long)job0;
         CK(cudaMemcpyAsync(jobc, &c->job0_h, sizeof(unsigned long long), cudaMemcpyHostToDevice, c->stream));
     }
-    if(clear && !c->tiles) {
+    if(clear) {
         const int64_t a0 = c->groups_h[g0].acc_base;
         const int64_t a1 = g1 < ngall ? c->groups_h[g1].acc_base : c->total_acc;
         CK(cudaMemsetAsync((float2 *)c->acc.p + a0, 0, (size_t)(a1 - a0) * sizeof(float2), c->stream));
@@ -595,32 +524,6 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     if(tgrid < 1) tgrid = 1;
     const GroupDev *G = (const GroupDev *)c->groups_d.p + g0;
     int ng = g1 - g0;
-    if(c->tiles) {
-        // trace, then bin the segments by receiver column block and evaluate
-        // tile by tile straight into the output (no accumulator, no scale pass)
-        const long long b0 = c->tg_h[g0].bin_base;
-        const long long b1 = g1 < ngall ? c->tg_h[g1].bin_base : c->nbins;
-        CK(cudaMemsetAsync(c->tcnt.p, 0, (size_t)(c->nbins + 1) * sizeof(unsigned int), c->stream));
-        CK(cudaMemsetAsync(c->twork.p, 0, (size_t)(c->nbins + 1) * sizeof(float), c->stream));
-        CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, nullptr, (int)tgrid, tblock,
-                               c->stream, stage_bytes));
-        CK(cudaEventRecord(c->ev[1], c->stream));
-        const TileGroupDev *TG = (const TileGroupDev *)c->tg_d.p + g0;
-        CK(launch_tile_binning(c->segs.p, c->seg_cap, ctr, ctr, G, ng, TG, (unsigned int *)c->tcnt.p,
-                               (float *)c->twork.p, (unsigned int *)c->toff.p, (unsigned int *)c->torder.p, b0, b1,
-                               c->ndb_max, (unsigned int *)c->tlist.p, c->list_cap, c->sm_count, c->stream));
-        CK(cudaEventRecord(c->ev[4], c->stream));
-        const unsigned long long ntiles = (unsigned long long)(b1 - b0) * c->ndb_max;
-        const int tgrid2 = c->sm_count * tile_ctas_per_sm(c->nfreq_max, c->gauss, c->coherent);
-        CK(launch_tiles(c->segs.p, G, ng, TG, (const double *)c->freqs_d.p, (const unsigned int *)c->tlist.p,
-                        (const unsigned int *)c->toff.p, (const unsigned int *)c->torder.p, ntiles, c->ndb_max,
-                        c->nfreq_max, c->list_cap, (float2 *)c->out.p, ctr, c->gauss, c->coherent, tgrid2,
-                        c->stream));
-        CK(cudaEventRecord(c->ev[2], c->stream));
-        CK(cudaEventRecord(c->ev[3], c->stream));
-        c->last_overlapped = false;
-        return;
-    }
     // mixed TL runs driven by the host: influence kernels on stream2 take the
     // segment blocks the trace publishes while it runs (no kernel waits for
     // another; the host relaunches them until the trace's end event)
@@ -958,25 +861,10 @@ void run_arrivals(bhcb_ctx *c)
 
 // TL runs whose segments do not fit in max_memory at once: trace the groups in
 // contiguous waves, halving a wave (by jobs) until its segments fit.
-// the tiled influence's bin lists were too short: make room for what the
-// binning counted (and a margin) before the run is repeated
-void grow_list(bhcb_ctx *c)
-{
-    const unsigned long long need = c->last.nlist + c->last.nlist / 4 + 1024;
-    if(need * sizeof(unsigned int) > c->max_memory) throw MemError("tiled influence lists exceed max_memory");
-    c->list_cap = std::max(c->list_cap * 2, need);
-    c->tlist.ensure(c->list_cap * sizeof(unsigned int));
-}
-
 int run_range(bhcb_ctx *c, int g0, int g1, bhcb_stats &acc)
 {
     do_launch_range(c, g0, g1, true, true);
     do_sync(c);
-    for(int k = 0; k < 4 && (c->last.err_bits & (1u << ERR_LIST_OVERFLOW)); ++k) {
-        grow_list(c);
-        do_launch_range(c, g0, g1, true, true);
-        do_sync(c);
-    }
     if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
         if(g1 - g0 <= 1)
             throw MemError("one environment's segments exceed max_memory; raise bhcb_init.max_memory");
@@ -1027,10 +915,6 @@ int run_checked(bhcb_ctx *c)
     for(int attempt = 0; attempt < 8; ++attempt) {
         do_launch(c, true);
         do_sync(c);
-        if(c->last.err_bits & (1u << ERR_LIST_OVERFLOW)) {
-            grow_list(c);
-            continue;
-        }
         if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
             // grow the segment buffer and run again
             size_t rec = c->xkind ? sizeof(XSeg) : seg_record_bytes(c->precision == BHCB_PREC_FP64);
@@ -1214,7 +1098,6 @@ int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
         if(init->max_memory) c->max_memory = init->max_memory;
         c->share = init->share_trajectory != 0;
         c->overlap = (init->flags & BHCB_FLAG_SERIAL_INFLUENCE) == 0;
-        c->tiled_opt = (init->flags & BHCB_FLAG_SEGMENT_INFLUENCE) == 0;
         c->output_cb = init->output_callback;
     }
     int ndev = 0;
@@ -1713,10 +1596,7 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
             if(tr < t.trace_ms) { t.trace_ms = tr; t.stage_kb = kb; }
         }
         c->stage_cap = (unsigned int)t.stage_kb * 1024u;
-        // the segment-by-segment influence is persistent over a chosen number of
-        // CTAs per SM; the tiled one runs as many as fit
         for(int k : {2, 3, 4, 5, 6, 8, 10, 12}) {
-            if(c->tiles) break;
             c->influence_ctas_per_sm = k;
             timed(tr, inf);
             if(inf < t.influence_ms) { t.influence_ms = inf; t.influence_ctas_per_sm = k; }

@@ -23,7 +23,6 @@ enum : uint32_t {
     ERR_RAYINIT = 2, ERR_BOUNDARY_SEG_NAN = 3, ERR_BOUNDARY_CONDITION_TYPE = 4,
     ERR_INVALID_SSP_TYPE = 5, ERR_OUTSIDE_ALTIMETRY = 6, ERR_OUTSIDE_BATHYMETRY = 7,
     ERR_OUTSIDE_SSP = 8, ERR_QUAD_ISEG = 9,
-    ERR_LIST_OVERFLOW = 29,          // the tiled influence's bin lists need more room (this runtime's own)
     ERR_STAGE_WAIT = 30,             // a shared-memory table staging wait ran out (this runtime's own)
     ERR_SEG_OVERFLOW = 31,
 };
@@ -270,26 +269,6 @@ struct RunCounters {
     unsigned int overflow_job;    // first job that could not store its segments
     unsigned int pad;
     unsigned long long chunk_counter;   // influence work queue (32-segment chunks)
-    unsigned long long nlist;     // tiled influence: (segment, column block) entries the binning needs
-    unsigned long long tile_counter;    // tiled influence work queue
-};
-
-// Tiled influence of the mixed-precision TL path: the receiver grid of every
-// (group, source depth) is cut into column blocks of TILE_COLS ranges ("bins";
-// each segment is listed in the bins its receiver columns touch) and depth
-// blocks of TILE_DEPTHS depths; one CTA owns a (bin, depth block) tile, one
-// thread per depth, and keeps the tile's fields for all frequencies in
-// registers, so no contribution goes through a global atomic.
-constexpr int TILE_COLS = 4;
-constexpr int TILE_DEPTHS = 256;
-struct TileGroupDev {
-    int64_t bin_base;        // first bin of the group; bins are [isz][column block]
-    int32_t ncb, ndb;        // column blocks, depth blocks
-    int32_t uniform_r;       // ranges equally spaced: the phase turns by a fixed rotation per column
-    int32_t pad;
-    double rstep;            // range spacing (m) when uniform_r
-    float dz_mean;           // mean receiver depth spacing (work estimate of the tile order)
-    float pad2;
 };
 
 } // namespace bhcb

@@ -44,12 +44,6 @@ enum { BHCB_PREC_FP64 = 0, BHCB_PREC_MIXED = 1 };
    not waited for). This flag keeps the influence after the trace in stream
    order, for callers that need bhcb_launch not to block (e.g. stream capture). */
 #define BHCB_FLAG_SERIAL_INFLUENCE 1
-/* Mixed-precision TL runs on rectilinear receiver grids evaluate the
-   contributions tile by tile (receiver column blocks, all frequencies of a
-   trace group at once) after the trace; this flag selects the segment-by-
-   segment influence instead (overlapped with the trace unless
-   BHCB_FLAG_SERIAL_INFLUENCE is also set). */
-#define BHCB_FLAG_SEGMENT_INFLUENCE 2
 
 /* Context options; mirrors bhcInit (include/bhc/structs.hpp:490-546). */
 typedef struct bhcb_init {
