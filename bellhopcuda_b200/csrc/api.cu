@@ -34,6 +34,7 @@ template<typename R> cudaError_t launch_influence(const void *, unsigned long lo
                                                   const GroupDev *, int, const double *, float2 *,
                                                   RunCounters *, bool, bool, int, cudaStream_t);
 cudaError_t launch_scale(const float2 *, float2 *, const GroupDev *, int, int, cudaStream_t);
+cudaError_t launch_set_counter(unsigned long long *, unsigned long long, cudaStream_t);
 size_t seg_record_bytes(bool fp64);
 template<typename R> cudaError_t launch_arr_gather(const void *, unsigned long long, const GroupDev *, int,
                                                    const double *, bool, bool, ArrCand *, uint64_t *, uint32_t *,
@@ -129,7 +130,13 @@ struct bhcb_ctx {
     void (*output_cb)(const char *) = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;   // influence launches beside the trace
-    bool overlap = true;              // mixed TL runs: influence overlaps the trace
+    bool overlap = false;             // mixed TL runs: influence overlaps the trace (BHCB_FLAG_OVERLAP_INFLUENCE)
+    // the serial TL step captured once into a CUDA graph and replayed
+    bool use_graphs = true;
+    int graph_state = 0;              // 0: next launch direct, 1: next launch captures, 2: replay
+    cudaGraph_t lgraph = nullptr;
+    cudaGraphExec_t lexec = nullptr;
+    bool capturing = false;           // the step is being captured: events are recorded as external nodes
     // ev: 0 start, 1 trace end, 2 influence end, 3 scale end, 4 first influence launch
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
@@ -155,7 +162,6 @@ struct bhcb_ctx {
     std::vector<EnvDev> envdev_h;    // the prepared environments (counts; plans the staging)
 
     DevBuf arena, groups_d, freqs_d, acc, out, segs, counters;
-    unsigned long long job0_h = 0;   // staging for the job counter's start value
     DevBuf blk_state, scan;          // published segment blocks; queue of an overlapped launch
     bool last_overlapped = false;
 
@@ -260,9 +266,21 @@ void prepare_arrivals(bhcb_ctx *c)
     }
 }
 
+void drop_graph(bhcb_ctx *c);
+
+// Records step event k on stream st; inside a capture as an external event
+// node, so that the replayed graph records it like a direct launch does (its
+// times stay readable).
+cudaError_t record_event(bhcb_ctx *c, int k, cudaStream_t st)
+{
+    return c->capturing ? cudaEventRecordWithFlags(c->ev[k], st, cudaEventRecordExternal)
+                        : cudaEventRecord(c->ev[k], st);
+}
+
 void do_prepare(bhcb_ctx *c)
 {
     if(c->envs.empty()) throw StateError("no environment: call bhcb_setup or bhcb_add_env first");
+    drop_graph(c);
     CK(cudaSetDevice(c->device));
     c->groups_h.clear();
     c->fields.clear();
@@ -479,21 +497,20 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     const int ngall = (int)c->groups_h.size();
     const long long job0 = c->groups_h[g0].job_base;
     const long long job1 = g1 < ngall ? (long long)c->groups_h[g1].job_base : c->njobs;
+    // counters cleared, overflow job set to "none", job counter to the first
+    // job: memsets and a one-thread kernel, so that a captured step refers to
+    // no host memory
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(RunCounters) + 64, c->stream));
     RunCounters *ctr = (RunCounters *)c->counters.p;
-    unsigned long long init_overflow = 0xffffffffull;
-    CK(cudaMemcpyAsync(&ctr->overflow_job, &init_overflow, 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(&ctr->overflow_job, 0xff, sizeof(ctr->overflow_job), c->stream));
     unsigned long long *jobc = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
-    if(job0) {
-        c->job0_h = (unsigned long long)job0;
-        CK(cudaMemcpyAsync(jobc, &c->job0_h, sizeof(unsigned long long), cudaMemcpyHostToDevice, c->stream));
-    }
+    if(job0) CK(launch_set_counter(jobc, (unsigned long long)job0, c->stream));
     if(clear) {
         const int64_t a0 = c->groups_h[g0].acc_base;
         const int64_t a1 = g1 < ngall ? c->groups_h[g1].acc_base : c->total_acc;
         CK(cudaMemsetAsync((float2 *)c->acc.p + a0, 0, (size_t)(a1 - a0) * sizeof(float2), c->stream));
     }
-    CK(cudaEventRecord(c->ev[0], c->stream));
+    CK(record_event(c, 0, c->stream));
     if(c->xkind) {
         // ray-centred / Cerveny / simple Gaussian beams: FP64 trace with the
         // kind's influence prologue, then its influence kernel and scaling
@@ -502,16 +519,16 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         long long xgrid = std::min<long long>((job1 - job0 + 63) / 64, (long long)c->sm_count * 16);
         CK(launch_trace_x(Gx, ngx, job1, (XSeg *)c->segs.p, c->seg_cap, ctr, jobc, c->xkind, (int)std::max(1LL, xgrid),
                           64, c->stream));
-        CK(cudaEventRecord(c->ev[1], c->stream));
+        CK(record_event(c, 1, c->stream));
         c->last_overlapped = false;
         int nzmax = 1;   // receiver depths per range, the most of the launched groups
         for(int g = g0; g < g1; ++g) nzmax = std::max(nzmax, c->fields[c->groups_h[g].field_index].nrzp);
         CK(launch_influence_x((const XSeg *)c->segs.p, c->seg_cap, Gx, ngx, (const double *)c->freqs_d.p,
                               (float2 *)c->acc.p, ctr, c->xkind, nzmax, c->sm_count * 16, c->stream));
-        CK(cudaEventRecord(c->ev[2], c->stream));
+        CK(record_event(c, 2, c->stream));
         CK(launch_scale_x((const float2 *)c->acc.p, (float2 *)c->out.p, Gx, ngx, (const double *)c->freqs_d.p, ctr,
                           c->sm_count * 2, c->stream));
-        CK(cudaEventRecord(c->ev[3], c->stream));
+        CK(record_event(c, 3, c->stream));
         return;
     }
     int tblock = c->trace_block;
@@ -536,7 +553,7 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         c->scan.ensure(64);
         blk = (unsigned int *)c->blk_state.p;
         CK(cudaMemsetAsync(blk, 0, nblk * sizeof(unsigned int), c->stream));
-        CK(cudaEventRecord(c->ev[0], c->stream));
+        CK(record_event(c, 0, c->stream));
     }
     if(fp64)
         CK(launch_trace<double>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
@@ -544,14 +561,14 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     else
         CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
                                c->stream, stage_bytes));
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(record_event(c, 1, c->stream));
     if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
     if(ovl) {
         const int igrid = c->sm_count * c->influence_ctas_per_sm;
         unsigned long long *scan = (unsigned long long *)c->scan.p;
         const double *fq = (const double *)c->freqs_d.p;
         CK(cudaStreamWaitEvent(c->stream2, c->ev[0], 0));
-        CK(cudaEventRecord(c->ev[4], c->stream2));
+        CK(record_event(c, 4, c->stream2));
         for(;;) {
             cudaError_t q = cudaEventQuery(c->ev[1]);
             if(q == cudaSuccess) break;
@@ -566,10 +583,10 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         CK(cudaMemsetAsync(scan, 0, sizeof(unsigned long long), c->stream2));
         CK(launch_influence_mixed(c->segs.p, c->seg_cap, G, ng, fq, (float2 *)c->acc.p, ctr, c->gauss,
                                   c->coherent, igrid, c->stream2, blk, scan));
-        CK(cudaEventRecord(c->ev[2], c->stream2));
+        CK(record_event(c, 2, c->stream2));
         CK(cudaStreamWaitEvent(c->stream, c->ev[2], 0));
         CK(launch_scale((const float2 *)c->acc.p, (float2 *)c->out.p, G, ng, c->sm_count * 2, c->stream));
-        CK(cudaEventRecord(c->ev[3], c->stream));
+        CK(record_event(c, 3, c->stream));
         return;
     }
     // the influence grid covers the buffer capacity; chunks past the stored
@@ -581,9 +598,9 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     else
         CK(launch_influence<float>(c->segs.p, c->seg_cap, G, ng, (const double *)c->freqs_d.p,
                                    (float2 *)c->acc.p, ctr, c->gauss, c->coherent, igrid, c->stream));
-    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(record_event(c, 2, c->stream));
     CK(launch_scale((const float2 *)c->acc.p, (float2 *)c->out.p, G, ng, c->sm_count * 2, c->stream));
-    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(record_event(c, 3, c->stream));
 }
 
 void do_launch(bhcb_ctx *c, bool host_driven)
@@ -591,18 +608,69 @@ void do_launch(bhcb_ctx *c, bool host_driven)
     do_launch_range(c, 0, (int)c->groups_h.size(), true, host_driven);
 }
 
+void drop_graph(bhcb_ctx *c)
+{
+    if(c->lexec) cudaGraphExecDestroy(c->lexec);
+    if(c->lgraph) cudaGraphDestroy(c->lgraph);
+    c->lexec = nullptr;
+    c->lgraph = nullptr;
+    c->graph_state = 0;
+}
+
+// One step of a prepared batch. Serial TL steps run directly the first time
+// (one-time kernel set-up happens outside any capture), are captured into a
+// CUDA graph the second time, and replay that graph afterwards; whatever
+// changes the prepared state or the launch shape drops the graph.
+void launch_step(bhcb_ctx *c)
+{
+    const bool overlapped = c->overlap && c->precision != BHCB_PREC_FP64 && c->mode == MODE_TL;
+    if(!c->use_graphs || overlapped || c->mode != MODE_TL || c->graph_state == 0) {
+        do_launch(c, c->overlap);
+        if(c->use_graphs && !overlapped && c->mode == MODE_TL) c->graph_state = 1;
+        return;
+    }
+    if(c->graph_state == 1) {
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        try {
+            do_launch(c, false);
+        } catch(...) {
+            c->capturing = false;
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(c->stream, &g);
+            if(g) cudaGraphDestroy(g);
+            throw;
+        }
+        c->capturing = false;
+        CK(cudaStreamEndCapture(c->stream, &c->lgraph));
+        CK(cudaGraphInstantiate(&c->lexec, c->lgraph, 0));
+        c->graph_state = 2;
+    }
+    c->last_overlapped = false;
+    CK(cudaGraphLaunch(c->lexec, c->stream));
+}
+
+// elapsed time between two recorded events (0 if the pair has no timing)
+float event_ms(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    if(cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        ms = 0.f;
+    }
+    return ms;
+}
+
 int do_sync(bhcb_ctx *c)
 {
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaMemcpy(&c->last, c->counters.p, sizeof(RunCounters), cudaMemcpyDeviceToHost));
-    float t0 = 0, t1 = 0, t2 = 0;
-    CK(cudaEventElapsedTime(&t0, c->ev[0], c->ev[1]));
+    float t0 = event_ms(c->ev[0], c->ev[1]), t1 = 0, t2 = 0;
     float span = 0;
     if(c->mode == MODE_TL) {
-        CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
-        CK(cudaEventElapsedTime(&t2, c->ev[0], c->ev[3]));
-        if(c->last_overlapped) CK(cudaEventElapsedTime(&span, c->ev[4], c->ev[2]));
-        else span = t1;
+        t1 = event_ms(c->ev[1], c->ev[2]);
+        t2 = event_ms(c->ev[0], c->ev[3]);
+        span = c->last_overlapped ? event_ms(c->ev[4], c->ev[2]) : t1;
     } else {
         t2 = t0;
     }
@@ -787,7 +855,7 @@ void run_arrivals(bhcb_ctx *c)
     RunCounters *ctr = (RunCounters *)c->counters.p;
     unsigned long long *cursor = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
     const int grid = c->sm_count * 16;
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(record_event(c, 1, c->stream));
     // 1. count
     CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), c->stream));
     if(fp64)
@@ -850,7 +918,7 @@ void run_arrivals(bhcb_ctx *c)
         for(size_t k = 0; k < n; ++k) c->hit_begin[fld[k] + 1]++;
         for(size_t f = 0; f < c->fields.size(); ++f) c->hit_begin[f + 1] += c->hit_begin[f];
     }
-    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(record_event(c, 2, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     float t1 = 0;
     CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
@@ -913,7 +981,7 @@ int run_waves(bhcb_ctx *c)
 int run_checked(bhcb_ctx *c)
 {
     for(int attempt = 0; attempt < 8; ++attempt) {
-        do_launch(c, true);
+        launch_step(c);
         do_sync(c);
         if(c->last.err_bits & (1u << ERR_SEG_OVERFLOW)) {
             // grow the segment buffer and run again
@@ -928,6 +996,7 @@ int run_checked(bhcb_ctx *c)
             }
             c->seg_cap = std::min(maxcap, std::max(c->seg_cap * 2, (unsigned long long)(c->last.nseg * 1.25)));
             c->segs.ensure(c->seg_cap * rec);
+            drop_graph(c);   // the segment buffer moved
             continue;
         }
         if(c->last.err_bits) {
@@ -1097,7 +1166,8 @@ int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
         c->precision = init->precision == BHCB_PREC_FP64 ? BHCB_PREC_FP64 : BHCB_PREC_MIXED;
         if(init->max_memory) c->max_memory = init->max_memory;
         c->share = init->share_trajectory != 0;
-        c->overlap = (init->flags & BHCB_FLAG_SERIAL_INFLUENCE) == 0;
+        c->overlap = (init->flags & BHCB_FLAG_OVERLAP_INFLUENCE) != 0;
+        c->use_graphs = (init->flags & BHCB_FLAG_NO_GRAPH) == 0;
         c->output_cb = init->output_callback;
     }
     int ndev = 0;
@@ -1121,6 +1191,7 @@ void bhcb_close(bhcb_ctx *c)
     if(!c) return;
     cudaSetDevice(c->device);
     if(c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
     if(c->stream2) cudaStreamSynchronize(c->stream2);
     for(DevBuf *b : {&c->arena, &c->groups_d, &c->freqs_d, &c->acc, &c->out, &c->segs, &c->counters, &c->cand,
                      &c->keys0, &c->keys1, &c->vals0, &c->vals1, &c->hist, &c->narr_d, &c->arr_d, &c->hits_d,
@@ -1203,7 +1274,7 @@ int bhcb_launch(bhcb_ctx *c)
             return BHCB_OK;
         }
         if(c->mode == MODE_EIGEN) c->rays.assign(c->fields.size(), RaySet{});
-        do_launch(c, c->overlap);
+        launch_step(c);
         return BHCB_OK;
     });
 }
@@ -1566,8 +1637,10 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         if(c->mode != MODE_TL) throw StateError("the autotuner covers TL runs");
         if(c->xkind) throw StateError("the autotuner covers geometric Cartesian beams ('G', 'B')");
         const int reps = std::max(1, std::min<int>(repeats, 16));
-        const bool overlap = c->overlap;
+        const bool overlap = c->overlap, graphs = c->use_graphs;
         c->overlap = false;   // time the trace and the influence separately
+        c->use_graphs = false;   // every shape launched directly
+        drop_graph(c);
         auto timed = [&](double &tr, double &inf) {
             tr = inf = 1e300;
             for(int r = 0; r < reps; ++r) {
@@ -1603,6 +1676,8 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         }
         c->influence_ctas_per_sm = t.influence_ctas_per_sm;
         c->overlap = overlap;
+        c->use_graphs = graphs;
+        drop_graph(c);
         if(out) *out = t;
         char b[160];
         snprintf(b, sizeof b, "autotune: trace %d threads/CTA, %d KB staged (%.3f ms), influence %d CTAs/SM (%.3f ms)",
@@ -1624,6 +1699,7 @@ int bhcb_set_tuning(bhcb_ctx *c, const bhcb_tuning *t)
         c->trace_block = t->trace_block;
         c->influence_ctas_per_sm = t->influence_ctas_per_sm;
         c->stage_cap = (unsigned int)t->stage_kb * 1024u;
+        drop_graph(c);
         return BHCB_OK;
     });
 }

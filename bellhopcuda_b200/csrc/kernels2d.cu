@@ -466,7 +466,15 @@ __global__ void scale_kernel(const float2 *__restrict__ acc, float2 *__restrict_
     }
 }
 
+__global__ void set_counter_kernel(unsigned long long *p, unsigned long long v) { *p = v; }
+
 // ---------------------------------------------------------------- launchers
+cudaError_t launch_set_counter(unsigned long long *p, unsigned long long v, cudaStream_t st)
+{
+    set_counter_kernel<<<1, 1, 0, st>>>(p, v);
+    return cudaGetLastError();
+}
+
 template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroups, long long njobs,
                                               void *segs, unsigned long long cap, RunCounters *ctr,
                                               unsigned long long *job_counter, unsigned int *blk_state,

@@ -51,9 +51,9 @@ F_INFL = 40.0
 ORACLE_STEPS_PER_TRACE = 20993289
 ORACLE_EVALS_ALL_FREQS = 6440570521
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one full-size
-# influence launch (10 frequencies), from the ncu capture summarised in
-# profiles/influence_kernel_rd_gauss.md: 863.87 MB read + 343.98 MB written.
-INFLUENCE_DRAM_BYTES = 1207.85e6
+# influence launch (10 frequencies) of the current build, from the ncu capture
+# summarised in profiles/influence_kernel_rd_gauss.md (None until captured).
+INFLUENCE_DRAM_BYTES = None
 
 
 def log(*a):
@@ -159,10 +159,10 @@ def probe_fp_peak(gpu):
 
 
 # ------------------------------------------------------------- environment
-def make_env(tmp, rank):
+def make_env(tmp, rank, rays=0):
     from bellhopcuda_b200 import workloads as W
     from bellhopcuda_b200.envfile import write_env
-    spec = W.rd_gauss(seed=1002 + rank)
+    spec = W.rd_gauss(seed=1002 + rank) if not rays else W.rd_gauss(seed=1002 + rank, nalpha=rays)
     root = write_env(spec, os.path.join(tmp, "rd_gauss_%d" % rank))
     return spec, root, W.rd_gauss_freqs()
 
@@ -179,8 +179,10 @@ def tl_rms(a, b):
 
 # ------------------------------------------------------------- our arm
 def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=None):
-    """Device time per step of the prepared run (tables resident in HBM).
-    tune: None to run the autotuner first (untimed), else a shape to apply."""
+    """Device time per step of the prepared run (tables resident in HBM): each
+    step replays the CUDA graph of trace + influence + scale that the first
+    two launches set up. tune: None to run the autotuner first (untimed), else a
+    shape to apply."""
     t = B.Tracer(gpu=gpu, precision=precision)
     t.setup(root)
     t.set_frequencies(0, freqs)
@@ -332,6 +334,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--rays", type=int, default=0,
+                    help="profiling only: trace this many rays of the fan instead of 20001 (the line says so)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling only: the serial mixed run alone (no e2e, FP64 or CPU legs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -360,8 +366,20 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     fp32_peak, fp64_peak = probe_fp_peak(local)
     with tempfile.TemporaryDirectory() as tmp:
-        spec, root, freqs = make_env(tmp, rank)
+        spec, root, freqs = make_env(tmp, rank, args.rays)
         nf = len(freqs)
+        if args.profile:
+            # profiling driver: the serial mixed run only (influence after the trace)
+            shape = {"trace_block": 32, "influence_ctas_per_sm": 8, "stage_kb": 64}   # fixed: no tuning launches
+            t, times, stats, _ = time_arm(B, torch, root, freqs, B.PREC_MIXED, args.steps, args.warmup, local,
+                                          flush, tune=shape)
+            t.close()
+            print(json.dumps({"profile": "serial mixed run", "rays": spec.nalpha, "steps": args.steps,
+                              "ms_per_step": statistics.mean(times),
+                              "trace_ms": statistics.mean(x["trace_ms"] for x in stats),
+                              "influence_ms": statistics.mean(x["influence_ms"] for x in stats),
+                              "contributions": stats[-1]["evals"], "segments": stats[-1]["segments"]}))
+            return 0
         # ---- headline: mixed precision, shared trajectory
         barrier()
         with ClockSampler(local) as clk:
@@ -387,16 +405,17 @@ def main():
                     "mixed_speedup": (world * nf * 1000.0 / ms64) and value / (world * nf * 1000.0 / ms64),
                     "tl_rms_err_db_mixed_vs_fp64_max_over_freqs": max(errs),
                     "trace_ms": stats64[-1]["trace_ms"], "influence_ms": stats64[-1]["influence_ms"]}
+        # ---- the kernels' own times inside the timed steps (events in the graph)
+        kernels = {"trace_kernel_ms": statistics.mean(x["trace_ms"] for x in stats),
+                   "influence_kernel_ms": statistics.mean(x["influence_ms"] for x in stats)}
         # ---- end to end through the C ABI with host buffers
         e2e_times, h2d, d2h = time_e2e(B, torch, root, freqs, max(1, args.steps), local, tune=tuning)
         e2e_s = max_over_ranks(sum(e2e_times) / 1000.0)
         e2e = {"value": world * nf * len(e2e_times) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
-        # ---- roofline of the dominant kernel
-        # the influence overlaps the trace: its time is the span from its first
-        # launch to the last one's end (includes the part hidden under the trace)
-        infl_ms = statistics.mean(s_["influence_span_ms"] for s_ in stats)
-        trace_ms = statistics.mean(s_["trace_ms"] for s_ in stats)
+        # ---- roofline of the dominant kernel, on its own launch time
+        infl_ms = kernels["influence_kernel_ms"]
+        trace_ms = kernels["trace_kernel_ms"]
         dom = "influence_kernel" if infl_ms >= trace_ms else "trace_kernel"
         if dom == "influence_kernel":
             work = F_INFL * ORACLE_EVALS_ALL_FREQS
@@ -435,7 +454,8 @@ def main():
                                     "stage_kb": tuning["stage_kb"],
                                     "chosen_by": "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-        "gpu_launches": 3 * args.steps, "fp64_trace": fp64,
+        "gpu_launches": 3 * args.steps, "fp64_trace": fp64, "kernels": kernels,
+        "launch": "CUDA graph replay of memsets + trace + influence + scale per step",
     }
     if rank == 0:
         print(json.dumps(line))

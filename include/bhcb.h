@@ -37,13 +37,21 @@ enum {
 
 enum { BHCB_PREC_FP64 = 0, BHCB_PREC_MIXED = 1 };
 
+/* TL runs evaluate the influence after the trace in stream order (the
+   default; this flag is kept for callers that set it). bhcb_launch then only
+   enqueues work: its first launch after bhcb_prepare runs the kernels
+   directly, the second captures the step (counter set-up, trace, influence,
+   ScalePressure) into a CUDA graph, and later launches replay that graph. */
+#define BHCB_FLAG_SERIAL_INFLUENCE 1
 /* Mixed-precision TL runs overlap the influence with the trace: bhcb_run and
    bhcb_launch relaunch influence kernels on a second stream for the segment
    blocks the running trace has published, so bhcb_launch returns only once the
    trace has ended (the final influence and scale kernels are still enqueued,
-   not waited for). This flag keeps the influence after the trace in stream
-   order, for callers that need bhcb_launch not to block (e.g. stream capture). */
-#define BHCB_FLAG_SERIAL_INFLUENCE 1
+   not waited for). Not captured in a graph. On B200 the concurrent influence
+   slows the latency-bound trace, so this is off unless asked for. */
+#define BHCB_FLAG_OVERLAP_INFLUENCE 2
+/* Launch the kernels of every step directly instead of replaying a CUDA graph. */
+#define BHCB_FLAG_NO_GRAPH 4
 
 /* Context options; mirrors bhcInit (include/bhc/structs.hpp:490-546). */
 typedef struct bhcb_init {

@@ -9,7 +9,7 @@ oracle run over the whole ray fan on the host's threads:
   beam-receiver contributions.
 * C2 — range-dependent Gaussian beams, 20001 rays, 501 x 2001 receivers, 10
   frequencies sharing one trajectory, run as the benchmark runs it (prepare,
-  autotune, host-driven launch with the influence overlapped on the trace);
+  autotune, launch: trace, influence and scale, replayed from a CUDA graph);
   the 50 Hz and 500 Hz fields against the oracle, and the FP64 trace's step
   count equal to the oracle's.
 * C3 — the 256-environment batch in one run; the first four seeded
@@ -88,8 +88,9 @@ def test_c2_full_bench_sequence(workdir):
         t.set_frequencies(0, freqs)
         t.prepare()
         t.autotune(repeats=1)
-        t.launch()
-        t.sync()
+        for _ in range(3):   # direct, captured, replayed
+            t.launch()
+            t.sync()
         st = t.stats()
         fields = {i: t.field(0, i)[0] for i in (0, len(freqs) - 1)}
     assert st["err_bits"] == 0

@@ -45,3 +45,36 @@ def test_graph_replays_match_regular_run(precision, tmp_path):
                 got = out.cpu().numpy()
                 rms, n = tl_rms(got[0], ref[0])
                 assert n > 100 and rms < 0.05, (k, rms)
+
+
+@pytest.mark.parametrize("precision", [B.PREC_MIXED, B.PREC_FP64])
+def test_batched_step_graph_replays(precision, tmp_path):
+    """bhcb_launch on a prepared batch: the first launch runs the kernels
+    directly, the second captures the step (several environments, several
+    frequencies sharing one trajectory) into a CUDA graph, later launches replay
+    it. Every launch gives the fields of a run without graphs."""
+    envs = [W.rd_gauss(nalpha=401, nrz=61, nrr=201, nbty=40), W.munk_tl(nalpha=301, nrz=51, nrr=151, beam="B")]
+    freqs = [[50.0, 158.1, 500.0], [50.0, 200.0]]
+    roots = [write_env(s, os.path.join(str(tmp_path), "b%d" % i)) for i, s in enumerate(envs)]
+
+    def setup(t):
+        for i, r in enumerate(roots):
+            t.add_env(r)
+            t.set_frequencies(i, freqs[i])
+
+    with B.Tracer(precision=precision, graphs=False) as t:
+        setup(t)
+        t.run()
+        ref = [[t.field(i, k) for k in range(len(freqs[i]))] for i in range(len(roots))]
+    with B.Tracer(precision=precision) as t:
+        setup(t)
+        t.prepare()
+        for step in range(4):
+            t.launch()
+            t.sync()
+            st = t.stats()
+            assert st["err_bits"] == 0 and st["evals"] > 0
+            for i in range(len(roots)):
+                for k in range(len(freqs[i])):
+                    rms, n = tl_rms(t.field(i, k)[0], ref[i][k][0])
+                    assert n > 100 and rms < 0.01, (step, i, k, rms)
