@@ -46,7 +46,7 @@ class BhcbError(RuntimeError):
 
 class Tuning(C.Structure):
     _fields_ = [("trace_block", C.c_int32), ("influence_ctas_per_sm", C.c_int32), ("stage_kb", C.c_int32),
-                ("trace_ms", C.c_double), ("influence_ms", C.c_double)]
+                ("trace_ms", C.c_double), ("influence_ms", C.c_double), ("trace_lanes", C.c_int32)]
 
 
 class Init(C.Structure):
@@ -390,10 +390,11 @@ class Tracer:
         t = Tuning()
         self._check(self._lib.bhcb_autotune(self._h, repeats, C.byref(t)))
         return {"trace_block": t.trace_block, "influence_ctas_per_sm": t.influence_ctas_per_sm,
-                "stage_kb": t.stage_kb, "trace_ms": t.trace_ms, "influence_ms": t.influence_ms}
+                "stage_kb": t.stage_kb, "trace_ms": t.trace_ms, "influence_ms": t.influence_ms,
+                "trace_lanes": t.trace_lanes}
 
-    def set_tuning(self, trace_block: int, influence_ctas_per_sm: int, stage_kb: int = 32):
-        t = Tuning(trace_block, influence_ctas_per_sm, stage_kb, 0.0, 0.0)
+    def set_tuning(self, trace_block: int, influence_ctas_per_sm: int, stage_kb: int = 32, trace_lanes: int = 32):
+        t = Tuning(trace_block, influence_ctas_per_sm, stage_kb, 0.0, 0.0, trace_lanes)
         self._check(self._lib.bhcb_set_tuning(self._h, C.byref(t)))
 
     def stream_ptr(self) -> int:

@@ -26,7 +26,7 @@ namespace bhcb {
 template<typename R> cudaError_t launch_trace(const GroupDev *, int, long long, void *,
                                               unsigned long long, RunCounters *,
                                               unsigned long long *, unsigned int *, int, int, cudaStream_t,
-                                              unsigned int);
+                                              unsigned int, int);
 cudaError_t launch_influence_mixed(const void *, unsigned long long, const GroupDev *, int, const double *,
                                    float2 *, RunCounters *, bool, bool, int, cudaStream_t, unsigned int *,
                                    unsigned long long *);
@@ -143,6 +143,7 @@ struct bhcb_ctx {
     // launch shapes (bhcb_autotune picks them by timing the prepared workload)
     int trace_block = 32;           // threads per trace CTA (one ray each)
     int influence_ctas_per_sm = 8;  // persistent influence CTAs per SM
+    int trace_lanes = 32;           // rays per trace warp
 
     std::vector<EnvSlot> envs;
     bool prepared = false;
@@ -537,7 +538,9 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         size_t off[ST_COUNT];
         stage_bytes = std::max<unsigned int>(stage_bytes, (unsigned int)stage_plan(c->envdev_h[g], c->stage_cap, off));
     }
-    long long tgrid = std::min<long long>((job1 - job0 + tblock - 1) / tblock, (long long)c->sm_count * 16);
+    // rays per CTA: trace_lanes of each warp's 32 lanes take rays
+    const long long rays_per_cta = std::max(1, tblock * c->trace_lanes / 32);
+    long long tgrid = std::min<long long>((job1 - job0 + rays_per_cta - 1) / rays_per_cta, (long long)c->sm_count * 32);
     if(tgrid < 1) tgrid = 1;
     const GroupDev *G = (const GroupDev *)c->groups_d.p + g0;
     int ng = g1 - g0;
@@ -557,10 +560,10 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
     }
     if(fp64)
         CK(launch_trace<double>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
-                                c->stream, stage_bytes));
+                                c->stream, stage_bytes, c->trace_lanes));
     else
         CK(launch_trace<float>(G, ng, job1, c->segs.p, c->seg_cap, ctr, jobc, blk, (int)tgrid, tblock,
-                               c->stream, stage_bytes));
+                               c->stream, stage_bytes, c->trace_lanes));
     CK(record_event(c, 1, c->stream));
     if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
     if(ovl) {
@@ -1662,6 +1665,13 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
             if(tr < t.trace_ms) { t.trace_ms = tr; t.trace_block = tb; }
         }
         c->trace_block = t.trace_block;
+        t.trace_lanes = c->trace_lanes;
+        for(int ln : {16, 32}) {   // rays per trace warp: 16 diverge less, if the warps fit
+            c->trace_lanes = ln;
+            timed(tr, inf);
+            if(tr < t.trace_ms) { t.trace_ms = tr; t.trace_lanes = ln; }
+        }
+        c->trace_lanes = t.trace_lanes;
         t.stage_kb = (int32_t)(c->stage_cap / 1024);
         for(int kb : {0, 32, 64}) {   // shared-memory table staging
             c->stage_cap = (unsigned int)kb * 1024u;
@@ -1680,8 +1690,9 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         drop_graph(c);
         if(out) *out = t;
         char b[160];
-        snprintf(b, sizeof b, "autotune: trace %d threads/CTA, %d KB staged (%.3f ms), influence %d CTAs/SM (%.3f ms)",
-                 t.trace_block, t.stage_kb, t.trace_ms, t.influence_ctas_per_sm, t.influence_ms);
+        snprintf(b, sizeof b, "autotune: trace %d threads/CTA, %d rays/warp, %d KB staged (%.3f ms), influence %d CTAs/SM "
+                 "(%.3f ms)", t.trace_block, t.trace_lanes, t.stage_kb, t.trace_ms, t.influence_ctas_per_sm,
+                 t.influence_ms);
         c->msg(b);
         return BHCB_OK;
     });
@@ -1696,9 +1707,12 @@ int bhcb_set_tuning(bhcb_ctx *c, const bhcb_tuning *t)
             throw std::invalid_argument("influence_ctas_per_sm must be in 1..64");
         if(t->stage_kb < 0 || t->stage_kb > (int32_t)(STAGE_MAX_BYTES / 1024))
             throw std::invalid_argument("stage_kb must be in 0..64");
+        if(t->trace_lanes != 0 && t->trace_lanes != 16 && t->trace_lanes != 32)
+            throw std::invalid_argument("trace_lanes must be 16 or 32 (0: 32)");
         c->trace_block = t->trace_block;
         c->influence_ctas_per_sm = t->influence_ctas_per_sm;
         c->stage_cap = (unsigned int)t->stage_kb * 1024u;
+        c->trace_lanes = t->trace_lanes ? t->trace_lanes : 32;
         drop_graph(c);
         return BHCB_OK;
     });

@@ -28,10 +28,11 @@
 namespace bhcb {
 
 // R: ray state; RecR: segment record (float for the mixed kernel's FP32 influence).
+// lanes: rays per warp (16 or 32); the other lanes only help stage the tables.
 template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_kernel(
     const GroupDev *__restrict__ groups, int ngroups, long long njobs, SegRec<RecR> *segs,
     unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, unsigned int *blk_state,
-    unsigned int stage_budget)
+    unsigned int stage_budget, int lanes)
 {
     // tables of the group this CTA's first rays belong to, staged in shared memory
     extern __shared__ __align__(16) unsigned char s_tab[];
@@ -41,6 +42,8 @@ template<typename R, typename RecR> __global__ void __launch_bounds__(64) trace_
     const int gs = find_group(groups, ngroups, hint);
     const bool staged = stage_budget > 0 && stage_env_tables(groups[gs].env, s_env, s_tab, stage_budget, &s_bar, ctr);
     for(;;) {
+        // a warp with fewer rays takes fewer divergent paths per step
+        if((int)(threadIdx.x & 31) >= lanes) break;
         long long job = (long long)atomicAdd(job_counter, 1ull);
         if(job >= njobs) break;
         const int gi = find_group(groups, ngroups, job);
@@ -478,7 +481,8 @@ cudaError_t launch_set_counter(unsigned long long *p, unsigned long long v, cuda
 template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroups, long long njobs,
                                               void *segs, unsigned long long cap, RunCounters *ctr,
                                               unsigned long long *job_counter, unsigned int *blk_state,
-                                              int grid, int block, cudaStream_t st, unsigned int stage_bytes)
+                                              int grid, int block, cudaStream_t st, unsigned int stage_bytes,
+                                              int lanes)
 {
     // the ray state is FP64 in both precisions (the mixed precision writes FP32
     // segment records for its FP32 influence kernel): the trajectory, and with it
@@ -492,7 +496,7 @@ template<typename R> cudaError_t launch_trace(const GroupDev *groups, int ngroup
     }
     if(stage_bytes > STAGE_MAX_BYTES) stage_bytes = STAGE_MAX_BYTES;
     trace_kernel<double, R><<<grid, block, stage_bytes, st>>>(groups, ngroups, njobs, (SegRec<R> *)segs, cap, ctr,
-                                                              job_counter, blk_state, stage_bytes);
+                                                              job_counter, blk_state, stage_bytes, lanes);
     return cudaGetLastError();
 }
 
@@ -535,10 +539,10 @@ cudaError_t launch_scale(const float2 *acc, float2 *out, const GroupDev *groups,
 
 template cudaError_t launch_trace<float>(const GroupDev *, int, long long, void *, unsigned long long,
                                          RunCounters *, unsigned long long *, unsigned int *, int, int,
-                                         cudaStream_t, unsigned int);
+                                         cudaStream_t, unsigned int, int);
 template cudaError_t launch_trace<double>(const GroupDev *, int, long long, void *, unsigned long long,
                                           RunCounters *, unsigned long long *, unsigned int *, int, int,
-                                          cudaStream_t, unsigned int);
+                                          cudaStream_t, unsigned int, int);
 template cudaError_t launch_influence<float>(const void *, unsigned long long, const GroupDev *, int,
                                              const double *, float2 *, RunCounters *, bool, bool, int,
                                              cudaStream_t);

@@ -190,7 +190,7 @@ def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=N
     if tune is None:
         t.tuning = t.autotune(repeats=1)
     else:
-        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"])
+        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"], tune.get("trace_lanes", 32))
         t.tuning = tune
     s = torch.cuda.ExternalStream(t.stream_ptr(), device=gpu)
     for _ in range(warmup):
@@ -218,7 +218,7 @@ def time_e2e(B, torch, root, freqs, steps, gpu, tune=None):
     pinned host memory, all inside the timed window."""
     t = B.Tracer(gpu=gpu, precision=B.PREC_MIXED)
     if tune is not None:
-        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"])
+        t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"], tune.get("trace_lanes", 32))
     nf = len(freqs)
     t.setup(root)
     t.set_frequencies(0, freqs)
@@ -452,6 +452,7 @@ def main():
                    "launch_shape": {"trace_block": tuning["trace_block"],
                                     "influence_ctas_per_sm": tuning["influence_ctas_per_sm"],
                                     "stage_kb": tuning["stage_kb"],
+                                    "trace_lanes": tuning.get("trace_lanes", 32),
                                     "chosen_by": "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 3 * args.steps, "fp64_trace": fp64, "kernels": kernels,

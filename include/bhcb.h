@@ -296,6 +296,7 @@ typedef struct bhcb_tuning {
     int32_t influence_ctas_per_sm;  /* persistent influence CTAs per SM */
     int32_t stage_kb;               /* shared memory (KB, 0..64) a trace CTA stages environment tables into */
     double trace_ms, influence_ms;  /* best times measured with the chosen shape */
+    int32_t trace_lanes;            /* rays per trace warp (16 or 32; 0 = 32): fewer rays diverge less per step */
 } bhcb_tuning;
 int bhcb_autotune(bhcb_ctx *ctx, int32_t repeats, bhcb_tuning *out);
 int bhcb_set_tuning(bhcb_ctx *ctx, const bhcb_tuning *tuning);
