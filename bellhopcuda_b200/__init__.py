@@ -70,6 +70,30 @@ class EnvInfo(C.Structure):
                 ("beam_type", C.c_char * 8)]
 
 
+_PD = C.POINTER(C.c_double)
+_PF = C.POINTER(C.c_float)
+
+
+class EnvDesc(C.Structure):
+    """bhcb_env_desc: a 2-D environment in memory (the values bhcParams<false>
+    holds after bhc::setup, include/bhc/bhc.hpp:58-452)."""
+    _fields_ = [("title", C.c_char_p), ("freq0", C.c_double), ("top_opt", C.c_char * 6),
+                ("bot_opt", C.c_char * 6), ("fg", C.c_double * 4), ("nbio", C.c_int32), ("bio", _PD),
+                ("top_hs", C.c_double * 7), ("bot_hs", C.c_double * 7), ("nssp", C.c_int32),
+                ("ssp_z", _PD), ("ssp_alphaR", _PD), ("ssp_betaR", _PD), ("ssp_rho", _PD),
+                ("ssp_alphaI", _PD), ("ssp_betaI", _PD), ("bot_depth", C.c_double),
+                ("ati_type", C.c_char * 2), ("bty_type", C.c_char * 2), ("nati", C.c_int32),
+                ("nbty", C.c_int32), ("ati_r_km", _PD), ("ati_z", _PD), ("ati_geo", _PD),
+                ("bty_r_km", _PD), ("bty_z", _PD), ("bty_geo", _PD), ("nsbp", C.c_int32), ("sbp", _PD),
+                ("nsz", C.c_int32), ("nrz", C.c_int32), ("nrr", C.c_int32), ("nalpha", C.c_int32),
+                ("isingle", C.c_int32), ("sz", _PF), ("rz", _PF), ("rr_km", _PD), ("alpha_deg", _PD),
+                ("run_type", C.c_char * 7), ("cerv_type", C.c_char * 2), ("deltas", C.c_double),
+                ("box_z", C.c_double), ("box_r_km", C.c_double), ("eps_mult", C.c_double),
+                ("rloop", C.c_double), ("nimage", C.c_int32), ("ibeam_window", C.c_int32),
+                ("component", C.c_char), ("nquad_r", C.c_int32), ("quad_r_km", _PD), ("quad_c", _PD),
+                ("nbrc", C.c_int32), ("ntrc", C.c_int32), ("brc", _PD), ("trc", _PD)]
+
+
 # bhcb_arrival / bhcb_eigen_hit (the reference's Arrival and EigenHit records)
 ARRIVAL_DTYPE = np.dtype([("NTopBnc", "<i4"), ("NBotBnc", "<i4"), ("SrcDeclAngle", "<f4"),
                           ("SrcAzimAngle", "<f4"), ("RcvrDeclAngle", "<f4"), ("RcvrAzimAngle", "<f4"),
@@ -141,6 +165,10 @@ SIGNATURES = [
     ("bhcb_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),
     ("bhcb_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("bhcb_version", C.c_char_p, []),
+    ("bhcb_add_env_desc", C.c_int, [C.c_void_p, C.POINTER(EnvDesc), C.POINTER(C.c_int32)]),
+    ("bhcb_read_env_desc", C.c_int, [C.c_char_p, C.POINTER(C.POINTER(EnvDesc)), C.c_char_p, C.c_size_t]),
+    ("bhcb_free_env_desc", None, [C.POINTER(EnvDesc)]),
+    ("bhcb_ssp_at", C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_double)]),
 ]
 
 
@@ -158,6 +186,40 @@ def load_library():
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+class EnvDescription:
+    """An environment read into memory by the library (bhcb_read_env_desc):
+    `desc` is the EnvDesc, editable in place (scalars; the arrays stay the
+    library's); released with close() or on garbage collection."""
+
+    def __init__(self, file_root: str):
+        lib = load_library()
+        p = C.POINTER(EnvDesc)()
+        msg = C.create_string_buffer(512)
+        rc = lib.bhcb_read_env_desc(file_root.encode(), C.byref(p), msg, 512)
+        if rc != 0:
+            raise BhcbError(rc, msg.value.decode(errors="replace"))
+        self._p = p
+        self.desc = p.contents
+
+    def close(self):
+        if self._p:
+            load_library().bhcb_free_env_desc(self._p)
+            self._p = None
+            self.desc = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def check_env(file_root: str) -> dict:
@@ -236,6 +298,19 @@ class Tracer:
         idx = C.c_int32()
         self._check(self._lib.bhcb_add_env(self._h, file_root.encode(), C.byref(idx)))
         return idx.value
+
+    def add_env_desc(self, desc) -> int:
+        """Append an in-memory environment (an EnvDesc, or an EnvDescription)."""
+        d = desc.desc if isinstance(desc, EnvDescription) else desc
+        idx = C.c_int32()
+        self._check(self._lib.bhcb_add_env_desc(self._h, C.byref(d), C.byref(idx)))
+        return idx.value
+
+    def ssp_at(self, env: int, r: float, z: float) -> float:
+        """Sound speed (m/s) of environment env at range r and depth z (m)."""
+        c = C.c_double()
+        self._check(self._lib.bhcb_ssp_at(self._h, env, float(r), float(z), C.byref(c)))
+        return c.value
 
     def clear(self):
         self._check(self._lib.bhcb_clear(self._h))

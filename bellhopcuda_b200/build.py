@@ -19,7 +19,7 @@ BUILD = os.path.join(ROOT, "_build")
 
 CU_SOURCES = ["kernels2d.cu", "influence_mixed.cu", "arrivals.cu", "kernels3d.cu", "api.cu", "api3d.cu",
               "noalloc.cu", "nn_gemm.cu", "nn_ops.cu", "influence_x.cu", "influence3d_x.cu", "nx2d.cu"]
-CPP_SOURCES = ["host/ldi.cpp", "host/env2d.cpp"]
+CPP_SOURCES = ["host/ldi.cpp", "host/env2d.cpp", "host/envdesc.cpp", "host/bhc_cxx.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # FP64 ray tracers (2-D, 3-D, Nx2D, the ray-centred / Cerveny / SGB prologues,
 # the allocation-free fused kernel) and the FP64 influence / arrival gathers:

@@ -1235,6 +1235,55 @@ int bhcb_add_env(bhcb_ctx *c, const char *root, int32_t *idx)
     });
 }
 
+int bhcb_add_env_desc(bhcb_ctx *c, const bhcb_env_desc *desc, int32_t *idx)
+{
+    return guarded(c, [&]() -> int {
+        if(!desc) throw std::invalid_argument("environment descriptor is NULL");
+        if(c->is3d()) throw StateError("the context holds 3-D environments: bhcb_clear first");
+        EnvSlot S;
+        S.root = "";
+        S.in = env_from_desc(*desc);
+        S.freqs = {S.in.freq0};
+        preprocess(S.in, S.in.freq0);   // validate now, like bhc::setup's Validate pass
+        c->envs.push_back(std::move(S));
+        c->prepared = false;
+        if(idx) *idx = (int32_t)c->envs.size() - 1;
+        return BHCB_OK;
+    });
+}
+
+int bhcb_read_env_desc(const char *root, bhcb_env_desc **desc, char *msg, size_t n)
+{
+    if(msg && n) msg[0] = 0;
+    if(!root || !desc) return BHCB_ERR_ARG;
+    *desc = nullptr;
+    try {
+        EnvInput in = read_env_files(root);
+        preprocess(in, in.freq0);   // the same validation as bhcb_add_env
+        *desc = desc_from_env(in);
+        return BHCB_OK;
+    } catch(const std::exception &e) {
+        if(msg && n) snprintf(msg, n, "%s", e.what());
+        return BHCB_ERR_INPUT;
+    }
+}
+
+void bhcb_free_env_desc(bhcb_env_desc *desc)
+{
+    if(desc) free_desc(desc);
+}
+
+int bhcb_ssp_at(bhcb_ctx *c, int32_t env, double r, double z, double *cout)
+{
+    return guarded(c, [&]() -> int {
+        if(!cout) throw std::invalid_argument("output pointer is NULL");
+        if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
+        const EnvSlot &S = c->envs[env];
+        *cout = ssp_at(preprocess(S.in, S.in.freq0), r, z);
+        return BHCB_OK;
+    });
+}
+
 int bhcb_setup(bhcb_ctx *c, const char *root)
 {
     int r = bhcb_clear(c);

@@ -31,17 +31,6 @@ template<typename T> void read_vector(LdiReader &f, int32_t &n, std::vector<T> &
     for(int i = 0; i < n; ++i) f.read(x[i]);
 }
 
-// SubTab (src/common_setup.hpp:306-334): FMA sub-tabulation
-template<typename T> void subtab(std::vector<T> &x, int n)
-{
-    const T m999 = (T)(sizeof(T) == 4 ? -999.9f : -999.9);
-    const T p01 = (T)(sizeof(T) == 4 ? 0.01f : 0.01);
-    if(n >= 3 && std::fabs(x[2] - m999) < p01) {
-        if(std::fabs(x[1] - m999) < p01) x[1] = x[0];
-        T dx = (x[1] - x[0]) / (T)(n - 1), x0 = x[0];
-        for(int i = 0; i < n; ++i) x[i] = std::fma((T)i, dx, x0);
-    }
-}
 
 void read_bdry_file(const std::string &path, BdryIn &b)
 {

@@ -8,6 +8,7 @@
 // the modules' Validate/Preprocess steps (src/module/*.hpp) for one frequency.
 #pragma once
 #include <array>
+#include <cmath>
 #include <complex>
 #include <cstdint>
 #include <string>
@@ -127,8 +128,32 @@ struct Env3Tables {
     std::vector<std::string> warnings;
 };
 
+// SubTab (src/common_setup.hpp:306-334): FMA sub-tabulation of a vector read
+// as (first, last, -999.9 marker)
+template<typename T> void subtab(std::vector<T> &x, int n)
+{
+    const T m999 = (T)(sizeof(T) == 4 ? -999.9f : -999.9);
+    const T p01 = (T)(sizeof(T) == 4 ? 0.01f : 0.01);
+    if(n >= 3 && x.size() >= 3 && std::fabs(x[2] - m999) < p01) {
+        if(std::fabs(x[1] - m999) < p01) x[1] = x[0];
+        T dx = (x[1] - x[0]) / (T)(n - 1), x0 = x[0];
+        if((int)x.size() < n) x.resize(n);
+        for(int i = 0; i < n; ++i) x[i] = std::fma((T)i, dx, x0);
+    }
+}
+
 EnvInput read_env_files(const std::string &fileroot, bool o3d = false);
 EnvTables preprocess(const EnvInput &in, double freq);
 Env3Tables preprocess3d(const EnvInput &in, double freq);
+
+} // namespace bhcb
+
+struct bhcb_env_desc;
+namespace bhcb {
+// in-memory 2-D environments of the C ABI (envdesc.cpp)
+EnvInput env_from_desc(const bhcb_env_desc &d);
+bhcb_env_desc *desc_from_env(const EnvInput &in);   // owns its arrays; free_desc releases it
+void free_desc(bhcb_env_desc *d);
+double ssp_at(const EnvTables &T, double r, double z);   // sound speed (m/s) at range r, depth z (m)
 
 } // namespace bhcb

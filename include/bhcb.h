@@ -90,6 +90,58 @@ int bhcb_setup(bhcb_ctx *ctx, const char *file_root);
 int bhcb_add_env(bhcb_ctx *ctx, const char *file_root, int32_t *env_index);
 int bhcb_clear(bhcb_ctx *ctx);
 
+/* In-memory 2-D environment (the values bhcParams<false> holds after
+   bhc::setup and the extsetup_* calls, include/bhc/bhc.hpp:58-452; the .env
+   grammar's values, src/api.cpp:253-277). Vectors are complete (not
+   sub-tabulated): nsz source depths (m), nrz receiver depths (m), nrr ranges
+   (km), nalpha launch angles (degrees; nalpha 0 = estimated as
+   EstimateNumAngles does, src/module/rayangles.hpp:212-238, over -20..20). An
+   altimetry / bathymetry with 0 points is flat. All arrays are read during
+   the call only. */
+typedef struct bhcb_env_desc {
+    const char *title;
+    double freq0;
+    char top_opt[6], bot_opt[6];        /* TopOpt, BotOpt (SSP type, bc, atten units, ...) */
+    double fg[4];                       /* Francois-Garrison T, S, pH, z_bar (TopOpt[3] 'F') */
+    int32_t nbio;                       /* biological layers (TopOpt[3] 'B'): 5 doubles each */
+    const double *bio;                  /* z1 z2 f0 q a0 */
+    double top_hs[7], bot_hs[7];        /* halfspaces: zTemp alphaR betaR rho alphaI betaI Mz */
+    int32_t nssp;                       /* SSP nodes */
+    const double *ssp_z, *ssp_alphaR, *ssp_betaR, *ssp_rho, *ssp_alphaI, *ssp_betaI;
+    double bot_depth;                   /* depth of the bottom (m) */
+    char ati_type[2], bty_type[2];      /* boundary file types ('L' / 'C', 'S' / 'L') */
+    int32_t nati, nbty;                 /* points; 0 = flat boundary */
+    const double *ati_r_km, *ati_z, *ati_geo;   /* geo: 5 per point (long format), may be NULL */
+    const double *bty_r_km, *bty_z, *bty_geo;
+    int32_t nsbp;                       /* source beam pattern points (0 = omnidirectional) */
+    const double *sbp;                  /* (angle deg, level dB) pairs */
+    int32_t nsz, nrz, nrr, nalpha, isingle;
+    const float *sz, *rz;
+    const double *rr_km, *alpha_deg;
+    char run_type[7];                   /* Beam->RunType */
+    char cerv_type[2];                  /* Cerveny beam width / curvature options (Beam->Type[1..2]) */
+    double deltas, box_z, box_r_km;     /* step (m, 0 = automatic), beam box */
+    double eps_mult, rloop;             /* Cerveny epsilon multiplier and rLoop */
+    int32_t nimage, ibeam_window;
+    char component;
+    int32_t nquad_r;                    /* quad SSP ('Q'): ranges (km) and c[iz * nquad_r + ir] */
+    const double *quad_r_km, *quad_c;
+    int32_t nbrc, ntrc;                 /* reflection tables ('F'): (theta deg, |R|, phase deg) triples */
+    const double *brc, *trc;
+} bhcb_env_desc;
+/* bhc::setup from parameters in memory (the extsetup_* route): append the
+   environment described by desc, like bhcb_add_env does for a file. */
+int bhcb_add_env_desc(bhcb_ctx *ctx, const bhcb_env_desc *desc, int32_t *env_index);
+/* Read FileRoot.env (+ side files) as a 2-D environment into a descriptor the
+   library allocates (arrays included); release it with bhcb_free_env_desc.
+   Needs no GPU. msg (may be NULL) receives the reason of a failure. */
+int bhcb_read_env_desc(const char *file_root, bhcb_env_desc **desc, char *msg, size_t n);
+void bhcb_free_env_desc(bhcb_env_desc *desc);
+/* bhc::get_ssp (include/bhc/bhc.hpp:440-452): sound speed (m/s) of
+   environment env_index at range r (m) and depth z (m), interpolated as the
+   tracer does (SSP types N, C, S, P, Q). Needs no GPU. */
+int bhcb_ssp_at(bhcb_ctx *ctx, int32_t env_index, double r, double z, double *c);
+
 /* Multi-frequency extension (no reference counterpart: the reference traces
    one freq0 per bhc::run, include/bhc/bhc.hpp:174-179): evaluate env_index at
    the nfreq given frequencies instead of its file frequency. */

@@ -16,6 +16,7 @@ import bellhopcuda_b200 as B  # noqa: E402
 import oracle_ctypes  # noqa: E402
 from cases import CASES  # noqa: E402
 from bellhopcuda_b200.envfile import EnvSpec, write_env  # noqa: E402
+from bellhopcuda_b200 import workloads as W  # noqa: E402
 
 
 def header_functions():
@@ -256,3 +257,19 @@ def test_reader3d_accepts_reference_inputs(name, workdir):
         assert info["nrays"] > 0
     except B.BhcbError as e:
         assert "not supported" in str(e), str(e)
+
+
+def test_env_desc_reads_file(workdir):
+    """bhcb_read_env_desc gives the file's values (ranges in km, angles in degrees)."""
+    spec = W.munk_tl(nalpha=301, nrz=51, nrr=201)
+    root = write_env(spec, os.path.join(workdir, "desc_munk"))
+    with B.EnvDescription(root) as e:
+        d = e.desc
+        assert d.nsz == 1 and d.nrz == 51 and d.nrr == 201 and d.nalpha == 301
+        assert abs(d.rr_km[200] - spec.rr_km[1]) < 1e-9
+        assert d.alpha_deg[0] == spec.alpha[0] and d.alpha_deg[300] == spec.alpha[1]
+        assert d.nssp == len(spec.ssp_z)
+        assert d.run_type[:2] == spec.run_type[:2].encode()
+        assert abs(d.freq0 - spec.freq) < 1e-12
+    with pytest.raises(B.BhcbError):
+        B.EnvDescription(os.path.join(workdir, "no_such_env"))
