@@ -288,14 +288,19 @@ def cpu_baseline(spec, freqs, tmp):
 def run_reference_arm(args, rank, world):
     """The reference's CPU implementation on the same workload: each step is
     one whole TL field (the full 20001-ray fan over the 501 x 2001 grid) at
-    one of the ten frequencies, the frequencies taken in turn, so K steps
-    cover the ten fields K / 10 times. Measured, not extrapolated."""
+    one of the ten frequencies. The reference's time per field falls with
+    frequency (wider beams at low frequency), so the frequencies are taken
+    lowest, highest, second lowest, second highest, ...: every even number of
+    steps pairs slow and fast fields, and ten steps cover all ten. Measured,
+    not extrapolated."""
     if rank != 0:
         return 0
     from bellhopcuda_b200 import workloads as W
     with tempfile.TemporaryDirectory() as tmp:
         spec = W.rd_gauss()
-        freqs = W.rd_gauss_freqs()
+        ladder = W.rd_gauss_freqs()
+        n = len(ladder)
+        freqs = [ladder[(k // 2) if k % 2 == 0 else n - 1 - k // 2] for k in range(n)]
         try:
             for i in range(max(args.warmup, 0)):
                 reference_field(spec, freqs[i % len(freqs)], tmp, "w%d" % i)
