@@ -60,9 +60,18 @@ template<typename R, typename RecR> __device__ __forceinline__ bool infl_prologu
 {
     double rA = inf.x.x, rB = p1.x.x;
     V2<double> d = sub2(p1.x, p0.x);
-    double rlen = sqrt(dot2(d, d));
-    if(rlen < 1.0e3 * spacing_d(p1.x.x)) return false;   // IsSmallValue: duplicate point
-    V2<double> rayt = div2(d, rlen);
+    // IsSmallValue(rlen): duplicate point. rlen = |d| is needed only by
+    // segments that reach a receiver column; when |d|^2 exceeds four times the
+    // squared threshold, rlen is above the threshold whatever the rounding,
+    // and the square root waits until the segment is stored.
+    const double dd = dot2(d, d);
+    const double small_len = 1.0e3 * spacing_d(p1.x.x);
+    double rlen = 0.0;
+    const bool long_seg = dd > 4.0 * small_len * small_len;
+    if(!long_seg) {
+        rlen = sqrt(dd);
+        if(rlen < small_len) return false;
+    }
     double phaseq = (double)p0.q.x;
     if((phaseq <= 0.0 && inf.qOld > 0.0) || (phaseq >= 0.0 && inf.qOld < 0.0))
         inf.phase += BHCB_PI / FLTD(2.0);
@@ -93,6 +102,8 @@ template<typename R, typename RecR> __device__ __forceinline__ bool infl_prologu
     inf.ir = ir;
     inf.x = p1.x;
     if(first < 0) return false;
+    if(long_seg) rlen = sqrt(dd);
+    const V2<double> rayt = div2(d, rlen);
     rec.x0r = p0.x.x;
     rec.x0z = p0.x.y;
     rec.tau0r = p0.taur;

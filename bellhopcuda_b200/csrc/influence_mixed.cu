@@ -5,8 +5,11 @@
 // beams, src/influence.hpp:423-473,897-1024) and reduces them into the
 // range-major accumulator acc[field][isz][ir][iz].
 //
-// Work layout. Each warp takes 32 segments from a dynamic queue (heaviest
-// first). For each frequency of the segments' trace group:
+// Work layout. Each warp takes work items from a dynamic queue, heaviest
+// first: an item is 32 segments (one chunk of one ray) at one frequency of
+// their trace group (beside a running trace, a whole published chunk with all
+// its frequencies), so that the heaviest chunk's frequencies spread over
+// several warps instead of one warp ending the launch alone. For the item:
 // Beside a running trace (blk_state set), a launch takes only the chunks the
 // tracer has published and exits when the rest are not ready; the host
 // relaunches it until the trace ends (no kernel waits for another).
@@ -263,15 +266,26 @@ influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long lon
     __shared__ SegFreqM s_p[MW][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned long long nchunks = (nseg + 31) / 32;
+    // frequencies per chunk: items are (chunk, frequency) pairs, except beside
+    // a running trace, where an item is a whole published chunk
+    int fsplit = 0;
+    if(!blk_state) {
+        for(int g = lane; g < ngroups; g += 32) fsplit = max(fsplit, groups[g].nfreq);
+        for(int o = 16; o > 0; o >>= 1) fsplit = max(fsplit, __shfl_xor_sync(0xffffffffu, fsplit, o));
+        fsplit = max(fsplit, 1);
+    }
+    const unsigned long long nitems = fsplit ? nchunks * (unsigned long long)fsplit : nchunks;
     unsigned int evals = 0;
     for(;;) {
-        unsigned long long ch = 0;
-        if(lane == 0) ch = atomicAdd(queue, 1ull);
-        ch = __shfl_sync(0xffffffffu, ch, 0);
-        if(ch >= nchunks) break;
+        unsigned long long it = 0;
+        if(lane == 0) it = atomicAdd(queue, 1ull);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if(it >= nitems) break;
         // segments are stored in trace order, so the last chunks hold the
         // far-range segments with the widest beams: take the heaviest first
-        ch = nchunks - 1 - ch;
+        it = nitems - 1 - it;
+        const unsigned long long ch = fsplit ? it / (unsigned long long)fsplit : it;
+        const int fsel = fsplit ? (int)(it - ch * (unsigned long long)fsplit) : -1;
         if(blk_state) {
             // running beside the trace: take a chunk (a 32-slot block of one
             // ray) only once the tracer has published it; skipped blocks are
@@ -301,7 +315,8 @@ influence_kernel_mixed(const SegRec<float> *__restrict__ segs, unsigned long lon
         }
         int maxf = nfreq;
         for(int o = 16; o > 0; o >>= 1) maxf = max(maxf, __shfl_xor_sync(0xffffffffu, maxf, o));
-        for(int f = 0; f < maxf; ++f) {
+        const int f0 = fsel >= 0 ? fsel : 0, f1 = fsel >= 0 ? min(fsel + 1, maxf) : maxf;
+        for(int f = f0; f < f1; ++f) {
             int cnt = 0;
             SegFreqM &mine = s_p[w][lane];
             if(valid && f < nfreq) {

@@ -62,6 +62,7 @@ template<typename R> struct RayState2 {
     BdState top, bot;
     HsDev htop, hbot;
     SegState iSeg;
+    SspSegCache sc;
     double dBegTop, dBegBot;
     double alpha;
     R c;
@@ -73,6 +74,7 @@ template<typename R> __device__ __forceinline__ bool ray_init2d(const EnvDev &e,
                                                                 RayState2<R> &st, RunCounters *ctr)
 {
     st.iSeg = SegState{0, 0};
+    ssp_cache_init(st.sc, e);
     const double alpha = e.alpha[ialpha];
     st.alpha = alpha;
     const double SrcDecl = (180.0 / BHCB_PI) * alpha;
@@ -126,7 +128,7 @@ template<typename R> __device__ __forceinline__ bool ray_update2d(RayState2<R> &
                                                                   const EnvDev &e, RunCounters *ctr)
 {
     bool tr = false, br = false;
-    step2d(st.p0, p1, st.top, st.bot, e, st.iSeg, small, tr, br, ctr);
+    step2d(st.p0, p1, st.top, st.bot, e, st.iSeg, small, tr, br, ctr, &st.sc);
     get_bdry_seg(p1.x, (double)p1.t.x, st.top, e.btop, e.ntop, e.top_long, st.htop, true, false, ctr);
     get_bdry_seg(p1.x, (double)p1.t.x, st.bot, e.bbot, e.nbot, e.bot_long, st.hbot, false, false, ctr);
     distances(p1.x, st.top, st.bot, dEndTop, dEndBot);

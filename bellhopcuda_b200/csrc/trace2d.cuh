@@ -183,6 +183,93 @@ template<typename R, bool NEED_RHO = false> __device__ __forceinline__ void eval
     }
 }
 
+// Register copy of the SSP segment a ray is in, for the 1-D profile types
+// C, S and P: the segment's depth bounds and its coefficients, reloaded only
+// when update_seg would move the segment. It holds the table values
+// themselves and eval_ssp_cached does eval_ssp's arithmetic on them, so the
+// results are the same; it saves the dependent table loads of every
+// evaluation on the ray's step chain.
+struct SspSegCache {
+    int type;          // e.ssp_type; other types take eval_ssp
+    int iz;            // segment held (-1: none)
+    bool down, up;     // update_seg may move the segment down / up from iz
+    double z0, z1;     // e.z[iz], e.z[iz + 1]
+    double k0, k1, k2, k3, k4, k5, k6, k7;   // C: c, cz (re, im); S, P: the four complex coefficients
+};
+
+__device__ __forceinline__ void ssp_cache_init(SspSegCache &sc, const EnvDev &e)
+{
+    sc.type = e.ssp_type;
+    sc.iz = -1;
+}
+
+template<typename R> __device__ __forceinline__ void eval_ssp_cached(
+    V2<double> x, V2<R> t, SSPOut<R> &o, const EnvDev &e, SegState &s, SspSegCache &sc, RunCounters *ctr)
+{
+    if(sc.type != SSP_CLINEAR && sc.type != SSP_CUBIC && sc.type != SSP_PCHIP) {
+        eval_ssp(x, t, o, e, s, ctr);
+        return;
+    }
+    const bool tpos = t.y >= (R)0;
+    // the segment update_seg would leave unchanged (src/ssp.hpp:36-51)
+    bool move = sc.iz != s.z;
+    if(!move)
+        move = tpos ? ((sc.down && x.y < sc.z0) || (sc.up && x.y >= sc.z1))
+                    : ((sc.up && x.y > sc.z1) || (sc.down && x.y <= sc.z0));
+    if(move) {
+        const int n = e.nssp;
+        update_seg(x.y, tpos, e.z, n, s.z);
+        const int iz = s.z;
+        sc.iz = iz;
+        sc.down = iz > 0;
+        sc.up = iz < n - 2;
+        sc.z0 = e.z[iz];
+        sc.z1 = e.z[iz + 1];
+        if(sc.type == SSP_CLINEAR) {
+            sc.k0 = e.c[2 * iz];
+            sc.k1 = e.c[2 * iz + 1];
+            sc.k2 = e.cz[2 * iz];
+            sc.k3 = e.cz[2 * iz + 1];
+        } else {
+            const double *C = e.coef;
+            sc.k0 = C[2 * iz];
+            sc.k1 = C[2 * iz + 1];
+            sc.k2 = C[2 * (n + iz)];
+            sc.k3 = C[2 * (n + iz) + 1];
+            sc.k4 = C[2 * (2 * n + iz)];
+            sc.k5 = C[2 * (2 * n + iz) + 1];
+            sc.k6 = C[2 * (3 * n + iz)];
+            sc.k7 = C[2 * (3 * n + iz) + 1];
+        }
+    }
+    const double dz = x.y - sc.z0;
+    o.crr = o.crz = o.czz = (R)0;
+    o.rho = (R)0;
+    if(sc.type == SSP_CLINEAR) {
+        o.c = (R)sc.k0 + (R)dz * (R)sc.k2;
+        o.ci = (R)sc.k1 + (R)dz * (R)sc.k3;
+        o.gradc = mk2<R>((R)0, (R)sc.k2);
+    } else if(sc.type == SSP_CUBIC) {
+        // SplineALL (src/curves.hpp:190-204)
+        const R h = (R)dz;
+        const R c1r = (R)sc.k0, c1i = (R)sc.k1, c2r = (R)sc.k2, c2i = (R)sc.k3;
+        const R c3r = (R)sc.k4, c3i = (R)sc.k5, c4r = (R)sc.k6, c4i = (R)sc.k7;
+        const R half = (R)0.5, sixth = (R)(double)(1.0f / 6.0f);
+        o.c = c1r + h * (c2r + h * (half * c3r + sixth * h * c4r));
+        o.ci = c1i + h * (c2i + h * (half * c3i + sixth * h * c4i));
+        o.gradc = mk2<R>((R)0, c2r + h * (c3r + h * half * c4r));
+        o.czz = c3r + h * c4r;
+    } else {
+        const R xt = (R)dz;
+        const R a0 = (R)sc.k0, a0i = (R)sc.k1, a1 = (R)sc.k2, a1i = (R)sc.k3;
+        const R a2 = (R)sc.k4, a2i = (R)sc.k5, a3 = (R)sc.k6, a3i = (R)sc.k7;
+        o.c = a0 + (a1 + (a2 + a3 * xt) * xt) * xt;
+        o.ci = a0i + (a1i + (a2i + a3i * xt) * xt) * xt;
+        o.gradc = mk2<R>((R)0, a1 + ((R)2 * a2 + (R)3 * a3 * xt) * xt);
+        o.czz = (R)2 * a2 + (R)6 * a3 * xt;
+    }
+}
+
 // src/boundary.hpp:66-227 (2-D branch)
 __device__ __forceinline__ void get_bdry_seg(
     V2<double> x, double tx, BdState &bs, const BdryPtDev *bd, int n, bool islong, HsDev &hs,
@@ -350,11 +437,14 @@ __device__ __forceinline__ void step_to_bdry(
 // src/step.hpp:589-649 (interface curvature correction)
 template<typename R> __device__ __forceinline__ void step2d(
     const RayPt<R> &ray0, RayPt<R> &ray2, const BdState &top, const BdState &bot,
-    const EnvDev &e, SegState &iSeg, int &small, bool &tr, bool &br, RunCounters *ctr)
+    const EnvDev &e, SegState &iSeg, int &small, bool &tr, bool &br, RunCounters *ctr,
+    SspSegCache *sc = nullptr)
 {
     StepGeo g{&e};
     SSPOut<R> o0, o1, o2;
-    eval_ssp(ray0.x, ray0.t, o0, e, iSeg, ctr);
+#define BHCB_STEP_SSP(X, T, O) \
+    do { if(sc) eval_ssp_cached(X, T, O, e, iSeg, *sc, ctr); else eval_ssp(X, T, O, e, iSeg, ctr); } while(0)
+    BHCB_STEP_SSP(ray0.x, ray0.t, o0);
     R cnn0 = o0.crr * ray0.t.y * ray0.t.y - (R)2 * o0.crz * ray0.t.x * ray0.t.y
         + o0.czz * ray0.t.x * ray0.t.x;
     V2<R> pq0p = scl2(-cnn0, ray0.q), pq0q = scl2(o0.c, ray0.p);
@@ -370,7 +460,7 @@ template<typename R> __device__ __forceinline__ void step2d(
     ray1.p = add2(ray0.p, scl2((R)halfh, pq0p));
     ray1.q = add2(ray0.q, scl2((R)halfh, pq0q));
 
-    eval_ssp(ray1.x, ray1.t, o1, e, iSeg, ctr);
+    BHCB_STEP_SSP(ray1.x, ray1.t, o1);
     R cnn1 = o1.crr * ray1.t.y * ray1.t.y - (R)2 * o1.crz * ray1.t.x * ray1.t.y
         + o1.czz * ray1.t.x * ray1.t.x;
     V2<R> pq1p = scl2(-cnn1, ray1.q), pq1q = scl2(o1.c, ray1.p);
@@ -397,7 +487,8 @@ template<typename R> __device__ __forceinline__ void step2d(
     ray2.Phase = ray0.Phase;
     ray2.ntop = ray0.ntop;
     ray2.nbot = ray0.nbot;
-    eval_ssp(ray2.x, ray2.t, o2, e, iSeg, ctr);
+    BHCB_STEP_SSP(ray2.x, ray2.t, o2);
+#undef BHCB_STEP_SSP
     ray2.c = o2.c;
     if(iSeg.z != s0.z || iSeg.r != s0.r) {
         // iSeg.r only moves for the quad SSP; a depth crossing takes precedence
