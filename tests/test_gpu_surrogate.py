@@ -11,24 +11,58 @@ from bellhopcuda_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def _cpu_net(model, torch):
-    """The network's forward in float64 on the CPU from the model's bf16 weights."""
-    def lin(l, x):
-        w = l.wb.double().cpu().requires_grad_(True)
-        b = l.b.double().cpu().requires_grad_(True)
-        return w, b, x @ w.T + b
+def _bf(t):
+    """Round a float64 tensor to bfloat16 and back (the GPU's storage points)."""
+    return t.to(__import__("torch").bfloat16).double()
 
-    def mlp(m, x):
-        ps = []
-        for i, l in enumerate(m.layers):
-            w, b, z = lin(l, x)
-            ps += [w, b]
-            x = torch.nn.functional.gelu(z, approximate="tanh") if l.gelu else z
-        return x, ps
-    return mlp
+
+def _gelu(z, torch):
+    c = 0.7978845608028654   # sqrt(2 / pi), tanh form
+    u = c * (z + 0.044715 * z ** 3)
+    return 0.5 * z * (1.0 + torch.tanh(u))
+
+
+def _dgelu(z, torch):
+    c = 0.7978845608028654
+    u = c * (z + 0.044715 * z ** 3)
+    th = torch.tanh(u)
+    return 0.5 * (1.0 + th) + 0.5 * z * (1.0 - th ** 2) * c * (1.0 + 3 * 0.044715 * z ** 2)
+
+
+def _cpu_forward(m, x, torch):
+    """One MLP in float64 on the CPU, rounding to bf16 where the GPU stores bf16:
+    layer outputs and the kept pre-activations."""
+    xs, pres = [], []
+    for l in m.layers:
+        W = l.wb.double().cpu()
+        z = x @ W.T + l.b.double().cpu()
+        xs.append(x)
+        if l.gelu:
+            pres.append(_bf(z))
+            x = _bf(_gelu(z, torch))
+        else:
+            pres.append(None)
+            x = _bf(z)
+    return x, xs, pres
+
+
+def _cpu_backward(m, dz, xs, pres, torch):
+    """Gradients (gw, gb) of every layer, last to first, with the GPU's bf16
+    rounding of the propagated pre-activation gradients."""
+    grads = []
+    for i in range(len(m.layers) - 1, -1, -1):
+        l = m.layers[i]
+        grads.append((dz.T @ xs[i], dz.sum(0)))
+        if i > 0:
+            W = l.wb.double().cpu()
+            dz = _bf((dz @ W) * _dgelu(pres[i - 1], torch))
+    return grads[::-1]
 
 
 def test_gradients_match_cpu_float64():
+    """Forward and every parameter gradient of the tensor-core network against
+    a float64 CPU restatement that rounds to bf16 at the same storage points.
+    What remains is FP32 accumulation order and bf16 rounding ties: 1e-2."""
     import torch
     model = S.Surrogate(seed=3)
     rng = np.random.default_rng(0)
@@ -42,30 +76,31 @@ def test_gradients_match_cpu_float64():
     model.backward(dpred)
     torch.cuda.synchronize()
     model.ops.check()
-    # float64 restatement on the CPU
-    mlp = _cpu_net(model, torch)
-    b, pb = mlp(model.branch, x.double().cpu())
-    t, pt = mlp(model.trunk, model.phi.double().cpu())
-    beta = model.pbias.double().cpu().requires_grad_(True)
-    p64 = b @ t.T + beta
-    # bf16 activations between layers: about 1 % relative, measured on the whole output
-    d = pred.cpu().double() - p64.detach()
-    assert float(d.norm() / p64.detach().norm()) < 0.02
-    l64 = ((p64 - y.double().cpu()) ** 2).mean()
-    l64.backward()
+    b, bx, bp = _cpu_forward(model.branch, x.double().cpu(), torch)
+    t, tx, tp = _cpu_forward(model.trunk, model.phi.double().cpu(), torch)
+    p64 = b @ t.T + model.pbias.double().cpu()
+    d = pred.cpu().double() - p64
+    assert float(d.norm() / p64.norm()) < 1e-2
+    # the loss gradient the GPU stored (bf16), propagated on the CPU
+    dp = dpred.cpu().double()
+    ref_dp = _bf(2.0 * (pred.cpu().double() - y.cpu().double()) / (Bn * S.NP))
+    assert float((dp - ref_dp).norm() / ref_dp.norm()) < 1e-2
+    db = _bf(dp @ t)
+    dt = _bf(dp.T @ b)
     got = []
     for m in (model.branch, model.trunk):
         for l in m.layers:
             got += [l.gw, l.gb]
-    ref = pb + pt
-    for g, r in zip(got, ref):
+    ref = []
+    for gw, gb in _cpu_backward(model.branch, db, bx, bp, torch) + _cpu_backward(model.trunk, dt, tx, tp, torch):
+        ref += [gw, gb]
+    for k, (g, r) in enumerate(zip(got, ref)):
         g = g.double().cpu().flatten()
-        r = r.grad.flatten()
-        cos = float((g @ r) / (g.norm() * r.norm() + 1e-300))
+        r = r.flatten()
         rel = float((g - r).norm() / (r.norm() + 1e-300))
-        assert cos > 0.99 and rel < 0.1, (cos, rel)
+        assert rel < 1e-2, (k, rel)
     g = model.gpb.double().cpu()
-    assert float((g - beta.grad).norm() / beta.grad.norm()) < 0.05
+    assert float((g - dp.sum(0)).norm() / dp.sum(0).norm()) < 1e-3
 
 
 def test_training_reduces_error_and_fallback_is_the_trace(tmp_path):
