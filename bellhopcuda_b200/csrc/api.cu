@@ -1144,7 +1144,7 @@ int run3_checked(bhcb_ctx *c)
     bhcb_stats st{};
     uint32_t wb = 0;
     const uint32_t eb = run3_run(c->r3, c->stream, c->sm_count, c->max_memory, c->opt_max_narr, c->allow_merging,
-                                 st, wb);
+                                 c->precision == BHCB_PREC_MIXED, st, wb);
     c->stats = st;
     c->err_bits = eb;
     c->warn_bits = wb;

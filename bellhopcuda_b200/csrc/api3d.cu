@@ -39,7 +39,7 @@ size_t nx_record_bytes();
 cudaError_t launch_trace3d(const GroupDev *, int, long long, SegRec3 *, unsigned long long, RunCounters *,
                            unsigned long long *, int, cudaStream_t);
 cudaError_t launch_influence3d(const SegRec3 *, unsigned long long, const GroupDev *, int, float2 *, RunCounters *,
-                               int, cudaStream_t);
+                               int, cudaStream_t, bool);
 cudaError_t launch_sqrt3d(float2 *, long long, int, cudaStream_t);
 cudaError_t launch_arr_gather3d(const SegRec3 *, unsigned long long, const GroupDev *, int, bool, ArrCand *,
                                 uint64_t *, uint32_t *, unsigned long long, unsigned long long *, RunCounters *,
@@ -95,6 +95,7 @@ struct Run3 {
     std::vector<RaySet3> raysets;     // per environment
     bool raycen = false;              // geometric beams in ray-centred coordinates ('g', 'b')
     bool nx2d = false;                // N x 2-D rays (RunType(6) '2')
+    bool mixed = false;               // Cartesian TL contributions in mixed precision (BHCB_PREC_MIXED)
     int sm_count = 148;
 };
 
@@ -525,7 +526,7 @@ void run_jobs(Run3 *r, long long j0, long long j1, cudaStream_t st, int sm_count
                                      (int)r->groups_h.size(), (float2 *)r->field.p, ctr, nzt, sm_count * 16, st));
         } else if(rc.err_bits == 0) {
             CK(launch_influence3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
-                                  (int)r->groups_h.size(), (float2 *)r->field.p, ctr, igrid, st));
+                                  (int)r->groups_h.size(), (float2 *)r->field.p, ctr, igrid, st, r->mixed));
         }
         CK(cudaEventRecord(e2, st));
         RunCounters rc2{};
@@ -609,10 +610,11 @@ uint32_t trace_rays3(Run3 *r, RaySet3 &R, cudaStream_t st, uint32_t &warn_bits)
 } // namespace
 
 uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, int32_t opt_max_narr,
-                  int32_t allow_merging, bhcb_stats &stats, uint32_t &warn_bits)
+                  int32_t allow_merging, bool mixed, bhcb_stats &stats, uint32_t &warn_bits)
 {
     auto t0 = std::chrono::steady_clock::now();
     uint64_t h2d = 0;
+    r->mixed = mixed;
     r->max_memory = max_memory;
     r->opt_max_narr = opt_max_narr;
     r->allow_merging = allow_merging;

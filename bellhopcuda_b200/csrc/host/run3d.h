@@ -22,8 +22,10 @@ int run3_count(const Run3 *r);
 int run3_add_env(Run3 *r, const std::string &root);
 // builds the tables, traces every ray of every environment and evaluates the
 // fields; fills the statistics; returns the tracer's error bits (0 = clean)
+// mixed: TL contributions of Cartesian geometric beams in mixed precision (the
+// trace stays FP64)
 uint32_t run3_run(Run3 *r, cudaStream_t st, int sm_count, uint64_t max_memory, int32_t opt_max_narr,
-                  int32_t allow_merging, bhcb_stats &stats, uint32_t &warn_bits);
+                  int32_t allow_merging, bool mixed, bhcb_stats &stats, uint32_t &warn_bits);
 // arrivals runs (RunType 'A' / 'a'): storage [cell][max_narr], cells in the field layout
 bool run3_is_arrivals(const Run3 *r);
 // eigen-hit runs ('E'): copies up to max_hits hits of env (reference order) to

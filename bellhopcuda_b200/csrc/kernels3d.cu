@@ -347,6 +347,50 @@ __device__ __forceinline__ float2 tl_field3(const Contrib3 &o, bool gauss, bool 
     return make_float2((float)v, 0.0f);
 }
 
+// The TL contribution of one receiver in the mixed precision (FP32 q, beam
+// window, amplitude and weight with the SFU's approximations; the delay's
+// phase omega tau is formed and reduced mod 2 pi in FP64, the rest in FP32).
+// Same tests and formulas as geo_core3 + tl_field3.
+__device__ __forceinline__ bool geo_tl3_mixed(const SegRec3 &R, double s, double n1, double n2, bool gauss,
+                                              bool coherent, double omega, float2 &out)
+{
+    const float sf = (float)s;
+    const float rq0 = (float)R.rcp_q0, rq1 = (float)R.rcp_qhat0;
+    const float q00 = fmaf(sf, (float)R.dq[0], (float)R.q0[0]) * rq0;
+    const float q10 = fmaf(sf, (float)R.dq[2], (float)R.q0[2]) * rq0;
+    const float q01 = fmaf(sf, (float)R.dq[1], (float)R.q0[1]) * rq1;
+    const float q11 = fmaf(sf, (float)R.dq[3], (float)R.q0[3]) * rq1;
+    const float qF = q00 * q11 - q10 * q01;
+    const float eps2 = (float)(DBL_EPS * DBL_EPS);
+    if(q00 * q00 + q10 * q10 < eps2 || q01 * q01 + q11 * q11 < eps2) return false;
+    if(fabsf(qF) < (float)DBL_EPS) return false;
+    const float iq = 1.0f / qF;
+    const float n1f = (float)n1, n2f = (float)n2;
+    const float n1p = fabsf((q11 * n1f - q01 * n2f) * iq);
+    const float n2p = fabsf((q00 * n2f - q10 * n1f) * iq);
+    const float dist = gauss ? n1p + n2p : fmaxf(n1p, n2p);
+    if(dist > (gauss ? 4.0f : 1.0f)) return false;
+    const float cnst = (float)R.cnst_num * rsqrtf(fabsf(qF));
+    const float w = gauss ? __expf(-0.5f * (n1p * n1p + n2p * n2p)) : (1.0f - n1p) * (1.0f - n2p);
+    const float att = __expf((float)(omega * (R.tau0i + s * R.dtaui)));
+    if(coherent) {
+        float ph = (float)R.phase0;
+        if((qF <= 0.0f && R.qold > 0.0) || (qF >= 0.0f && R.qold < 0.0)) ph += (float)(BHCB_PI / 2.0);
+        const double a = omega * (R.tau0r + s * R.dtaur);
+        const float ar = (float)(a - 6.28318530717958647692 * rint(a * 0.15915494309189533577));
+        float sa, ca;
+        __sincosf(ph - ar, &sa, &ca);
+        const float cw = cnst * w * att;
+        out = make_float2(cw * ca, cw * sa);
+    } else {
+        float v = cnst * att;
+        v = v * v * w;
+        if(gauss) v *= (float)(2.0 * BHCB_PI);
+        out = make_float2(v, 0.0f);
+    }
+    return true;
+}
+
 // first index with (double)rz >= z (n if none)
 __device__ __forceinline__ int first_depth_at_or_above(const float *rz, int n, double z)
 {
@@ -404,7 +448,8 @@ __device__ __forceinline__ bool pair_outside_beam(const SegRec3 &R, double dxr, 
 // INFL_EIG_COUNT / INFL_EIG_FILL: the same for eigenray hits (RecordEigenHit,
 // src/eigenrays.hpp:24-40), keyed by (trace group, ray, step, position in the
 // receiver-range walk, bearing, depth) — the reference's single-threaded order.
-enum { INFL_TL = 0, INFL_ARR_COUNT = 1, INFL_ARR_FILL = 2, INFL_EIG_COUNT = 3, INFL_EIG_FILL = 4 };
+// INFL_TL_MIXED: INFL_TL with the receiver's contribution in mixed precision.
+enum { INFL_TL = 0, INFL_ARR_COUNT = 1, INFL_ARR_FILL = 2, INFL_EIG_COUNT = 3, INFL_EIG_FILL = 4, INFL_TL_MIXED = 5 };
 template<int MODE>
 __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
     const SegRec3 *__restrict__ segs, unsigned long long nseg, const GroupDev *__restrict__ groups, int ngroups,
@@ -525,6 +570,15 @@ __global__ void __launch_bounds__(32 * WARPS3) influence3d_kernel(
                 const double sv = (dxr * R.rayt[0] + dyr * R.rayt[1] + dz * R.rayt[2]) / R.rlen;
                 const double n1 = fabs(dxr * R.e1[0] + dyr * R.e1[1] + dz * R.e1[2]);
                 const double n2 = fabs(dxr * R.e2[0] + dyr * R.e2[1] + dz * R.e2[2]);
+                if(MODE == INFL_TL_MIXED) {
+                    float2 v;
+                    if(!geo_tl3_mixed(R, sv, n1, n2, E.gaussian != 0, E.coherent != 0,
+                                      FLTD(2.0) * BHCB_PI * E.freq0, v))
+                        continue;
+                    ++nevals;
+                    atomicAdd(field + s_poff[w][pi] + (long long)iz * E.nrr, v);
+                    continue;
+                }
                 Contrib3 o;
                 if(!geo_core3(R, sv, n1, n2, E.gaussian != 0, o)) continue;
                 ++nevals;
@@ -642,11 +696,16 @@ cudaError_t launch_trace3d(const GroupDev *groups, int ngroups, long long job_en
 }
 
 cudaError_t launch_influence3d(const SegRec3 *segs, unsigned long long nseg, const GroupDev *groups, int ngroups,
-                               float2 *field, RunCounters *ctr, int grid, cudaStream_t st)
+                               float2 *field, RunCounters *ctr, int grid, cudaStream_t st, bool mixed)
 {
     if(nseg == 0) return cudaSuccess;
-    influence3d_kernel<INFL_TL><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, field, ctr, nullptr,
-                                                               nullptr, nullptr, 0, nullptr, ArrKeyBits{});
+    if(mixed)
+        influence3d_kernel<INFL_TL_MIXED><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, field, ctr,
+                                                                         nullptr, nullptr, nullptr, 0, nullptr,
+                                                                         ArrKeyBits{});
+    else
+        influence3d_kernel<INFL_TL><<<grid, 32 * WARPS3, 0, st>>>(segs, nseg, groups, ngroups, field, ctr, nullptr,
+                                                                   nullptr, nullptr, 0, nullptr, ArrKeyBits{});
     return cudaGetLastError();
 }
 

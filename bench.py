@@ -212,6 +212,34 @@ def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=N
     return t, times, stats, fields
 
 
+def time_c4(B, tmp, rank, runs=3):
+    """The 3-D workload (51,984 rays, 36 bearings x 101 depths x 501 ranges,
+    Gaussian beams, hexahedral SSP) as one TL run per step in both precisions:
+    the run's own trace and influence times (device events), median of
+    `runs` runs after one untimed run. Not part of the headline metric."""
+    from bellhopcuda_b200 import workloads as W
+    files = W.c4_3d(run_type="CB   3")
+    root = os.path.join(tmp, "c4_%d" % rank)
+    for suffix, text in files.items():
+        with open(root + suffix, "w") as f:
+            f.write(text)
+    out = {"workload": "C4: 3-D Gaussian-beam TL, 361 x 144 rays, 36 x 101 x 501 receivers, 200 Hz"}
+    for name, prec in (("fp64", B.PREC_FP64), ("mixed", B.PREC_MIXED)):
+        with B.Tracer(precision=prec) as t:
+            t.setup3d(root)
+            t.run()
+            st = []
+            for _ in range(runs):
+                t.run()
+                st.append(t.stats())
+        tot = sorted(x["trace_ms"] + x["influence_ms"] for x in st)[len(st) // 2]
+        out[name] = {"run_ms": tot, "trace_ms": statistics.median(x["trace_ms"] for x in st),
+                     "influence_ms": statistics.median(x["influence_ms"] for x in st),
+                     "contributions": int(st[-1]["evals"])}
+    out["mixed_speedup"] = out["fp64"]["run_ms"] / out["mixed"]["run_ms"]
+    return out
+
+
 def time_e2e(B, torch, root, freqs, steps, gpu, tune=None):
     """Same metric through the public C ABI with host buffers: setup reads the
     files, prepare uploads the tables, run, and every field copied back to
@@ -339,6 +367,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the 3-D (C4) TL timing")
     ap.add_argument("--rays", type=int, default=0,
                     help="profiling only: trace this many rays of the fan instead of 20001 (the line says so)")
     ap.add_argument("--profile", action="store_true",
@@ -442,6 +471,7 @@ def main():
                                      F_STEP * ORACLE_STEPS_PER_TRACE / (trace_ms * 1e-3) / 1e12,
                                      "influence_kernel_ms": infl_ms},
                     "fp64_peak_tflops": fp64_peak}
+        c4 = None if args.no_c4 else time_c4(B, tmp, rank)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(spec, freqs, tmp)
@@ -460,7 +490,7 @@ def main():
                                     "trace_lanes": tuning.get("trace_lanes", 32),
                                     "chosen_by": "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-        "gpu_launches": 3 * args.steps, "fp64_trace": fp64, "kernels": kernels,
+        "gpu_launches": 3 * args.steps, "fp64_trace": fp64, "kernels": kernels, "c4_3d_tl": c4,
         "launch": "CUDA graph replay of memsets + trace + influence + scale per step",
     }
     if rank == 0:

@@ -45,12 +45,15 @@ def to_file_order(u):
 TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p and not p.endswith("_ray.npz")]
 
 
+@pytest.mark.parametrize("precision", [B.PREC_FP64, B.PREC_MIXED])
 @pytest.mark.parametrize("path", TL3D, ids=[os.path.basename(p)[:-4] for p in TL3D])
-def test_3d_field_matches_reference(path, workdir):
+def test_3d_field_matches_reference(path, precision, workdir):
+    """Both precisions: the mixed one evaluates the Cartesian beams' TL
+    contributions in FP32 (the trace stays FP64); same 0.5 dB bound."""
     g = np.load(path)
-    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    root = os.path.join(workdir, os.path.basename(path)[:-4] + "_%d" % precision)
     write_case(g, root)
-    with B.Tracer(precision=B.PREC_FP64) as t:
+    with B.Tracer(precision=precision) as t:
         t.setup3d(root)
         t.run()
         u = t.field3d(0)

@@ -44,13 +44,16 @@ def files_sha(files):
     return h.hexdigest()
 
 
-def test_c4_bearings_tl(workdir):
+@pytest.mark.parametrize("precision", [B.PREC_FP64, B.PREC_MIXED])
+def test_c4_bearings_tl(precision, workdir):
+    """FP64 within 0.1 dB of the reference; the mixed precision (FP32
+    contributions) within the north-star 0.5 dB."""
     g = np.load(os.path.join(GOLD, "c4_bearings_tl.npz"))
     files = W.c4_3d(run_type="CB   3", ntheta=2)
     assert files_sha(files) == str(g["sha"]), "the seeded C4 generator no longer gives the fixture's inputs"
-    root = os.path.join(workdir, "c4_tl")
+    root = os.path.join(workdir, "c4_tl_%d" % precision)
     write_files(files, root)
-    with B.Tracer(precision=B.PREC_FP64) as t:
+    with B.Tracer(precision=precision) as t:
         t.setup3d(root)
         t.run()
         u = t.field3d(0)
@@ -64,9 +67,10 @@ def test_c4_bearings_tl(workdir):
     m = b < 100.0
     d = np.abs(a[m] - b[m])
     rms = float(np.sqrt(np.mean(d ** 2)))
-    print("C4 2-bearing TL: rms %.2e dB over %d receivers, steps %d" % (rms, int(m.sum()), st["steps"]))
+    print("C4 2-bearing TL, precision %d: rms %.2e dB over %d receivers, steps %d" % (
+        precision, rms, int(m.sum()), st["steps"]))
     assert m.sum() > 50000
-    assert rms < 0.1
+    assert rms < (0.1 if precision == B.PREC_FP64 else 0.5)
 
 
 def test_c4_bearings_arrivals(workdir):
