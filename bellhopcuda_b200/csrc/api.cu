@@ -40,6 +40,9 @@ template<typename R> cudaError_t launch_arr_gather(const void *, unsigned long l
                                                    const double *, bool, bool, ArrCand *, uint64_t *, uint32_t *,
                                                    unsigned long long, unsigned long long *, RunCounters *,
                                                    ArrKeyBits, int, cudaStream_t);
+cudaError_t launch_arr_gather_x(const XSeg *, unsigned long long, const GroupDev *, int, const double *, int, bool,
+                                ArrCand *, uint64_t *, uint32_t *, unsigned long long, unsigned long long *,
+                                RunCounters *, ArrKeyBits, int, int, cudaStream_t);
 size_t radix_sort_hist_entries(unsigned long long n);
 cudaError_t radix_sort_pairs(uint64_t *, uint32_t *, uint64_t *, uint32_t *, unsigned long long, int, uint32_t *,
                              int *, cudaStream_t);
@@ -105,12 +108,13 @@ constexpr unsigned long long MAXN_STEPS_HOST = 100000;   // steps per ray (inclu
 
 int run_mode_of(char r0)
 {
-    if(r0 == 'A' || r0 == 'a') return MODE_ARR;
+    if(r0 == 'A' || r0 == 'a' || r0 == 'V' || r0 == 'v') return MODE_ARR;   // 'V' / 'v': also eigen hits
     if(r0 == 'E') return MODE_EIGEN;
     if(r0 == 'C' || r0 == 'S' || r0 == 'I') return MODE_TL;
     if(r0 == 'R') return MODE_RAY;
     throw std::runtime_error(std::string("RunType '") + r0 + "' is not supported by this entry point "
-                             "(TL 'C'/'S'/'I', arrivals 'A'/'a', eigen hits 'E', rays 'R')");
+                             "(TL 'C'/'S'/'I', arrivals 'A'/'a', arrivals and eigen hits 'V'/'v', eigen hits 'E', "
+                             "rays 'R')");
 }
 
 int bits_for(unsigned long long n)   // bits to hold values 0..n-1 (at least 1)
@@ -168,9 +172,10 @@ struct bhcb_ctx {
 
     // arrivals / eigen runs (RunType 'A', 'a', 'E')
     int mode = MODE_TL;
+    bool also_eigen = false;         // RunType 'V' / 'v': an arrivals run that also records eigen hits
     int32_t opt_max_narr = 0, allow_merging = 1;
     int32_t max_narr = 0;
-    ArrKeyBits kb{};
+    ArrKeyBits kb{}, kb_eig{};       // ordering keys of the arrivals (or eigen) pass and of the eigen pass of 'V' runs
     unsigned long long ncand = 0;
     DevBuf cand, keys0, keys1, vals0, vals1, hist, narr_d, arr_d, hits_d, hitfield_d;
     const uint64_t *sorted_keys = nullptr;
@@ -231,25 +236,35 @@ void prepare_arrivals(bhcb_ctx *c)
         max_nrr = std::max(max_nrr, F.nrr);
         max_nrzp = std::max(max_nrzp, F.nrzp);
     }
-    ArrKeyBits kb{};
     const int bis = bits_for(MAXN_STEPS_HOST), bjob = bits_for((unsigned long long)max_njobs);
-    if(c->mode == MODE_ARR) {
-        kb.eigen = 0;
-        kb.sh_walk = 0;
-        kb.sh_is = 0;
-        kb.sh_job = bis;
-        kb.sh_cell = bis + bjob;
-        kb.total_bits = kb.sh_cell + bits_for((unsigned long long)c->total_field);
-    } else {
-        kb.eigen = 1;
-        kb.sh_walk = bits_for((unsigned long long)max_nrzp);
-        kb.sh_is = kb.sh_walk + bits_for((unsigned long long)max_nrr);
-        kb.sh_job = kb.sh_is + bis;
-        kb.sh_cell = kb.sh_job + bjob;
-        kb.total_bits = kb.sh_cell + bits_for((unsigned long long)c->fields.size());
-    }
-    if(kb.total_bits > 64)
-        throw MemError("arrival ordering key needs more than 64 bits; split the run");
+    auto layout = [&](bool eigen) {
+        ArrKeyBits kb{};
+        if(!eigen) {
+            kb.eigen = 0;
+            kb.sh_walk = 0;
+            kb.sh_is = 0;
+            kb.sh_job = bis;
+            kb.sh_cell = bis + bjob;
+            kb.total_bits = kb.sh_cell + bits_for((unsigned long long)c->total_field);
+        } else {
+            kb.eigen = 1;
+            // within a step: Cartesian and simple Gaussian beams walk the ranges,
+            // then the depths; ray-centred beams the depths, then the ranges
+            const bool depth_outer = c->xkind == INFL_GEO_RAYCEN;
+            const int lo_bits = bits_for((unsigned long long)(depth_outer ? max_nrr : max_nrzp));
+            const int hi_bits = bits_for((unsigned long long)(depth_outer ? max_nrzp : max_nrr));
+            kb.sh_walk = lo_bits;
+            kb.sh_is = kb.sh_walk + hi_bits;
+            kb.sh_job = kb.sh_is + bis;
+            kb.sh_cell = kb.sh_job + bjob;
+            kb.total_bits = kb.sh_cell + bits_for((unsigned long long)c->fields.size());
+        }
+        if(kb.total_bits > 64)
+            throw MemError("arrival ordering key needs more than 64 bits; split the run");
+        return kb;
+    };
+    const ArrKeyBits kb = layout(c->mode != MODE_ARR);
+    c->kb_eig = c->also_eigen ? layout(true) : kb;
     c->kb = kb;
     if(c->mode == MODE_ARR) {
         size_t cells = (size_t)c->total_field;
@@ -258,6 +273,7 @@ void prepare_arrivals(bhcb_ctx *c)
             // like the reference (src/mode/arr.hpp:80-98): as many arrivals per
             // receiver as a quarter of max_memory holds, at most 1000
             uint64_t m = (c->max_memory / 4) / (cells * sizeof(ArrivalRec) + 1);
+            if(c->also_eigen) m /= 2;   // half the room goes to the eigen hits (src/mode/arr.hpp:87)
             mx = (int32_t)std::min<uint64_t>(m, 1000);
         }
         if(mx <= 0) throw MemError("insufficient memory to allocate arrivals");
@@ -291,6 +307,7 @@ void do_prepare(bhcb_ctx *c)
     c->njobs = 0;
     bool fp64 = c->precision == BHCB_PREC_FP64;
     c->mode = run_mode_of(c->envs[0].in.run_type[0]);
+    c->also_eigen = c->envs[0].in.run_type[0] == 'V' || c->envs[0].in.run_type[0] == 'v';
     for(auto &S : c->envs)
         if(run_mode_of(S.in.run_type[0]) != c->mode)
             throw std::runtime_error("a batch must use one run mode (TL, arrivals or eigen hits)");
@@ -521,6 +538,7 @@ void do_launch_range(bhcb_ctx *c, int g0, int g1, bool clear, bool host_driven)
         CK(launch_trace_x(Gx, ngx, job1, (XSeg *)c->segs.p, c->seg_cap, ctr, jobc, c->xkind, (int)std::max(1LL, xgrid),
                           64, c->stream));
         CK(record_event(c, 1, c->stream));
+        if(c->mode != MODE_TL) return;   // arrivals / hits: run_arrivals after the trace
         c->last_overlapped = false;
         int nzmax = 1;   // receiver depths per range, the most of the launched groups
         for(int g = g0; g < g1; ++g) nzmax = std::max(nzmax, c->fields[c->groups_h[g].field_index].nrzp);
@@ -848,8 +866,10 @@ void write_rays(const bhcb_ctx *c, const Field &F, const RaySet &R, const std::s
     }
 }
 
-// Arrivals / eigen hits of the traced segments: count, gather, order, replay.
-void run_arrivals(bhcb_ctx *c)
+// Candidates of the traced segments under key layout kb: count, gather, and
+// order them; returns their number (c->sorted_keys / sorted_vals point at the
+// order).
+unsigned long long gather_sorted(bhcb_ctx *c, const ArrKeyBits &kb)
 {
     const bool fp64 = c->precision == BHCB_PREC_FP64;
     const GroupDev *G = (const GroupDev *)c->groups_d.p;
@@ -858,15 +878,19 @@ void run_arrivals(bhcb_ctx *c)
     RunCounters *ctr = (RunCounters *)c->counters.p;
     unsigned long long *cursor = (unsigned long long *)((uint8_t *)c->counters.p + sizeof(RunCounters));
     const int grid = c->sm_count * 16;
-    CK(record_event(c, 1, c->stream));
+    int nzmax = 1;   // receiver depths per range, the most of the batch (ray-centred / simple Gaussian)
+    for(const Field &F : c->fields) nzmax = std::max(nzmax, F.nrzp);
     // 1. count
     CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), c->stream));
-    if(fp64)
+    if(c->xkind)
+        CK(launch_arr_gather_x((const XSeg *)c->segs.p, c->seg_cap, G, ng, fq, c->xkind, true, nullptr, nullptr,
+                               nullptr, 0, cursor, ctr, kb, nzmax, grid, c->stream));
+    else if(fp64)
         CK(launch_arr_gather<double>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, true, nullptr, nullptr, nullptr, 0,
-                                     cursor, ctr, c->kb, grid, c->stream));
+                                     cursor, ctr, kb, grid, c->stream));
     else
         CK(launch_arr_gather<float>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, true, nullptr, nullptr, nullptr, 0,
-                                    cursor, ctr, c->kb, grid, c->stream));
+                                    cursor, ctr, kb, grid, c->stream));
     unsigned long long n = 0;
     CK(cudaMemcpyAsync(&n, &ctr->nevals, sizeof n, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -883,43 +907,73 @@ void run_arrivals(bhcb_ctx *c)
     c->hist.ensure(radix_sort_hist_entries(nn) * sizeof(uint32_t));
     // 2. gather
     CK(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), c->stream));
-    if(fp64)
+    if(c->xkind)
+        CK(launch_arr_gather_x((const XSeg *)c->segs.p, c->seg_cap, G, ng, fq, c->xkind, false, (ArrCand *)c->cand.p,
+                               (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, kb, nzmax, grid,
+                               c->stream));
+    else if(fp64)
         CK(launch_arr_gather<double>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, false, (ArrCand *)c->cand.p,
-                                     (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, c->kb, grid,
+                                     (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, kb, grid,
                                      c->stream));
     else
         CK(launch_arr_gather<float>(c->segs.p, c->seg_cap, G, ng, fq, c->gauss, false, (ArrCand *)c->cand.p,
-                                    (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, c->kb, grid,
+                                    (uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, n, cursor, ctr, kb, grid,
                                     c->stream));
     // 3. order
     int in1 = 0;
     CK(radix_sort_pairs((uint64_t *)c->keys0.p, (uint32_t *)c->vals0.p, (uint64_t *)c->keys1.p,
-                        (uint32_t *)c->vals1.p, n, c->kb.total_bits, (uint32_t *)c->hist.p, &in1, c->stream));
+                        (uint32_t *)c->vals1.p, n, kb.total_bits, (uint32_t *)c->hist.p, &in1, c->stream));
     c->sorted_keys = (const uint64_t *)(in1 ? c->keys1.p : c->keys0.p);
     c->sorted_vals = (const uint32_t *)(in1 ? c->vals1.p : c->vals0.p);
-    // 4. replay / emit
+    return n;
+}
+
+// Eigen hits in sorted order, copied to the host with the field of each.
+void emit_eigen_hits(bhcb_ctx *c, unsigned long long n, const ArrKeyBits &kb)
+{
+    const size_t nn = std::max<size_t>(n, 1);
+    c->hits_d.ensure(nn * sizeof(EigenHitRec));
+    c->hitfield_d.ensure(nn * sizeof(int32_t));
+    CK(launch_eigen_emit(c->sorted_vals, (const ArrCand *)c->cand.p, n, (EigenHitRec *)c->hits_d.p,
+                         (int32_t *)c->hitfield_d.p, kb.sh_cell, c->sorted_keys, c->sm_count, c->stream));
+    c->hits_h.resize(n);
+    std::vector<int32_t> fld(n);
+    if(n) {
+        CK(cudaMemcpyAsync(c->hits_h.data(), c->hits_d.p, n * sizeof(EigenHitRec), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaMemcpyAsync(fld.data(), c->hitfield_d.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->hit_begin.assign(c->fields.size() + 1, 0);
+    for(size_t k = 0; k < n; ++k) c->hit_begin[fld[k] + 1]++;
+    for(size_t f = 0; f < c->fields.size(); ++f) c->hit_begin[f + 1] += c->hit_begin[f];
+}
+
+// Arrivals / eigen hits of the traced segments: count, gather, order, replay
+// (AddArr) or emit (RecordEigenHit). 'V' / 'v' runs take both passes over the
+// same segments, as the reference records the hit of every contribution it
+// hands to AddArr (src/influence.hpp:443-450).
+void run_arrivals(bhcb_ctx *c)
+{
+    const GroupDev *G = (const GroupDev *)c->groups_d.p;
+    const int ng = (int)c->groups_h.size();
+    const double *fq = (const double *)c->freqs_d.p;
+    CK(record_event(c, 1, c->stream));
+    unsigned long long n = gather_sorted(c, c->kb);
+    unsigned long long nevals = n;
     if(c->mode == MODE_ARR) {
         const size_t cells = (size_t)c->total_field;
         CK(cudaMemsetAsync(c->arr_d.p, 0, cells * (size_t)c->max_narr * sizeof(ArrivalRec), c->stream));
         CK(launch_arr_replay(c->sorted_keys, c->sorted_vals, (const ArrCand *)c->cand.p, n, G, ng, fq,
                              (long long)cells, c->kb.sh_cell, c->max_narr, c->allow_merging, (int32_t *)c->narr_d.p,
                              (ArrivalRec *)c->arr_d.p, c->sm_count, c->stream, false));
-    } else {
-        c->hits_d.ensure(nn * sizeof(EigenHitRec));
-        c->hitfield_d.ensure(nn * sizeof(int32_t));
-        CK(launch_eigen_emit(c->sorted_vals, (const ArrCand *)c->cand.p, n, (EigenHitRec *)c->hits_d.p,
-                             (int32_t *)c->hitfield_d.p, c->kb.sh_cell, c->sorted_keys, c->sm_count, c->stream));
-        c->hits_h.resize(n);
-        std::vector<int32_t> fld(n);
-        if(n) {
-            CK(cudaMemcpyAsync(c->hits_h.data(), c->hits_d.p, n * sizeof(EigenHitRec), cudaMemcpyDeviceToHost,
-                               c->stream));
-            CK(cudaMemcpyAsync(fld.data(), c->hitfield_d.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        if(c->also_eigen) {
+            CK(cudaStreamSynchronize(c->stream));   // the replay reads the candidates the eigen pass rewrites
+            n = gather_sorted(c, c->kb_eig);
+            emit_eigen_hits(c, n, c->kb_eig);
         }
-        CK(cudaStreamSynchronize(c->stream));
-        c->hit_begin.assign(c->fields.size() + 1, 0);
-        for(size_t k = 0; k < n; ++k) c->hit_begin[fld[k] + 1]++;
-        for(size_t f = 0; f < c->fields.size(); ++f) c->hit_begin[f + 1] += c->hit_begin[f];
+    } else {
+        emit_eigen_hits(c, n, c->kb);
     }
     CK(record_event(c, 2, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -927,7 +981,7 @@ void run_arrivals(bhcb_ctx *c)
     CK(cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]));
     c->stats.influence_ms = t1;
     c->stats.total_ms = c->stats.trace_ms + t1;
-    c->stats.evals = n;
+    c->stats.evals = nevals;
 }
 
 // TL runs whose segments do not fit in max_memory at once: trace the groups in
@@ -1073,7 +1127,7 @@ void write_arrivals(bhcb_ctx *c, const Field &F, const EnvSlot &S, const EnvTabl
                        arr.size() * sizeof(ArrivalRec), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const double RadDeg = 180.0 / 3.14159265358979323846;
-    const bool ascii = T.run_type[0] == 'A';
+    const bool ascii = T.run_type[0] == 'A' || T.run_type[0] == 'V';
     std::ofstream o(path, std::ios::binary);
     if(!o.good()) throw std::runtime_error("cannot open " + path);
     int nrz = (int)T.rz.size(), nrr = F.nrr, nsz = F.nsz;
@@ -1325,7 +1379,7 @@ int bhcb_launch(bhcb_ctx *c)
             run_rays(c);
             return BHCB_OK;
         }
-        if(c->mode == MODE_EIGEN) c->rays.assign(c->fields.size(), RaySet{});
+        if(c->mode == MODE_EIGEN || c->also_eigen) c->rays.assign(c->fields.size(), RaySet{});
         launch_step(c);
         return BHCB_OK;
     });
@@ -1356,7 +1410,7 @@ int bhcb_run(bhcb_ctx *c)
             run_rays(c);
             return BHCB_OK;
         }
-        if(c->mode == MODE_EIGEN) c->rays.assign(c->fields.size(), RaySet{});
+        if(c->mode == MODE_EIGEN || c->also_eigen) c->rays.assign(c->fields.size(), RaySet{});
         return run_checked(c);
     });
 }
@@ -1499,7 +1553,7 @@ int bhcb_eigen_hits(bhcb_ctx *c, int32_t env, int32_t ifreq, bhcb_eigen_hit *hit
             if(nhits) *nhits = n;
             return BHCB_OK;
         }
-        if(c->mode != MODE_EIGEN || !c->prepared) throw StateError("no eigen-hit run");
+        if((c->mode != MODE_EIGEN && !c->also_eigen) || !c->prepared) throw StateError("no eigen-hit run");
         if(env < 0 || env >= (int)c->envs.size()) throw std::invalid_argument("env_index out of range");
         const EnvSlot &S = c->envs[env];
         if(ifreq < 0 || ifreq >= (int)S.field_of_freq.size()) throw std::invalid_argument("ifreq out of range");
@@ -1534,6 +1588,10 @@ int bhcb_writeout(bhcb_ctx *c, int32_t env, int32_t ifreq, const char *root)
             const Field *F = find_field(c, env, ifreq);
             const EnvSlot &S = c->envs[env];
             write_arrivals(c, *F, S, S.tables[ifreq], S.freqs[ifreq], std::string(root) + ".arr");
+            if(c->also_eigen) {   // and the eigenrays (src/api.cpp:465-486)
+                const int fi = (int)(F - c->fields.data());
+                write_rays(c, *F, eigen_rays(c, fi), std::string(root) + ".ray");
+            }
             return BHCB_OK;
         }
         const Field *F = find_field(c, env, ifreq);
@@ -1644,11 +1702,11 @@ int bhcb_rays_shape(bhcb_ctx *c, int32_t env, int32_t ifreq, int64_t *nrays, int
             if(npoints) *npoints = np;
             return BHCB_OK;
         }
-        if(c->mode != MODE_RAY && c->mode != MODE_EIGEN)
-            throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E')");
+        if(c->mode != MODE_RAY && c->mode != MODE_EIGEN && !c->also_eigen)
+            throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E', 'V', 'v')");
         const Field *F = find_field(c, env, ifreq);
         const int fi = (int)(F - c->fields.data());
-        const RaySet &R = c->mode == MODE_EIGEN ? eigen_rays(c, fi) : c->rays[fi];
+        const RaySet &R = c->mode != MODE_RAY ? eigen_rays(c, fi) : c->rays[fi];
         if(!R.valid) throw StateError("no rays: run first");
         if(nrays) *nrays = (int64_t)R.jobs.size();
         if(npoints) *npoints = (int64_t)(R.rz.size() / 2);
@@ -1666,11 +1724,11 @@ int bhcb_copy_rays(bhcb_ctx *c, int32_t env, int32_t ifreq, int32_t *npts, int32
             run3_copy_rays(c->r3, env, c->stream, npts, bounces, alpha_deg, rz, rz_bytes);
             return BHCB_OK;
         }
-        if(c->mode != MODE_RAY && c->mode != MODE_EIGEN)
-            throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E')");
+        if(c->mode != MODE_RAY && c->mode != MODE_EIGEN && !c->also_eigen)
+            throw StateError("rays exist for 2-D ray runs ('R') and eigen runs ('E', 'V', 'v')");
         const Field *F = find_field(c, env, ifreq);
         const int fi = (int)(F - c->fields.data());
-        const RaySet &R = c->mode == MODE_EIGEN ? eigen_rays(c, fi) : c->rays[fi];
+        const RaySet &R = c->mode != MODE_RAY ? eigen_rays(c, fi) : c->rays[fi];
         if(!R.valid) throw StateError("no rays: run first");
         if(rz && rz_bytes < R.rz.size() * sizeof(double)) throw std::invalid_argument("rz buffer too small");
         if(npts) std::memcpy(npts, R.npts.data(), R.npts.size() * sizeof(int32_t));

@@ -711,10 +711,6 @@ EnvTables preprocess(const EnvInput &in, double freq)
     t.component = in.component;
     if(!ray_run && (bt == 'C' || bt == 'R') && (in.nimage < 1 || in.nimage > 3))
         env_error("Cerveny beams: the number of images must be 1, 2 or 3");
-    // ray-centred, Cerveny and simple Gaussian beams are TL-only in this build
-    if(!ray_run && (bt == 'g' || bt == 'b' || bt == 'S') && t.run_type[0] != 'C' && t.run_type[0] != 'S'
-       && t.run_type[0] != 'I')
-        env_error(std::string("beam type '") + bt + "' with arrivals or eigenrays is not supported by this build");
 
     char st = in.top_opt[0];
     switch(st) {

@@ -460,6 +460,27 @@ __device__ __forceinline__ bool geo_core(const XSeg &S, double s, double n1, dou
     return true;
 }
 
+// InfluenceGeoCore's beam test and the parts ApplyContribution hands to
+// AddArr / RecordEigenHit (src/influence.hpp:432-451, 897-1024): amplitude
+// cnst w, phase and complex delay; false outside the beam.
+__device__ __forceinline__ bool geo_parts(const XSeg &S, double s, double n1, double freq, bool gauss, double &amp,
+                                          double &ph, double &dr, double &di)
+{
+    const double qF = S.q0r + s * S.dqr;
+    double sigma = fabs(qF * S.rcp_q0);
+    const double sig0 = sigma;
+    if(gauss) sigma = max(sigma, min(FLTD(0.2) * freq * S.tau1r, BHCB_PI * (S.c0 / freq)));   // AdjustSigma
+    if(n1 >= (gauss ? 4.0 : 1.0) * sigma) return false;
+    const double cnst = S.amp / sqrt(fabs(qF));
+    const double w = gauss ? exp(FLTD(-0.5) * (n1 / sigma) * (n1 / sigma)) * (sig0 / sigma) : (sigma - n1) / sigma;
+    amp = cnst * w;
+    const bool caustic = (qF <= 0.0 && S.q0r > 0.0) || (qF >= 0.0 && S.q0r < 0.0);
+    ph = caustic ? S.ph_b : S.ph_a;
+    dr = S.tau0r + s * S.dtaur;
+    di = S.tau0i + s * S.dtaui;
+    return true;
+}
+
 // FlipBeamForImage / FlipNormalForImage (src/influence.hpp:362-377)
 __device__ __forceinline__ V2<double> flip_x(V2<double> x, int image, const EnvDev &e)
 {
@@ -617,6 +638,109 @@ template<int KIND> __global__ void __launch_bounds__(128) influence_x_kernel(
     if((threadIdx.x & 31) == 0 && evals) atomicAdd(&ctr->nevals, (unsigned long long)evals);
 }
 
+// Arrival candidates (RunType 'A' / 'a') and eigen hits ('E') of the
+// ray-centred geometric ('g', 'b') and simple Gaussian ('S') records, one
+// thread per (record, receiver depth), in the form arrivals.cu sorts and
+// replays: ArrCand with the key (receiver cell, ray, step) for AddArr, or
+// (field, ray, step, walk) for RecordEigenHit, the walk restating the
+// reference's loop order within a step: receiver depth, then the ranges from
+// A towards B for ray-centred beams (src/influence.hpp:1088-1180); the
+// receiver range, then the depth for simple Gaussian beams, which reach only
+// depths within RadMax of the ray when the run is not TL (src/influence.hpp:
+// 1440-1480). COUNT: only counts (ctr->nevals).
+template<int KIND, bool COUNT> __global__ void __launch_bounds__(128) arr_gather_x_kernel(
+    const XSeg *__restrict__ segs, unsigned long long cap, const GroupDev *__restrict__ groups, int ngroups,
+    const double *__restrict__ freqs, ArrCand *cands, uint64_t *keys, uint32_t *vals, unsigned long long cand_cap,
+    unsigned long long *cursor, RunCounters *ctr, ArrKeyBits kb, int nzmax)
+{
+    const unsigned long long nseg = min(__ldcg(&ctr->nseg), cap);
+    const unsigned long long nitems = nseg * (unsigned long long)nzmax;
+    unsigned long long count = 0;
+    for(unsigned long long it = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; it < nitems;
+        it += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = it / (unsigned)nzmax;
+        const int iz = (int)(it - k * (unsigned)nzmax);
+        const XSeg &S = segs[k];
+        if(S.job < 0) continue;
+        const GroupDev &G = groups[find_group(groups, ngroups, S.job)];
+        const EnvDev &e = *G.env;
+        if(iz >= e.nrz_per_range) continue;
+        const int local = (int)((long long)S.job - G.job_base);
+        const int nal = e.isingle > 0 ? 1 : e.nalpha;
+        const int isz = local / nal;
+        const int ialpha = e.isingle > 0 ? e.isingle - 1 : local % nal;
+        const double freq = freqs[G.freq_base];
+        const double zR = (double)e.rz[iz];
+        auto emit = [&](int ir, int hi_walk, int lo_walk, double amp, double ph, double dr, double di) {
+            if(COUNT) {
+                ++count;
+                return;
+            }
+            const unsigned long long i = atomicAdd(cursor, 1ull);
+            if(i >= cand_cap) return;
+            ArrCand c;
+            uint64_t key;
+            if(kb.eigen) {
+                key = ((uint64_t)G.field_index << kb.sh_cell) | ((uint64_t)local << kb.sh_job)
+                      | ((uint64_t)S.is << kb.sh_is) | ((uint64_t)hi_walk << kb.sh_walk) | (uint64_t)lo_walk;
+                c.amp = c.phase = c.delay_re = c.delay_im = 0.0;
+                c.rcvr_decl = 0.f;
+                c.ntop = S.is;      // eigen: step index
+                c.nbot = ir;        // eigen: receiver range index
+                c.job = iz | (isz << 20);
+            } else {
+                const long long cell = G.field_base + ((long long)isz * e.nrz_per_range + iz) * e.nrr + ir;
+                key = ((uint64_t)cell << kb.sh_cell) | ((uint64_t)local << kb.sh_job) | (uint64_t)S.is;
+                c.amp = amp;
+                c.phase = ph;
+                c.delay_re = dr;
+                c.delay_im = di;
+                c.rcvr_decl = (float)S.rcvr_decl;
+                c.ntop = S.ntop;
+                c.nbot = S.nbot;
+                c.job = S.job;
+            }
+            c.aux = ialpha;
+            c.rcvr_azim = 0.f;
+            cands[i] = c;
+            keys[i] = key;
+            vals[i] = (uint32_t)i;
+        };
+        if(KIND == INFL_GEO_RAYCEN) {
+            double nA, rA, nB, rB;
+            int irA, irB;
+            if(!S.valid) {
+                nA = 1e10;
+                rA = 1e10;
+                irA = 0;
+            } else {
+                n_r_ir(nA, rA, irA, mk2(S.xa, S.za), mk2(S.nxa, S.nza), zR, e);
+            }
+            n_r_ir(nB, rB, irB, mk2(S.xb, S.zb), mk2(S.nxb, S.nzb), zR, e);
+            if(irA == irB) continue;
+            const int up = irB <= irA ? 0 : 1;
+            int walk = 0;
+            for(int ir = irA + up; ir != irB + up; ir += 2 * up - 1, ++walk) {
+                const double s = (e.rr[ir] - rA) / (rB - rA);
+                const double n1 = fabs(nA + s * (nB - nA));
+                double amp, ph, dr, di;
+                if(geo_parts(S, s, n1, freq, e.gaussian, amp, ph, dr, di)) emit(ir, iz, walk, amp, ph, dr, di);
+            }
+        } else {   // INFL_SGB
+            const double deltaz = zR - S.zb;
+            if(!(fabs(deltaz) < S.radmax)) continue;
+            const double cpa = fabs(deltaz * S.drab) / sqrt(S.drab * S.drab + S.dzab * S.dzab);
+            const double ds = sqrt(deltaz * deltaz - cpa * cpa);
+            const double sx1 = S.sint + ds;
+            const double thet = atan(cpa / sx1);
+            const double cnst = S.amp / sqrt(sx1);
+            const double w = exp(-S.sgb_a * thet * thet);
+            emit(S.ir, S.ir, iz, cnst * w, S.ph_a, S.tau0r + S.t1y * deltaz, S.tau0i);
+        }
+    }
+    if(COUNT && count) atomicAdd(&ctr->nevals, count);
+}
+
 // ScalePressure, 2-D (src/influence.hpp:1556-1627, with PostProcessTL's
 // source sound speed, src/mode/tl.cpp:106-180) fused with the transpose
 // acc[f][isz][ir][iz] -> out[f][isz][iz][ir].
@@ -717,6 +841,34 @@ cudaError_t launch_influence_x(const XSeg *segs, unsigned long long cap, const G
         influence_x_kernel<INFL_SGB><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, freqs, acc, ctr, nzmax);
         break;
     default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_arr_gather_x(const XSeg *segs, unsigned long long cap, const GroupDev *groups, int ngroups,
+                                const double *freqs, int kind, bool count, ArrCand *cands, uint64_t *keys,
+                                uint32_t *vals, unsigned long long cand_cap, unsigned long long *cursor,
+                                RunCounters *ctr, ArrKeyBits kb, int nzmax, int grid, cudaStream_t st)
+{
+    if(nzmax < 1) nzmax = 1;
+    if(kind == INFL_GEO_RAYCEN) {
+        if(count)
+            arr_gather_x_kernel<INFL_GEO_RAYCEN, true><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, freqs, cands,
+                                                                             keys, vals, cand_cap, cursor, ctr, kb,
+                                                                             nzmax);
+        else
+            arr_gather_x_kernel<INFL_GEO_RAYCEN, false><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, freqs,
+                                                                              cands, keys, vals, cand_cap, cursor,
+                                                                              ctr, kb, nzmax);
+    } else if(kind == INFL_SGB) {
+        if(count)
+            arr_gather_x_kernel<INFL_SGB, true><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, freqs, cands, keys,
+                                                                      vals, cand_cap, cursor, ctr, kb, nzmax);
+        else
+            arr_gather_x_kernel<INFL_SGB, false><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, freqs, cands,
+                                                                       keys, vals, cand_cap, cursor, ctr, kb, nzmax);
+    } else {
+        return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }

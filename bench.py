@@ -240,6 +240,40 @@ def time_c4(B, tmp, rank, runs=3):
     return out
 
 
+def run_gemm(dims, warmup, launches=20):
+    """The surrogate's tcgen05 GEMM (bhcb_nn_gemm) on random bf16 operands:
+    C[M][N] = A[M][K] B[N][K]^T + bias with the given epilogue (default bf16
+    output), timed with CUDA events over `launches` launches after `warmup`."""
+    import torch
+    from bellhopcuda_b200 import surrogate as S
+    M, N, K = dims[:3]
+    epi = dims[3] if len(dims) > 3 else S.EPI_BF16
+    ops = S._Ops()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(M, K, device="cuda", generator=g).bfloat16()
+    Bm = torch.randn(N, K, device="cuda", generator=g).bfloat16()
+    out = torch.empty(M, N, device="cuda", dtype=torch.float32 if epi == S.EPI_F32 else torch.bfloat16)
+    bias = torch.zeros(N, device="cuda")
+    aux = torch.empty(M, N, device="cuda", dtype=torch.bfloat16) if epi in (S.EPI_GELU, S.EPI_DGELU) else None
+    kw = {"aux_out": aux} if epi == S.EPI_GELU else ({"aux_in": aux} if epi == S.EPI_DGELU else {})
+    if aux is not None:
+        aux.zero_()
+    for _ in range(max(warmup, 1)):
+        ops.gemm(A, Bm, out, epi, bias=bias, **kw)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(launches):
+        ops.gemm(A, Bm, out, epi, bias=bias, **kw)
+    e1.record()
+    torch.cuda.synchronize()
+    ops.check()
+    ms = e0.elapsed_time(e1) / launches
+    print(json.dumps({"gemm": [M, N, K], "epilogue": epi, "ms": ms, "tflops": 2.0 * M * N * K / (ms * 1e-3) / 1e12,
+                      "launches": launches}))
+    return 0
+
+
 def time_e2e(B, torch, root, freqs, steps, gpu, tune=None):
     """Same metric through the public C ABI with host buffers: setup reads the
     files, prepare uploads the tables, run, and every field copied back to
@@ -368,6 +402,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 3-D (C4) TL timing")
+    ap.add_argument("--gemm", type=int, nargs="+", metavar="M N K [EPI]",
+                    help="time the surrogate's tensor-core GEMM (bhcb_nn_gemm) alone and exit")
     ap.add_argument("--rays", type=int, default=0,
                     help="profiling only: trace this many rays of the fan instead of 20001 (the line says so)")
     ap.add_argument("--profile", action="store_true",
@@ -381,6 +417,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.gemm:
+        return run_gemm(args.gemm, args.warmup)
 
     import torch
     import bellhopcuda_b200 as B

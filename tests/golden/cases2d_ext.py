@@ -205,4 +205,18 @@ CASES2D_EXT = {
     # simple Gaussian beams ('S')
     "x2d_sgb_munk": lambda: _munk_small("CS RR "),
     "x2d_sgb_shallow_incoherent": lambda: _shallow_small("IS RR "),
+    # arrivals (binary .arr) and eigen hits (the .ray of the re-traced hit rays)
+    # with ray-centred geometric and simple Gaussian beams
+    "x2d_arr_raycen_hat_munk": lambda: _munk_small("ag RR ", nrz=11, nrr=21),
+    "x2d_arr_raycen_gauss_shallow": lambda: _shallow_small("ab RR ", nrz=6, nrr=11, nalpha=151),
+    "x2d_arr_sgb_munk": lambda: _munk_small("aS RR ", nrz=6, nrr=11),
+    "x2d_arr_sgb_shallow": lambda: _shallow_small("aS RR ", nrz=6, nrr=11, nalpha=151),
+    "x2d_eig_raycen_hat_munk": lambda: _munk_small("Eg RR ", nrz=3, rz=(800.0, 3000.0), nrr=4, rr_km=(20.0, 50.0)),
+    "x2d_eig_raycen_gauss_shallow": lambda: _shallow_small("Eb RR ", nrz=3, rz=(25.0, 75.0), nrr=3,
+                                                           rr_km=(3.0, 7.0)),
+    "x2d_eig_sgb_munk": lambda: _munk_small("ES RR ", nrz=3, rz=(800.0, 3000.0), nrr=4, rr_km=(20.0, 50.0)),
+    # arrivals and eigen hits in one run ('v': binary .arr and the .ray of the hits)
+    "x2d_arr_v_cart_hat_munk": lambda: _munk_small("vG RR ", nrz=3, rz=(800.0, 3000.0), nrr=4, rr_km=(20.0, 50.0)),
+    "x2d_arr_v_raycen_gauss_shallow": lambda: _shallow_small("vb RR ", nrz=3, rz=(25.0, 75.0), nrr=3,
+                                                             rr_km=(3.0, 7.0)),
 }

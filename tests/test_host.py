@@ -102,13 +102,13 @@ def test_reader_rejects_bad_box(workdir):
 
 def test_reader_rejects_unsupported_beam(workdir):
     """Cerveny beams are TL-only (as in the reference); ray-centred and simple
-    Gaussian beams with arrivals are outside this build."""
+    Gaussian beams take arrivals and eigen runs."""
     root = _write(workdir, "cerveny", run_type="AC RR ")
     with pytest.raises(B.BhcbError, match="does not support eigenrays or arrivals"):
         B.check_env(root)
-    root = _write(workdir, "raycen_arr", run_type="Ag RR ")
-    with pytest.raises(B.BhcbError, match="not supported"):
-        B.check_env(root)
+    for rt in ("Ag RR ", "ab RR ", "ES RR "):
+        root = _write(workdir, "x_" + rt[:2], run_type=rt)
+        assert B.check_env(root)["run_type"].startswith(rt[:2])
 
 
 def test_reader_missing_file(workdir):
@@ -167,8 +167,11 @@ def test_reader2d_ext_sizes_match_reference_fixture(name, workdir):
     root = os.path.join(workdir, name)
     write_fixture_files(g, root)
     info = B.check_env(root)
-    nsz, nrz, nrr = g["field"].shape
-    assert (info["nsz"], info["nrz"], info["nrr"]) == (nsz, nrz, nrr)
+    if "field" in g.files:          # TL: the .shd grid
+        nsz, nrz, nrr = g["field"].shape
+        assert (info["nsz"], info["nrz"], info["nrr"]) == (nsz, nrz, nrr)
+    elif "narr" in g.files:         # arrivals: the .arr grid
+        assert (info["nsz"], info["nrz"], info["nrr"]) == (len(g["sz"]), len(g["rz"]), len(g["rr"]))
     assert info["nalpha"] > 0
 
 
