@@ -1051,9 +1051,7 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
         env_error(std::string("3-D beam type '") + bt + "' is not supported by this build (geometric 'G', 'B', 'g', 'b')");
     if(!ray_run3 && (bt == 'g' || bt == 'b') && t.run_type[0] != 'C' && t.run_type[0] != 'S' && t.run_type[0] != 'I')
         env_error("3-D ray-centred beams with arrivals or eigenrays are not supported by this build");
-    if(t.nx2d) {   // Nx2D: ray, TL and arrival runs with Cartesian geometric beams
-        if(t.run_type[0] == 'E')
-            env_error("Nx2D eigenray runs are not supported by this build (TL, arrival and ray runs are)");
+    if(t.nx2d) {   // Nx2D: ray, TL, arrival and eigen runs with Cartesian geometric beams
         if(!ray_run3 && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
             env_error(std::string("Nx2D beam type '") + bt + "' is not supported by this build (Cartesian 'G' / 'B')");
         if(t.beam_type[3] == 'S') env_error("Nx2D beam shift is not supported by this build");

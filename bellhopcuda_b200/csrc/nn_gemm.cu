@@ -32,6 +32,7 @@ namespace bhcb {
 namespace {
 
 constexpr int BM = 128, BN = 128, BK = 64, STAGES = 2;
+constexpr int GROUP_M = 16;  // tile rows per L2 group of the launch order (8192^3: 1094 -> 1143 TFLOP/s)
 constexpr int TILE_A = BM * BK * 2;   // 16 KiB
 constexpr int TILE_B = BN * BK * 2;
 constexpr int SMEM_BYTES = STAGES * (TILE_A + TILE_B) + 1024 + 256;
@@ -152,7 +153,22 @@ __global__ void __launch_bounds__(128, 3) gemm_tc_kernel(const __grid_constant__
     __shared__ int s_fail;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    // Tile order: the launch order walks groups of GROUP_M tile rows, a column
+    // of GROUP_M tiles at a time, so the CTAs resident together share GROUP_M
+    // panels of A and a band of B panels that fit in L2 (instead of every B
+    // panel against a few A rows).
+    int m_t, n_t;
+    {
+        const int num_m = (int)gridDim.y, num_n = (int)gridDim.x;
+        const int t = (int)blockIdx.y * num_n + (int)blockIdx.x;
+        const int per_group = GROUP_M * num_n;
+        const int first_m = (t / per_group) * GROUP_M;
+        const int gsz = min(num_m - first_m, GROUP_M);
+        const int r = t - (t / per_group) * per_group;
+        m_t = first_m + r % gsz;
+        n_t = r / gsz;
+    }
+    const int m0 = m_t * BM, n0 = n_t * BN;
     const int nk = (K + BK - 1) / BK;
     if(threadIdx.x == 0) {
         s_fail = 0;

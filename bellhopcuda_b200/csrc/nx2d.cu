@@ -502,7 +502,11 @@ __global__ void __launch_bounds__(128) influence_nx_kernel(const SegRec<double> 
 // candidates (ApplyContribution with itheta = ibeta and AddArr,
 // src/influence.hpp:434-451; ReceiverAngles 2-D form, src/influence.hpp:
 // 123-136: receiver azimuth = the source azimuth) keyed (receiver cell, ray,
-// step) for the shared radix sort and per-cell replay. One thread per record.
+// step) for the shared radix sort and per-cell replay. With kb.eigen, the same
+// contributions as eigen hits (RecordEigenHit with itheta = ibeta), keyed
+// (trace group, ray, step, walk position of the receiver range, bearing,
+// depth): the 2-D Cartesian walk visits the bracketed ranges towards point1,
+// then the depths (src/influence.hpp:1295-1406). One thread per record.
 // COUNT: counts into ctr->nevals; otherwise candidate i at atomicAdd(cursor).
 template<bool COUNT>
 __global__ void __launch_bounds__(128) arr_gather_nx_kernel(const SegRec<double> *__restrict__ segs,
@@ -553,6 +557,24 @@ __global__ void __launch_bounds__(128) arr_gather_nx_kernel(const SegRec<double>
                 }
                 const unsigned long long i = atomicAdd(cursor, 1ull);
                 if(i >= cand_cap) continue;
+                if(kb.eigen) {
+                    ArrCand c;
+                    c.amp = c.phase = c.delay_re = c.delay_im = 0.0;
+                    c.rcvr_decl = 0.f;
+                    c.ntop = S.is;                   // step
+                    c.nbot = ir;                     // receiver range
+                    c.job = S.job;
+                    c.aux = J.ibeta;                 // itheta = ibeta (src/influence.hpp:439)
+                    c.rcvr_azim = __int_as_float(iz);
+                    cands[i] = c;
+                    const int walk = S.tx > 0.0 ? ir : E.nrr - 1 - ir;
+                    const int gidx = (int)(&G - groups);
+                    keys[i] = ((uint64_t)gidx << kb.sh_cell) | ((uint64_t)local << kb.sh_job)
+                              | ((uint64_t)S.is << kb.sh_is) | ((uint64_t)walk << kb.sh_walk)
+                              | ((uint64_t)J.ibeta << kb.sh_theta) | (uint64_t)iz;
+                    vals[i] = (uint32_t)i;
+                    continue;
+                }
                 const double w = gauss ? exp(FLTD(-0.5) * (n1 / sigma) * (n1 / sigma)) * (sig0 / sigma)
                                        : (sigma - n1) / sigma;
                 const bool caustic = (qF <= 0.0 && S.q0 > 0.0) || (qF >= 0.0 && S.q0 < 0.0);

@@ -51,9 +51,10 @@ F_INFL = 40.0
 ORACLE_STEPS_PER_TRACE = 20993289
 ORACLE_EVALS_ALL_FREQS = 6440570521
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one full-size
-# influence launch (10 frequencies) of the current build, from the ncu capture
-# summarised in profiles/influence_kernel_rd_gauss.md (None until captured).
-INFLUENCE_DRAM_BYTES = None
+# influence launch (10 frequencies) of the current build: 863.68 MB read +
+# 506.92 MB written, from a one-pass ncu capture of the full workload
+# summarised in profiles/influence_kernel_rd_gauss.md.
+INFLUENCE_DRAM_BYTES = 863.68e6 + 506.92e6
 
 
 def log(*a):

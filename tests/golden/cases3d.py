@@ -236,6 +236,21 @@ def munk3d_nx2d_arr_gauss():
                        rr_range=(7, 5.0, 30.0))
 
 
+def munk3d_nx2d_eig_gauss():
+    """Nx2D eigen hits ('E'): the hits of each receiver bearing's plane
+    (itheta = ibeta), on a sparse receiver grid."""
+    return _munk_slice("EB   2", alpha=(121, -20.3, 20.3), theta=[0.0, 2.0, 5.0], nrz_range=(3, 800.0, 2800.0),
+                       rr_range=(4, 8.0, 26.0))
+
+
+def seamount3d_nx2d_arr_hat():
+    """Nx2D arrivals with hat beams over the seamount grid on four bearings
+    (reflections off the triangles projected on each plane)."""
+    f = seamount3d_gauss()
+    f[".env"] = f[".env"].replace("'CB   3'", "'aG   2'").replace("101\n0 10 /", "11\n0 10 /")
+    return f
+
+
 def seamount3d_nx2d_ray():
     f = seamount3d_ray()
     f[".env"] = f[".env"].replace("'R    3'", "'R    2'")
@@ -273,4 +288,6 @@ CASES3D = {
     "munk3d_nx2d_ray": munk3d_nx2d_ray,
     "seamount3d_nx2d_ray": seamount3d_nx2d_ray,
     "munk3d_nx2d_arr_gauss": munk3d_nx2d_arr_gauss,
+    "munk3d_nx2d_eig_gauss": munk3d_nx2d_eig_gauss,
+    "seamount3d_nx2d_arr_hat": seamount3d_nx2d_arr_hat,
 }
