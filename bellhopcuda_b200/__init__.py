@@ -28,6 +28,7 @@ PREC_MIXED = 1
 FLAG_SERIAL_INFLUENCE = 1   # BHCB_FLAG_SERIAL_INFLUENCE (the default)
 FLAG_OVERLAP_INFLUENCE = 2  # BHCB_FLAG_OVERLAP_INFLUENCE
 FLAG_NO_GRAPH = 4           # BHCB_FLAG_NO_GRAPH
+FLAG_PIPELINE = 8           # BHCB_FLAG_PIPELINE
 
 ERR_NAMES = {
     2: "BHC_ERR_RAYINIT", 3: "BHC_ERR_BOUNDARY_SEG_CONTAINS_NAN",
@@ -252,10 +253,11 @@ class Tracer:
 
     def __init__(self, gpu: int = 0, precision: int = PREC_MIXED, max_memory: int = 0,
                  share_trajectory: bool = True, serial_influence: bool = False, overlap_influence: bool = False,
-                 graphs: bool = True):
+                 graphs: bool = True, pipeline: bool = False):
         self._lib = load_library()
         flags = (FLAG_SERIAL_INFLUENCE if serial_influence else 0) | \
-            (FLAG_OVERLAP_INFLUENCE if overlap_influence else 0) | (0 if graphs else FLAG_NO_GRAPH)
+            (FLAG_OVERLAP_INFLUENCE if overlap_influence else 0) | (0 if graphs else FLAG_NO_GRAPH) | \
+            (FLAG_PIPELINE if pipeline else 0)
         init = Init(gpu, precision, max_memory, 1 if share_trajectory else 0, flags, None)
         h = C.c_void_p()
         rc = self._lib.bhcb_open(C.byref(init), C.byref(h))

@@ -135,6 +135,19 @@ struct bhcb_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;   // influence launches beside the trace
     bool overlap = false;             // mixed TL runs: influence overlaps the trace (BHCB_FLAG_OVERLAP_INFLUENCE)
+    // pipelined TL steps (BHCB_FLAG_PIPELINE): slot k % 2 of launch k; slot 0
+    // uses segs / counters / acc, slot 1 the pipe_* buffers
+    bool pipeline = false;
+    cudaStream_t pstream[3] = {nullptr, nullptr, nullptr};   // trace streams of slots 0 / 1, influence stream
+    DevBuf pipe_segs, pipe_counters, pipe_acc;
+    // per slot: 0 trace start, 1 trace end, 2 influence start, 3 influence end, 4 scale end
+    cudaEvent_t pev[2][5] = {};
+    cudaEvent_t pev_ctx = nullptr;    // the context stream's position at the first launch
+    cudaEvent_t pev_pair = nullptr;   // scale end of the last launch of the previous pair
+    long long pipe_k = 0;             // launches since the last prepare
+    bool pipe_inflight = false;       // launches not yet waited for by bhcb_sync
+    int pipe_used = 0;                // slots (bit mask) launched since the last bhcb_sync
+    int pipe_last = 0;                // slot of the last launch
     // the serial TL step captured once into a CUDA graph and replayed
     bool use_graphs = true;
     int graph_state = 0;              // 0: next launch direct, 1: next launch captures, 2: replay
@@ -631,11 +644,92 @@ void do_launch(bhcb_ctx *c, bool host_driven)
 
 void drop_graph(bhcb_ctx *c)
 {
+    // pipelined launches in flight finish first (their slots are rebuilt)
+    for(auto &st : c->pstream)
+        if(st) cudaStreamSynchronize(st);
+    c->pipe_inflight = false;
+    c->pipe_k = 0;
     if(c->lexec) cudaGraphExecDestroy(c->lexec);
     if(c->lgraph) cudaGraphDestroy(c->lgraph);
     c->lexec = nullptr;
     c->lgraph = nullptr;
     c->graph_state = 0;
+}
+
+// Pipelined TL step (BHCB_FLAG_PIPELINE), geometric Cartesian beams.
+// Launches go in pairs: launches 2j and 2j + 1 trace at the same time (each on
+// its own stream, into its own slot: segment records, counters, accumulator),
+// then their influence and ScalePressure run one after the other on the
+// influence stream, and the next pair's traces wait for the pair's last
+// scale. Two latency-bound traces share the SMs well (each issues on a few
+// per cent of the cycles), while a trace beside an influence launch is
+// starved of issue slots, so traces never overlap influences. The context
+// stream waits for each launch's fields.
+void launch_pipelined(bhcb_ctx *c)
+{
+    const bool fp64 = c->precision == BHCB_PREC_FP64;
+    const int P = (int)(c->pipe_k & 1);
+    const size_t seg_bytes = (size_t)c->seg_cap * seg_record_bytes(fp64);
+    const size_t ctr_bytes = sizeof(RunCounters) + 64;
+    const size_t acc_bytes = (size_t)std::max<int64_t>(c->total_acc, 1) * sizeof(float2);
+    if(P == 1) {
+        c->pipe_segs.ensure(seg_bytes);
+        c->pipe_counters.ensure(ctr_bytes);
+        c->pipe_acc.ensure(acc_bytes);
+    }
+    void *segs = P ? c->pipe_segs.p : c->segs.p;
+    RunCounters *ctr = (RunCounters *)(P ? c->pipe_counters.p : c->counters.p);
+    float2 *acc = (float2 *)(P ? c->pipe_acc.p : c->acc.p);
+    unsigned long long *jobc = (unsigned long long *)((uint8_t *)ctr + sizeof(RunCounters));
+    cudaStream_t A = c->pstream[P], Bs = c->pstream[2];
+    cudaEvent_t *ev = c->pev[P];
+    if(!c->pipe_inflight) {   // the first launch follows the context stream's work
+        CK(cudaEventRecord(c->pev_ctx, c->stream));
+        for(auto st : c->pstream) CK(cudaStreamWaitEvent(st, c->pev_ctx, 0));
+    }
+    // the previous pair's influences are done (and with them the slot's last user)
+    if(c->pipe_k >= 2) CK(cudaStreamWaitEvent(A, c->pev_pair, 0));
+    CK(cudaEventRecord(ev[0], A));
+    CK(cudaMemsetAsync(ctr, 0, ctr_bytes, A));
+    CK(cudaMemsetAsync(&ctr->overflow_job, 0xff, sizeof(ctr->overflow_job), A));
+    CK(cudaMemsetAsync(acc, 0, acc_bytes, A));
+    const GroupDev *G = (const GroupDev *)c->groups_d.p;
+    const int ng = (int)c->groups_h.size();
+    const int tblock = c->trace_block;
+    unsigned int stage_bytes = 0;
+    for(int g = 0; g < ng; ++g) {
+        size_t off[ST_COUNT];
+        stage_bytes = std::max<unsigned int>(stage_bytes, (unsigned int)stage_plan(c->envdev_h[g], c->stage_cap, off));
+    }
+    const long long rays_per_cta = std::max(1, tblock * c->trace_lanes / 32);
+    long long tgrid = std::min<long long>((c->njobs + rays_per_cta - 1) / rays_per_cta, (long long)c->sm_count * 32);
+    if(tgrid < 1) tgrid = 1;
+    if(fp64)
+        CK(launch_trace<double>(G, ng, c->njobs, segs, c->seg_cap, ctr, jobc, nullptr, (int)tgrid, tblock, A,
+                                stage_bytes, c->trace_lanes));
+    else
+        CK(launch_trace<float>(G, ng, c->njobs, segs, c->seg_cap, ctr, jobc, nullptr, (int)tgrid, tblock, A,
+                               stage_bytes, c->trace_lanes));
+    CK(cudaEventRecord(ev[1], A));
+    CK(cudaStreamWaitEvent(Bs, ev[1], 0));
+    CK(cudaEventRecord(ev[2], Bs));
+    const int igrid = c->sm_count * c->influence_ctas_per_sm;
+    if(fp64)
+        CK(launch_influence<double>(segs, c->seg_cap, G, ng, (const double *)c->freqs_d.p, acc, ctr, c->gauss,
+                                    c->coherent, igrid, Bs));
+    else
+        CK(launch_influence<float>(segs, c->seg_cap, G, ng, (const double *)c->freqs_d.p, acc, ctr, c->gauss,
+                                   c->coherent, igrid, Bs));
+    CK(cudaEventRecord(ev[3], Bs));
+    CK(launch_scale(acc, (float2 *)c->out.p, G, ng, c->sm_count * 2, Bs));
+    CK(cudaEventRecord(ev[4], Bs));
+    if(P == 1) CK(cudaEventRecord(c->pev_pair, Bs));   // a pair ends
+    CK(cudaStreamWaitEvent(c->stream, ev[4], 0));
+    c->pipe_last = P;
+    c->pipe_used |= 1 << P;
+    ++c->pipe_k;
+    c->pipe_inflight = true;
+    c->last_overlapped = false;
 }
 
 // One step of a prepared batch. Serial TL steps run directly the first time
@@ -644,6 +738,10 @@ void drop_graph(bhcb_ctx *c)
 // changes the prepared state or the launch shape drops the graph.
 void launch_step(bhcb_ctx *c)
 {
+    if(c->pipeline && c->mode == MODE_TL && !c->xkind && !c->overlap) {
+        launch_pipelined(c);
+        return;
+    }
     const bool overlapped = c->overlap && c->precision != BHCB_PREC_FP64 && c->mode == MODE_TL;
     if(!c->use_graphs || overlapped || c->mode != MODE_TL || c->graph_state == 0) {
         do_launch(c, c->overlap);
@@ -685,10 +783,30 @@ float event_ms(cudaEvent_t a, cudaEvent_t b)
 int do_sync(bhcb_ctx *c)
 {
     CK(cudaStreamSynchronize(c->stream));
-    CK(cudaMemcpy(&c->last, c->counters.p, sizeof(RunCounters), cudaMemcpyDeviceToHost));
+    const bool piped = c->pipe_inflight;
+    if(piped) {   // the last pipelined launch: its slot's counters and events
+        for(auto &st : c->pstream) CK(cudaStreamSynchronize(st));
+        c->pipe_inflight = false;
+    }
+    const int used = c->pipe_used;
+    c->pipe_used = 0;
+    const int P = c->pipe_last;
+    CK(cudaMemcpy(&c->last, piped && P ? c->pipe_counters.p : c->counters.p, sizeof(RunCounters),
+                  cudaMemcpyDeviceToHost));
+    if(piped && (used & (1 << (P ^ 1)))) {   // the other slot's launch: its error and warning bits too
+        RunCounters o{};
+        CK(cudaMemcpy(&o, P ? c->counters.p : c->pipe_counters.p, sizeof(RunCounters), cudaMemcpyDeviceToHost));
+        c->last.err_bits |= o.err_bits;
+        c->last.warn_bits |= o.warn_bits;
+    }
     float t0 = event_ms(c->ev[0], c->ev[1]), t1 = 0, t2 = 0;
     float span = 0;
-    if(c->mode == MODE_TL) {
+    if(piped) {
+        t0 = event_ms(c->pev[P][0], c->pev[P][1]);
+        t1 = event_ms(c->pev[P][2], c->pev[P][3]);
+        t2 = event_ms(c->pev[P][0], c->pev[P][4]);
+        span = t1;
+    } else if(c->mode == MODE_TL) {
         t1 = event_ms(c->ev[1], c->ev[2]);
         t2 = event_ms(c->ev[0], c->ev[3]);
         span = c->last_overlapped ? event_ms(c->ev[4], c->ev[2]) : t1;
@@ -1225,6 +1343,7 @@ int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
         c->share = init->share_trajectory != 0;
         c->overlap = (init->flags & BHCB_FLAG_OVERLAP_INFLUENCE) != 0;
         c->use_graphs = (init->flags & BHCB_FLAG_NO_GRAPH) == 0;
+        c->pipeline = (init->flags & BHCB_FLAG_PIPELINE) != 0;
         c->output_cb = init->output_callback;
     }
     int ndev = 0;
@@ -1239,6 +1358,15 @@ int bhcb_open(const bhcb_init *init, bhcb_ctx **out)
     if(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) return BHCB_ERR_CUDA;
     for(auto &e : c->ev)
         if(cudaEventCreate(&e) != cudaSuccess) return BHCB_ERR_CUDA;
+    if(c->pipeline) {
+        for(auto &st : c->pstream)
+            if(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return BHCB_ERR_CUDA;
+        for(auto &row : c->pev)
+            for(auto &e : row)
+                if(cudaEventCreate(&e) != cudaSuccess) return BHCB_ERR_CUDA;
+        if(cudaEventCreateWithFlags(&c->pev_ctx, cudaEventDisableTiming) != cudaSuccess) return BHCB_ERR_CUDA;
+        if(cudaEventCreateWithFlags(&c->pev_pair, cudaEventDisableTiming) != cudaSuccess) return BHCB_ERR_CUDA;
+    }
     *out = c.release();
     return BHCB_OK;
 }
@@ -1250,12 +1378,21 @@ void bhcb_close(bhcb_ctx *c)
     if(c->stream) cudaStreamSynchronize(c->stream);
     drop_graph(c);
     if(c->stream2) cudaStreamSynchronize(c->stream2);
+    for(auto &st : c->pstream)
+        if(st) cudaStreamSynchronize(st);
     for(DevBuf *b : {&c->arena, &c->groups_d, &c->freqs_d, &c->acc, &c->out, &c->segs, &c->counters, &c->cand,
                      &c->keys0, &c->keys1, &c->vals0, &c->vals1, &c->hist, &c->narr_d, &c->arr_d, &c->hits_d,
-                     &c->hitfield_d, &c->blk_state, &c->scan})
+                     &c->hitfield_d, &c->blk_state, &c->scan, &c->pipe_segs, &c->pipe_counters, &c->pipe_acc})
         b->release();
     for(auto &e : c->ev)
         if(e) cudaEventDestroy(e);
+    for(auto &row : c->pev)
+        for(auto &e : row)
+            if(e) cudaEventDestroy(e);
+    if(c->pev_ctx) cudaEventDestroy(c->pev_ctx);
+    if(c->pev_pair) cudaEventDestroy(c->pev_pair);
+    for(auto &st : c->pstream)
+        if(st) cudaStreamDestroy(st);
     if(c->stream) cudaStreamDestroy(c->stream);
     if(c->stream2) cudaStreamDestroy(c->stream2);
     run3_free(c->r3);

@@ -179,12 +179,17 @@ def tl_rms(a, b):
 
 
 # ------------------------------------------------------------- our arm
-def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=None):
-    """Device time per step of the prepared run (tables resident in HBM): each
-    step replays the CUDA graph of trace + influence + scale that the first
-    two launches set up. tune: None to run the autotuner first (untimed), else a
-    shape to apply."""
-    t = B.Tracer(gpu=gpu, precision=precision)
+def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=None, pipeline=False):
+    """Device time per step of the prepared run (tables resident in HBM).
+    Serial: each step replays the CUDA graph of trace + influence + scale that
+    the first two launches set up, L2 flushed before each step, timed one by
+    one. Pipelined (BHCB_FLAG_PIPELINE): the `steps` launches go back to back,
+    the trace of each beside the influence of the previous one, timed as a
+    whole from the first launch to the last field; every step writes and reads
+    its own 655 MB of segment records (more than the 126 MB L2), and L2 is
+    flushed once before the first. tune: None to run the autotuner first
+    (untimed), else a shape to apply."""
+    t = B.Tracer(gpu=gpu, precision=precision, pipeline=pipeline)
     t.setup(root)
     t.set_frequencies(0, freqs)
     t.prepare()
@@ -194,21 +199,57 @@ def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=N
         t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"], tune.get("trace_lanes", 32))
         t.tuning = tune
     s = torch.cuda.ExternalStream(t.stream_ptr(), device=gpu)
+    if pipeline and tune is None:
+        # concurrent trace and influence share each SM's registers: pick the
+        # shape by timing pipelined launches (untimed tuning, like autotune)
+        best = None
+        base = dict(t.tuning)
+        for tb, k in ((base["trace_block"], base["influence_ctas_per_sm"]), (32, 6), (32, 5), (64, 6), (32, 4)):
+            t.set_tuning(tb, k, base["stage_kb"], base.get("trace_lanes", 32))
+            for _ in range(2):
+                t.launch()
+            t.sync()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(4):
+                t.launch()
+            e1.record(s)
+            t.sync()
+            ms = e0.elapsed_time(e1) / 4
+            if best is None or ms < best[0]:
+                best = (ms, tb, k)
+        t.tuning = dict(base, trace_block=best[1], influence_ctas_per_sm=best[2], chosen_by_pipeline=True)
+        t.set_tuning(best[1], best[2], base["stage_kb"], base.get("trace_lanes", 32))
     for _ in range(warmup):
         t.launch()
         t.sync()
     times, stats = [], []
-    for _ in range(steps):
+    if pipeline:
         with torch.cuda.stream(s):
-            flush.zero_()          # evict L2 (256 MiB > 126 MB) outside the timed window
+            flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        t.launch()
+        for _ in range(steps):
+            t.launch()
         e1.record(s)
         t.sync()
-        times.append(e0.elapsed_time(e1))
-        stats.append(t.stats())
+        total = e0.elapsed_time(e1)
+        times = [total / steps] * steps
+        stats = [t.stats()]
+    else:
+        for _ in range(steps):
+            with torch.cuda.stream(s):
+                flush.zero_()          # evict L2 (256 MiB > 126 MB) outside the timed window
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            t.launch()
+            e1.record(s)
+            t.sync()
+            times.append(e0.elapsed_time(e1))
+            stats.append(t.stats())
     fields = [t.field(0, i)[0] for i in range(len(freqs))]
     return t, times, stats, fields
 
@@ -403,6 +444,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 3-D (C4) TL timing")
+    ap.add_argument("--serial", action="store_true",
+                    help="time the steps one at a time (graph replay) instead of pipelined launches")
     ap.add_argument("--gemm", type=int, nargs="+", metavar="M N K [EPI]",
                     help="time the surrogate's tensor-core GEMM (bhcb_nn_gemm) alone and exit")
     ap.add_argument("--rays", type=int, default=0,
@@ -455,9 +498,10 @@ def main():
             return 0
         # ---- headline: mixed precision, shared trajectory
         barrier()
+        pipe = not args.serial
         with ClockSampler(local) as clk:
             t, times, stats, fields_mixed = time_arm(B, torch, root, freqs, B.PREC_MIXED, args.steps,
-                                                     args.warmup, local, flush)
+                                                     args.warmup, local, flush, pipeline=pipe)
             barrier()
         clocks = clk.summary()
         total_s = max_over_ranks(sum(times) / 1000.0)
@@ -466,11 +510,19 @@ def main():
         st = stats[-1]
         tuning = t.tuning
         t.close()
-        # ---- FP64 per-frequency tracer (the plain GPU trace)
+        # ---- the same steps one at a time (graph replay, L2 flushed before each)
+        serial = None
+        if pipe:
+            ts_, times_s, _, _ = time_arm(B, torch, root, freqs, B.PREC_MIXED, max(2, args.steps // 2),
+                                          args.warmup, local, flush, tune=tuning, pipeline=False)
+            ts_.close()
+            ms_s = max_over_ranks(statistics.mean(times_s))
+            serial = {"ms_per_step": ms_s, "value": world * nf * 1000.0 / ms_s,
+                      "launch": "one step at a time: CUDA graph replay of memsets + trace + influence + scale"}
         fp64 = None
         if not args.no_fp64:
             t64, times64, stats64, fields64 = time_arm(B, torch, root, freqs, B.PREC_FP64,
-                                                       max(1, args.steps // 2), 1, local, flush)
+                                                       max(2, args.steps // 2), 1, local, flush, pipeline=pipe)
             t64.close()
             ms64 = max_over_ranks(statistics.mean(times64))
             errs = [tl_rms(fields_mixed[i], fields64[i]) for i in range(nf)]
@@ -521,16 +573,23 @@ def main():
         "config": dict(CONFIG),
         "detail": {"frequencies_share_one_trajectory": True, "fields_per_step": nf, "rays": int(st["rays"]),
                    "steps_traced": int(st["steps"]), "contributions": int(st["evals"]),
-                   "l2": "flushed (256 MiB write) before every timed step",
+                   "l2": ("each step writes and reads its own 655 MB of segment records (> 126 MB L2); L2 flushed "
+                          "(256 MiB write) once before the timed steps") if pipe else
+                         "flushed (256 MiB write) before every timed step",
                    "parallelism": "replicas per GPU (one environment per rank)",
                    "launch_shape": {"trace_block": tuning["trace_block"],
                                     "influence_ctas_per_sm": tuning["influence_ctas_per_sm"],
                                     "stage_kb": tuning["stage_kb"],
                                     "trace_lanes": tuning.get("trace_lanes", 32),
-                                    "chosen_by": "bhcb_autotune before the warm-up (untimed)"}},
+                                    "chosen_by": "bhcb_autotune, then timed pipelined launches of five shapes "
+                                                 "(before the warm-up, untimed)" if tuning.get("chosen_by_pipeline")
+                                    else "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 3 * args.steps, "fp64_trace": fp64, "kernels": kernels, "c4_3d_tl": c4,
-        "launch": "CUDA graph replay of memsets + trace + influence + scale per step",
+        "launch": ("pipelined launches (BHCB_FLAG_PIPELINE): the trace of step k+1 beside the influence of step k "
+                   "on two streams, double-buffered segment records and accumulators; steps timed as a whole")
+                  if pipe else "CUDA graph replay of memsets + trace + influence + scale per step",
+        "serial_steps": serial,
     }
     if rank == 0:
         print(json.dumps(line))

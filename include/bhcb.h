@@ -52,6 +52,17 @@ enum { BHCB_PREC_FP64 = 0, BHCB_PREC_MIXED = 1 };
 #define BHCB_FLAG_OVERLAP_INFLUENCE 2
 /* Launch the kernels of every step directly instead of replaying a CUDA graph. */
 #define BHCB_FLAG_NO_GRAPH 4
+/* Pipelined TL steps (geometric Cartesian beams): successive bhcb_launch
+   calls of a prepared batch go in pairs whose two traces run at the same time
+   (internal streams, one buffer slot of segment records, counters and
+   accumulator each: twice their device memory), then their influence and
+   ScalePressure one after the other; the next pair's traces start when the
+   pair's last scale ends. bhcb_launch returns at once; work enqueued on the
+   context stream after a launch waits for that launch's fields; bhcb_sync
+   waits for every launch. The first launch after bhcb_prepare or bhcb_sync is
+   ordered after the work already on the context stream; later launches are
+   not, until the next bhcb_sync. */
+#define BHCB_FLAG_PIPELINE 8
 
 /* Context options; mirrors bhcInit (include/bhc/structs.hpp:490-546). */
 typedef struct bhcb_init {

@@ -78,3 +78,39 @@ def test_batched_step_graph_replays(precision, tmp_path):
                 for k in range(len(freqs[i])):
                     rms, n = tl_rms(t.field(i, k)[0], ref[i][k][0])
                     assert n > 100 and rms < 0.01, (step, i, k, rms)
+
+
+@pytest.mark.parametrize("precision", [B.PREC_MIXED, B.PREC_FP64])
+def test_pipelined_launches_match_serial(precision, workdir):
+    """BHCB_FLAG_PIPELINE: five launches back to back (the trace of one beside
+    the influence of the previous, two buffer slots), one sync; the fields
+    equal a serial run's (float atomics: 1e-5 of the field maximum) and the
+    counters are the last launch's."""
+    spec = W.munk_tl(nalpha=401, nrz=51, nrr=201, beam="B")
+    root = write_env(spec, os.path.join(workdir, "pipe_%d" % precision))
+    freqs = [50.0, 100.0, 200.0]
+    with B.Tracer(precision=precision) as t:
+        t.setup(root)
+        t.set_frequencies(0, freqs)
+        t.run()
+        ref = [t.field(0, i) for i in range(len(freqs))]
+        st_ref = t.stats()
+    with B.Tracer(precision=precision, pipeline=True) as t:
+        t.setup(root)
+        t.set_frequencies(0, freqs)
+        t.prepare()
+        for _ in range(5):
+            t.launch()
+        t.sync()
+        st = t.stats()
+        got = [t.field(0, i) for i in range(len(freqs))]
+        # and again after the sync (the first launch of an epoch)
+        t.launch()
+        t.sync()
+        again = [t.field(0, i) for i in range(len(freqs))]
+    assert st["err_bits"] == 0
+    assert st["steps"] == st_ref["steps"] and st["segments"] == st_ref["segments"]
+    for a, b, c in zip(got, ref, again):
+        tol = 1e-5 * np.abs(b).max()
+        np.testing.assert_allclose(a, b, rtol=0, atol=tol)
+        np.testing.assert_allclose(c, b, rtol=0, atol=tol)
