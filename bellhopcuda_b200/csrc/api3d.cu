@@ -19,6 +19,9 @@
 
 namespace bhcb {
 
+cudaError_t launch_arr_gather3d_rc(const XSeg3 *, unsigned long long, const GroupDev *, int, bool, ArrCand *,
+                                   uint64_t *, uint32_t *, unsigned long long, unsigned long long *, RunCounters *,
+                                   ArrKeyBits, int, int, cudaStream_t);
 cudaError_t launch_rays_nx(const GroupDev *, int, const long long *, const int *, int, const long long *, double *,
                            int *, int *, RunCounters *, bool, int, cudaStream_t);
 cudaError_t launch_rays3d(const GroupDev *, int, const long long *, const int *, int, const long long *, double *,
@@ -282,7 +285,8 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
     if(r->rayrun) return;   // trajectories only: no segments, fields or arrivals
     if(r->eigen) {
-        // ordering key (low to high): depth | bearing | walk position | step | ray | trace group
+        // ordering key (low to high): depth | bearing | walk position | step | ray | trace group;
+        // ray-centred beams walk depth, then bearing, then the ranges: walk | bearing | depth
         int mz = 1, mt = 1, mr = 1, mj = 1;
         for(const auto &S : r->envs) {
             mz = std::max(mz, (int)S.T.rz.size());
@@ -292,9 +296,10 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         for(const GroupDev &G : r->groups_h) mj = std::max(mj, G.njobs);
         ArrKeyBits kb{};
         kb.eigen = 1;
-        kb.sh_theta = bits((unsigned long long)mz);
+        const int lo = r->raycen ? mr : mz, hi = r->raycen ? mz : mr;
+        kb.sh_theta = bits((unsigned long long)lo);
         kb.sh_walk = kb.sh_theta + bits((unsigned long long)mt);
-        kb.sh_is = kb.sh_walk + bits((unsigned long long)mr);
+        kb.sh_is = kb.sh_walk + bits((unsigned long long)hi);
         kb.sh_job = kb.sh_is + bits(100000);   // steps per ray (MaxN)
         kb.sh_cell = kb.sh_job + bits((unsigned long long)mj);
         kb.total_bits = kb.sh_cell + bits((unsigned long long)r->groups_h.size());
@@ -359,6 +364,13 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
     // Nx2D: 2-D records on the bearing planes; 3-D: SegRec3
     auto gather = [&](bool count, ArrCand *c, uint64_t *k, uint32_t *v, unsigned long long cap,
                       unsigned long long *cur) {
+        if(r->raycen) {
+            int nzt = 1;   // (depth, bearing) pairs per record, the most of the batch
+            for(const auto &S : r->envs) nzt = std::max(nzt, (int)(S.T.rz.size() * S.T.theta.size()));
+            return launch_arr_gather3d_rc((const XSeg3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
+                                          (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, nzt,
+                                          sm_count * 16, st);
+        }
         return r->nx2d ? launch_arr_gather_nx(r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
                                               (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, igrid, st)
                        : launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,

@@ -1049,8 +1049,6 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     // ray runs trace geometric rays whatever the beam type (src/mode/ray.cpp:44-86)
     if(!ray_run3 && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' ' || bt == 'g' || bt == 'b'))
         env_error(std::string("3-D beam type '") + bt + "' is not supported by this build (geometric 'G', 'B', 'g', 'b')");
-    if(!ray_run3 && (bt == 'g' || bt == 'b') && t.run_type[0] != 'C' && t.run_type[0] != 'S' && t.run_type[0] != 'I')
-        env_error("3-D ray-centred beams with arrivals or eigenrays are not supported by this build");
     if(t.nx2d) {   // Nx2D: ray, TL, arrival and eigen runs with Cartesian geometric beams
         if(!ray_run3 && !(bt == 'G' || bt == 'B' || bt == '^' || bt == ' '))
             env_error(std::string("Nx2D beam type '") + bt + "' is not supported by this build (Cartesian 'G' / 'B')");

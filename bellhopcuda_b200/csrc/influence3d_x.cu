@@ -282,7 +282,128 @@ __global__ void __launch_bounds__(128) influence3d_rc_kernel(const XSeg3 *__rest
     if((threadIdx.x & 31) == 0 && evals) atomicAdd(&ctr->nevals, (unsigned long long)evals);
 }
 
+// Arrival candidates (RunType 'A' / 'a') and eigen hits ('E') of the same
+// contributions, one thread per (record, receiver depth, bearing), for the
+// shared sort and replay (arrivals.cu): arrivals keyed (receiver cell, ray,
+// step) with the receiver angles of the segment's direction (ReceiverAngles,
+// src/influence.hpp:123-138, rayt = point1.x - point0.x); eigen hits keyed
+// (trace group, ray, step, depth, bearing, walk position from A towards B),
+// the reference's loop order within a step (src/influence.hpp:1088-1180).
+// COUNT: counts into ctr->nevals; otherwise candidate i at atomicAdd(cursor).
+template<bool COUNT>
+__global__ void __launch_bounds__(128) arr_gather3d_rc_kernel(const XSeg3 *__restrict__ segs, unsigned long long cap,
+                                                              const GroupDev *__restrict__ groups, int ngroups,
+                                                              ArrCand *cands, uint64_t *keys, uint32_t *vals,
+                                                              unsigned long long cand_cap, unsigned long long *cursor,
+                                                              RunCounters *ctr, ArrKeyBits kb, int nzt)
+{
+    const unsigned long long nseg = min(__ldcg(&ctr->nseg), cap);
+    const unsigned long long nitems = nseg * (unsigned long long)nzt;
+    unsigned long long count = 0;
+    for(unsigned long long it = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; it < nitems;
+        it += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = it / (unsigned)nzt;
+        const int rem = (int)(it - k * (unsigned)nzt);
+        const XSeg3 &R = segs[k];
+        if(R.job < 0) continue;
+        const int g = find_group(groups, ngroups, R.job);
+        const GroupDev &G = groups[g];
+        const Env3Dev &E = *G.env3;
+        if(rem >= E.nrz * E.ntheta) continue;
+        const int iz = rem / E.ntheta, itheta = rem - iz * E.ntheta;
+        const double zR = (double)E.rz[iz];
+        const double tcx = E.tcs[2 * itheta], tcy = E.tcs[2 * itheta + 1];
+        double mA, nA, rA, mB, nB, rB;
+        int irA, irB;
+        if(!m_n_r_ir(R.x0, R.n1a, R.n2a, R.ta, R.xs, R.ys, zR, tcx, tcy, E, mA, nA, rA, irA)) continue;
+        if(!m_n_r_ir(R.x1, R.n1b, R.n2b, R.tb, R.xs, R.ys, zR, tcx, tcy, E, mB, nB, rB, irB)) continue;
+        if(E.gaussian) {
+            if(R.maxr_m <= min(fabs(mA), fabs(mB)) && mA * mB >= 0.0) continue;
+            if(R.maxr_n <= min(fabs(nA), fabs(nB)) && nA * nB >= 0.0) continue;
+        }
+        if(irA == irB) continue;
+        const int local = (int)(R.job - G.job_base);
+        const Job3 J = job_indices3(E, local);
+        const long long row = G.field_base
+            + ((((long long)J.isz * E.nsx + J.isx) * E.nsy + J.isy) * E.ntheta + itheta) * E.nrz * E.nrr
+            + (long long)iz * E.nrr;
+        const int up = irB <= irA ? 0 : 1;
+        int walk = 0;
+        for(int ir = irA + up; ir != irB + up; ir += 2 * up - 1, ++walk) {
+            const double s = (E.rr[ir] - rA) / (rB - rA);
+            const double n1 = fabs(nA + s * (nB - nA));
+            const double n2 = fabs(mA + s * (mB - mA));
+            double q00 = R.q0[0] + s * R.dq[0], q01 = R.q0[1] + s * R.dq[1];
+            double q10 = R.q0[2] + s * R.dq[2], q11 = R.q0[3] + s * R.dq[3];
+            q00 *= R.rcp_q0;
+            q10 *= R.rcp_q0;
+            q01 *= R.rcp_qhat0;
+            q11 *= R.rcp_qhat0;
+            const double qF = q00 * q11 - q10 * q01;
+            if(nearly_zero(qF)) continue;
+            const double n1p = fabs((-q01 * n2 + q11 * n1) / qF);
+            const double n2p = fabs((q00 * n2 - q10 * n1) / qF);
+            if(!E.gaussian && max(n1p, n2p) > 1.0) continue;
+            if(COUNT) {
+                ++count;
+                continue;
+            }
+            const unsigned long long i = atomicAdd(cursor, 1ull);
+            if(i >= cand_cap) continue;
+            ArrCand c;
+            uint64_t key;
+            if(kb.eigen) {
+                c.amp = c.phase = c.delay_re = c.delay_im = 0.0;
+                c.rcvr_decl = 0.f;
+                c.ntop = R.is;
+                c.nbot = ir;
+                c.job = R.job;
+                c.aux = itheta;
+                c.rcvr_azim = __int_as_float(iz);
+                key = ((uint64_t)g << kb.sh_cell) | ((uint64_t)local << kb.sh_job) | ((uint64_t)R.is << kb.sh_is)
+                      | ((uint64_t)iz << kb.sh_walk) | ((uint64_t)itheta << kb.sh_theta) | (uint64_t)walk;
+            } else {
+                const double w = E.gaussian ? exp(FLTD(-0.5) * (n1p * n1p + n2p * n2p))
+                                            : (FLTD(1.0) - n1p) * (FLTD(1.0) - n2p);
+                double ph = R.phase0;
+                if((qF <= 0.0 && R.qold > 0.0) || (qF >= 0.0 && R.qold < 0.0)) ph += BHCB_PI / FLTD(2.0);
+                const double tx = R.x1[0] - R.x0[0], ty = R.x1[1] - R.x0[1], tz = R.x1[2] - R.x0[2];
+                c.amp = R.cnst_num / sqrt(fabs(qF)) * w;
+                c.phase = ph;
+                c.delay_re = R.tau0r + s * R.dtaur;
+                c.delay_im = R.tau0i + s * R.dtaui;
+                c.rcvr_decl = (float)((180.0 / BHCB_PI) * atan2(tz, sqrt(tx * tx + ty * ty)));
+                c.rcvr_azim = (float)((180.0 / BHCB_PI) * atan2(ty, tx));
+                c.ntop = R.ntop;
+                c.nbot = R.nbot;
+                c.job = R.job;
+                c.aux = 0;
+                key = ((uint64_t)(row + ir) << kb.sh_cell) | ((uint64_t)local << kb.sh_job) | (uint64_t)R.is;
+            }
+            cands[i] = c;
+            keys[i] = key;
+            vals[i] = (uint32_t)i;
+        }
+    }
+    if(COUNT && count) atomicAdd(&ctr->nevals, count);
+}
+
 } // namespace
+
+cudaError_t launch_arr_gather3d_rc(const XSeg3 *segs, unsigned long long cap, const GroupDev *groups, int ngroups,
+                                   bool count, ArrCand *cands, uint64_t *keys, uint32_t *vals,
+                                   unsigned long long cand_cap, unsigned long long *cursor, RunCounters *ctr,
+                                   ArrKeyBits kb, int nzt, int grid, cudaStream_t st)
+{
+    if(nzt < 1) nzt = 1;
+    if(count)
+        arr_gather3d_rc_kernel<true><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, cands, keys, vals, cand_cap,
+                                                           cursor, ctr, kb, nzt);
+    else
+        arr_gather3d_rc_kernel<false><<<grid, 128, 0, st>>>(segs, cap, groups, ngroups, cands, keys, vals, cand_cap,
+                                                            cursor, ctr, kb, nzt);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_trace3d_rc(const GroupDev *groups, int ngroups, long long job_end, XSeg3 *segs,
                               unsigned long long cap, RunCounters *ctr, unsigned long long *job_counter, int grid,

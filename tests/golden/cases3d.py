@@ -236,6 +236,18 @@ def munk3d_nx2d_arr_gauss():
                        rr_range=(7, 5.0, 30.0))
 
 
+def munk3d_raycen_arr_gauss():
+    """Arrivals ('a') of Gaussian beams in ray-centred coordinates ('b'),
+    the depth / bearing / range walk of Step_InfluenceGeoRayCen."""
+    return _munk_slice("ab   3", nrz_range=(6, 500.0, 3000.0), rr_range=(7, 5.0, 30.0))
+
+
+def munk3d_raycen_eig_hat():
+    """Eigen hits ('E') of hat beams in ray-centred coordinates ('g')."""
+    return _munk_slice("Eg   3", alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0), theta=[0.0, 2.0, 5.0],
+                       nrz_range=(3, 800.0, 2800.0), rr_range=(4, 8.0, 26.0))
+
+
 def munk3d_nx2d_eig_gauss():
     """Nx2D eigen hits ('E'): the hits of each receiver bearing's plane
     (itheta = ibeta), on a sparse receiver grid."""
@@ -289,5 +301,7 @@ CASES3D = {
     "seamount3d_nx2d_ray": seamount3d_nx2d_ray,
     "munk3d_nx2d_arr_gauss": munk3d_nx2d_arr_gauss,
     "munk3d_nx2d_eig_gauss": munk3d_nx2d_eig_gauss,
+    "munk3d_raycen_arr_gauss": munk3d_raycen_arr_gauss,
+    "munk3d_raycen_eig_hat": munk3d_raycen_eig_hat,
     "seamount3d_nx2d_arr_hat": seamount3d_nx2d_arr_hat,
 }
