@@ -86,6 +86,8 @@ struct Run3 {
     bool ran = false;
     // arrivals runs (RunType 'A' / 'a') and eigen-hit runs ('E')
     bool arrivals = false, eigen = false;
+    bool also_eigen = false;          // 'V' / 'v': an arrivals run that also records the eigen hits
+    ArrKeyBits kb_eig{};              // the eigen pass of 'V' / 'v' runs
     std::vector<EigenHitRec> hits_h;   // in the reference's single-threaded order
     std::vector<int32_t> hit_group;    // environment of each hit
     DevBuf hits_d, hitgrp_d;
@@ -205,7 +207,8 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         e.coherent = T.run_type[0] == 'C';
         e.beam2 = T.beam_type[2];
         e.run0 = T.run_type[0];
-        e.arrivals = T.nx2d && (T.run_type[0] == 'A' || T.run_type[0] == 'a');   // records carry the receiver angle
+        e.arrivals = T.nx2d && (T.run_type[0] == 'A' || T.run_type[0] == 'a' || T.run_type[0] == 'V' ||
+                                T.run_type[0] == 'v');   // records carry the receiver angle
         d.hex = T.ssp_type == SSP_HEXAHEDRAL;
         d.hnx = (int)T.hx.size(); d.hny = (int)T.hy.size(); d.hnz = (int)T.hz.size();
         d.top = T.top;
@@ -265,10 +268,14 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     CK(cudaMemcpyAsync(r->groups_d.p, r->groups_h.data(), r->groups_h.size() * sizeof(GroupDev),
                        cudaMemcpyHostToDevice, st));
     r->counters.ensure(sizeof(RunCounters) + 64);
-    // one run type per batch: TL ('C', 'S', 'I'), arrivals ('A', 'a') or eigen hits ('E')
-    auto kind = [](char t) { return (t == 'A' || t == 'a') ? 1 : (t == 'E' ? 2 : (t == 'R' ? 3 : 0)); };
+    // one run type per batch: TL ('C', 'S', 'I'), arrivals ('A', 'a'), arrivals and
+    // eigen hits ('V', 'v') or eigen hits ('E')
+    auto kind = [](char t) {
+        return (t == 'A' || t == 'a') ? 1 : (t == 'V' || t == 'v') ? 4 : (t == 'E' ? 2 : (t == 'R' ? 3 : 0));
+    };
     const int k0 = kind(r->envs[0].T.run_type[0]);
-    r->arrivals = k0 == 1;
+    r->arrivals = k0 == 1 || k0 == 4;
+    r->also_eigen = k0 == 4;
     r->eigen = k0 == 2;
     r->rayrun = k0 == 3;
     r->raysets.assign(r->envs.size(), RaySet3{});
@@ -284,9 +291,10 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         if(kind(S.T.run_type[0]) != k0) throw std::runtime_error("a 3-D batch must use one run type");
     auto bits = [](unsigned long long n) { int b = 1; while(b < 64 && (1ull << b) < n) ++b; return b; };
     if(r->rayrun) return;   // trajectories only: no segments, fields or arrivals
-    if(r->eigen) {
-        // ordering key (low to high): depth | bearing | walk position | step | ray | trace group;
-        // ray-centred beams walk depth, then bearing, then the ranges: walk | bearing | depth
+    // eigen-hit ordering key (low to high): depth | bearing | walk position |
+    // step | ray | trace group; ray-centred beams walk depth, then bearing,
+    // then the ranges: walk | bearing | depth
+    auto eigen_layout = [&]() {
         int mz = 1, mt = 1, mr = 1, mj = 1;
         for(const auto &S : r->envs) {
             mz = std::max(mz, (int)S.T.rz.size());
@@ -304,11 +312,15 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
         kb.sh_cell = kb.sh_job + bits((unsigned long long)mj);
         kb.total_bits = kb.sh_cell + bits((unsigned long long)r->groups_h.size());
         if(kb.total_bits > 64) throw MemError("eigen-hit ordering key needs more than 64 bits; split the batch");
-        r->kb = kb;
-        r->hits_h.clear();
-        r->hit_group.clear();
+        return kb;
+    };
+    r->hits_h.clear();
+    r->hit_group.clear();
+    if(r->eigen) {
+        r->kb = eigen_layout();
         return;
     }
+    if(r->also_eigen) r->kb_eig = eigen_layout();
     if(!r->arrivals) {
         r->field.ensure(std::max<int64_t>(r->total_field, 1) * sizeof(float2));
         return;
@@ -328,7 +340,8 @@ void prepare3(Run3 *r, cudaStream_t st, uint64_t &h2d)
     if(mx <= 0) {
         // as the reference (src/mode/arr.hpp:80-98): what a quarter of
         // max_memory holds per receiver, at most 1000
-        const uint64_t m = (r->max_memory / 4) / (cells * sizeof(ArrivalRec) + 1);
+        uint64_t m = (r->max_memory / 4) / (cells * sizeof(ArrivalRec) + 1);
+        if(r->also_eigen) m /= 2;   // half the room goes to the eigen hits (src/mode/arr.hpp:87)
         mx = (int32_t)std::min<uint64_t>(m, 1000);
     }
     if(mx <= 0) throw MemError("insufficient memory to allocate arrivals");
@@ -360,35 +373,38 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, st));
-    CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), st));
     // Nx2D: 2-D records on the bearing planes; 3-D: SegRec3
     auto gather = [&](bool count, ArrCand *c, uint64_t *k, uint32_t *v, unsigned long long cap,
-                      unsigned long long *cur) {
+                      unsigned long long *cur, const ArrKeyBits &kb) {
         if(r->raycen) {
             int nzt = 1;   // (depth, bearing) pairs per record, the most of the batch
             for(const auto &S : r->envs) nzt = std::max(nzt, (int)(S.T.rz.size() * S.T.theta.size()));
             return launch_arr_gather3d_rc((const XSeg3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
-                                          (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, nzt,
+                                          (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, kb, nzt,
                                           sm_count * 16, st);
         }
         return r->nx2d ? launch_arr_gather_nx(r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
-                                              (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, igrid, st)
+                                              (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, kb, igrid, st)
                        : launch_arr_gather3d((const SegRec3 *)r->segs.p, nseg, (const GroupDev *)r->groups_d.p,
-                                             (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, r->kb, igrid, st);
+                                             (int)r->groups_h.size(), count, c, k, v, cap, cur, ctr, kb, igrid, st);
     };
-    CK(gather(true, nullptr, nullptr, nullptr, 0, nullptr));
-    unsigned long long n = 0;
-    CK(cudaMemcpyAsync(&n, &ctr->nevals, sizeof n, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    const size_t per = sizeof(ArrCand) + 2 * sizeof(uint64_t) + 2 * sizeof(uint32_t);
-    const size_t fixed = r->segs.bytes + r->arr_d.bytes + r->narr_d.bytes + (64u << 20);
-    const size_t avail = r->max_memory > fixed ? r->max_memory - fixed : 0;
-    if((size_t)n * per + radix_sort_hist_entries(n) * 4 > avail && j1 - j0 > 1) {
-        cudaEventDestroy(e0); cudaEventDestroy(e1);
-        return false;
-    }
-    if(n > 0xffffffffull) throw MemError("more than 2^32 arrival candidates in one wave; lower max_memory");
-    if(n) {
+    // one pass: count, gather, order, then replay (AddArr) or emit the eigen
+    // hits (RecordEigenHit); 'V' / 'v' runs take an eigen pass after the
+    // arrivals pass, over the same segments
+    unsigned long long n_first = 0;
+    auto pass = [&](const ArrKeyBits &kb, bool eig, bool first) -> bool {
+        CK(cudaMemsetAsync(&ctr->nevals, 0, sizeof(unsigned long long), st));
+        CK(gather(true, nullptr, nullptr, nullptr, 0, nullptr, kb));
+        unsigned long long n = 0;
+        CK(cudaMemcpyAsync(&n, &ctr->nevals, sizeof n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const size_t per = sizeof(ArrCand) + 2 * sizeof(uint64_t) + 2 * sizeof(uint32_t);
+        const size_t fixed = r->segs.bytes + r->arr_d.bytes + r->narr_d.bytes + (64u << 20);
+        const size_t avail = r->max_memory > fixed ? r->max_memory - fixed : 0;
+        if(first && (size_t)n * per + radix_sort_hist_entries(n) * 4 > avail && j1 - j0 > 1) return false;
+        if(n > 0xffffffffull) throw MemError("more than 2^32 arrival candidates in one wave; lower max_memory");
+        if(first) n_first = n;
+        if(!n) return true;
         r->cand.ensure(n * sizeof(ArrCand));
         r->keys0.ensure(n * sizeof(uint64_t));
         r->keys1.ensure(n * sizeof(uint64_t));
@@ -396,13 +412,13 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
         r->vals1.ensure(n * sizeof(uint32_t));
         r->hist.ensure(std::max<size_t>(radix_sort_hist_entries(n), 1) * sizeof(uint32_t));
         CK(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
-        CK(gather(false, (ArrCand *)r->cand.p, (uint64_t *)r->keys0.p, (uint32_t *)r->vals0.p, n, cursor));
+        CK(gather(false, (ArrCand *)r->cand.p, (uint64_t *)r->keys0.p, (uint32_t *)r->vals0.p, n, cursor, kb));
         int in1 = 0;
         CK(radix_sort_pairs((uint64_t *)r->keys0.p, (uint32_t *)r->vals0.p, (uint64_t *)r->keys1.p,
-                            (uint32_t *)r->vals1.p, n, r->kb.total_bits, (uint32_t *)r->hist.p, &in1, st));
+                            (uint32_t *)r->vals1.p, n, kb.total_bits, (uint32_t *)r->hist.p, &in1, st));
         const uint64_t *k = (const uint64_t *)(in1 ? r->keys1.p : r->keys0.p);
         const uint32_t *v = (const uint32_t *)(in1 ? r->vals1.p : r->vals0.p);
-        if(r->eigen) {
+        if(eig) {
             r->hits_d.ensure(n * sizeof(EigenHitRec));
             r->hitgrp_d.ensure(n * sizeof(int32_t));
             CK(launch_eigen_emit3(v, (const ArrCand *)r->cand.p, n, (const GroupDev *)r->groups_d.p,
@@ -416,12 +432,22 @@ bool apply_arrivals(Run3 *r, long long j0, long long j1, unsigned long long nseg
             CK(cudaMemcpyAsync(r->hit_group.data() + h0, r->hitgrp_d.p, n * sizeof(int32_t),
                                cudaMemcpyDeviceToHost, st));
         } else {
-        CK(launch_arr_replay(k, v, (const ArrCand *)r->cand.p, n, (const GroupDev *)r->groups_d.p,
-                             (int)r->groups_h.size(), nullptr, (long long)r->total_field, r->kb.sh_cell,
-                             r->max_narr, r->allow_merging, (int32_t *)r->narr_d.p, (ArrivalRec *)r->arr_d.p,
-                             sm_count, st, true));
+            CK(launch_arr_replay(k, v, (const ArrCand *)r->cand.p, n, (const GroupDev *)r->groups_d.p,
+                                 (int)r->groups_h.size(), nullptr, (long long)r->total_field, kb.sh_cell,
+                                 r->max_narr, r->allow_merging, (int32_t *)r->narr_d.p, (ArrivalRec *)r->arr_d.p,
+                                 sm_count, st, true));
         }
+        return true;
+    };
+    if(!pass(r->kb, r->eigen, true)) {
+        cudaEventDestroy(e0); cudaEventDestroy(e1);
+        return false;
     }
+    if(r->also_eigen) {
+        CK(cudaStreamSynchronize(st));   // the replay reads the candidates the eigen pass rewrites
+        pass(r->kb_eig, true, false);
+    }
+    const unsigned long long n = n_first;
     CK(cudaEventRecord(e1, st));
     RunCounters rc{};
     CK(cudaMemcpyAsync(&rc, ctr, sizeof rc, cudaMemcpyDeviceToHost, st));
@@ -745,7 +771,7 @@ bool run3_is_arrivals(const Run3 *r) { return r->arrivals; }
 int64_t run3_eigen_hits(Run3 *r, int env, void *hits, int64_t max_hits)
 {
     ran_env(r, env);
-    if(!r->eigen) throw StateError("not an eigen-hit run");
+    if(!r->eigen && !r->also_eigen) throw StateError("not an eigen-hit run");
     int64_t n = 0;
     EigenHitRec *out = reinterpret_cast<EigenHitRec *>(hits);
     for(size_t k = 0; k < r->hits_h.size(); ++k) {
@@ -789,7 +815,7 @@ static void write_arrivals3(Run3 *r, const Env3Slot &S, const std::string &path,
     run3_copy_arrivals(r, (int)(&S - r->envs.data()), narr.data(), narr.size() * 4, arr.data(),
                        arr.size() * sizeof(ArrivalRec), st);
     const double RadDeg = 180.0 / 3.14159265358979323846;
-    const bool ascii = T.run_type[0] == 'A';
+    const bool ascii = T.run_type[0] == 'A' || T.run_type[0] == 'V';   // src/mode/arr.cpp:95-100
     std::ofstream o(path, std::ios::binary);
     if(!o.good()) throw std::runtime_error("cannot open " + path);
     const int nsx = (int)T.sx.size(), nsy = (int)T.sy.size(), nsz = (int)T.sz.size();
@@ -857,14 +883,15 @@ static void write_arrivals3(Run3 *r, const Env3Slot &S, const std::string &path,
 }
 
 // .shd, 3-D: WriteHeader and WriteOutTL (src/mode/tl.cpp:38-101, 195-248)
-bool run3_has_rays(const Run3 *r) { return r->rayrun || r->eigen; }
+bool run3_has_rays(const Run3 *r) { return r->rayrun || r->eigen || r->also_eigen; }
 
-// RunType 'R': the traced rays; 'E': the hit rays re-traced up to their hit
+// RunType 'R': the traced rays; 'E', 'V', 'v': the hit rays re-traced up to their hit
 // (EigenModePostWorker, src/mode/eigen.cpp:24-45) on first use, in hit order
 static const RaySet3 &rays_of_env(Run3 *r, int env, cudaStream_t st)
 {
     const Env3Slot &S = ran_env(r, env);
-    if(!r->rayrun && !r->eigen) throw StateError("rays exist for ray runs ('R') and eigen runs ('E')");
+    if(!r->rayrun && !r->eigen && !r->also_eigen)
+        throw StateError("rays exist for ray runs ('R') and eigen runs ('E', 'V', 'v')");
     RaySet3 &R = r->raysets[env];
     if(R.valid) return R;
     if(r->rayrun) throw StateError("no rays: run first");
@@ -952,6 +979,7 @@ void run3_writeout(Run3 *r, int env, const std::string &root, cudaStream_t st)
     }
     if(r->arrivals) {
         write_arrivals3(r, S, root + ".arr", st);
+        if(r->also_eigen) write_rays3(r, env, root + ".ray", st);   // src/api.cpp:465-486
         return;
     }
     const Env3Tables &T = S.T;

@@ -503,7 +503,9 @@ template<bool O3D, bool R3D> void collect(Internal &in, bhcOutputs<O3D, R3D> &o,
         }
         o.uAllSources = new cpxf[n];
         check(ctx, bhcb_copy_field(ctx, 0, 0, o.uAllSources, n * sizeof(cpxf)), "copy field");
-    } else if(run0 == 'A' || run0 == 'a') {
+    }
+    const bool combined = run0 == 'V' || run0 == 'v';   // arrivals and eigen hits in one run
+    if(run0 == 'A' || run0 == 'a' || combined) {
         int32_t nsz = 0, nrz = 0, nrr = 0, mx = 0;
         check(ctx, bhcb_arrivals_shape(ctx, 0, 0, &nsz, &nrz, &nrr, &mx), "arrivals shape");
         const size_t cells = (size_t)nsz * nrz * nrr;
@@ -528,7 +530,8 @@ template<bool O3D, bool R3D> void collect(Internal &in, bhcOutputs<O3D, R3D> &o,
             for(size_t i = 0; i < per; ++i) m = std::max(m, o.arrinfo->NArr[s * per + i]);
             o.arrinfo->MaxNPerSource[s] = m;
         }
-    } else if(run0 == 'E') {
+    }
+    if(run0 == 'E' || combined) {
         int64_t nh = 0;
         check(ctx, bhcb_eigen_hits(ctx, 0, 0, nullptr, 0, &nh), "eigen hits");
         std::vector<bhcb_eigen_hit> h((size_t)nh);
@@ -540,7 +543,7 @@ template<bool O3D, bool R3D> void collect(Internal &in, bhcOutputs<O3D, R3D> &o,
             o.eigen->hits[i] = EigenHit{h[i].is, h[i].itheta, h[i].ir, h[i].iz, h[i].isx, h[i].isy, h[i].isz,
                                         h[i].ialpha, h[i].ibeta};
     }
-    if(run0 == 'R' || run0 == 'E') {   // trajectories: rays of a ray run, hit rays of an eigen run
+    if(run0 == 'R' || run0 == 'E' || combined) {   // trajectories: rays of a ray run, hit rays of an eigen run
         int64_t nrays = 0, npts = 0;
         if(bhcb_rays_shape(ctx, 0, 0, &nrays, &npts) == BHCB_OK && nrays > 0) {
             // 2 doubles (r, z) per point from a 2-D context, 3 (x, y, z) from a

@@ -1028,7 +1028,7 @@ Env3Tables preprocess3d(const EnvInput &in, double freq)
     t.freq0 = freq;
     std::memcpy(t.run_type, in.run_type, 7);
     switch(t.run_type[0]) {   // src/module/runtype.hpp:53-78
-    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'R': break;
+    case 'C': case 'S': case 'I': case 'A': case 'a': case 'E': case 'V': case 'v': case 'R': break;
     default: env_error("unknown RunType");
     }
     const bool ray_run3 = t.run_type[0] == 'R';

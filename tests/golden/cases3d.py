@@ -269,6 +269,24 @@ def seamount3d_nx2d_ray():
     return f
 
 
+def munk3d_v_hat():
+    """Arrivals and eigen hits in one run ('v', binary arrivals) with hat beams."""
+    return _munk_slice("vG   3", alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0), theta=[0.0, 2.0, 5.0],
+                       nrz_range=(3, 800.0, 2800.0), rr_range=(4, 8.0, 26.0))
+
+
+def munk3d_raycen_v_gauss():
+    """'v' with Gaussian beams in ray-centred coordinates ('b')."""
+    return _munk_slice("vb   3", alpha=(121, -20.3, 20.3), beta=(21, -8.0, 8.0), theta=[0.0, 2.0, 5.0],
+                       nrz_range=(3, 800.0, 2800.0), rr_range=(4, 8.0, 26.0))
+
+
+def munk3d_nx2d_v_gauss():
+    """Nx2D 'v': arrivals and the eigen hits of each receiver bearing's plane."""
+    return _munk_slice("vB   2", alpha=(121, -20.3, 20.3), theta=[0.0, 2.0, 5.0], nrz_range=(3, 800.0, 2800.0),
+                       rr_range=(4, 8.0, 26.0))
+
+
 CASES3D = {
     "munk3d_gauss": munk3d_gauss,
     "munk3d_hat": munk3d_hat,
@@ -304,4 +322,7 @@ CASES3D = {
     "munk3d_raycen_arr_gauss": munk3d_raycen_arr_gauss,
     "munk3d_raycen_eig_hat": munk3d_raycen_eig_hat,
     "seamount3d_nx2d_arr_hat": seamount3d_nx2d_arr_hat,
+    "munk3d_v_hat": munk3d_v_hat,
+    "munk3d_raycen_v_gauss": munk3d_raycen_v_gauss,
+    "munk3d_nx2d_v_gauss": munk3d_nx2d_v_gauss,
 }

@@ -4,7 +4,8 @@ Runs the reference's own bellhopcxx (compiled from its sources by
 oracle/Makefile into oracle/_ref/) as a 3-D run (-3), or an Nx2D run (-4) for
 cases whose RunType(6) is '2', on every case of
 tests/golden/cases3d.py and stores, per case, the input files' text and the
-scaled complex field (TL runs) or the arrivals (RunType 'a') as
+scaled complex field (TL runs), the arrivals (RunType 'a'), the rays
+('R', 'E') or the arrivals with the hit rays ('v') as
 tests/golden/<case>.npz. The GPU tests write the input
 files back from the fixture, so they need neither the reference nor this
 script at run time. Run from the repository root:
@@ -53,33 +54,37 @@ def main(names=None):
             if r.returncode != 0:
                 raise SystemExit("reference failed on %s:\n%s%s" % (name, r.stdout[-2000:], r.stderr[-2000:]))
             texts = {"file_" + suffix[1:]: np.array(text) for suffix, text in files.items()}
+            rays = {}
             if os.path.exists(root + ".ray"):
-                # ray runs ('R') and eigen hits ('E'): the reference writes the
-                # traced rays (eigen: the hit rays re-traced, in hit order, so each
-                # ray's take-off angle in radians and point count, the hit's step +
-                # 2, pin the hit list) with their points (x, y, z)
+                # ray runs ('R') and eigen hits ('E', 'V', 'v'): the reference
+                # writes the traced rays (eigen: the hit rays re-traced, in hit
+                # order, so each ray's take-off angle in radians and point count,
+                # the hit's step + 2, pin the hit list) with their points (x, y, z)
                 R = read_ray(root + ".ray")
                 npts = np.array([len(x["xy"]) for x in R["rays"]], np.int32)
                 # points of the first (at most) 64 rays keep the fixture small
                 nkeep = min(len(npts), 64)
-                np.savez_compressed(os.path.join(HERE, name + ".npz"),
-                                    alpha=np.array([x["alpha"] for x in R["rays"]]), npts=npts,
-                                    bnc=np.array([[x["ntop"], x["nbot"]] for x in R["rays"]], np.int32).reshape(-1, 2),
-                                    xyz=np.concatenate([x["xy"] for x in R["rays"][:nkeep]]) if nkeep
-                                    else np.zeros((0, 3)), xyz_rays=np.int32(nkeep), **texts)
+                rays = dict(alpha=np.array([x["alpha"] for x in R["rays"]]), npts=npts,
+                            bnc=np.array([[x["ntop"], x["nbot"]] for x in R["rays"]], np.int32).reshape(-1, 2),
+                            xyz=np.concatenate([x["xy"] for x in R["rays"][:nkeep]]) if nkeep
+                            else np.zeros((0, 3)), xyz_rays=np.int32(nkeep))
                 print(name, "rays", len(R["rays"]), "points", int(npts.sum()), "%.1fs" % (time.time() - t0))
-                continue
             if os.path.exists(root + ".arr"):
                 # arrivals: per receiver (source, bearing, depth, range) the
-                # count and the records, flattened with offsets
+                # count and the records, flattened with offsets; a combined run
+                # ('V', 'v') keeps its hit rays beside them under eig_*
                 A = read_arr_binary(root + ".arr")
                 narr = np.array([len(a) for src in A["sources"] for a in src["arrivals"]], np.int32)
                 recs = np.concatenate([a for src in A["sources"] for a in src["arrivals"]] or
                                       [np.zeros((0, 10), np.float32)])
+                eig = {"eig_" + k: v for k, v in rays.items()}
                 np.savez_compressed(os.path.join(HERE, name + ".npz"), narr=narr, arr=recs, rr=A["rr"],
                                     rz=A["rz"], sz=A["sz"], theta=A["theta"],
-                                    maxn=np.array([s["maxn"] for s in A["sources"]], np.int32), **texts)
+                                    maxn=np.array([s["maxn"] for s in A["sources"]], np.int32), **eig, **texts)
                 print(name, "arrivals", int(narr.sum()), "max", int(narr.max()), "%.1fs" % (time.time() - t0))
+                continue
+            if rays:
+                np.savez_compressed(os.path.join(HERE, name + ".npz"), **rays, **texts)
                 continue
             shd = read_shd(root + ".shd")
             np.savez_compressed(os.path.join(HERE, name + ".npz"), field=shd["field"],

@@ -42,7 +42,7 @@ def to_file_order(u):
     return np.transpose(u, (1, 2, 3, 0, 4, 5))
 
 
-TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p and not p.endswith("_ray.npz")]
+TL3D = [p for p in GOLD if "_arr_" not in p and "_eig_" not in p and "_v_" not in p and not p.endswith("_ray.npz")]
 
 
 @pytest.mark.parametrize("precision", [B.PREC_FP64, B.PREC_MIXED])
@@ -152,9 +152,12 @@ def test_3d_arrivals_match_reference(path, workdir):
         t.run()
         narr, arr = t.arrivals()
         t.writeout(root + "_gpu")
+    check_arrivals(narr, arr, g, root, os.path.basename(path)[:-4])
+
+
+def check_arrivals(narr, arr, g, root, name):
     narr = narr.reshape(-1)
     assert narr.sum() > 0
-    name = os.path.basename(path)[:-4]
     if name in NX2D_GRID_RAY_DIFF:
         # Nx2D rays over a boundary grid: about one ray in a hundred leaves the
         # reference's trajectory (see test_3d_rays_match_reference), and its
@@ -203,15 +206,19 @@ def test_3d_eigen_hits_match_reference(path, workdir):
         t.setup3d(root)
         t.run()
         hits = t.eigen_hits(0)
-    assert len(hits) == len(g["alpha"]) > 0
-    np.testing.assert_array_equal(hits["is"] + 2, g["npts"])
+    check_hits(hits, g, g["alpha"], g["npts"], "'E")
+
+
+def check_hits(hits, g, alpha, npts, run_tag):
+    assert len(hits) == len(alpha) > 0
+    np.testing.assert_array_equal(hits["is"] + 2, npts)
     # the take-off angle of each hit's ray: elevation fan from the .env (alpha1, alpha2, n)
     txt = str(g["file_env"]).splitlines()
-    k = [i for i, ln in enumerate(txt) if ln.strip().startswith("'E")][0]
+    k = [i for i, ln in enumerate(txt) if ln.strip().startswith(run_tag)][0]
     na = int(txt[k + 1].split()[0])
     a1, a2 = (float(v) for v in txt[k + 2].replace("/", " ").split()[:2])
     fan = np.deg2rad(np.linspace(a1, a2, na))
-    np.testing.assert_allclose(fan[hits["ialpha"]], g["alpha"], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(fan[hits["ialpha"]], alpha, rtol=1e-9, atol=1e-12)
 
 
 RAY3D = sorted(p for p in GOLD if p.endswith("_ray.npz"))
@@ -272,5 +279,33 @@ def test_3d_eigenrays_match_reference(path, workdir):
         rays = t.rays(dim=3)
         t.writeout(root + "_gpu")
     compare_rays3d(rays, g)
+    from bellhopcuda_b200.rayfile import read_ray
+    assert len(read_ray(root + "_gpu.ray")["rays"]) == len(rays)
+
+
+V3D = sorted(p for p in GOLD if "_v_" in p)
+
+
+@pytest.mark.parametrize("path", V3D, ids=[os.path.basename(p)[:-4] for p in V3D])
+def test_3d_combined_arrivals_and_eigen_hits(path, workdir):
+    """RunType 'v': arrivals and eigen hits of one 3-D / Nx2D run, against
+    the reference's .arr and .ray outputs of that run: the arrivals as in
+    test_3d_arrivals_match_reference, the hits and their re-traced rays as in
+    the eigen tests."""
+    g = np.load(path)
+    root = os.path.join(workdir, os.path.basename(path)[:-4])
+    write_case(g, root)
+    with B.Tracer(precision=B.PREC_FP64) as t:
+        t.set_arrival_options(1000, True)
+        t.setup3d(root)
+        t.run()
+        narr, arr = t.arrivals()
+        hits = t.eigen_hits(0)
+        rays = t.rays(dim=3)
+        t.writeout(root + "_gpu")
+    check_arrivals(narr, arr, g, root, os.path.basename(path)[:-4])
+    check_hits(hits, g, g["eig_alpha"], g["eig_npts"], "'v")
+    eig = {k[4:]: g[k] for k in g.files if k.startswith("eig_")}
+    compare_rays3d(rays, eig)
     from bellhopcuda_b200.rayfile import read_ray
     assert len(read_ray(root + "_gpu.ray")["rays"]) == len(rays)
