@@ -1,4 +1,13 @@
-"""Neural-operator TL surrogate for the 2-D coherent hat-beam workload (C5).
+"""Neural-operator TL surrogate for the 2-D surrogate workload (C5).
+
+The fields are incoherent Gaussian-beam TL (RunType 'IB') by default, or
+coherent hat-beam TL ('CG'). A coherent field on the 128 x 256 grid is
+sampled far below the Nyquist rate of its interference fringes (wavelengths of
+3-30 m against receiver spacings of 39 m in depth and 78 m in range), so at a
+receiver it behaves like a Rayleigh-faded amplitude about the incoherent mean,
+whose 20 log10 spread is about 5.6 dB: the error floor of any predictor that
+varies smoothly with the environment. The incoherent field is the learnable
+quantity.
 
 A DeepONet-style operator maps an environment to its TL grid:
 
@@ -455,43 +464,35 @@ def infer(model: Surrogate, P, idx: Sequence[int], threshold_db: float = 1.0, ma
     return out, fb.cpu().numpy(), {"surrogate_s": t_sur, "fallback_s": t_fb}
 
 
-# ---------------------------------------------------------------------- CLI
-def main(argv=None):
-    """Generate fields with the plain FP64 tracer, train, evaluate on the test
-    split (90/5/5 by seed order), report one JSON line."""
-    import argparse
-    import json
-    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--n", type=int, default=100000, help="environments (train + val + test)")
-    ap.add_argument("--seed", type=int, default=1005)
-    ap.add_argument("--epochs", type=int, default=20)
-    ap.add_argument("--batch", type=int, default=256)
-    ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--threshold-db", type=float, default=1.0)
-    ap.add_argument("--infer-batch", type=int, default=4096)
-    ap.add_argument("--chunk", type=int, default=2048, help="environments per trace launch")
-    ap.add_argument("--save", default="", help="write the weights (.npz)")
-    ap.add_argument("--tmpdir", default="")
-    a = ap.parse_args(argv)
+# ------------------------------------------------------------ C5 end to end
+def run_c5(n: int = 100000, seed: int = 1005, run_type: str = "IB", fan_deg: float = W.C5_FAN_DEG,
+           epochs: int = 40, batch: int = 256, lr: float = 1e-3, threshold_db: float = 1.0,
+           infer_batch: int = 4096, chunk: int = 2048, tmpdir: str = "", log=None, save: str = "") -> Dict:
+    """Generate n fields with the plain FP64 tracer, train on the first 90 %,
+    calibrate the fallback margin on the next 5 % and evaluate on the last
+    5 %: the surrogate's own errors, the fallback rate at threshold_db, the
+    errors of the returned fields, and the time of the surrogate with its
+    fallback against the plain FP64 trace of the same test fields through
+    the same call (trace_tl)."""
     torch = _torch()
-    log = lambda m: print(m, flush=True)
-    P = W.c5_params(a.n, a.seed)
-    n_tr, n_va = int(a.n * 0.90), int(a.n * 0.05)
-    tr, va, te = list(range(n_tr)), list(range(n_tr, n_tr + n_va)), list(range(n_tr + n_va, a.n))
-    tmp = a.tmpdir or tempfile.mkdtemp(prefix="c5_")
-    Y = torch.empty((a.n, NP), device="cuda")
-    gen = trace_tl(P, list(range(a.n)), Y, chunk=a.chunk, tmpdir=tmp, log=log)
-    X = torch.tensor(features(P, list(range(a.n))), device="cuda").bfloat16()
+    P = W.c5_params(n, seed, run_type, fan_deg)
+    n_tr, n_va = int(n * 0.90), int(n * 0.05)
+    tr, va, te = list(range(n_tr)), list(range(n_tr, n_tr + n_va)), list(range(n_tr + n_va, n))
+    tmp = tmpdir or tempfile.mkdtemp(prefix="c5_")
+    Y = torch.empty((n, NP), device="cuda")
+    gen = trace_tl(P, list(range(n)), Y, chunk=chunk, tmpdir=tmp, log=log)
+    X = torch.tensor(features(P, list(range(n))), device="cuda").bfloat16()
     model = Surrogate(seed=0)
-    log("parameters %d" % model.params())
+    if log:
+        log("parameters %d" % model.params())
     t0 = time.time()
-    hist = model.train(X[:n_tr], Y[:n_tr], epochs=a.epochs, batch=a.batch, lr=a.lr, log=log)
+    hist = model.train(X[:n_tr], Y[:n_tr], epochs=epochs, batch=batch, lr=lr, log=log)
     torch.cuda.synchronize()
     t_train = time.time() - t0
     # error head on the training fields' actual errors
     rms = torch.empty(n_tr, device="cuda")
-    for c0 in range(0, n_tr, a.infer_batch):
-        xb = X[c0:c0 + a.infer_batch]
+    for c0 in range(0, n_tr, infer_batch):
+        xb = X[c0:c0 + infer_batch]
         pred = model.forward(xb, keep=False)
         model.ops.row_rms(pred, Y[c0:c0 + xb.shape[0]], rms[c0:c0 + xb.shape[0]])
     rms *= TL_SCALE
@@ -505,35 +506,75 @@ def main(argv=None):
     tv *= TL_SCALE
     ratio = (tv / pv.clamp_min(1e-6)).cpu().numpy()
     margin = float(np.quantile(ratio, 0.95))
-    # test split: throughput with fallback, errors of what is returned
-    tl, fb, tm = infer(model, P, te, threshold_db=a.threshold_db, margin=margin, batch=a.infer_batch, tmpdir=tmp)
+    # test split: the plain FP64 trace and the surrogate with its fallback,
+    # each timed twice, interleaved (the faster of the two counts)
+    plain_rows = torch.empty((len(te), NP), device="cuda")
+    t_plain, t_with = [], []
+    for _ in range(2):
+        t_plain.append(trace_tl(P, te, plain_rows, tmpdir=tmp)["trace_s"])
+        tl, fb, tm = infer(model, P, te, threshold_db=threshold_db, margin=margin, batch=infer_batch, tmpdir=tmp)
+        t_with.append(tm["surrogate_s"] + tm["fallback_s"])
     ref = Y[n_tr + n_va:] * TL_SCALE + TL_MEAN
     err = torch.empty(len(te), device="cuda")
     model.ops.row_rms(tl, ref, err)
     err = err.cpu().numpy()
-    sur_only, _, tm0 = infer(model, P, te, threshold_db=1e9, batch=a.infer_batch, tmpdir=tmp)
+    sur_only, _, tm0 = infer(model, P, te, threshold_db=1e9, batch=infer_batch, tmpdir=tmp)
     e0 = torch.empty(len(te), device="cuda")
     model.ops.row_rms(sur_only, ref, e0)
     e0 = e0.cpu().numpy()
+    phi = float(fb.mean())
     out = {
-        "fields": a.n, "train_fields": n_tr, "test_fields": len(te), "params": model.params(),
-        "generate_s": gen["trace_s"], "generate_fields_per_s": a.n / gen["trace_s"],
-        "train_s": t_train, "epochs": a.epochs, "train_rms_db": hist,
+        "fields": n, "run_type": run_type, "fan_deg": fan_deg, "train_fields": n_tr, "test_fields": len(te),
+        "params": model.params(), "generate_s": gen["trace_s"], "generate_fields_per_s": n / gen["trace_s"],
+        "train_s": t_train, "epochs": epochs, "train_rms_db": hist,
         "surrogate_only_fields_per_s": len(te) / tm0["surrogate_s"], "surrogate_only_rms_db_mean": float(e0.mean()),
         "surrogate_only_rms_db_median": float(np.median(e0)),
-        "margin": margin, "fallback_rate": float(fb.mean()),
-        "fields_per_s_with_fallback": len(te) / (tm["surrogate_s"] + tm["fallback_s"]),
+        "surrogate_only_within_1db": float((e0 <= 1.0).mean()),
+        "threshold_db": threshold_db, "margin": margin, "fallback_rate": phi,
+        "fields_per_s_with_fallback": len(te) / min(t_with), "with_fallback_s": t_with,
+        "plain_fp64_fields_per_s": len(te) / min(t_plain), "plain_s": t_plain,
+        "speedup_with_fallback": min(t_plain) / min(t_with),
+        # the same from the per-field costs: the surrogate pass for every
+        # field plus the plain trace's time for the fallback fraction
+        "speedup_accounted": 1.0 / (tm0["surrogate_s"] / min(t_plain) + phi),
         "returned_rms_db_mean": float(err.mean()), "returned_rms_db_p95": float(np.quantile(err, 0.95)),
         "returned_within_1db": float((err <= 1.0).mean()),
-        "plain_fp64_fields_per_s": a.n / gen["trace_s"],
+        "returned_within_threshold": float((err <= threshold_db).mean()),
+        "accepted_rms_db_mean": float(e0[~fb].mean()) if (~fb).any() else None,
+        "accepted_within_1db": float((e0[~fb] <= 1.0).mean()) if (~fb).any() else None,
     }
     pe = (model.predict_error(X[n_tr + n_va:]) * margin).cpu().numpy()
     for thr in (2.0, 3.0, 6.0):
         acc = pe <= thr
         out["accepted_at_%gdb" % thr] = float(acc.mean())
         out["accepted_rms_db_mean_at_%gdb" % thr] = float(e0[acc].mean()) if acc.any() else None
-    if a.save:
-        np.savez_compressed(a.save, **model.state())
+    if save:
+        np.savez_compressed(save, **model.state())
+    return out
+
+
+# ---------------------------------------------------------------------- CLI
+def main(argv=None):
+    """Generate fields with the plain FP64 tracer, train, evaluate on the test
+    split (90/5/5 by seed order), report one JSON line."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--n", type=int, default=100000, help="environments (train + val + test)")
+    ap.add_argument("--seed", type=int, default=1005)
+    ap.add_argument("--run-type", default="IB", help="RunType of the fields: IB (incoherent Gaussian beams) or CG")
+    ap.add_argument("--fan-deg", type=float, default=W.C5_FAN_DEG, help="launch angles -fan .. fan (degrees)")
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--threshold-db", type=float, default=1.0)
+    ap.add_argument("--infer-batch", type=int, default=4096)
+    ap.add_argument("--chunk", type=int, default=2048, help="environments per trace launch")
+    ap.add_argument("--save", default="", help="write the weights (.npz)")
+    ap.add_argument("--tmpdir", default="")
+    a = ap.parse_args(argv)
+    out = run_c5(a.n, a.seed, a.run_type, a.fan_deg, a.epochs, a.batch, a.lr, a.threshold_db, a.infer_batch,
+                 a.chunk, a.tmpdir, log=lambda m: print(m, flush=True), save=a.save)
     print(json.dumps(out))
     return out
 

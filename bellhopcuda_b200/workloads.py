@@ -147,18 +147,24 @@ def c4_3d(seed=1004, run_type="CB   3", scale=1.0, nalpha=361, nbeta=144, ntheta
 
 C5_NZ, C5_NR = 128, 256
 C5_RR_KM = (0.08, 20.0)
+# launch angles -89 .. 89 degrees: the fan reaches every receiver of the grid
+# (with -60 .. 60 a cone beside the source that no ray enters stays at the
+# 130 dB clamp, up to 90 % of the first 300 m of range)
+C5_FAN_DEG = 89.0
 
 
-def c5_params(n, seed=1005):
+def c5_params(n, seed=1005, run_type="IB", fan_deg=C5_FAN_DEG):
     """Seeded parameters of n surrogate environments (one row each):
-    depth, bottom cp, source depth, frequency, 8 SSP mode amplitudes."""
+    depth, bottom cp, source depth, frequency, 8 SSP mode amplitudes; and
+    the RunType of their fields ('IB': incoherent Gaussian beams, the
+    default; 'CG': coherent hat beams) and the launch fan's half-angle."""
     rng = np.random.Generator(np.random.PCG64(seed))
     depth = rng.uniform(1000.0, 5000.0, n)
     cp = rng.uniform(1500.0, 1800.0, n)
     zs = rng.uniform(10.0, 500.0, n)
     f = np.exp(rng.uniform(math.log(50.0), math.log(500.0), n))
     a = rng.normal(0.0, 2.0, (n, 8))
-    return dict(depth=depth, cp=cp, zs=zs, f=f, a=a)
+    return dict(depth=depth, cp=cp, zs=zs, f=f, a=a, run_type=run_type, fan_deg=float(fan_deg))
 
 
 def c5_ssp(depth, a):
@@ -182,10 +188,11 @@ def c5_env(P, i) -> EnvSpec:
         title="surrogate env %d" % i, freq=f, ssp_type="C", top_bc="V", atten_unit="W",
         ssp_z=z, ssp_cp=c, bot_bc="A", bot_hs=(depth, cp, 0.0, 1.8, 0.8, 0.0),
         nsz=1, sz=(zs,), nrz=C5_NZ, rz=(0.0, depth), nrr=C5_NR, rr_km=C5_RR_KM,
-        run_type="CG RR ", nalpha=c5_nalpha(depth, f), alpha=(-60.0, 60.0), deltas=0.0,
+        run_type=P.get("run_type", "IB")[:2] + " RR ", nalpha=c5_nalpha(depth, f),
+        alpha=(-P.get("fan_deg", C5_FAN_DEG), P.get("fan_deg", C5_FAN_DEG)), deltas=0.0,
         box_z=depth + 100.0, box_r_km=C5_RR_KM[1] + 1.0)
 
 
-def c5_envs(n=100000, seed=1005) -> List[EnvSpec]:
-    P = c5_params(n, seed)
+def c5_envs(n=100000, seed=1005, run_type="IB") -> List[EnvSpec]:
+    P = c5_params(n, seed, run_type)
     return [c5_env(P, i) for i in range(n)]

@@ -435,6 +435,20 @@ def run_reference_arm(args, rank, world):
 
 
 # ------------------------------------------------------------------ main
+def run_surrogate(tmp):
+    """C5: 100,000 seeded environments traced by the plain FP64 tracer
+    (incoherent Gaussian beams), the neural operator trained on 90 % of them
+    (40 epochs, tcgen05 GEMMs), the fallback margin calibrated on 5 %, and the
+    last 5 % answered by the surrogate with the FP64 trace as fallback at the
+    1 dB bound, timed against the plain trace of the same fields."""
+    from bellhopcuda_b200 import surrogate as S
+    o = S.run_c5(n=100000, epochs=40, threshold_db=1.0, tmpdir=tmp)
+    o["train_rms_db"] = o["train_rms_db"][-1]
+    o["workload"] = ("C5: 100,000 fields 128 x 256, 64-node SSP = Munk + 8 modes N(0, 2 m/s), depth 1000-5000 m, "
+                     "cp 1500-1800, source 10-500 m, 50-500 Hz; incoherent Gaussian beams, launch angles +-89 deg")
+    return o
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,6 +458,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 3-D (C4) TL timing")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the C5 surrogate run (100,000 traced fields, training, test split)")
     ap.add_argument("--serial", action="store_true",
                     help="time the steps one at a time (graph replay) instead of pipelined launches")
     ap.add_argument("--gemm", type=int, nargs="+", metavar="M N K [EPI]",
@@ -563,6 +579,9 @@ def main():
                                      "influence_kernel_ms": infl_ms},
                     "fp64_peak_tflops": fp64_peak}
         c4 = None if args.no_c4 else time_c4(B, tmp, rank)
+        sur = None
+        if rank == 0 and world == 1 and not args.no_surrogate:
+            sur = run_surrogate(tmp)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(spec, freqs, tmp)
@@ -586,6 +605,7 @@ def main():
                                     else "bhcb_autotune before the warm-up (untimed)"}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 3 * args.steps, "fp64_trace": fp64, "kernels": kernels, "c4_3d_tl": c4,
+        "surrogate": sur,
         "launch": ("pipelined launches (BHCB_FLAG_PIPELINE): the trace of step k+1 beside the influence of step k "
                    "on two streams, double-buffered segment records and accumulators; steps timed as a whole")
                   if pipe else "CUDA graph replay of memsets + trace + influence + scale per step",

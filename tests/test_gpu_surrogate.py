@@ -122,3 +122,17 @@ def test_training_reduces_error_and_fallback_is_the_trace(tmp_path):
     tl2, fb2, tm2 = S.infer(model, P, idx[64:], threshold_db=1e9, tmpdir=str(tmp_path))
     assert not fb2.any() and tm2["fallback_s"] == 0.0
     assert torch.isfinite(tl2).all()
+
+
+def test_trained_surrogate_gains_over_the_plain_trace(tmp_path):
+    """The C5 pipeline on 30,000 incoherent Gaussian-beam fields (27,000 for
+    training, 30 epochs) judged at a 2 dB acceptance bound: part of the test
+    split is answered by the network, what is returned stays within the bound,
+    and the surrogate with its fallback costs less than the plain FP64 trace of
+    the same fields. (The full C5 run, 100,000 fields at the 1 dB bound, is
+    reported by bench.py's `surrogate` key.)"""
+    o = S.run_c5(n=30000, epochs=30, threshold_db=2.0, tmpdir=str(tmp_path))
+    assert o["surrogate_only_rms_db_mean"] < 3.0, o["surrogate_only_rms_db_mean"]
+    assert o["fallback_rate"] < 0.95, o["fallback_rate"]
+    assert o["returned_within_threshold"] >= 0.95, o["returned_within_threshold"]
+    assert o["speedup_accounted"] > 1.0, o["speedup_accounted"]
