@@ -1884,10 +1884,11 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         if(c->mode != MODE_TL) throw StateError("the autotuner covers TL runs");
         if(c->xkind) throw StateError("the autotuner covers geometric Cartesian beams ('G', 'B')");
         const int reps = std::max(1, std::min<int>(repeats, 16));
-        const bool overlap = c->overlap, graphs = c->use_graphs;
+        const bool overlap = c->overlap, graphs = c->use_graphs, pipeline = c->pipeline;
         c->overlap = false;   // time the trace and the influence separately
         c->use_graphs = false;   // every shape launched directly
-        drop_graph(c);
+        drop_graph(c);        // (also drains pipelined launches)
+        c->pipeline = false;  // one launch at a time on the context stream
         auto timed = [&](double &tr, double &inf) {
             tr = inf = 1e300;
             for(int r = 0; r < reps; ++r) {
@@ -1931,6 +1932,7 @@ int bhcb_autotune(bhcb_ctx *c, int32_t repeats, bhcb_tuning *out)
         c->influence_ctas_per_sm = t.influence_ctas_per_sm;
         c->overlap = overlap;
         c->use_graphs = graphs;
+        c->pipeline = pipeline;
         drop_graph(c);
         if(out) *out = t;
         char b[160];

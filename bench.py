@@ -194,7 +194,7 @@ def time_arm(B, torch, root, freqs, precision, steps, warmup, gpu, flush, tune=N
     t.set_frequencies(0, freqs)
     t.prepare()
     if tune is None:
-        t.tuning = t.autotune(repeats=1)
+        t.tuning = t.autotune(repeats=2)
     else:
         t.set_tuning(tune["trace_block"], tune["influence_ctas_per_sm"], tune["stage_kb"], tune.get("trace_lanes", 32))
         t.tuning = tune
