@@ -276,3 +276,20 @@ def test_env_desc_reads_file(workdir):
         assert abs(d.freq0 - spec.freq) < 1e-12
     with pytest.raises(B.BhcbError):
         B.EnvDescription(os.path.join(workdir, "no_such_env"))
+
+
+def test_c5_environments_follow_run_type_and_fan(workdir):
+    """The surrogate workload's environments: the same seeded parameters for
+    either field type; 'IB' with a +-89 degree fan by default, 'CG' on
+    request; the reader takes both."""
+    from bellhopcuda_b200 import workloads as W
+    P = W.c5_params(4, seed=5)
+    Q = W.c5_params(4, seed=5, run_type="CG", fan_deg=60.0)
+    for k in ("depth", "cp", "zs", "f", "a"):
+        np.testing.assert_array_equal(P[k], Q[k])
+    a, b = W.c5_env(P, 1), W.c5_env(Q, 1)
+    assert a.run_type.startswith("IB") and b.run_type.startswith("CG")
+    assert tuple(a.alpha) == (-89.0, 89.0) and tuple(b.alpha) == (-60.0, 60.0)
+    for name, spec in (("ib", a), ("cg", b)):
+        info = B.check_env(write_env(spec, os.path.join(workdir, name)))
+        assert info["nrz"] == W.C5_NZ and info["nrr"] == W.C5_NR
