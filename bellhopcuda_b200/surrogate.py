@@ -464,6 +464,32 @@ def infer(model: Surrogate, P, idx: Sequence[int], threshold_db: float = 1.0, ma
     return out, fb.cpu().numpy(), {"surrogate_s": t_sur, "fallback_s": t_fb}
 
 
+# ------------------------------------------------------------ calibration
+ACCEPT_PRECISION = 0.975   # accepted fields within the threshold, on the validation split
+
+
+def calibrate_margin(pred_err: np.ndarray, err: np.ndarray, threshold_db: float,
+                     precision: float = ACCEPT_PRECISION, min_accept: int = 50) -> float:
+    """The margin m of the fallback rule (a field falls back when m x its
+    predicted error exceeds threshold_db), from the validation split's
+    predicted and actual errors: the fields are accepted in order of predicted
+    error up to the largest count (at least min_accept) whose actual errors
+    stay within threshold_db for a `precision` fraction of them, and m puts
+    the cut at that count's predicted error. Without such a count, m is the
+    95th percentile of actual / predicted error (accepted fields then stay
+    within the threshold in about 95 % of cases)."""
+    order = np.argsort(pred_err, kind="stable")
+    ok = err[order] <= threshold_db
+    prec = np.cumsum(ok) / np.arange(1, len(ok) + 1)
+    good = np.nonzero(prec[min_accept - 1:] >= precision)[0] if len(ok) >= min_accept else np.zeros(0, int)
+    if len(good):
+        k = int(good[-1]) + min_accept
+        cut = float(pred_err[order][k - 1])
+        if cut > 0.0:
+            return threshold_db / cut * (1.0 - 1e-6)
+    return float(np.quantile(err / np.maximum(pred_err, 1e-6), 0.95))
+
+
 # ------------------------------------------------------------ C5 end to end
 def run_c5(n: int = 100000, seed: int = 1005, run_type: str = "IB", fan_deg: float = W.C5_FAN_DEG,
            epochs: int = 40, batch: int = 256, lr: float = 1e-3, threshold_db: float = 1.0,
@@ -497,20 +523,19 @@ def run_c5(n: int = 100000, seed: int = 1005, run_type: str = "IB", fan_deg: flo
         model.ops.row_rms(pred, Y[c0:c0 + xb.shape[0]], rms[c0:c0 + xb.shape[0]])
     rms *= TL_SCALE
     model.train_error_head(X[:n_tr], rms)
-    # calibrate the margin on the validation split: accepted fields must stay
-    # below the threshold in 95 % of cases
+    # calibrate the acceptance on the validation split
     pv = model.predict_error(X[n_tr:n_tr + n_va])
     tv = torch.empty(n_va, device="cuda")
     pred = model.forward(X[n_tr:n_tr + n_va], keep=False)
     model.ops.row_rms(pred, Y[n_tr:n_tr + n_va], tv)
     tv *= TL_SCALE
-    ratio = (tv / pv.clamp_min(1e-6)).cpu().numpy()
-    margin = float(np.quantile(ratio, 0.95))
+    margin = calibrate_margin(pv.cpu().numpy(), tv.cpu().numpy(), threshold_db)
     # test split: the plain FP64 trace and the surrogate with its fallback,
-    # each timed twice, interleaved (the faster of the two counts)
+    # each timed three times, interleaved (the fastest counts: both go through
+    # files and the reader, whose time varies by tens of per cent)
     plain_rows = torch.empty((len(te), NP), device="cuda")
     t_plain, t_with = [], []
-    for _ in range(2):
+    for _ in range(3):
         t_plain.append(trace_tl(P, te, plain_rows, tmpdir=tmp)["trace_s"])
         tl, fb, tm = infer(model, P, te, threshold_db=threshold_db, margin=margin, batch=infer_batch, tmpdir=tmp)
         t_with.append(tm["surrogate_s"] + tm["fallback_s"])

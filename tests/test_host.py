@@ -293,3 +293,23 @@ def test_c5_environments_follow_run_type_and_fan(workdir):
     for name, spec in (("ib", a), ("cg", b)):
         info = B.check_env(write_env(spec, os.path.join(workdir, name)))
         assert info["nrz"] == W.C5_NZ and info["nrr"] == W.C5_NR
+
+
+def test_surrogate_acceptance_calibration():
+    """The fallback rule's margin: on the calibration fields, the accepted
+    ones (smallest predicted errors) stay within the threshold for at least
+    97.5 % of them; without enough such fields the 95th-percentile rule."""
+    from bellhopcuda_b200.surrogate import calibrate_margin, ACCEPT_PRECISION
+    rng = np.random.default_rng(3)
+    pe = rng.uniform(0.5, 3.0, 5000)
+    err = pe * rng.lognormal(0.0, 0.2, 5000)
+    m = calibrate_margin(pe, err, 1.0)
+    acc = pe * m <= 1.0
+    assert acc.sum() >= 50 and (err[acc] <= 1.0).mean() >= ACCEPT_PRECISION
+    # one more field accepted would break the precision target
+    nxt = np.sort(pe[~acc])[0]
+    acc2 = pe <= nxt
+    assert acc2.sum() == acc.sum() + 1 and (err[acc2] <= 1.0).mean() < ACCEPT_PRECISION
+    # no field within the threshold: the 95th-percentile margin accepts none
+    m2 = calibrate_margin(pe, err + 5.0, 1.0)
+    assert not (pe * m2 <= 1.0).any()
