@@ -78,32 +78,41 @@ def test_c1_full(precision, workdir):
 
 
 def test_c2_full_bench_sequence(workdir):
-    """The benchmark's own sequence on the full C2 workload."""
+    """The benchmark's own sequences on the full C2 workload: one step at a
+    time (direct, captured, replayed) and its headline, pipelined launches
+    (five back to back after the warm-up, the last one's fields checked)."""
     spec = W.rd_gauss()
     freqs = W.rd_gauss_freqs()
     assert (spec.nalpha, spec.nrz, spec.nrr, len(freqs)) == (20001, 501, 2001, 10)
     root = write_env(spec, os.path.join(workdir, "c2_full"))
-    with B.Tracer(precision=B.PREC_MIXED) as t:
-        t.setup(root)
-        t.set_frequencies(0, freqs)
-        t.prepare()
-        t.autotune(repeats=1)
-        for _ in range(3):   # direct, captured, replayed
-            t.launch()
-            t.sync()
-        st = t.stats()
-        fields = {i: t.field(0, i)[0] for i in (0, len(freqs) - 1)}
-    assert st["err_bits"] == 0
-    assert st["fields"] == 10 and st["groups"] == 1   # one shared trajectory
-    for i in (0, len(freqs) - 1):
-        s = W.rd_gauss(freq=freqs[i])
-        ref = oracle_field("c2_%d" % i, s)
-        rms, mx, n = tl_err(fields[i], ref["field"][0])
-        print("C2 mixed %.1f Hz: rms %.4f dB max %.2f dB over %d receivers; steps %d/%d" % (
-            freqs[i], rms, mx, n, st["steps"], ref["nsteps"]))
-        assert n > 300000   # 1.0 M receivers, about half of them above 100 dB at 500 Hz
-        assert rms < RMS_MIXED
-        assert st["steps"] == ref["nsteps"]
+    runs = {}
+    for pipe in (False, True):
+        with B.Tracer(precision=B.PREC_MIXED, pipeline=pipe) as t:
+            t.setup(root)
+            t.set_frequencies(0, freqs)
+            t.prepare()
+            t.autotune(repeats=2)
+            for _ in range(3):   # serial: direct, captured, replayed
+                t.launch()
+                t.sync()
+            if pipe:
+                for _ in range(5):
+                    t.launch()
+                t.sync()
+            st = t.stats()
+            runs[pipe] = (st, {i: t.field(0, i)[0] for i in (0, len(freqs) - 1)})
+    for pipe, (st, fields) in runs.items():
+        assert st["err_bits"] == 0
+        assert st["fields"] == 10 and st["groups"] == 1   # one shared trajectory
+        for i in (0, len(freqs) - 1):
+            s = W.rd_gauss(freq=freqs[i])
+            ref = oracle_field("c2_%d" % i, s)
+            rms, mx, n = tl_err(fields[i], ref["field"][0])
+            print("C2 mixed%s %.1f Hz: rms %.4f dB max %.2f dB over %d receivers; steps %d/%d" % (
+                " pipelined" if pipe else "", freqs[i], rms, mx, n, st["steps"], ref["nsteps"]))
+            assert n > 300000   # 1.0 M receivers, about half of them above 100 dB at 500 Hz
+            assert rms < RMS_MIXED
+            assert st["steps"] == ref["nsteps"]
 
 
 def test_c2_full_fp64(workdir):
