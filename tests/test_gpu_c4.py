@@ -47,7 +47,7 @@ def files_sha(files):
 @pytest.mark.parametrize("precision", [B.PREC_FP64, B.PREC_MIXED])
 def test_c4_bearings_tl(precision, workdir):
     """FP64 within 0.1 dB of the reference; the mixed precision (FP32
-    contributions) within the north-star 0.5 dB."""
+    contributions) within the 0.5 dB TL bound."""
     g = np.load(os.path.join(GOLD, "c4_bearings_tl.npz"))
     files = W.c4_3d(run_type="CB   3", ntheta=2)
     assert files_sha(files) == str(g["sha"]), "the seeded C4 generator no longer gives the fixture's inputs"

@@ -15,7 +15,7 @@ oracle run over the whole ray fan on the host's threads:
 * C3 — the 256-environment batch in one run; the first four seeded
   environments of the batch against the oracle.
 
-Tolerances (north star): TL = -20 log10|p| within 0.5 dB RMS over receivers
+Tolerances: TL = -20 log10|p| within 0.5 dB RMS over receivers
 where the oracle TL < 100 dB (mixed precision), 0.1 dB RMS for the FP64 path.
 """
 import os

@@ -1,6 +1,6 @@
 """GPU parity: the product (through the C ABI) against the oracle.
 
-Tolerance (north star): TL = -20 log10|p| within 0.5 dB RMS over receivers where
+Tolerance: TL = -20 log10|p| within 0.5 dB RMS over receivers where
 the oracle TL < 100 dB; the FP64 tracer is also held to a tighter RMS bound.
 """
 import os
