@@ -723,6 +723,320 @@ struct ShdReader {
     }
 };
 
+// List-directed text (the reference's LDIFile as its output readers use it):
+// list() starts a read statement at the next line; values are separated by
+// blanks or commas, strings may be quoted, and a statement continues onto
+// the following lines until it has its values.
+struct ListIn {
+    std::vector<std::string> lines;
+    size_t li = 0, pos = 0;
+    bool started = false;
+    explicit ListIn(const std::string &p)
+    {
+        std::ifstream f(p);
+        if(!f.good()) throw std::runtime_error("cannot open " + p);
+        std::string l;
+        while(std::getline(f, l)) lines.push_back(l);
+    }
+    void list()
+    {
+        if(started) { ++li; pos = 0; }
+        started = true;
+    }
+    bool eof()
+    {
+        size_t k = started ? li + 1 : li;
+        for(; k < lines.size(); ++k)
+            if(lines[k].find_first_not_of(" \t\r,") != std::string::npos) return false;
+        return true;
+    }
+    std::string token()
+    {
+        for(;;) {
+            if(li >= lines.size()) throw std::runtime_error("end of file in a list-directed read");
+            const std::string &l = lines[li];
+            while(pos < l.size() && (l[pos] == ' ' || l[pos] == '\t' || l[pos] == '\r' || l[pos] == ',')) ++pos;
+            if(pos >= l.size()) { ++li; pos = 0; continue; }
+            if(l[pos] == '\'' || l[pos] == '"') {
+                const char q = l[pos];
+                const size_t e = l.find(q, pos + 1);
+                std::string t = l.substr(pos + 1, (e == std::string::npos ? l.size() : e) - pos - 1);
+                pos = e == std::string::npos ? l.size() : e + 1;
+                return t;
+            }
+            size_t e = pos;
+            while(e < l.size() && l[e] != ' ' && l[e] != '\t' && l[e] != '\r' && l[e] != ',') ++e;
+            std::string t = l.substr(pos, e - pos);
+            pos = e;
+            return t;
+        }
+    }
+    double real() { return std::stod(token()); }
+    int32_t integer() { return (int32_t)std::lround(std::stod(token())); }
+};
+
+// Fortran sequential unformatted records ([int32 n][n bytes][int32 n], the
+// reference's UnformattedIFile): rec() moves to the next record, get() reads
+// the record's values in order.
+struct SeqIn {
+    std::vector<char> b;
+    size_t next = 0, cur = 0, end = 0;
+    explicit SeqIn(const std::string &p)
+    {
+        std::ifstream f(p, std::ios::binary);
+        if(!f.good()) throw std::runtime_error("cannot open " + p);
+        b.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    }
+    void rec()
+    {
+        int32_t n = 0;
+        if(next + 4 > b.size()) throw std::runtime_error("end of file in an unformatted read");
+        std::memcpy(&n, b.data() + next, 4);
+        if(n < 0 || next + 8 + (size_t)n > b.size()) throw std::runtime_error("bad record in an unformatted file");
+        cur = next + 4;
+        end = cur + (size_t)n;
+        next = end + 4;
+    }
+    template<typename T> T get()
+    {
+        T v;
+        if(cur + sizeof(T) > end) throw std::runtime_error("record too short in an unformatted file");
+        std::memcpy(&v, b.data() + cur, sizeof(T));
+        cur += sizeof(T);
+        return v;
+    }
+};
+
+// ReadOutArrivals (src/mode/arr.cpp:275-428): header (dimension, frequency,
+// source and receiver coordinates), then per source its largest arrival
+// count and per receiver the count and the records. MaxNArr is the largest
+// count in the file within what the arrival memory of maxMemory holds
+// (src/mode/arr.hpp:74-104); counts above it are cut, with a warning.
+template<bool O3D, bool R3D> void read_arrivals(Internal &in, bhcParams<O3D> &params, bhcOutputs<O3D, R3D> &outputs,
+                                                const std::string &path, bool ascii)
+{
+    std::unique_ptr<ListIn> A;
+    std::unique_ptr<SeqIn> Bf;
+    if(ascii) A.reset(new ListIn(path)); else Bf.reset(new SeqIn(path));
+    auto beginv = [&]() { if(ascii) A->list(); else Bf->rec(); };
+    auto rd_f = [&]() -> double { return ascii ? A->real() : (double)Bf->get<float>(); };
+    auto rd_d = [&]() -> double { return ascii ? A->real() : Bf->get<double>(); };
+    auto rd_i = [&]() -> int32_t { return ascii ? A->integer() : Bf->get<int32_t>(); };
+    std::string dim;
+    if(ascii) {
+        A->list();
+        dim = "'" + A->token() + "'";
+    } else {
+        Bf->rec();
+        char t[4];
+        for(char &c : t) c = Bf->get<char>();
+        dim.assign(t, 4);
+    }
+    if(dim != (O3D ? "'3D'" : "'2D'"))
+        throw std::runtime_error(std::string("incorrect dimensionality in arrivals file, must be ") +
+                                 (O3D ? "'3D'" : "'2D'") + ", got " + dim);
+    beginv();
+    params.freqinfo->freq0 = (float)rd_f();
+    Position &P = *params.Pos;
+    auto rd_array_d = [&](double *&v, int32_t &n) {
+        beginv();
+        n = rd_i();
+        if(n < 1) throw std::runtime_error("bad coordinate count in arrivals file");
+        resize(v, (size_t)n);
+        for(int32_t i = 0; i < n; ++i) v[i] = rd_d();
+    };
+    auto rd_array_f = [&](float *&v, int32_t &n) {
+        beginv();
+        n = rd_i();
+        if(n < 1) throw std::runtime_error("bad coordinate count in arrivals file");
+        resize(v, (size_t)n);
+        for(int32_t i = 0; i < n; ++i) v[i] = (float)rd_f();
+    };
+    if constexpr(O3D) {
+        rd_array_d(P.Sx, P.NSx);
+        rd_array_d(P.Sy, P.NSy);
+    } else {
+        P.NSx = P.NSy = 1;
+    }
+    rd_array_f(P.Sz, P.NSz);
+    rd_array_f(P.Rz, P.NRz);
+    rd_array_d(P.Rr, P.NRr);
+    if constexpr(O3D) {
+        rd_array_d(P.theta, P.Ntheta);
+    } else {
+        P.Ntheta = 1;
+    }
+    if(params.Beam->RunType[4] == 'I')
+        throw std::runtime_error("arrivals readout (and writeout) is not compatible with an irregular grid");
+    P.NRz_per_range = P.NRz;
+    P.RrInKm = false;
+    const size_t nsrc = (size_t)P.NSx * P.NSy * P.NSz;
+    const size_t per_src = (size_t)P.Ntheta * P.NRz * P.NRr;
+    const size_t cells = nsrc * per_src;
+    // every record first (the arrays are sized by the largest count)
+    std::vector<int32_t> narr(cells, 0), maxn(nsrc, 0);
+    std::vector<std::vector<Arrival>> recs(cells);
+    const double DegRad = kPi / 180.0;
+    for(int32_t isz = 0; isz < P.NSz; ++isz)
+        for(int32_t isx = 0; isx < P.NSx; ++isx)
+            for(int32_t isy = 0; isy < P.NSy; ++isy) {
+                const size_t src = ((size_t)isz * P.NSx + isx) * P.NSy + isy;
+                beginv();
+                maxn[src] = rd_i();
+                for(size_t k = 0; k < per_src; ++k) {
+                    // GetFieldAddr order: [isz][isx][isy][itheta][iz][ir]
+                    const size_t cell = src * per_src + k;
+                    beginv();
+                    const int32_t n = rd_i();
+                    if(n < 0) throw std::runtime_error("negative arrival count in arrivals file");
+                    narr[cell] = n;
+                    recs[cell].resize((size_t)n);
+                    for(int32_t a = 0; a < n; ++a) {
+                        Arrival &R = recs[cell][a];
+                        beginv();
+                        R.a = (float)rd_f();
+                        R.Phase = (float)(DegRad * (ascii ? A->real() : (double)Bf->get<float>()));
+                        const float d1 = (float)rd_f(), d2 = (float)rd_f();
+                        R.delay = cpxf(d1, d2);
+                        R.SrcDeclAngle = (float)rd_f();
+                        R.SrcAzimAngle = O3D ? (float)rd_f() : 0.f;
+                        R.RcvrDeclAngle = (float)rd_f();
+                        R.RcvrAzimAngle = O3D ? (float)rd_f() : 0.f;
+                        if(ascii) {
+                            R.NTopBnc = A->integer();
+                            R.NBotBnc = A->integer();
+                        } else {
+                            R.NTopBnc = (int32_t)Bf->get<float>();
+                            R.NBotBnc = (int32_t)Bf->get<float>();
+                        }
+                    }
+                }
+            }
+    int64_t mem = (int64_t)in.init.maxMemory - (int64_t)(cells * sizeof(int32_t)) - (int64_t)(nsrc * sizeof(int32_t)) - 96;
+    mem = std::max<int64_t>(mem, 0);
+    const int64_t fit = mem / (int64_t)(cells * sizeof(Arrival));
+    if(fit == 0) throw std::runtime_error("insufficient memory to allocate arrivals");
+    int32_t most = 1;
+    for(int32_t n : narr) most = std::max(most, n);
+    const int32_t mx = (int32_t)std::min<int64_t>(most, std::min<int64_t>(fit, 0x7fffffff));
+    free_outputs(outputs);
+    outputs.arrinfo = new ArrInfo{};
+    outputs.eigen = new EigenInfo{};
+    outputs.rayinfo = new RayInfo<O3D, R3D>{};
+    ArrInfo &I = *outputs.arrinfo;
+    I.MaxNArr = mx;
+    I.AllowMerging = in.init.numThreads == 1;
+    I.NArr = new int32_t[cells];
+    I.Arr = new Arrival[cells * (size_t)mx]();
+    I.MaxNPerSource = new int32_t[nsrc];
+    for(size_t s2 = 0; s2 < nsrc; ++s2) I.MaxNPerSource[s2] = maxn[s2];
+    for(size_t c = 0; c < cells; ++c) {
+        const int32_t keep = std::min(narr[c], mx);
+        if(keep < narr[c]) {
+            char m[160];
+            snprintf(m, sizeof m, "%d arrivals in file at receiver cell %zu, but only memory for %d", narr[c], c, keep);
+            say(in, m);
+        }
+        I.NArr[c] = keep;
+        for(int32_t a = 0; a < keep; ++a) I.Arr[c * (size_t)mx + a] = recs[c][a];
+    }
+}
+
+// ReadOutRay (src/mode/ray.cpp:203-370): header (title, frequency, source
+// and angle counts, boundary depths, 'rz' or 'xyz'), then per ray its
+// take-off angle, its point count with the last point's bounce counts, and
+// its points. Nx2D rays (xyz in the file) come back in their plane's
+// (range from the first point, depth) coordinates.
+template<bool O3D, bool R3D> void read_rays(Internal &in, bhcParams<O3D> &params, bhcOutputs<O3D, R3D> &outputs,
+                                            const std::string &path)
+{
+    ListIn L(path);
+    L.list();
+    set_title(params.Title, L.token().c_str());
+    L.list();
+    params.freqinfo->freq0 = L.real();
+    L.list();
+    const int32_t nsx = L.integer(), nsy = L.integer(), nsz = L.integer();
+    if(nsx != params.Pos->NSx || nsy != params.Pos->NSy || nsz != params.Pos->NSz) {
+        char m[160];
+        snprintf(m, sizeof m, "NSx = %d, NSy = %d, NSz = %d in the ray file, but %d, %d, %d in the setup", nsx, nsy,
+                 nsz, params.Pos->NSx, params.Pos->NSy, params.Pos->NSz);
+        say(in, m);
+    }
+    L.list();
+    (void)L.integer();
+    (void)L.integer();
+    L.list();
+    (void)L.real();
+    (void)L.real();
+    L.list();
+    const std::string dim = L.token();
+    if(dim != (O3D ? "xyz" : "rz"))
+        throw std::runtime_error("dimensionality in the ray file is '" + dim + "', must be " + (O3D ? "'xyz'" : "'rz'"));
+    struct One {
+        double alpha;
+        int32_t n, ntop, nbot;
+        std::vector<double> pts;
+    };
+    std::vector<One> rays;
+    const int nc = O3D ? 3 : 2;
+    while(!L.eof()) {
+        One r;
+        L.list();
+        r.alpha = L.real();
+        if(!std::isfinite(r.alpha)) break;
+        L.list();
+        r.n = L.integer();
+        r.ntop = L.integer();
+        r.nbot = L.integer();
+        if(r.n <= 0) throw std::runtime_error("<= 0 points in a ray of the ray file");
+        if(r.ntop < 0 || r.nbot < 0) throw std::runtime_error("invalid number of bounces in a ray of the ray file");
+        r.pts.resize((size_t)r.n * nc);
+        for(int32_t k = 0; k < r.n; ++k) {
+            L.list();
+            for(int c = 0; c < nc; ++c) r.pts[(size_t)k * nc + c] = L.real();
+        }
+        rays.push_back(std::move(r));
+    }
+    free_outputs(outputs);
+    outputs.arrinfo = new ArrInfo{};
+    outputs.eigen = new EigenInfo{};
+    outputs.rayinfo = new RayInfo<O3D, R3D>{};
+    RayInfo<O3D, R3D> &RI = *outputs.rayinfo;
+    RI.NRays = (int32_t)rays.size();
+    RI.results = new RayResult<O3D, R3D>[rays.size() ? rays.size() : 1]();
+    for(size_t i = 0; i < rays.size(); ++i) {
+        const One &r = rays[i];
+        RayResult<O3D, R3D> &res = RI.results[i];
+        res.Nsteps = r.n;
+        res.SrcDeclAngle = O3D ? r.alpha * (180.0 / kPi) : r.alpha;
+        res.ray = new rayPt<R3D>[r.n]();
+        double tx = 1.0, ty = 0.0;
+        if constexpr(O3D && !R3D) {
+            // the plane's radial direction: first to last point (OceanToRayX)
+            const double *p0 = &r.pts[0], *p1 = &r.pts[(size_t)(r.n - 1) * 3];
+            const double dx = p1[0] - p0[0], dy = p1[1] - p0[1], l = std::sqrt(dx * dx + dy * dy);
+            if(l > 0) { tx = dx / l; ty = dy / l; }
+        }
+        for(int32_t k = 0; k < r.n; ++k) {
+            const double *q = &r.pts[(size_t)k * nc];
+            if constexpr(!O3D) {
+                res.ray[k].x.x = q[0];
+                res.ray[k].x.y = q[1];
+            } else if constexpr(R3D) {
+                res.ray[k].x.x = q[0];
+                res.ray[k].x.y = q[1];
+                res.ray[k].x.z = q[2];
+            } else {
+                res.ray[k].x.x = (q[0] - r.pts[0]) * tx + (q[1] - r.pts[1]) * ty;
+                res.ray[k].x.y = q[2];
+            }
+        }
+        res.ray[r.n - 1].NumTopBnc = r.ntop;
+        res.ray[r.n - 1].NumBotBnc = r.nbot;
+    }
+}
+
 template<typename F> auto guard(const char *what, const void *internal, F &&fn) -> decltype(fn())
 {
     try {
@@ -882,6 +1196,21 @@ template<bool O3D, bool R3D> bool readout(bhcParams<O3D> &params, bhcOutputs<O3D
 {
     return guard("readout", params.internal, [&]() -> bool {
         if(!FileRoot) throw std::runtime_error("FileRoot is null");
+        // the mode of the setup's RunType picks the file (GetMode, src/api.cpp:367-382)
+        const char run0 = params.Beam->RunType[0];
+        Internal &in = internal_of(params);
+        if(run0 == 'A' || run0 == 'a') {
+            read_arrivals(in, params, outputs, std::string(FileRoot) + ".arr", run0 == 'A');
+            return true;
+        }
+        if(run0 == 'V' || run0 == 'v') throw std::runtime_error("ReadOutArrivals called while not in arrivals mode");
+        if(run0 == 'R') {
+            read_rays(in, params, outputs, std::string(FileRoot) + ".ray");
+            return true;
+        }
+        if(run0 == 'E') return true;   // the eigenray mode reads nothing back
+        if(run0 != 'C' && run0 != 'S' && run0 != 'I')
+            throw std::runtime_error(std::string("invalid RunType ") + run0);
         // .shd (src/mode/tl.cpp:38-248): 10 header records, then one record
         // per (Sx, Sy, bearing, Sz, receiver depth) row of NRr complex values
         ShdReader r(std::string(FileRoot) + ".shd");

@@ -11,8 +11,15 @@
 //   bhc_api_check nonblocking <file root>
 //       extsetup_blocking(false): run returns at once, postprocess waits,
 //       completedCallback fires once, progress ends at 100.
+//   bhc_api_check readout <2|3|4> <file root>
+//       setup from the files (2-D, 3-D or Nx2D) and readout of the run's
+//       output file (.arr for RunType 'A' / 'a', .ray for 'R'); prints the
+//       counts and sums the test compares with its own reading of the file;
+//       needs no GPU.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -190,8 +197,69 @@ static int check_nonblocking(const char *root)
     return failures ? 1 : 0;
 }
 
+template<bool O3D, bool R3D> static int check_readout(const char *root)
+{
+    using namespace bhc;
+    bhcParams<O3D> p;
+    bhcOutputs<O3D, R3D> o;
+    if(!setup(make_init(root), p, o)) return 2;
+    if(!readout(p, o, root)) {
+        finalize(p, o);
+        return 3;
+    }
+    const char run0 = p.Beam->RunType[0];
+    if(run0 == 'A' || run0 == 'a') {
+        const ArrInfo &A = *o.arrinfo;
+        const Position &P = *p.Pos;
+        const size_t cells = (size_t)P.NSx * P.NSy * P.NSz * P.Ntheta * P.NRz * P.NRr;
+        double s[10] = {0};
+        long long total = 0;
+        for(size_t c = 0; c < cells; ++c)
+            for(int k = 0; k < A.NArr[c]; ++k) {
+                const Arrival &r = A.Arr[c * A.MaxNArr + k];
+                ++total;
+                s[0] += r.a; s[1] += r.Phase; s[2] += r.delay.real(); s[3] += r.delay.imag();
+                s[4] += r.SrcDeclAngle; s[5] += r.SrcAzimAngle; s[6] += r.RcvrDeclAngle; s[7] += r.RcvrAzimAngle;
+                s[8] += r.NTopBnc; s[9] += r.NBotBnc;
+            }
+        int maxsrc = 0;
+        for(int k = 0; k < P.NSx * P.NSy * P.NSz; ++k) maxsrc = std::max(maxsrc, A.MaxNPerSource[k]);
+        std::printf("arr %d %d %d %d %d %d %.9g %lld %d %d", P.NSx, P.NSy, P.NSz, P.Ntheta, P.NRz, P.NRr,
+                    (double)p.freqinfo->freq0, total, A.MaxNArr, maxsrc);
+        for(double v : s) std::printf(" %.17g", v);
+        std::printf("\n");
+    } else if(run0 == 'R') {
+        const RayInfo<O3D, R3D> &R = *o.rayinfo;
+        long long pts = 0;
+        double s[6] = {0};
+        for(int i = 0; i < R.NRays; ++i) {
+            const RayResult<O3D, R3D> &r = R.results[i];
+            pts += r.Nsteps;
+            s[0] += r.SrcDeclAngle;
+            for(int k = 0; k < r.Nsteps; ++k) {
+                s[1] += r.ray[k].x.x;
+                s[2] += r.ray[k].x.y;
+                if constexpr(R3D) s[3] += r.ray[k].x.z;
+            }
+            s[4] += r.ray[r.Nsteps - 1].NumTopBnc;
+            s[5] += r.ray[r.Nsteps - 1].NumBotBnc;
+        }
+        std::printf("ray %d %lld", R.NRays, pts);
+        for(double v : s) std::printf(" %.17g", v);
+        std::printf("\n");
+    }
+    finalize(p, o);
+    std::printf(failures ? "FAILED %d\n" : "OK\n", failures);
+    return failures ? 1 : 0;
+}
+
 int main(int argc, char **argv)
 {
+    if(argc >= 4 && std::strcmp(argv[1], "readout") == 0) {
+        const int d = std::atoi(argv[2]);
+        return d == 3 ? check_readout<true, true>(argv[3]) : d == 4 ? check_readout<true, false>(argv[3])
+                                                                    : check_readout<false, false>(argv[3]);
+    }
     if(argc >= 3 && std::strcmp(argv[1], "params") == 0) return check_params(argv[2]);
     if(argc >= 4 && std::strcmp(argv[1], "run") == 0) return check_run(argv[2], argv[3], argc >= 5 ? argv[4] : nullptr);
     if(argc >= 3 && std::strcmp(argv[1], "nonblocking") == 0) return check_nonblocking(argv[2]);

@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 
+import numpy as np
 import pytest
 
 from bellhopcuda_b200 import build as BUILD
@@ -51,3 +52,95 @@ def test_params_roundtrip(tmp_path):
     assert r.stdout.strip().endswith("OK")
     env = open(os.path.join(tmp_path, "edited.env")).read()
     assert "'R~'" in env and os.path.exists(os.path.join(tmp_path, "edited.bty"))
+
+
+def _arr_ascii(text: str, is3d: bool) -> dict:
+    """The ASCII arrivals file as the test reads it: one statement per line."""
+    lines = [ln.replace(",", " ").split() for ln in text.splitlines() if ln.strip()]
+    k = 2
+    dims = []
+    for _ in range(6 if is3d else 3):
+        dims.append(int(lines[k][0]))
+        k += 1
+    if is3d:
+        nsx, nsy, nsz, nrz, nrr, nth = dims
+    else:
+        (nsz, nrz, nrr), nsx, nsy, nth = dims, 1, 1, 1
+    nf = 10 if is3d else 8
+    maxn, recs = [], []
+    for _ in range(nsz * nsx * nsy):
+        maxn.append(int(lines[k][0]))
+        k += 1
+        for _ in range(nth * nrz * nrr):
+            n = int(lines[k][0])
+            k += 1
+            for _ in range(n):
+                recs.append([float(v) for v in lines[k][:nf]])
+                k += 1
+    return dict(dims=(nsx, nsy, nsz, nth, nrz, nrr), freq=float(lines[1][0]), maxn=maxn,
+                recs=np.array(recs).reshape(-1, nf))
+
+
+@pytest.mark.parametrize("case", ["ro2d_A", "ro2d_a", "ro2d_R", "ro3d_A", "ro3d_a", "ro3d_R", "ronx_a", "ronx_R"])
+def test_readout_reference_files(case, tmp_path):
+    """bhc::readout of .arr (ASCII and binary) and .ray files that the
+    reference itself wrote (2-D, 3-D, Nx2D; tests/golden/make_golden_readout.py):
+    the coordinates, counts and every record come back (sums compared with the
+    test's own reading of the file)."""
+    from bellhopcuda_b200.arrfile import read_arr_binary
+    from bellhopcuda_b200.rayfile import read_ray
+    g = np.load(os.path.join(HERE, "golden", "readout_cases.npz"))
+    dim, suffix = int(g[case + "_dim"]), str(g[case + "_suffix"])
+    root = os.path.join(str(tmp_path), case)
+    with open(root + ".env", "w") as f:
+        f.write(str(g[case + "_env"]))
+    data = g[case + "_out"].tobytes()
+    with open(root + suffix, "wb") as f:
+        f.write(data)
+    exe = build_check(str(tmp_path))
+    r = subprocess.run([exe, "readout", str(dim), root], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = [ln for ln in r.stdout.splitlines() if ln.startswith(("arr ", "ray "))][0].split()
+    is3d = dim != 2
+    if suffix == ".arr":
+        if case.endswith("_a"):
+            A = read_arr_binary(root + ".arr")
+            dims = (len(A["sx"]), len(A["sy"]), len(A["sz"]), len(A["theta"]), len(A["rz"]), len(A["rr"]))
+            recs = np.concatenate([a for s in A["sources"] for a in s["arrivals"]]).astype(np.float64)
+            maxn, freq = [s["maxn"] for s in A["sources"]], A["freq"]
+        else:
+            A = _arr_ascii(data.decode(), is3d)
+            dims, recs, maxn, freq = A["dims"], A["recs"], A["maxn"], A["freq"]
+        assert tuple(int(v) for v in out[1:7]) == dims
+        assert abs(float(out[7]) - freq) <= 1e-6 * freq
+        assert int(out[8]) == len(recs) > 0
+        assert int(out[9]) >= max(maxn) and int(out[10]) == max(maxn)
+        if not is3d:   # 2-D records carry no azimuths
+            z = np.zeros((len(recs), 1))
+            recs = np.hstack([recs[:, :5], z, recs[:, 5:6], z, recs[:, 6:]])
+        phase = np.float32(np.deg2rad(recs[:, 1]))
+        want = [recs[:, 0].astype(np.float32).sum(), phase.astype(np.float64).sum()] + \
+            [recs[:, k].astype(np.float32).astype(np.float64).sum() for k in range(2, 10)]
+        got = [float(v) for v in out[11:21]]
+        np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-9)
+    else:
+        R = read_ray(root + ".ray")
+        rays = R["rays"]
+        assert int(out[1]) == len(rays) > 0
+        assert int(out[2]) == sum(len(x["xy"]) for x in rays)
+        alpha = sum(np.rad2deg(x["alpha"]) if is3d else x["alpha"] for x in rays)
+        sx = sy = sz = 0.0
+        for x in rays:
+            p = x["xy"]
+            if dim == 4:   # Nx2D: range along the plane from the first point, depth
+                d = p[-1, :2] - p[0, :2]
+                t = d / np.hypot(*d) if np.hypot(*d) > 0 else np.array([1.0, 0.0])
+                sx += ((p[:, :2] - p[0, :2]) @ t).sum()
+                sy += p[:, 2].sum()
+            else:
+                sx += p[:, 0].sum()
+                sy += p[:, 1].sum()
+                sz += p[:, 2].sum() if dim == 3 else 0.0
+        got = [float(v) for v in out[3:9]]
+        want = [alpha, sx, sy, sz, sum(x["ntop"] for x in rays), sum(x["nbot"] for x in rays)]
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-6 * max(1.0, abs(sx)))
