@@ -1256,7 +1256,20 @@ template<bool O3D> bool writeenv(bhcParams<O3D> &params, const char *FileRoot)
     return guard("writeenv", params.internal, [&]() -> bool {
         if(!FileRoot) throw std::runtime_error("FileRoot is null");
         if constexpr(O3D) {
-            throw std::runtime_error("writeenv covers 2-D parameters");
+            // 3-D and Nx2D parameters are the setup's files (this library runs
+            // them from FileRoot): write them again under the new root
+            Internal &in = internal_of(params);
+            if(in.root.empty()) throw std::runtime_error("3-D and Nx2D setups need FileRoot");
+            bool any = false;
+            for(const char *ext : {".env", ".ssp", ".bty", ".ati", ".sbp", ".trc", ".brc"}) {
+                std::ifstream src(in.root + ext, std::ios::binary);
+                if(!src.good()) continue;
+                std::ofstream dst(std::string(FileRoot) + ext, std::ios::binary);
+                if(!dst.good()) throw std::runtime_error(std::string("cannot write ") + FileRoot + ext);
+                dst << src.rdbuf();
+                any = any || std::strcmp(ext, ".env") == 0;
+            }
+            if(!any) throw std::runtime_error("cannot read " + in.root + ".env");
         } else {
             DescOf d(params);
             write_env_files(d.d, FileRoot);

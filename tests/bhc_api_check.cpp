@@ -11,6 +11,9 @@
 //   bhc_api_check nonblocking <file root>
 //       extsetup_blocking(false): run returns at once, postprocess waits,
 //       completedCallback fires once, progress ends at 100.
+//   bhc_api_check writeenv <2|3|4> <file root> <new root>
+//       setup from the files, writeenv to the new root, setup from those;
+//       the two setups agree. Needs no GPU.
 //   bhc_api_check readout <2|3|4> <file root>
 //       setup from the files (2-D, 3-D or Nx2D) and readout of the run's
 //       output file (.arr for RunType 'A' / 'a', .ray for 'R'); prints the
@@ -253,8 +256,33 @@ template<bool O3D, bool R3D> static int check_readout(const char *root)
     return failures ? 1 : 0;
 }
 
+template<bool O3D, bool R3D> static int check_writeenv(const char *root, const char *newroot)
+{
+    using namespace bhc;
+    bhcParams<O3D> p;
+    bhcOutputs<O3D, R3D> o;
+    if(!setup(make_init(root), p, o)) return 2;
+    EXPECT(writeenv(p, newroot));
+    bhcParams<O3D> q;
+    bhcOutputs<O3D, R3D> qo;
+    EXPECT(setup(make_init(newroot), q, qo));
+    EXPECT(std::strncmp(p.Title, q.Title, 80) == 0);
+    EXPECT(p.Pos->NSz == q.Pos->NSz && p.Pos->NRz == q.Pos->NRz && p.Pos->NRr == q.Pos->NRr);
+    EXPECT(p.Pos->Ntheta == q.Pos->Ntheta && p.Beam->RunType[0] == q.Beam->RunType[0]);
+    finalize(q, qo);
+    finalize(p, o);
+    std::printf(failures ? "FAILED %d\n" : "OK\n", failures);
+    return failures ? 1 : 0;
+}
+
 int main(int argc, char **argv)
 {
+    if(argc >= 5 && std::strcmp(argv[1], "writeenv") == 0) {
+        const int d = std::atoi(argv[2]);
+        return d == 3 ? check_writeenv<true, true>(argv[3], argv[4])
+                      : d == 4 ? check_writeenv<true, false>(argv[3], argv[4])
+                               : check_writeenv<false, false>(argv[3], argv[4]);
+    }
     if(argc >= 4 && std::strcmp(argv[1], "readout") == 0) {
         const int d = std::atoi(argv[2]);
         return d == 3 ? check_readout<true, true>(argv[3]) : d == 4 ? check_readout<true, false>(argv[3])

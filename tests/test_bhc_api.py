@@ -144,3 +144,23 @@ def test_readout_reference_files(case, tmp_path):
         got = [float(v) for v in out[3:9]]
         want = [alpha, sx, sy, sz, sum(x["ntop"] for x in rays), sum(x["nbot"] for x in rays)]
         np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-6 * max(1.0, abs(sx)))
+
+
+@pytest.mark.parametrize("case", ["seamount3d_gauss", "hex3d_nx2d_hat", "munk3d_gauss"])
+def test_writeenv_3d_and_nx2d(case, tmp_path):
+    """writeenv of a 3-D / Nx2D setup writes its files under the new root
+    (.env and the boundary / SSP files), which set up the same run."""
+    g = np.load(os.path.join(HERE, "golden", case + ".npz"))
+    root = os.path.join(str(tmp_path), case)
+    for k in g.files:
+        if k.startswith("file_"):
+            with open(root + "." + k[5:], "w") as f:
+                f.write(str(g[k]))
+    dim = "4" if "nx2d" in case else "3"
+    exe = build_check(str(tmp_path))
+    new = os.path.join(str(tmp_path), "copy")
+    r = subprocess.run([exe, "writeenv", dim, root, new], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip().endswith("OK"), r.stdout + r.stderr
+    for k in g.files:
+        if k.startswith("file_"):
+            assert open(new + "." + k[5:]).read() == str(g[k])
