@@ -43,6 +43,7 @@ struct Internal {
     std::atomic<int> progress{100};
     std::atomic<bool> ok{true};
     std::string error;
+    std::ofstream prt;           // FileRoot.prt when there is no prtCallback
 };
 
 Internal *state(const void *p) { return static_cast<Internal *>(const_cast<void *>(p)); }
@@ -51,6 +52,15 @@ void say(const Internal &in, const std::string &m)
 {
     if(in.init.outputCallback) in.init.outputCallback(m.c_str());
     else std::printf("%s\n", m.c_str());
+}
+
+// PRT text: to prtCallback, else to FileRoot.prt (opened by setup), else
+// stdout (PrintFileEmu, src/util/prtfileemu.hpp:30-60)
+void prt(Internal &in, const std::string &m)
+{
+    if(in.init.prtCallback) in.init.prtCallback(m.c_str());
+    else if(in.prt.is_open()) in.prt << m << std::flush;
+    else std::printf("%s", m.c_str());
 }
 
 std::string last_error(bhcb_ctx *ctx)
@@ -1056,6 +1066,23 @@ template<typename F> auto guard(const char *what, const void *internal, F &&fn) 
 } // namespace
 
 // ------------------------------------------------------------------ setup
+// the parameters' summary that setup and echo write as PRT text
+template<bool O3D> std::string echo_text(const bhcParams<O3D> &params)
+{
+    std::ostringstream o;
+    o << "bhcb (B200) - " << params.Title << "\n";
+    o << " frequency = " << params.freqinfo->freq0 << " Hz\n";
+    o << " number of sources = " << params.Pos->NSz << ", receiver depths = " << params.Pos->NRz
+      << ", receiver ranges = " << params.Pos->NRr << "\n";
+    if(!O3D) {
+        o << " SSP type '" << params.ssp->Type << "', " << params.ssp->NPts << " points, depth "
+          << params.Bdry->Bot.hs.Depth << " m\n";
+        o << " run type '" << std::string(params.Beam->RunType, 7) << "', beams " << params.Angles->alpha.n
+          << "\n";
+    }
+    return o.str();
+}
+
 template<bool O3D, bool R3D> bool setup(const bhcInit &init, bhcParams<O3D> &params, bhcOutputs<O3D, R3D> &outputs)
 {
     std::memset(static_cast<void *>(&params), 0, sizeof params);
@@ -1066,6 +1093,10 @@ template<bool O3D, bool R3D> bool setup(const bhcInit &init, bhcParams<O3D> &par
     in->dim = !O3D ? 2 : (R3D ? 3 : 4);
     params.internal = in;
     alloc_params(params);
+    if(!init.prtCallback && !in->root.empty()) {
+        in->prt.open(in->root + ".prt");
+        if(!in->prt.is_open()) say(*in, "could not open print file " + in->root + ".prt");
+    }
     return guard("setup", in, [&]() -> bool {
         if constexpr(!O3D) {
             if(!in->root.empty()) {
@@ -1111,6 +1142,9 @@ template<bool O3D, bool R3D> bool setup(const bhcInit &init, bhcParams<O3D> &par
                 }
             }
         }
+        // the input echo as PRT text (the reference's readers write it while
+        // they read); a setup from the defaults without a callback prints none
+        if(init.prtCallback || in->prt.is_open()) prt(*in, echo_text(params));
         return true;
     });
 }
@@ -1118,20 +1152,7 @@ template<bool O3D, bool R3D> bool setup(const bhcInit &init, bhcParams<O3D> &par
 template<bool O3D> bool echo(bhcParams<O3D> &params)
 {
     return guard("echo", params.internal, [&]() -> bool {
-        Internal &in = internal_of(params);
-        std::ostringstream o;
-        o << "bhcb (B200) - " << params.Title << "\n";
-        o << " frequency = " << params.freqinfo->freq0 << " Hz\n";
-        o << " number of sources = " << params.Pos->NSz << ", receiver depths = " << params.Pos->NRz
-          << ", receiver ranges = " << params.Pos->NRr << "\n";
-        if(!O3D) {
-            o << " SSP type '" << params.ssp->Type << "', " << params.ssp->NPts << " points, depth "
-              << params.Bdry->Bot.hs.Depth << " m\n";
-            o << " run type '" << std::string(params.Beam->RunType, 7) << "', beams " << params.Angles->alpha.n
-              << "\n";
-        }
-        if(in.init.prtCallback) in.init.prtCallback(o.str().c_str());
-        else std::printf("%s", o.str().c_str());
+        prt(internal_of(params), echo_text(params));
         return true;
     });
 }

@@ -271,6 +271,22 @@ template<bool O3D, bool R3D> static int check_writeenv(const char *root, const c
     EXPECT(p.Pos->Ntheta == q.Pos->Ntheta && p.Beam->RunType[0] == q.Beam->RunType[0]);
     finalize(q, qo);
     finalize(p, o);
+    // without a prtCallback the PRT text goes to FileRoot.prt
+    bhcInit quiet = make_init(newroot);
+    quiet.prtCallback = nullptr;
+    bhcParams<O3D> r;
+    bhcOutputs<O3D, R3D> ro;
+    EXPECT(setup(quiet, r, ro));
+    EXPECT(echo(r));
+    finalize(r, ro);
+    FILE *f = std::fopen((std::string(newroot) + ".prt").c_str(), "r");
+    EXPECT(f != nullptr);
+    if(f) {
+        char line[256] = {0};
+        EXPECT(std::fgets(line, sizeof line, f) != nullptr);
+        EXPECT(std::strstr(line, "bhcb (B200)") != nullptr);
+        std::fclose(f);
+    }
     std::printf(failures ? "FAILED %d\n" : "OK\n", failures);
     return failures ? 1 : 0;
 }
