@@ -1,4 +1,5 @@
-"""Reader for binary BELLHOP arrivals files (``.arr`` written for RunType 'a').
+"""Readers for BELLHOP arrivals files (``.arr``): binary (RunType 'a') and
+ASCII ('A').
 
 Layout follows the reference writer (src/mode/arr.cpp:88-239): Fortran
 sequential unformatted records ([int32 n][n bytes][int32 n]); a header of
@@ -49,5 +50,48 @@ def read_arr_binary(path: str) -> dict:
             narr = int(np.frombuffer(next(recs), "<i4", 1)[0])
             arrs = [np.frombuffer(next(recs), "<f4", nf).copy() for _ in range(narr)]
             src.append(np.array(arrs, dtype=np.float32).reshape(narr, nf))
+        out.append(dict(maxn=maxn, arrivals=src))
+    return dict(dim=dim, freq=freq, sx=sx, sy=sy, sz=sz, rz=rz, rr=rr, theta=theta, sources=out)
+
+
+def read_arr_ascii(path: str) -> dict:
+    """2-D or 3-D ASCII arrivals (RunType 'A'), the same layout as the binary
+    file as list-directed text: the dimension ('2D' / '3D'), the frequency,
+    one line per coordinate array (count, values), then per source its
+    largest arrival count and per receiver the count and one line per
+    arrival. Returns the read_arr_binary dictionary (records as float32)."""
+    lines = [ln.replace(",", " ").split() for ln in open(path) if ln.strip()]
+    dim = "'" + lines[0][0].strip("'") + "'"
+    is3d = "3" in dim
+    freq = float(lines[1][0])
+    k = 2
+
+    def arr(dtype):
+        nonlocal k
+        n = int(lines[k][0])
+        vals = [float(v) for v in lines[k][1:1 + n]]
+        k += 1
+        while len(vals) < n:   # a list-directed statement may continue on the next lines
+            vals += [float(v) for v in lines[k]]
+            k += 1
+        return np.array(vals[:n], dtype)
+
+    sx = sy = np.zeros(1)
+    if is3d:
+        sx, sy = arr(np.float64), arr(np.float64)
+    sz, rz, rr = arr(np.float32), arr(np.float32), arr(np.float64)
+    theta = arr(np.float64) if is3d else np.zeros(1)
+    nf = 10 if is3d else 8
+    out = []
+    for _src in range(len(sz) * len(sx) * len(sy)):
+        maxn = int(lines[k][0])
+        k += 1
+        src = []
+        for _ in range(len(theta) * len(rz) * len(rr)):
+            narr = int(lines[k][0])
+            k += 1
+            a = np.array([[float(v) for v in lines[k + j][:nf]] for j in range(narr)], np.float32)
+            k += narr
+            src.append(a.reshape(narr, nf))
         out.append(dict(maxn=maxn, arrivals=src))
     return dict(dim=dim, freq=freq, sx=sx, sy=sy, sz=sz, rz=rz, rr=rr, theta=theta, sources=out)

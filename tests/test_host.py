@@ -313,3 +313,25 @@ def test_surrogate_acceptance_calibration():
     # no field within the threshold: the 95th-percentile margin accepts none
     m2 = calibrate_margin(pe, err + 5.0, 1.0)
     assert not (pe * m2 <= 1.0).any()
+
+
+def test_arrivals_ascii_and_binary_files_agree(workdir):
+    """The reference's ASCII ('A') and binary ('a') arrivals of one 2-D run
+    (tests/golden/make_golden_readout.py) read alike: the same receivers and
+    counts, values within the ASCII file's printed digits."""
+    from bellhopcuda_b200.arrfile import read_arr_ascii, read_arr_binary
+    g = np.load(os.path.join(HERE, "golden", "readout_cases.npz"))
+    paths = {}
+    for case in ("ro2d_A", "ro2d_a"):
+        paths[case] = os.path.join(workdir, case + ".arr")
+        with open(paths[case], "wb") as f:
+            f.write(g[case + "_out"].tobytes())
+    A, Bn = read_arr_ascii(paths["ro2d_A"]), read_arr_binary(paths["ro2d_a"])
+    assert A["dim"] == Bn["dim"] == "'2D'" and A["freq"] == Bn["freq"]
+    for k in ("sz", "rz", "rr"):
+        np.testing.assert_allclose(A[k], Bn[k], rtol=1e-6)
+    for sa, sb in zip(A["sources"], Bn["sources"]):
+        assert sa["maxn"] == sb["maxn"]
+        for a, b in zip(sa["arrivals"], sb["arrivals"]):
+            assert a.shape == b.shape
+            np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-6)
