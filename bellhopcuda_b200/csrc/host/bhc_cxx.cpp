@@ -1317,7 +1317,15 @@ template<bool O3D, bool R3D> bool get_ssp(bhcParams<O3D> &params, const VEC23<R3
     return guard("get_ssp", params.internal, [&]() -> bool {
         Internal &in = internal_of(params);
         if constexpr(O3D) {
-            throw std::runtime_error("get_ssp covers 2-D parameters");
+            // the setup's files' tables, interpolated on the host; an Nx2D
+            // point (range, depth) is taken on the plane along x through the
+            // origin, (r, 0, z) (the reference's Origin is left unset there)
+            if(in.root.empty()) throw std::runtime_error("3-D and Nx2D setups need FileRoot");
+            const bhcb::Env3Tables T = bhcb::preprocess3d(bhcb::read_env_files(in.root, true), params.freqinfo->freq0);
+            double c;
+            if constexpr(R3D) c = bhcb::ssp_at3(T, x.x, x.y, x.z);
+            else c = bhcb::ssp_at3(T, x.x, 0.0, x.y);
+            sound_speed = (float)c;
         } else {
             // host interpolation of the tables the tracer uses; no GPU needed
             (void)in;

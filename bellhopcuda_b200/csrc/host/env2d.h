@@ -155,5 +155,6 @@ EnvInput env_from_desc(const bhcb_env_desc &d);
 bhcb_env_desc *desc_from_env(const EnvInput &in);   // owns its arrays; free_desc releases it
 void free_desc(bhcb_env_desc *d);
 double ssp_at(const EnvTables &T, double r, double z);   // sound speed (m/s) at range r, depth z (m)
+double ssp_at3(const Env3Tables &T, double x, double y, double z);   // 3-D: at (x, y, z) (m)
 
 } // namespace bhcb

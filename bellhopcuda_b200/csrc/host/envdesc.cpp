@@ -252,4 +252,36 @@ double ssp_at(const EnvTables &T, double r, double z)
     }
 }
 
+// Sound speed at (x, y, z) of a 3-D environment: the hexahedral grid's
+// trilinear interpolation (src/ssp.hpp:220-305: c at the cell's four depth
+// columns from c + dz * dc/dz, then blended in x and y), or the 1-D profile in
+// depth.
+double ssp_at3(const Env3Tables &T, double x, double y, double z)
+{
+    if(T.ssp_type != SSP_HEXAHEDRAL) {
+        EnvTables P;
+        P.ssp_type = T.ssp_type;
+        P.z = T.z; P.c = T.c; P.cz = T.cz; P.n2 = T.n2; P.n2z = T.n2z; P.coef = T.coef;
+        return ssp_at(P, 0.0, z);
+    }
+    const int nx = (int)T.hx.size(), ny = (int)T.hy.size(), nz = (int)T.hz.size();
+    if(nx < 2 || ny < 2 || nz < 2) throw std::invalid_argument("hexahedral SSP grid has fewer than 2 nodes per axis");
+    if(x < T.hx[0] || x > T.hx[nx - 1] || y < T.hy[0] || y > T.hy[ny - 1])
+        throw std::invalid_argument("point outside the hexahedral SSP grid");
+    auto seg = [](const std::vector<double> &g, double v) {
+        int i = 0;
+        while(i < (int)g.size() - 2 && v >= g[i + 1]) ++i;
+        return i;
+    };
+    const int ix = seg(T.hx, x), iy = seg(T.hy, y), iz = seg(T.hz, z);
+    auto c_at = [&](int jx, int jy) {
+        return T.hc[((size_t)jx * ny + jy) * nz + iz] + (z - T.hz[iz]) * T.hcz[((size_t)jx * ny + jy) * (nz - 1) + iz];
+    };
+    const double c11 = c_at(ix, iy), c21 = c_at(ix + 1, iy), c12 = c_at(ix, iy + 1), c22 = c_at(ix + 1, iy + 1);
+    const double s1 = std::min(1.0, std::max(0.0, (x - T.hx[ix]) / (T.hx[ix + 1] - T.hx[ix])));
+    const double s2 = std::min(1.0, std::max(0.0, (y - T.hy[iy]) / (T.hy[iy + 1] - T.hy[iy])));
+    const double c1 = c11 + s2 * (c12 - c11), c2 = c21 + s2 * (c22 - c21);
+    return c1 + s1 * (c2 - c1);
+}
+
 } // namespace bhcb

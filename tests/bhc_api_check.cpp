@@ -14,6 +14,8 @@
 //   bhc_api_check writeenv <2|3|4> <file root> <new root>
 //       setup from the files, writeenv to the new root, setup from those;
 //       the two setups agree. Needs no GPU.
+//   bhc_api_check ssp <3|4> <file root> <x y z | r z>
+//       get_ssp of a 3-D or Nx2D setup at one point; needs no GPU.
 //   bhc_api_check readout <2|3|4> <file root>
 //       setup from the files (2-D, 3-D or Nx2D) and readout of the run's
 //       output file (.arr for RunType 'A' / 'a', .ray for 'R'); prints the
@@ -291,8 +293,32 @@ template<bool O3D, bool R3D> static int check_writeenv(const char *root, const c
     return failures ? 1 : 0;
 }
 
+// get_ssp of a 3-D (dim 3: x y z) or Nx2D (dim 4: r z) setup; prints c
+template<bool O3D, bool R3D> static int check_ssp(const char *root, int argc, char **argv)
+{
+    using namespace bhc;
+    bhcParams<O3D> p;
+    bhcOutputs<O3D, R3D> o;
+    if(!setup(make_init(root), p, o)) return 2;
+    VEC23<R3D> x{};
+    if constexpr(R3D) x = vec3{std::atof(argv[0]), std::atof(argv[1]), std::atof(argv[2])};
+    else x = vec2{std::atof(argv[0]), std::atof(argv[1])};
+    (void)argc;
+    float c = -1.f;
+    const bool ok = get_ssp<O3D, R3D>(p, x, c);
+    std::printf("ssp %d %.9g\n", ok ? 1 : 0, (double)c);
+    finalize(p, o);
+    return ok ? 0 : 5;
+}
+
 int main(int argc, char **argv)
 {
+    if(argc >= 6 && std::strcmp(argv[1], "ssp") == 0) {
+        const int d = std::atoi(argv[2]);
+        if(d == 3 && argc >= 7) return check_ssp<true, true>(argv[3], argc - 4, argv + 4);
+        if(d == 4) return check_ssp<true, false>(argv[3], argc - 4, argv + 4);
+        return 64;
+    }
     if(argc >= 5 && std::strcmp(argv[1], "writeenv") == 0) {
         const int d = std::atoi(argv[2]);
         return d == 3 ? check_writeenv<true, true>(argv[3], argv[4])

@@ -164,3 +164,64 @@ def test_writeenv_3d_and_nx2d(case, tmp_path):
     for k in g.files:
         if k.startswith("file_"):
             assert open(new + "." + k[5:]).read() == str(g[k])
+
+
+def _hex_table(text):
+    """x, y (km), z (m), c[ix, iy, iz] of a hexahedral .ssp file."""
+    t = text.split()
+    k = 0
+    nx = int(t[k]); x = np.array(t[k + 1:k + 1 + nx], float); k += 1 + nx
+    ny = int(t[k]); y = np.array(t[k + 1:k + 1 + ny], float); k += 1 + ny
+    nz = int(t[k]); z = np.array(t[k + 1:k + 1 + nz], float); k += 1 + nz
+    c = np.array(t[k:k + nx * ny * nz], float).reshape(nz, ny, nx).transpose(2, 1, 0)
+    return x, y, z, c
+
+
+def test_get_ssp_3d_and_nx2d(tmp_path):
+    """get_ssp of 3-D and Nx2D setups: the hexahedral grid's nodes, a point
+    halfway between two nodes in x (the mean of their c), and a 1-D profile's
+    nodes and midpoints (c-linear)."""
+    exe = build_check(str(tmp_path))
+
+    def ssp(dim, root, *x):
+        r = subprocess.run([exe, "ssp", str(dim), root] + ["%.17g" % v for v in x], capture_output=True,
+                           text=True, timeout=60)
+        assert r.returncode == 0, r.stdout + r.stderr
+        line = [ln for ln in r.stdout.splitlines() if ln.startswith("ssp ")][0].split()
+        return float(line[2])
+
+    def case(name):
+        g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+        root = os.path.join(str(tmp_path), name)
+        for k in g.files:
+            if k.startswith("file_"):
+                with open(root + "." + k[5:], "w") as f:
+                    f.write(str(g[k]))
+        return g, root
+
+    g, root = case("hex3d_gauss")
+    xk, yk, zk, c = _hex_table(str(g["file_ssp"]))
+    for ix, iy, iz in ((0, 0, 0), (1, 2, 3), (2, 1, 5), (1, 1, 2)):
+        got = ssp(3, root, xk[ix] * 1000.0, yk[iy] * 1000.0, zk[iz])
+        assert abs(got - c[ix, iy, iz]) <= 1e-3, (ix, iy, iz, got, c[ix, iy, iz])
+    got = ssp(3, root, 0.5 * (xk[0] + xk[1]) * 1000.0, yk[1] * 1000.0, zk[4])
+    assert abs(got - 0.5 * (c[0, 1, 4] + c[1, 1, 4])) <= 1e-3
+    g, root = case("munk3d_gauss")
+    env = str(g["file_env"]).splitlines()
+    k = [i for i, ln in enumerate(env) if ln.strip().startswith("'CVW")][0]
+    prof = []
+    for ln in env[k + 2:]:
+        vals = ln.replace("/", " ").split()
+        if len(vals) < 2 or not vals[0].replace(".", "", 1).isdigit():
+            break
+        prof.append((float(vals[0]), float(vals[1])))
+        if float(vals[0]) >= 5000.0:
+            break
+    zp, cp = np.array(prof).T
+    for i in (0, 10, 20):
+        assert abs(ssp(3, root, 100.0, -50.0, zp[i]) - cp[i]) <= 1e-3
+        mid = 0.5 * (zp[i] + zp[i + 1])
+        assert abs(ssp(3, root, 0.0, 0.0, mid) - 0.5 * (cp[i] + cp[i + 1])) <= 1e-3
+    g, root = case("hex3d_nx2d_hat")
+    xk, yk, zk, c = _hex_table(str(g["file_ssp"]))
+    assert abs(ssp(4, root, xk[2] * 1000.0, zk[3]) - c[2, 1, 3]) <= 1e-3   # (r, 0, z): y = 0 is node 1
