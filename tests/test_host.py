@@ -335,3 +335,27 @@ def test_arrivals_ascii_and_binary_files_agree(workdir):
         for a, b in zip(sa["arrivals"], sb["arrivals"]):
             assert a.shape == b.shape
             np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-6)
+
+
+def test_every_entry_rejects_null_arguments():
+    """The C ABI's error contract without a GPU: every entry point that takes a
+    context or buffers returns BHCB_ERR_ARG for null handles and zero sizes
+    instead of touching memory (the bhc:: layer above maps it to false)."""
+    import ctypes as C
+    lib = B.load_library()
+    host_only = {"bhcb_version", "bhcb_close", "bhcb_free_env_desc", "bhcb_read_env_desc", "bhcb_check_env",
+                 "bhcb_check_env3d", "bhcb_last_error", "bhcb_graph_destroy",
+                 "bhcb_nn_status"}   # reads the device's error word: no device here
+    checked = 0
+    for name, ret, args in B.SIGNATURES:
+        if name in host_only or not args or ret is None:
+            continue
+        vals = []
+        for a in args:
+            if a in (C.c_float, C.c_double, C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_int, C.c_size_t):
+                vals.append(a(0))
+            else:
+                vals.append(None)
+        assert getattr(lib, name)(*vals) == 1, name   # BHCB_ERR_ARG
+        checked += 1
+    assert checked >= 40
