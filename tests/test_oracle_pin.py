@@ -37,14 +37,15 @@ def test_oracle_matches_reference_golden(name):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_EXE), reason="reference build (oracle/_ref) not present")
-@pytest.mark.parametrize("seed", [1, 2])
+@pytest.mark.parametrize("seed", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_oracle_matches_reference_live(seed, workdir):
     from bellhopcuda_b200 import workloads as W
     rng = np.random.Generator(np.random.PCG64(seed))
     spec = W.rd_gauss(seed=100 + seed, nalpha=int(rng.integers(51, 201)), nrz=int(rng.integers(11, 41)),
                       nrr=int(rng.integers(21, 121)), nbty=int(rng.integers(5, 60)))
     spec.freq = float(rng.uniform(30, 400))
-    spec.run_type = ["CG RR ", "CB RR ", "IB RR "][seed % 3]
+    spec.run_type = ["CG RR ", "CB RR ", "IB RR ", "SB RR ", "SG RR ", "IG RR "][seed % 6]
+    spec.ssp_type = ["P", "C", "S", "N"][seed % 4]   # PCHIP, c-linear, spline, n2-linear
     root = write_env(spec, os.path.join(workdir, "live%d" % seed))
     subprocess.run([REF_EXE, "-2", "-1", root], check=True, capture_output=True)
     ref = read_shd(root + ".shd")["field"][0, 0, 0]
