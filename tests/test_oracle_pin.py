@@ -53,14 +53,17 @@ def test_oracle_matches_reference_live(seed, workdir):
     np.testing.assert_array_equal(got, ref)
 
 
-def test_oracle_arrivals_match_reference_counts(workdir):
+@pytest.mark.parametrize("seed,run_type", [(1002, "aG RR "), (1003, "aB RR "), (1004, "aB RR ")])
+def test_oracle_arrivals_match_reference_counts(seed, run_type, workdir):
+    """Arrivals (merging, one thread) of the oracle and of the reference's own
+    run: per receiver the count, amplitudes, delays and bounce counts equal."""
     if not os.path.exists(REF_EXE):
         pytest.skip("reference build (oracle/_ref) not present")
     import re
     from bellhopcuda_b200 import workloads as W
     from bellhopcuda_b200.arrfile import read_arr_binary
-    spec = W.rd_gauss(nalpha=151, nrz=7, nrr=15, nbty=20)
-    spec.run_type = "aG RR "
+    spec = W.rd_gauss(seed=seed, nalpha=151, nrz=7, nrr=15, nbty=20)
+    spec.run_type = run_type
     root = write_env(spec, os.path.join(workdir, "arr"))
     subprocess.run([REF_EXE, "-2", "-1", root], check=True, capture_output=True)
     A = read_arr_binary(root + ".arr")
