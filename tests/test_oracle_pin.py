@@ -78,3 +78,26 @@ def test_oracle_arrivals_match_reference_counts(seed, run_type, workdir):
         np.testing.assert_array_equal(oa["delay_re"], arrs[:, 2])
         np.testing.assert_array_equal(oa["NTopBnc"].astype(np.float32), arrs[:, 6])
         np.testing.assert_array_equal(oa["NBotBnc"].astype(np.float32), arrs[:, 7])
+
+
+@pytest.mark.parametrize("seed,run_type", [(1002, "EG RR "), (1005, "EB RR ")])
+def test_oracle_eigen_hits_match_reference(seed, run_type, workdir):
+    """Eigen hits (RecordEigenHit) of the oracle against the reference's own
+    single-threaded run: the reference writes one re-traced ray per hit, in hit
+    order, whose take-off angle and point count (the hit's step + 2) pin the
+    hit list."""
+    if not os.path.exists(REF_EXE):
+        pytest.skip("reference build (oracle/_ref) not present")
+    from bellhopcuda_b200 import workloads as W
+    from bellhopcuda_b200.rayfile import read_ray
+    spec = W.rd_gauss(seed=seed, nalpha=101, nrz=3, nrr=5, nbty=20)
+    spec.run_type = run_type
+    root = write_env(spec, os.path.join(workdir, "eig"))
+    subprocess.run([REF_EXE, "-2", "-1", root], check=True, capture_output=True)
+    rays = read_ray(root + ".ray")["rays"]
+    o = oracle_ctypes.run(spec)
+    hits = o["hits"]
+    assert len(hits) == o["neigen"] == len(rays) > 0
+    np.testing.assert_array_equal(hits["is"] + 2, [len(r["xy"]) for r in rays])
+    fan = np.linspace(spec.alpha[0], spec.alpha[1], spec.nalpha)
+    np.testing.assert_allclose(fan[hits["ialpha"]], [r["alpha"] for r in rays], rtol=0, atol=1e-9)
