@@ -522,7 +522,17 @@ template<bool O3D, bool R3D> void collect(Internal &in, bhcOutputs<O3D, R3D> &o,
         o.arrinfo->NArr = new int32_t[cells];
         o.arrinfo->Arr = new Arrival[cells * mx];
         o.arrinfo->MaxNArr = mx;
-        o.arrinfo->MaxNPerSource = new int32_t[nsz];
+        o.arrinfo->AllowMerging = in.init.numThreads == 1;
+        // MaxNPerSource is per source (NSx * NSy * NSz); in 3-D the shape's
+        // leading count also spans the bearings, whose cells follow their
+        // source's in the [isz][isx][isy][itheta][iz][ir] layout
+        int32_t nsrc = nsz;
+        if(in.dim != 2) {
+            int32_t d[6] = {0};
+            check(ctx, bhcb_field_shape3d(ctx, 0, d), "field shape");
+            nsrc = d[0] * d[1] * d[2];
+        }
+        o.arrinfo->MaxNPerSource = new int32_t[nsrc > 0 ? nsrc : 1];
         std::vector<bhcb_arrival> a(cells * mx);
         check(ctx, bhcb_copy_arrivals(ctx, 0, 0, o.arrinfo->NArr, cells * sizeof(int32_t), a.data(),
                                       a.size() * sizeof(bhcb_arrival)), "copy arrivals");
@@ -534,8 +544,8 @@ template<bool O3D, bool R3D> void collect(Internal &in, bhcOutputs<O3D, R3D> &o,
             r.a = a[i].a; r.Phase = a[i].phase;
             r.delay = cpxf(a[i].delay_re, a[i].delay_im);
         }
-        const size_t per = cells / (nsz ? nsz : 1);
-        for(int s = 0; s < nsz; ++s) {
+        const size_t per = cells / (nsrc ? nsrc : 1);
+        for(int s = 0; s < nsrc; ++s) {
             int32_t m = 0;
             for(size_t i = 0; i < per; ++i) m = std::max(m, o.arrinfo->NArr[s * per + i]);
             o.arrinfo->MaxNPerSource[s] = m;
@@ -608,6 +618,11 @@ template<bool O3D, bool R3D> void run_now(bhcParams<O3D> &p, bhcOutputs<O3D, R3D
         if(in.root.empty()) throw std::runtime_error("3-D and Nx2D runs read FileRoot's files (setup with FileRoot)");
         check(ctx, bhcb_setup3d(ctx, in.root.c_str()), "3-D setup");
         run0 = p.Beam->RunType[0];
+    }
+    if(run0 == 'A' || run0 == 'a' || run0 == 'V' || run0 == 'v') {
+        // merging as the reference's Arr mode decides it: only single-threaded
+        // runs merge (AllowMerging, src/mode/arr.hpp:78); MaxNArr from memory
+        check(ctx, bhcb_set_arrival_options(ctx, 0, in.init.numThreads == 1 ? 1 : 0), "arrival options");
     }
     in.progress = 10;
     check(ctx, bhcb_run(ctx), "run");

@@ -16,6 +16,8 @@
 //       the two setups agree. Needs no GPU.
 //   bhc_api_check ssp <3|4> <file root> <x y z | r z>
 //       get_ssp of a 3-D or Nx2D setup at one point; needs no GPU.
+//   bhc_api_check run3arr <file root>
+//       a 3-D arrivals run through bhc::run; counts and MaxNPerSource.
 //   bhc_api_check readout <2|3|4> <file root>
 //       setup from the files (2-D, 3-D or Nx2D) and readout of the run's
 //       output file (.arr for RunType 'A' / 'a', .ray for 'R'); prints the
@@ -311,8 +313,37 @@ template<bool O3D, bool R3D> static int check_ssp(const char *root, int argc, ch
     return ok ? 0 : 5;
 }
 
+// 3-D arrivals through bhc::run: the counts, their sum and MaxNPerSource
+static int check_run3_arrivals(const char *root)
+{
+    using namespace bhc;
+    bhcParams<true> p;
+    bhcOutputs<true, true> o;
+    bhcInit init = make_init(root);
+    init.numThreads = 1;   // single-threaded: arrivals merge, as in the reference's fixture run
+    if(!setup(init, p, o)) return 2;
+    if(!run(p, o)) return 3;
+    const Position &P = *p.Pos;
+    const size_t nsrc = (size_t)P.NSx * P.NSy * P.NSz, per = (size_t)P.Ntheta * P.NRz * P.NRr;
+    long long total = 0;
+    for(size_t s = 0; s < nsrc; ++s) {
+        int m = 0;
+        for(size_t k = 0; k < per; ++k) {
+            total += o.arrinfo->NArr[s * per + k];
+            m = std::max(m, o.arrinfo->NArr[s * per + k]);
+        }
+        EXPECT(o.arrinfo->MaxNPerSource[s] == m);
+        EXPECT(m <= o.arrinfo->MaxNArr);
+    }
+    std::printf("arr3 %zu %lld\n", nsrc, total);
+    finalize(p, o);
+    std::printf(failures ? "FAILED %d\n" : "OK\n", failures);
+    return failures ? 1 : 0;
+}
+
 int main(int argc, char **argv)
 {
+    if(argc >= 3 && std::strcmp(argv[1], "run3arr") == 0) return check_run3_arrivals(argv[2]);
     if(argc >= 6 && std::strcmp(argv[1], "ssp") == 0) {
         const int d = std::atoi(argv[2]);
         if(d == 3 && argc >= 7) return check_ssp<true, true>(argv[3], argc - 4, argv + 4);

@@ -106,3 +106,21 @@ def test_desc_route_matches_file_route(tmp_path):
     rms, _, n = tl_err(b, a)
     assert n > 1000 and rms < 1e-3
     assert abs(c - spec.ssp_cp[1]) < 1e-6
+
+
+def test_3d_arrivals_through_bhc(tmp_path):
+    """A 3-D arrivals run ('a', munk3d_arr_hat) through bhc::setup<true, true> /
+    run: the arrival counts sum to the reference's and MaxNPerSource holds each
+    source's largest count over all its bearings and receivers."""
+    HERE = os.path.dirname(os.path.abspath(__file__))
+    g = np.load(os.path.join(HERE, "golden", "munk3d_arr_hat.npz"))
+    root = os.path.join(str(tmp_path), "munk3d_arr_hat")
+    for k in g.files:
+        if k.startswith("file_"):
+            with open(root + "." + k[5:], "w") as f:
+                f.write(str(g[k]))
+    exe = build_check(str(tmp_path))
+    r = subprocess.run([exe, "run3arr", root], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("OK"), r.stdout + r.stderr
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("arr3 ")][0].split()
+    assert int(line[1]) == 1 and int(line[2]) == int(g["narr"].sum()) > 0
