@@ -5,9 +5,14 @@ workload (2-D, PCHIP SSP, 200-point bathymetry, 20001 rays over +-30 deg,
 
 A step is one pass of the hot path over the batch: trace every ray, evaluate
 every beam-receiver contribution for all 10 frequencies, post-process the 10
-TL fields. Our arm runs the mixed-precision tracer (FP32 bulk, FP64 positions /
-travel time / crossing solves) with the 10 frequencies sharing one trajectory;
-the FP64 per-frequency tracer is timed beside it.
+TL fields. Our arm runs the mixed-precision path (FP64 ray trace, FP32
+beam-receiver contributions) with the 10 frequencies sharing one trajectory,
+successive steps pipelined (two traces side by side, then their influences);
+beside it on the same line: the steps one at a time (`serial_steps`), the
+FP64 per-frequency tracer (`fp64_trace`), the 3-D workload (`c4_3d_tl`), the
+TL surrogate with its FP64 fallback (`surrogate`), the end-to-end rate through
+the C ABI with host buffers (`e2e`) and the reference's bellhopcxx on the host
+cores (`cpu_baseline`).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
