@@ -101,3 +101,22 @@ def test_oracle_eigen_hits_match_reference(seed, run_type, workdir):
     np.testing.assert_array_equal(hits["is"] + 2, [len(r["xy"]) for r in rays])
     fan = np.linspace(spec.alpha[0], spec.alpha[1], spec.nalpha)
     np.testing.assert_allclose(fan[hits["ialpha"]], [r["alpha"] for r in rays], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("tag,run_type", [("line", "CB RX "), ("line_hat", "IG RX "), ("irregular", "CB RI ")])
+def test_oracle_matches_reference_line_source_and_irregular_grid(tag, run_type, workdir):
+    """Line sources (RunType(4) 'X': ScalePressure's line-source constant)
+    and an irregular receiver grid (RunType(5) 'I': one depth per range) of
+    the oracle against the reference's own single-threaded runs, bit-exact."""
+    if not os.path.exists(REF_EXE):
+        pytest.skip("reference build (oracle/_ref) not present")
+    from bellhopcuda_b200 import workloads as W
+    spec = W.rd_gauss(seed=1010, nalpha=121, nrz=60 if tag == "irregular" else 31, nrr=60, nbty=30)
+    spec.freq = 120.0
+    spec.run_type = run_type
+    root = write_env(spec, os.path.join(workdir, tag))
+    subprocess.run([REF_EXE, "-2", "-1", root], check=True, capture_output=True)
+    ref = read_shd(root + ".shd")["field"][0, 0, 0]
+    got = oracle_ctypes.run(spec)["field"]
+    assert got.shape == ref.shape
+    np.testing.assert_array_equal(got, ref)
